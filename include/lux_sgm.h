@@ -1,0 +1,151 @@
+/* lux_sgm.h — C ABI of the B200 dense-stereo depth stage (liblux_sgm.so).
+ *
+ * This library replaces the CPU dense-stereo stage of Lux.Engine (mprovenz/lux). A C# host binds it with P/Invoke
+ * (`[LibraryImport]` or NativeLibrary.Load + `delegate* unmanaged`, as Lux.DepthModel/OnnxDepthNetwork.cs:52-55 does for
+ * ONNX Runtime). Plain pointers and sizes only; every function returns a status (0 = ok) and records a message that
+ * lux_sgm_last_error() returns. Status codes map onto the exceptions the reference throws (see LUX_ERR_*).
+ *
+ * Threading: a context serialises its own calls (internal mutex) and owns one CUDA stream; use one context per host
+ * thread for concurrency. Results do not depend on the schedule (the reference's guarantee, StereoAsyncApi.cs:44-47).
+ */
+#ifndef LUX_SGM_H
+#define LUX_SGM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define LUX_OK 0
+#define LUX_ERR_NEAR_FAR 1      /* InvalidOperationException "The near end has to be smaller than the fard end!" (DenseStereo.cs:43) */
+#define LUX_ERR_NONPOSITIVE 2   /* InvalidOperationException "Both the near and far end have to be positive!" (DenseStereo.cs:44) */
+#define LUX_ERR_BASELINE 3      /* InvalidOperationException "Baseline too small, check calibration." (DenseStereo.cs:63) */
+#define LUX_ERR_SKIPMODE 4      /* NotSupportedException "unrecognized sampling pattern" (DenseStereoSgm.cs:69) */
+#define LUX_ERR_BUDGET 5        /* NotSupportedException "StereoLayer memory budget exceeded" (DenseStereoSgm.cs:343), or the HBM budget */
+#define LUX_ERR_UPSAMPLE_SIZE 6 /* InvalidOperationException "Incorrect output depth size!" (DenseUpsampleLayer.cs:43) */
+#define LUX_ERR_INDEX 7         /* the reference indexes outside an array for these inputs (IndexOutOfRangeException) */
+#define LUX_ERR_ALLOC 8         /* device allocation failed */
+#define LUX_ERR_ARG 9           /* invalid argument (null pointer, bad size) */
+#define LUX_ERR_CUDA 10         /* a CUDA call failed */
+#define LUX_ERR_TIMEOUT 11      /* a bounded device-side wait gave up (the kernel returned without finishing) */
+#define LUX_ERR_UNSUPPORTED 12  /* inputs outside what this implementation supports (message says which) */
+#define LUX_ERR_CANCELED 13     /* OperationCanceledException: the request was canceled before it started */
+
+/* Rgba8Image (Lux.Engine/Pipeline/Registration/SparseLnrMatch.cs:8-13): 8-bit RGBA ("YUVA"), stride in pixels.
+ * on_device != 0: data is a device pointer of the context's GPU (no copy); else host memory. */
+typedef struct {
+  const uint8_t* data;
+  int32_t w, h, stride;
+  int32_t on_device;
+} lux_img_rgba8;
+
+/* CalibData (Lux.Engine/Pipeline/Registration/Triangulator.cs:8-19): row-major K, t, R, X_cam = R·X + t. */
+typedef struct {
+  float K[9], T[3], R[9];
+} lux_calib;
+
+/* StereoParams (Lux.Engine/Pipeline/Registration/DenseStereo.cs:15-21): the fields the dense path reads. */
+typedef struct {
+  int32_t margin;        /* Margin, 1 */
+  float plane_density;   /* PlaneDensity, 2.0 */
+  int32_t scale;         /* Scale, 32 */
+  int32_t skip_mode;     /* SkipMode, 0 or 2 */
+  uint16_t p1;           /* P1, 1 */
+  uint16_t reserved;
+  float p2scale;         /* P2Scale, 500 */
+  float guidance[4];     /* Guidance weights */
+  int32_t tile;          /* Tile T (even), 4 */
+} lux_stereo_params;
+
+typedef struct lux_sgm_ctx lux_sgm_ctx;
+typedef struct lux_layer lux_layer;
+
+/* Context: one GPU, one stream, an HBM budget that every request is admitted against (0 = no limit). */
+int lux_sgm_create(int device, uint64_t hbm_budget_bytes, lux_sgm_ctx** out);
+void lux_sgm_destroy(lux_sgm_ctx* ctx);
+const char* lux_sgm_last_error(const lux_sgm_ctx* ctx);
+/* Synchronises the context's stream. */
+int lux_sgm_sync(lux_sgm_ctx* ctx);
+/* The number of kernels this library has launched in this process (all contexts). */
+uint64_t lux_sgm_kernel_launches(void);
+/* The context's CUDA stream (a cudaStream_t), for callers that record events or order work against it. */
+void* lux_sgm_stream(lux_sgm_ctx* ctx);
+
+/* StereoParams defaults / L16Pyramid() (DenseStereo.cs:15-30). */
+void lux_sgm_default_params(lux_stereo_params* p);
+void lux_sgm_l16_pyramid(lux_stereo_params out[6]);
+
+/* DenseStereo.Planes (DenseStereo.cs:41-88). out must hold 4096 + align floats. Host only. */
+int lux_sgm_planes(float near_, float far_, const lux_calib* calibs, int32_t n_cams, float density, int32_t align, float* out,
+                   int32_t* n_out);
+
+/* DenseStereo.BoxFilter3 (DenseStereo.cs:93-123) of one image; dst is host memory of w*h*4 bytes (dense). */
+int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst);
+
+/* DenseLayer.Init + DenseLayer.Compute (DenseStereoSgm.cs:34-62, 181-232): one pyramid layer on the GPU.
+ * images: n_cams camera images (camera 0 = reference), box-FILTERED already unless prefilter != 0, which applies
+ * DenseStereo.BoxFilter3 to each on the device first (as DenseStereoPyramid.Run does, DenseStereoSgm.cs:335);
+ * gray[k] selects the grey cost weights; prev = the previous layer (NULL for a first layer: every pixel searches all
+ * planes). keep_pass1 keeps the aggregates after pass +1. The layer object owns its device state until
+ * lux_layer_destroy. */
+int lux_sgm_layer(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
+                  float near_, float far_, const lux_stereo_params* params, int32_t index, int32_t align, const lux_layer* prev,
+                  int32_t keep_pass1, int32_t prefilter, lux_layer** out);
+
+/* DenseStereoPyramid.Run (DenseStereoSgm.cs:331-353): box filter, six L16 layers with the 1 GiB align-8/align-2 choice.
+ * out receives six layer objects. */
+int lux_sgm_pyramid(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
+                    float near_, float far_, int32_t keep_pass1, lux_layer* out[6]);
+
+/* Layer facts (DenseLayer fields). */
+typedef struct {
+  int32_t w, h, index, align, n_planes, min_lo, max_hi, tile;
+  uint64_t volume;       /* sum of per-pixel caps: the element count of agg / raw */
+  float gpu_ms_cost;     /* device time of the matching-cost kernel (CUDA events on the context's stream) */
+  float gpu_ms_sgm;      /* device time of the two aggregation passes */
+  float gpu_ms_wta;      /* device time of the winner-take-all */
+  int32_t sgm_kernel;    /* 1 = the fast uniform-layer aggregation, 0 = the exact traversal replay */
+} lux_layer_info;
+int lux_layer_get_info(const lux_layer* layer, lux_layer_info* info);
+
+/* Copies a layer field into host memory: bytes must equal the field's size.
+ *   LUX_FIELD_DEPTH     float[w*h]        Depth (after WTA)
+ *   LUX_FIELD_PLANES    float[n_planes]   Planes
+ *   LUX_FIELD_SKIP      uint8[w*h]        Skip (0 computed, 0xff skipped)
+ *   LUX_FIELD_START / COUNT / CAP  uint16[w*h]
+ *   LUX_FIELD_OFFSETS   uint64[w*h+1]     CSR offsets of the ragged volume (pixel i: [off[i], off[i]+cap[i]))
+ *   LUX_FIELD_AGG       uint16[volume]    Agg (final aggregates)
+ *   LUX_FIELD_AGG_PASS1 uint16[volume]    AggPass1 (needs keep_pass1)
+ *   LUX_FIELD_RAW       uint8[volume]     Raw (entries of skipped pixels are 0)
+ *   LUX_FIELD_GUIDANCE  uint8[w*h*4]      Guidance */
+enum {
+  LUX_FIELD_DEPTH = 0,
+  LUX_FIELD_PLANES = 1,
+  LUX_FIELD_SKIP = 2,
+  LUX_FIELD_START = 3,
+  LUX_FIELD_COUNT = 4,
+  LUX_FIELD_CAP = 5,
+  LUX_FIELD_OFFSETS = 6,
+  LUX_FIELD_AGG = 7,
+  LUX_FIELD_AGG_PASS1 = 8,
+  LUX_FIELD_RAW = 9,
+  LUX_FIELD_GUIDANCE = 10,
+};
+int lux_layer_read(const lux_layer* layer, int32_t field, void* dst, uint64_t bytes);
+/* The device pointer of a field (valid until lux_layer_destroy), or NULL. */
+const void* lux_layer_device_ptr(const lux_layer* layer, int32_t field);
+void lux_layer_destroy(lux_layer* layer);
+
+/* DenseUpsampleLayer.Run (DenseUpsampleLayer.cs:35-48): prev depth pw×ph (host, or device when prev_on_device), guide RGBA8,
+ * output depth guide.w×guide.h into out_depth (host). prev_conf / out_conf optional (NULL). */
+int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int32_t ph, int32_t prev_on_device,
+                     const lux_img_rgba8* guide, int32_t set_w, int32_t set_h, float sigma, int32_t scale,
+                     const float* prev_conf, float* out_depth, float* out_conf);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,334 @@
+"""Host-side mirror of Lux.Engine's dense-stereo interface, backed by the CUDA library through its C ABI.
+
+Names and argument meanings follow the reference:
+  * StereoParams / StereoParams.l16_pyramid()      Lux.Engine/Pipeline/Registration/DenseStereo.cs:15-31
+  * DenseStereo.planes(...)                        DenseStereo.cs:41-88
+  * DenseStereo.box_filter3(...)                   DenseStereo.cs:93-123
+  * DenseLayer (init + compute on the GPU)         DenseStereoSgm.cs:13-232
+  * DenseStereoPyramid.run(...)                    DenseStereoSgm.cs:331-353
+  * DenseUpsampleLayer.run(...)                    DenseUpsampleLayer.cs:35-48
+Errors raise the exception class the reference throws (InvalidOperationError, NotSupportedError, IndexError), each
+carrying the C status code.
+"""
+import ctypes
+import struct
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+
+class LuxError(L.LuxError):
+    pass
+
+
+class InvalidOperationError(LuxError):
+    """InvalidOperationException of the reference (planes, upsample size)."""
+
+
+class NotSupportedError(LuxError):
+    """NotSupportedException of the reference (skip mode, memory budget)."""
+
+
+class LuxIndexError(LuxError, IndexError):
+    """The reference indexes outside an array for these inputs (IndexOutOfRangeException)."""
+
+
+_EXC = {1: InvalidOperationError, 2: InvalidOperationError, 3: InvalidOperationError, 6: InvalidOperationError,
+        4: NotSupportedError, 5: NotSupportedError, 7: LuxIndexError}
+
+
+def _raise(code, msg):
+    raise _EXC.get(code, LuxError)(code, msg)
+
+
+def _f32bits(u):
+    return struct.unpack("<f", struct.pack("<I", u))[0]
+
+
+@dataclass
+class StereoParams:
+    """StereoParams (DenseStereo.cs:15-21), the fields the dense path reads."""
+    margin: int = 1
+    plane_density: float = 2.0
+    scale: int = 32
+    skip_mode: int = 0
+    p1: int = 1
+    p2scale: float = 500.0
+    guidance: tuple = field(default_factory=lambda: (np.float32(_f32bits(0x3ef6384f)) / np.float32(6),
+                                                     np.float32(_f32bits(0x3ef6384f)) / np.float32(16),
+                                                     np.float32(_f32bits(0x3ef6384f)) / np.float32(16), np.float32(0)))
+    tile: int = 4
+
+    @staticmethod
+    def l16_pyramid() -> List["StereoParams"]:
+        """StereoParams.L16Pyramid(false) (DenseStereo.cs:24-30)."""
+        scales, tiles = (32, 16, 8, 4, 2, 1), (4, 8, 16, 32, 64, 64)
+        return [StereoParams(scale=scales[i], tile=tiles[i], skip_mode=2 if i >= 4 else 0) for i in range(6)]
+
+    def to_c(self):
+        p = L.Params()
+        p.margin, p.plane_density, p.scale, p.skip_mode = self.margin, self.plane_density, self.scale, self.skip_mode
+        p.p1, p.p2scale, p.tile = self.p1, self.p2scale, self.tile
+        for i in range(4):
+            p.guidance[i] = float(self.guidance[i])
+        return p
+
+
+@dataclass
+class CalibData:
+    """CalibData (Triangulator.cs:8-19): row-major K (3x3), T (3), R (3x3), X_cam = R·X + t."""
+    K: np.ndarray
+    T: np.ndarray
+    R: np.ndarray
+
+    def to_c(self):
+        c = L.Calib()
+        for i, v in enumerate(np.asarray(self.K, np.float32).reshape(9)):
+            c.K[i] = float(v)
+        for i, v in enumerate(np.asarray(self.T, np.float32).reshape(3)):
+            c.T[i] = float(v)
+        for i, v in enumerate(np.asarray(self.R, np.float32).reshape(9)):
+            c.R[i] = float(v)
+        return c
+
+
+def _calibs_c(calibs):
+    arr = (L.Calib * len(calibs))()
+    for i, c in enumerate(calibs):
+        arr[i] = c.to_c()
+    return arr
+
+
+def _img_c(img):
+    """A C image from a numpy (H, W, 4) uint8 array or a CUDA torch uint8 tensor of that shape."""
+    if hasattr(img, "data_ptr"):  # torch tensor
+        h, w, c = img.shape
+        assert c == 4 and img.is_contiguous()
+        return L.Img(img.data_ptr(), w, h, w, 1 if img.is_cuda else 0), img
+    a = np.ascontiguousarray(img, dtype=np.uint8)
+    h, w, c = a.shape
+    assert c == 4
+    return L.Img(a.ctypes.data, w, h, w, 0), a
+
+
+class Context:
+    """One GPU, one stream, an HBM budget (0 = none). Layers created through it keep their state on the device."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self.lib = L.load()
+        h = ctypes.c_void_p()
+        rc = self.lib.lux_sgm_create(device, hbm_budget_bytes, ctypes.byref(h))
+        if rc:
+            _raise(rc, "lux_sgm_create failed")
+        self.handle = h
+        self.device = device
+
+    def check(self, rc):
+        if rc:
+            _raise(rc, self.lib.lux_sgm_last_error(self.handle).decode())
+
+    def close(self):
+        if self.handle:
+            self.lib.lux_sgm_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def kernel_launches() -> int:
+    """Kernels the CUDA library has launched in this process."""
+    return int(L.load().lux_sgm_kernel_launches())
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class DenseStereo:
+    @staticmethod
+    def planes(near, far, calibs: Sequence[CalibData], density, align) -> np.ndarray:
+        """DenseStereo.Planes (DenseStereo.cs:41-88): metric plane depths, plane 0 = far .. n-1 = near."""
+        lib = L.load()
+        out = (ctypes.c_float * (4096 + max(int(align), 1) + 8))()
+        n = ctypes.c_int32()
+        cc = _calibs_c(calibs)
+        rc = lib.lux_sgm_planes(near, far, cc, len(calibs), density, align, out, ctypes.byref(n))
+        if rc:
+            _raise(rc, {1: "The near end has to be smaller than the fard end!", 2: "Both the near and far end have to be positive!",
+                        3: "Baseline too small, check calibration."}.get(rc, "planes failed"))
+        return np.frombuffer(out, dtype=np.float32, count=n.value).copy()
+
+    @staticmethod
+    def box_filter3(img, ctx: Optional[Context] = None) -> np.ndarray:
+        """DenseStereo.BoxFilter3 (DenseStereo.cs:93-123) on the GPU."""
+        ctx = ctx or default_context()
+        ci, keep = _img_c(img)
+        out = np.empty((ci.h, ci.w, 4), np.uint8)
+        ctx.check(ctx.lib.lux_sgm_box_filter3(ctx.handle, ctypes.byref(ci), out.ctypes.data))
+        return out
+
+
+class DenseLayer:
+    """A computed DenseLayer (DenseStereoSgm.cs:13-232) whose state lives on the GPU until close()."""
+
+    def __init__(self, ctx: Context, handle):
+        self.ctx = ctx
+        self.handle = handle
+        info = L.LayerInfo()
+        ctx.check(ctx.lib.lux_layer_get_info(handle, ctypes.byref(info)))
+        self.W, self.H, self.Index, self.Align = info.w, info.h, info.index, info.align
+        self.n_planes, self.MinLo, self.MaxHi, self.Tile = info.n_planes, info.min_lo, info.max_hi, info.tile
+        self.volume = info.volume
+        self.gpu_ms_cost, self.gpu_ms_sgm, self.gpu_ms_wta = info.gpu_ms_cost, info.gpu_ms_sgm, info.gpu_ms_wta
+        self.sgm_kernel = info.sgm_kernel
+
+    @staticmethod
+    def compute(images, gray, calibs, near, far, params: StereoParams, index=0, align=8, prev: Optional["DenseLayer"] = None,
+                keep_pass1=False, prefilter=False, ctx: Optional[Context] = None) -> "DenseLayer":
+        """DenseLayer.Init + Compute (DenseStereoSgm.cs:34-62, 181-232). images: RGBA8 (camera 0 = reference), box-filtered
+        already unless prefilter=True (then BoxFilter3 runs on the GPU first, as DenseStereoPyramid.Run does)."""
+        ctx = ctx or default_context()
+        arr = (L.Img * len(images))()
+        keep = []
+        for i, im in enumerate(images):
+            ci, k = _img_c(im)
+            arr[i] = ci
+            keep.append(k)
+        g = np.ascontiguousarray(np.asarray(gray, dtype=np.uint8))
+        cc = _calibs_c(calibs)
+        p = params.to_c()
+        out = ctypes.c_void_p()
+        rc = ctx.lib.lux_sgm_layer(ctx.handle, len(images), arr, g.ctypes.data, cc, near, far, ctypes.byref(p), index, align,
+                                   prev.handle if prev is not None else None, 1 if keep_pass1 else 0, 1 if prefilter else 0,
+                                   ctypes.byref(out))
+        ctx.check(rc)
+        return DenseLayer(ctx, out)
+
+    def _read(self, field_id, dtype, count):
+        out = np.empty(count, dtype=dtype)
+        self.ctx.check(self.ctx.lib.lux_layer_read(self.handle, field_id, out.ctypes.data, out.nbytes))
+        return out
+
+    @property
+    def Depth(self):
+        return self._read(L.FIELD_DEPTH, np.float32, self.W * self.H).reshape(self.H, self.W)
+
+    @property
+    def Planes(self):
+        return self._read(L.FIELD_PLANES, np.float32, self.n_planes)
+
+    @property
+    def Skip(self):
+        return self._read(L.FIELD_SKIP, np.uint8, self.W * self.H).reshape(self.H, self.W)
+
+    @property
+    def Start(self):
+        return self._read(L.FIELD_START, np.uint16, self.W * self.H).reshape(self.H, self.W)
+
+    @property
+    def Count(self):
+        return self._read(L.FIELD_COUNT, np.uint16, self.W * self.H).reshape(self.H, self.W)
+
+    @property
+    def Cap(self):
+        return self._read(L.FIELD_CAP, np.uint16, self.W * self.H).reshape(self.H, self.W)
+
+    @property
+    def Offsets(self):
+        return self._read(L.FIELD_OFFSETS, np.uint64, self.W * self.H + 1)
+
+    @property
+    def Agg(self):
+        """Final aggregates, CSR-flat: pixel i owns [Offsets[i], Offsets[i] + Cap[i])."""
+        return self._read(L.FIELD_AGG, np.uint16, self.volume)
+
+    @property
+    def AggPass1(self):
+        return self._read(L.FIELD_AGG_PASS1, np.uint16, self.volume)
+
+    @property
+    def Raw(self):
+        return self._read(L.FIELD_RAW, np.uint8, self.volume)
+
+    @property
+    def Guidance(self):
+        return self._read(L.FIELD_GUIDANCE, np.uint8, self.W * self.H * 4).reshape(self.H, self.W, 4)
+
+    def device_ptr(self, field_id):
+        return self.ctx.lib.lux_layer_device_ptr(self.handle, field_id)
+
+    def close(self):
+        if self.handle:
+            self.ctx.lib.lux_layer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DenseStereoPyramid:
+    @staticmethod
+    def run(images, gray, calibs, near=200.0, far=640000.0, keep_pass1=False, ctx: Optional[Context] = None) -> List[DenseLayer]:
+        """DenseStereoPyramid.Run (DenseStereoSgm.cs:331-353): the raw (unfiltered) camera images in, six layers out."""
+        ctx = ctx or default_context()
+        arr = (L.Img * len(images))()
+        keep = []
+        for i, im in enumerate(images):
+            ci, k = _img_c(im)
+            arr[i] = ci
+            keep.append(k)
+        g = np.ascontiguousarray(np.asarray(gray, dtype=np.uint8))
+        cc = _calibs_c(calibs)
+        outs = (ctypes.c_void_p * 6)()
+        ctx.check(ctx.lib.lux_sgm_pyramid(ctx.handle, len(images), arr, g.ctypes.data, cc, near, far, 1 if keep_pass1 else 0, outs))
+        return [DenseLayer(ctx, ctypes.c_void_p(outs[i])) for i in range(6)]
+
+
+@dataclass
+class UpsampleResult:
+    Depth: np.ndarray
+    W: int
+    H: int
+    Confidence: Optional[np.ndarray] = None
+
+
+class DenseUpsampleLayer:
+    Sigma = 12.0
+    Scale = 2
+
+    @staticmethod
+    def run(prev_depth, pw, ph, guide, set_w, set_h, sigma=12.0, scale=2, prev_confidence=None,
+            ctx: Optional[Context] = None) -> UpsampleResult:
+        """DenseUpsampleLayer.Run (DenseUpsampleLayer.cs:35-48) on the GPU."""
+        ctx = ctx or default_context()
+        gi, gkeep = _img_c(guide)
+        prev = np.ascontiguousarray(np.asarray(prev_depth, np.float32).reshape(-1))
+        out = np.empty(gi.w * gi.h, np.float32)
+        conf_out = None
+        conf_ptr = None
+        cin = None
+        if prev_confidence is not None:
+            cin = np.ascontiguousarray(np.asarray(prev_confidence, np.float32).reshape(-1))
+            conf_out = np.empty(gi.w * gi.h, np.float32)
+            conf_ptr = conf_out.ctypes.data
+        rc = ctx.lib.lux_sgm_upsample(ctx.handle, prev.ctypes.data, pw, ph, 0, ctypes.byref(gi), set_w, set_h, sigma, scale,
+                                      cin.ctypes.data if cin is not None else None, out.ctypes.data, conf_ptr)
+        ctx.check(rc)
+        return UpsampleResult(out.reshape(gi.h, gi.w), gi.w, gi.h,
+                              conf_out.reshape(gi.h, gi.w) if conf_out is not None else None)

@@ -1,0 +1,25 @@
+// Host-side geometry of the dense stage: plane list, flow matrices, skip masks, approximate reciprocals.
+// These run once per layer on a handful of values; the per-pixel work is on the GPU.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "../../include/lux_sgm.h"
+
+namespace lux {
+
+uint32_t host_rcp_bits(uint32_t b);    // IntelApprox.RcpBits (Lux.Engine/Imaging/IntelApprox.cs:21-29)
+uint32_t host_rsqrt_bits(uint32_t b);  // IntelApprox.RsqrtBits (IntelApprox.cs:32-45)
+float host_rcp(float x);
+const uint32_t* host_rcp_table();      // the 4096-entry table (uploaded to the device once per context)
+
+// DenseStereo.Planes (DenseStereo.cs:41-88); returns a LUX_ERR_* code.
+int host_planes(float near_, float far_, const lux_calib* calibs, int ncams, float density, int align, std::vector<float>& out);
+// Mat4D.FlowMatrix (ViewTransform.cs:126-133): column-major float M = (K_b·E_b)·(K_a·E_a)^-1 computed in double.
+void host_flow_matrix(const lux_calib& a, const lux_calib& b, float out[16]);
+// DenseLayer.SkipMask (DenseStereoSgm.cs:65-87); returns a LUX_ERR_* code.
+int host_skip_mask(int mode, int w, int h, std::vector<uint8_t>& m);
+// The plane-index boundaries of RangeFromPrevious (DenseStereoSgm.cs:94-96); returns whether they are non-decreasing.
+bool host_range_bounds(const std::vector<float>& planes, std::vector<float>& b);
+
+}  // namespace lux

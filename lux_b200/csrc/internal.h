@@ -1,0 +1,96 @@
+// Internal host-side interface between the C ABI (lux_sgm.cu) and the kernel files.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lux {
+
+constexpr int kMaxCams = 16;        // reference + up to 15 other cameras per layer (an L16 capture has 16 modules)
+// Every launch_* wrapper counts its kernels here (reported through lux_sgm_kernel_launches).
+void count_launches(int n);
+uint64_t kernel_launches();
+
+constexpr uint64_t kTimeoutNs = 20ull * 1000 * 1000 * 1000;  // bounded device waits: 20 s of %globaltimer
+
+// Layer geometry and per-pixel ranges, all device pointers.
+struct LayerGeom {
+  int W, H, n_planes, align, min_lo, max_hi, tile;
+  const float* planes;
+  const uchar4* guidance;
+  const uint8_t* skip;
+  const uint16_t* start;
+  const uint16_t* count;
+  const uint16_t* cap;
+  const uint64_t* off;
+  uint64_t volume;
+  bool uniform;  // every pixel searches [0, n) with cap n (first layer)
+};
+
+struct CostArgs {
+  const uint8_t* ref; int rw, rh;  // box-filtered reference image (dense RGBA8)
+  int n_others;
+  const uint8_t* other[kMaxCams];
+  int ow[kMaxCams], oh[kMaxCams];
+  float warp[kMaxCams][16];
+  uint16_t wq[kMaxCams][4];
+  float norm;                       // 0x3d17b426 / nOthers
+  int scale;
+};
+
+// prep.cu
+void launch_box_filter3(const uint8_t* src, int w, int h, int stride, uint8_t* dst, cudaStream_t s);
+void launch_guidance(const uint8_t* img0, int w0, int h0, int w, int h, int scale, uchar4* out, cudaStream_t s);
+// b: the n plane-index boundaries (device); monotone: b is non-decreasing (bisection gives the scan's answer)
+void launch_range_from_previous(const float* prev_depth, const uint8_t* prev_skip, int pw, int ph, const float* b, int monotone,
+                                int n, const uint32_t* rcp_table, int W, int H, int margin, uint16_t* start, uint16_t* count,
+                                int* minmax /* [0]=minLo [1]=maxHi, preset to INT_MAX, 0 */, void* scratch, cudaStream_t s);
+size_t range_from_previous_scratch_bytes(int pw, int ph);
+void launch_caps_offsets(const uint16_t* count, int npx, int align, uint16_t* cap, uint64_t* off, void* scratch, size_t scratch_bytes,
+                         cudaStream_t s);
+size_t caps_offsets_scratch_bytes(int npx);
+void launch_estimate_terms(const uint16_t* count, const uint8_t* skip, int npx, int align, unsigned long long* out_cost,
+                           cudaStream_t s);
+void launch_check_caps(const uint16_t* cap, int npx, int* err, cudaStream_t s);
+void launch_wta(const LayerGeom& g, const uint16_t* agg, float* depth, int* err, cudaStream_t s);
+void launch_fill_u16(uint16_t* p, size_t n, uint16_t v, cudaStream_t s);
+void launch_uniform_ranges(uint16_t* start, uint16_t* count, uint16_t* cap, uint64_t* off, int npx, int n, cudaStream_t s);
+// upsample chain (DenseUpsampleLayer.cs): g2 = NearestResize(ImageShift(guide)), then the bilateral upsample of 1/depth
+void launch_upsample(const float* prev, int pw, int ph, const uint8_t* guide, int gw, int gh, int gstride, float sigma,
+                     const uint32_t* rcp_table, uint8_t* g2, float* out_depth, const float* prev_conf, float* out_conf,
+                     cudaStream_t s);
+
+// cost.cu
+void launch_cost(const CostArgs& a, const LayerGeom& g, uint8_t* raw, int* err, cudaStream_t s);
+
+// sgm_emulate.cu: the exact replay of the reference's sheared-tile traversal on its line-buffer layout (any layer)
+struct EmuBuffers {
+  uint16_t* L; size_t Llen;
+  uint16_t* Min;
+  uint16_t* RangeS;
+  uint16_t* RangeC;
+  float4* Pix;
+  int* ticket;    // [2]
+  int* progress;  // [2 * bands]
+};
+size_t emu_line_buffer_elems(int W, int max_hi);
+void emu_init_buffers(const EmuBuffers& b, int W, int max_hi, int align, int bands, cudaStream_t s);
+void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xsw, uint16_t p1, float p2scale, const float gw[4],
+                        const uint8_t* raw, uint16_t* agg, int* err, cudaStream_t s);
+
+// sgm_uniform.cu: the fast aggregation of a uniform layer (every pixel searches all planes)
+struct UniformBuffers {
+  void* band_state;     // per CTA band: the last row's path states (boundary between CTA bands)
+  int* band_progress;   // per CTA band
+  int* ticket;          // [1]
+  void* side;           // per-row states of the two revisit-adjacent columns
+  void* edge_state;     // pass +1 final line-buffer row read by pass -1 (W+2 slots)
+  void* events;         // host-built revisit schedule
+};
+size_t uniform_supported_planes();
+bool uniform_fast_supported(int W, int H, int n_planes, int tile);
+size_t uniform_scratch_bytes(int W, int H, int n_planes, int tile);
+int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
+                    uint16_t* agg_pass1, float* depth, void* scratch, size_t scratch_bytes, int* err, cudaStream_t s);
+
+}  // namespace lux

@@ -1,0 +1,659 @@
+// C ABI of the dense-stereo depth stage (include/lux_sgm.h): contexts, device memory under an HBM budget, one layer,
+// the six-layer pyramid, and the upsample. The seams are DenseStereoPyramid.Run / DenseLayer (DenseStereoSgm.cs:331,
+// 34, 181) and DenseUpsampleLayer.Run (DenseUpsampleLayer.cs:35).
+#include <algorithm>
+#include <climits>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/lux_sgm.h"
+#include "host_geom.h"
+#include "internal.h"
+
+using namespace lux;
+
+struct lux_sgm_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t budget = 0;
+  uint64_t in_use = 0;
+  std::mutex mu;
+  std::string last_error;
+  uint32_t* d_rcp = nullptr;  // 4096-entry rcp table
+  int* d_err = nullptr;       // device error word of the current call
+  cudaEvent_t ev[4] = {};
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct lux_layer {
+  lux_sgm_ctx* ctx = nullptr;
+  int w = 0, h = 0, index = 0, align = 8, n = 0, min_lo = 0, max_hi = 0, tile = 4;
+  uint64_t volume = 0;
+  float ms_cost = 0.f, ms_sgm = 0.f, ms_wta = 0.f;
+  int sgm_kernel = 0;
+  std::vector<float> planes_h;
+  float* planes = nullptr;
+  uchar4* guidance = nullptr;
+  uint8_t* skip = nullptr;
+  uint16_t *start = nullptr, *count = nullptr, *cap = nullptr;
+  uint64_t* off = nullptr;
+  uint16_t* agg = nullptr;
+  uint16_t* agg_pass1 = nullptr;
+  uint8_t* raw = nullptr;
+  float* depth = nullptr;
+  std::vector<DevBuf> bufs;
+};
+
+namespace {
+
+int set_err(lux_sgm_ctx* ctx, int code, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+  }
+  return code;
+}
+
+const char* default_message(int code) {
+  switch (code) {
+    case LUX_ERR_NEAR_FAR: return "The near end has to be smaller than the fard end!";
+    case LUX_ERR_NONPOSITIVE: return "Both the near and far end have to be positive!";
+    case LUX_ERR_BASELINE: return "Baseline too small, check calibration.";
+    case LUX_ERR_SKIPMODE: return "unrecognized sampling pattern";
+    case LUX_ERR_BUDGET: return "StereoLayer memory budget exceeded: the BilateralUpsample fallback (mode 0) is not ported";
+    case LUX_ERR_UPSAMPLE_SIZE: return "Incorrect output depth size!";
+    case LUX_ERR_INDEX: return "Index was outside the bounds of the array (the reference indexes outside an array for these inputs)";
+    case LUX_ERR_TIMEOUT: return "a bounded device-side wait timed out";
+    default: return "error";
+  }
+}
+
+#define CK(call)                                                                                                   \
+  do {                                                                                                             \
+    cudaError_t e_ = (call);                                                                                       \
+    if (e_ != cudaSuccess) return set_err(ctx, LUX_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));     \
+  } while (0)
+
+// Device allocation from the stream-ordered pool, admitted against the context's HBM budget.
+int dev_alloc(lux_sgm_ctx* ctx, std::vector<DevBuf>& owner, size_t bytes, void** out) {
+  bytes = (bytes + 255) & ~(size_t)255;
+  if (bytes == 0) bytes = 256;
+  if (ctx->budget && ctx->in_use + bytes > ctx->budget)
+    return set_err(ctx, LUX_ERR_BUDGET, "HBM budget exceeded: %llu bytes in use + %llu requested > %llu budget",
+                   (unsigned long long)ctx->in_use, (unsigned long long)bytes, (unsigned long long)ctx->budget);
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, LUX_ERR_ALLOC, "device allocation of %llu bytes failed: %s", (unsigned long long)bytes, cudaGetErrorString(e));
+  }
+  ctx->in_use += bytes;
+  owner.push_back({p, bytes});
+  *out = p;
+  return LUX_OK;
+}
+
+void dev_free_all(lux_sgm_ctx* ctx, std::vector<DevBuf>& owner) {
+  for (auto& b : owner) {
+    cudaFreeAsync(b.p, ctx->stream);
+    ctx->in_use -= b.bytes;
+  }
+  owner.clear();
+}
+
+template <class T>
+int alloc_t(lux_sgm_ctx* ctx, std::vector<DevBuf>& owner, size_t count, T** out) {
+  void* p = nullptr;
+  int rc = dev_alloc(ctx, owner, count * sizeof(T), &p);
+  *out = static_cast<T*>(p);
+  return rc;
+}
+
+// Reads and clears the device error word.
+int take_device_error(lux_sgm_ctx* ctx) {
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (e) {
+    CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    return set_err(ctx, e, "%s", default_message(e));
+  }
+  return LUX_OK;
+}
+
+// Copies an image to the device as a dense RGBA8 buffer (or reuses a dense device image).
+int upload_image(lux_sgm_ctx* ctx, std::vector<DevBuf>& owner, const lux_img_rgba8& im, const uint8_t** out) {
+  if (!im.data || im.w <= 0 || im.h <= 0 || im.stride < im.w) return set_err(ctx, LUX_ERR_ARG, "invalid image");
+  if (im.on_device && im.stride == im.w) {
+    *out = im.data;
+    return LUX_OK;
+  }
+  uint8_t* d = nullptr;
+  int rc = alloc_t(ctx, owner, (size_t)im.w * im.h * 4, &d);
+  if (rc) return rc;
+  CK(cudaMemcpy2DAsync(d, (size_t)im.w * 4, im.data, (size_t)im.stride * 4, (size_t)im.w * 4, im.h,
+                       im.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+  *out = d;
+  return LUX_OK;
+}
+
+lux_stereo_params default_params() {
+  lux_stereo_params p;
+  std::memset(&p, 0, sizeof p);
+  p.margin = 1;
+  p.plane_density = 2.0f;
+  p.scale = 32;
+  p.skip_mode = 0;
+  p.p1 = 1;
+  p.p2scale = 500.0f;
+  uint32_t u = 0x3ef6384fu;
+  float g;
+  std::memcpy(&g, &u, 4);
+  p.guidance[0] = g / 6.0f;
+  p.guidance[1] = g / 16.0f;
+  p.guidance[2] = g / 16.0f;
+  p.guidance[3] = 0.0f;
+  p.tile = 4;
+  return p;
+}
+
+struct RangeResult {
+  int min_lo, max_hi_raw;
+};
+
+// RangeFromPrevious for a layer of size W×H with `planes` against the previous layer (device). start/count: device.
+int ranges_from_previous(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, const std::vector<float>& planes, const lux_layer* prev, int W,
+                         int H, int margin, uint16_t* start, uint16_t* count, RangeResult* rr) {
+  std::vector<float> b;
+  bool mono = host_range_bounds(planes, b);
+  float* db = nullptr;
+  int* mm = nullptr;
+  void* scratch = nullptr;
+  int rc;
+  if ((rc = alloc_t(ctx, tmp, b.size(), &db))) return rc;
+  if ((rc = alloc_t(ctx, tmp, 2, &mm))) return rc;
+  if ((rc = dev_alloc(ctx, tmp, range_from_previous_scratch_bytes(prev->w, prev->h), &scratch))) return rc;
+  int init[2] = {INT_MAX, 0};
+  CK(cudaMemcpyAsync(db, b.data(), b.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(mm, init, 8, cudaMemcpyHostToDevice, ctx->stream));
+  launch_range_from_previous(prev->depth, prev->skip, prev->w, prev->h, db, mono ? 1 : 0, (int)planes.size(), ctx->d_rcp, W, H,
+                             margin, start, count, mm, scratch, ctx->stream);
+  int res[2];
+  CK(cudaMemcpyAsync(res, mm, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  rr->min_lo = res[0];
+  rr->max_hi_raw = res[1];
+  return LUX_OK;
+}
+
+int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const int* iw, const int* ih, const uint8_t* gray,
+                const lux_calib* calibs, float near_, float far_, const lux_stereo_params& p, int index, int align, const lux_layer* prev,
+                int keep_pass1, lux_layer* L) {
+  int rc;
+  if (p.scale <= 0) return set_err(ctx, LUX_ERR_ARG, "scale must be positive");
+  if (p.tile < 2) return set_err(ctx, LUX_ERR_UNSUPPORTED, "tile %d: the GPU traversal needs a tile of at least 2", p.tile);
+  if (align <= 0) return set_err(ctx, LUX_ERR_ARG, "align must be positive");
+  L->ctx = ctx;
+  L->index = index;
+  L->align = align;
+  L->tile = p.tile;
+  if ((rc = host_planes(near_, far_, calibs, n_cams, p.plane_density, align, L->planes_h))) return set_err(ctx, rc, "%s", default_message(rc));
+  L->n = (int)L->planes_h.size();
+  if (n_cams < 2) return set_err(ctx, LUX_ERR_BASELINE, "%s", default_message(LUX_ERR_BASELINE));
+  if (n_cams > kMaxCams) return set_err(ctx, LUX_ERR_UNSUPPORTED, "at most %d cameras per layer", kMaxCams);
+  L->w = (iw[0] + p.scale - 1) / p.scale;
+  L->h = (ih[0] + p.scale - 1) / p.scale;
+  const int W = L->w, H = L->h;
+  const size_t npx = (size_t)W * H;
+  std::vector<uint8_t> skip;
+  if ((rc = host_skip_mask(p.skip_mode, W, H, skip))) return set_err(ctx, rc, "%s", default_message(rc));
+  auto& B = L->bufs;
+  if ((rc = alloc_t(ctx, B, (size_t)L->n, &L->planes))) return rc;
+  if ((rc = alloc_t(ctx, B, npx, &L->guidance))) return rc;
+  if ((rc = alloc_t(ctx, B, npx, &L->skip))) return rc;
+  if ((rc = alloc_t(ctx, B, npx, &L->start))) return rc;
+  if ((rc = alloc_t(ctx, B, npx, &L->count))) return rc;
+  if ((rc = alloc_t(ctx, B, npx, &L->cap))) return rc;
+  if ((rc = alloc_t(ctx, B, npx + 1, &L->off))) return rc;
+  if ((rc = alloc_t(ctx, B, npx, &L->depth))) return rc;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(L->planes, L->planes_h.data(), (size_t)L->n * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(L->skip, skip.data(), npx, cudaMemcpyHostToDevice, s));
+  launch_guidance(dimg[0], iw[0], ih[0], W, H, p.scale, L->guidance, s);
+  std::vector<DevBuf> tmp;
+  struct TmpGuard {
+    lux_sgm_ctx* c;
+    std::vector<DevBuf>* t;
+    ~TmpGuard() { dev_free_all(c, *t); }
+  } guard{ctx, &tmp};
+  bool uniform = prev == nullptr;
+  if (uniform) {  // DenseStereoSgm.cs:43-46
+    launch_uniform_ranges(L->start, L->count, L->cap, L->off, (int)npx, L->n, s);
+    L->min_lo = 0;
+    L->max_hi = ((L->n + align - 1) / align) * align;
+    L->volume = (uint64_t)npx * (uint64_t)L->n;
+  } else {
+    RangeResult rr;
+    if ((rc = ranges_from_previous(ctx, tmp, L->planes_h, prev, W, H, p.margin, L->start, L->count, &rr))) return rc;
+    L->min_lo = rr.min_lo;
+    L->max_hi = ((rr.max_hi_raw + align - 1) / align) * align;
+    void* scr = nullptr;
+    size_t sb = caps_offsets_scratch_bytes((int)npx);
+    if ((rc = dev_alloc(ctx, tmp, sb, &scr))) return rc;
+    launch_caps_offsets(L->count, (int)npx, align, L->cap, L->off, scr, sb, s);
+    CK(cudaMemcpyAsync(&L->volume, L->off + npx, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    launch_check_caps(L->cap, (int)npx, ctx->d_err, s);
+    if ((rc = take_device_error(ctx))) return rc;
+  }
+  if ((rc = alloc_t(ctx, B, L->volume + 8, &L->agg))) return rc;
+  if ((rc = alloc_t(ctx, B, L->volume + 8, &L->raw))) return rc;
+  CK(cudaMemsetAsync(L->agg, 0, (L->volume + 8) * 2, s));
+  if (!uniform) CK(cudaMemsetAsync(L->raw, 0, L->volume + 8, s));
+  if (keep_pass1) {
+    if ((rc = alloc_t(ctx, B, L->volume + 8, &L->agg_pass1))) return rc;
+  }
+  LayerGeom g;
+  g.W = W; g.H = H; g.n_planes = L->n; g.align = align; g.min_lo = L->min_lo; g.max_hi = L->max_hi; g.tile = p.tile;
+  g.planes = L->planes; g.guidance = L->guidance; g.skip = L->skip; g.start = L->start; g.count = L->count; g.cap = L->cap;
+  g.off = L->off; g.volume = L->volume; g.uniform = uniform;
+  // matching cost (DenseStereo.BuildContext + MatchingCost + Normalise)
+  CostArgs ca;
+  std::memset(&ca, 0, sizeof ca);
+  ca.ref = dimg[0]; ca.rw = iw[0]; ca.rh = ih[0];
+  ca.n_others = n_cams - 1;
+  for (int k = 1; k < n_cams; k++) {
+    ca.other[k - 1] = dimg[k];
+    ca.ow[k - 1] = iw[k];
+    ca.oh[k - 1] = ih[k];
+    host_flow_matrix(calibs[0], calibs[k], ca.warp[k - 1]);
+    static const uint16_t wg[4] = {12240, 0, 0, 0}, wc[4] = {8160, 680, 680, 0};
+    std::memcpy(ca.wq[k - 1], gray && gray[k] ? wg : wc, sizeof wg);
+  }
+  {
+    uint32_t u = 0x3d17b426u;
+    float f;
+    std::memcpy(&f, &u, 4);
+    volatile float nf = (float)ca.n_others;
+    ca.norm = f / nf;
+  }
+  ca.scale = p.scale;
+  CK(cudaEventRecord(ctx->ev[0], s));
+  launch_cost(ca, g, L->raw, ctx->d_err, s);
+  // aggregation: two passes over the sheared tiles, then WTA
+  CK(cudaEventRecord(ctx->ev[1], s));
+  const int bands = (H + p.tile - 1) / p.tile;
+  EmuBuffers eb;
+  eb.Llen = emu_line_buffer_elems(W, L->max_hi);
+  if ((rc = alloc_t(ctx, tmp, eb.Llen, &eb.L))) return rc;
+  if ((rc = alloc_t(ctx, tmp, (size_t)2 * (W + 2) * 4, &eb.Min))) return rc;
+  if ((rc = alloc_t(ctx, tmp, (size_t)2 * (W + 2), &eb.RangeS))) return rc;
+  if ((rc = alloc_t(ctx, tmp, (size_t)2 * (W + 2), &eb.RangeC))) return rc;
+  if ((rc = alloc_t(ctx, tmp, (size_t)2 * (W + 2), &eb.Pix))) return rc;
+  if ((rc = alloc_t(ctx, tmp, 2, &eb.ticket))) return rc;
+  if ((rc = alloc_t(ctx, tmp, (size_t)2 * bands, &eb.progress))) return rc;
+  emu_init_buffers(eb, W, L->max_hi, align, bands, s);
+  const int xsw = 0;  // LUX_SGM_XSW unset: the reference default
+  launch_sgm_emulate(g, eb, +1, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, ctx->d_err, s);
+  if (keep_pass1) CK(cudaMemcpyAsync(L->agg_pass1, L->agg, (L->volume + 8) * 2, cudaMemcpyDeviceToDevice, s));
+  launch_sgm_emulate(g, eb, -1, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, ctx->d_err, s);
+  CK(cudaEventRecord(ctx->ev[2], s));
+  launch_wta(g, L->agg, L->depth, ctx->d_err, s);
+  CK(cudaEventRecord(ctx->ev[3], s));
+  CK(cudaGetLastError());
+  if ((rc = take_device_error(ctx))) return rc;
+  CK(cudaEventElapsedTime(&L->ms_cost, ctx->ev[0], ctx->ev[1]));
+  CK(cudaEventElapsedTime(&L->ms_sgm, ctx->ev[1], ctx->ev[2]));
+  CK(cudaEventElapsedTime(&L->ms_wta, ctx->ev[2], ctx->ev[3]));
+  return LUX_OK;
+}
+
+void destroy_layer(lux_layer* L) {
+  if (!L) return;
+  if (L->ctx) {
+    dev_free_all(L->ctx, L->bufs);
+    cudaStreamSynchronize(L->ctx->stream);
+  }
+  delete L;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lux_sgm_create(int device, uint64_t hbm_budget_bytes, lux_sgm_ctx** out) {
+  if (!out) return LUX_ERR_ARG;
+  *out = nullptr;
+  lux_sgm_ctx* ctx = new lux_sgm_ctx();
+  ctx->device = device;
+  ctx->budget = hbm_budget_bytes;
+  auto fail = [&](int code) {
+    delete ctx;
+    return code;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return fail(LUX_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(LUX_ERR_CUDA);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;  // keep freed blocks in the pool: later requests of the same sizes allocate nothing new
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  if (cudaMalloc(&ctx->d_rcp, 4096 * 4) != cudaSuccess) return fail(LUX_ERR_ALLOC);
+  if (cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) return fail(LUX_ERR_ALLOC);
+  cudaMemcpy(ctx->d_rcp, host_rcp_table(), 4096 * 4, cudaMemcpyHostToDevice);
+  cudaMemset(ctx->d_err, 0, sizeof(int));
+  for (auto& e : ctx->ev) cudaEventCreate(&e);
+  *out = ctx;
+  return LUX_OK;
+}
+
+void lux_sgm_destroy(lux_sgm_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& e : ctx->ev) cudaEventDestroy(e);
+  cudaFree(ctx->d_rcp);
+  cudaFree(ctx->d_err);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* lux_sgm_last_error(const lux_sgm_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+
+uint64_t lux_sgm_kernel_launches(void) { return lux::kernel_launches(); }
+
+void* lux_sgm_stream(lux_sgm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int lux_sgm_sync(lux_sgm_ctx* ctx) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CK(cudaStreamSynchronize(ctx->stream));
+  return LUX_OK;
+}
+
+void lux_sgm_default_params(lux_stereo_params* p) {
+  if (p) *p = default_params();
+}
+
+void lux_sgm_l16_pyramid(lux_stereo_params out[6]) {  // StereoParams.L16Pyramid(false) (DenseStereo.cs:24-30)
+  static const int scales[6] = {32, 16, 8, 4, 2, 1}, tiles[6] = {4, 8, 16, 32, 64, 64};
+  for (int i = 0; i < 6; i++) {
+    out[i] = default_params();
+    out[i].scale = scales[i];
+    out[i].tile = tiles[i];
+    out[i].skip_mode = i >= 4 ? 2 : 0;
+    out[i].plane_density = 2.0f;
+  }
+}
+
+int lux_sgm_planes(float near_, float far_, const lux_calib* calibs, int32_t n_cams, float density, int32_t align, float* out,
+                   int32_t* n_out) {
+  if (!calibs || !out || !n_out) return LUX_ERR_ARG;
+  std::vector<float> pl;
+  int rc = host_planes(near_, far_, calibs, n_cams, density, align, pl);
+  if (rc) return rc;
+  std::memcpy(out, pl.data(), pl.size() * 4);
+  *n_out = (int32_t)pl.size();
+  return LUX_OK;
+}
+
+int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst) {
+  if (!ctx || !src || !dst) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  const uint8_t* d_src = nullptr;
+  uint8_t* d_dst = nullptr;
+  int rc = upload_image(ctx, tmp, *src, &d_src);
+  if (!rc) rc = alloc_t(ctx, tmp, (size_t)src->w * src->h * 4, &d_dst);
+  if (!rc) {
+    launch_box_filter3(d_src, src->w, src->h, src->w, d_dst, ctx->stream);
+    if (cudaMemcpyAsync(dst, d_dst, (size_t)src->w * src->h * 4, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+      rc = set_err(ctx, LUX_ERR_CUDA, "box filter copy failed");
+  }
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
+int lux_sgm_layer(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
+                  float near_, float far_, const lux_stereo_params* params, int32_t index, int32_t align, const lux_layer* prev,
+                  int32_t keep_pass1, int32_t prefilter, lux_layer** out) {
+  if (!ctx || !images || !calibs || !params || !out || n_cams <= 0) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  *out = nullptr;
+  if (n_cams > kMaxCams) return set_err(ctx, LUX_ERR_UNSUPPORTED, "at most %d cameras per layer", kMaxCams);
+  lux_layer* L = new lux_layer();
+  L->ctx = ctx;
+  std::vector<DevBuf> imgs;
+  std::vector<const uint8_t*> dimg((size_t)n_cams);
+  std::vector<int> iw((size_t)n_cams), ih((size_t)n_cams);
+  int rc = LUX_OK;
+  for (int k = 0; k < n_cams && !rc; k++) {
+    rc = upload_image(ctx, imgs, images[k], &dimg[k]);
+    iw[k] = images[k].w;
+    ih[k] = images[k].h;
+    if (!rc && prefilter) {  // DenseStereo.BoxFilter3 on the device
+      uint8_t* f = nullptr;
+      rc = alloc_t(ctx, imgs, (size_t)iw[k] * ih[k] * 4, &f);
+      if (!rc) launch_box_filter3(dimg[k], iw[k], ih[k], iw[k], f, ctx->stream);
+      dimg[k] = f;
+    }
+  }
+  if (!rc) rc = build_layer(ctx, n_cams, dimg.data(), iw.data(), ih.data(), gray, calibs, near_, far_, *params, index, align, prev,
+                            keep_pass1, L);
+  dev_free_all(ctx, imgs);
+  if (rc) {
+    destroy_layer(L);
+    return rc;
+  }
+  *out = L;
+  return LUX_OK;
+}
+
+int lux_sgm_pyramid(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
+                    float near_, float far_, int32_t keep_pass1, lux_layer* out[6]) {
+  if (!ctx || !images || !calibs || !out || n_cams <= 0) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  for (int i = 0; i < 6; i++) out[i] = nullptr;
+  if (n_cams > kMaxCams) return set_err(ctx, LUX_ERR_UNSUPPORTED, "at most %d cameras per layer", kMaxCams);
+  lux_stereo_params pars[6];
+  lux_sgm_l16_pyramid(pars);
+  std::vector<DevBuf> imgs;
+  std::vector<const uint8_t*> raw_img((size_t)n_cams);
+  std::vector<const uint8_t*> filt((size_t)n_cams);
+  std::vector<int> iw((size_t)n_cams), ih((size_t)n_cams);
+  int rc = LUX_OK;
+  for (int k = 0; k < n_cams && !rc; k++) {  // BoxFilter3 per camera, shared by all layers (DenseStereoSgm.cs:335)
+    rc = upload_image(ctx, imgs, images[k], &raw_img[k]);
+    iw[k] = images[k].w;
+    ih[k] = images[k].h;
+    uint8_t* f = nullptr;
+    if (!rc) rc = alloc_t(ctx, imgs, (size_t)iw[k] * ih[k] * 4, &f);
+    if (!rc) launch_box_filter3(raw_img[k], iw[k], ih[k], iw[k], f, ctx->stream);
+    filt[k] = f;
+  }
+  lux_layer* prev = nullptr;
+  for (int i = 0; i < 6 && !rc; i++) {
+    int align = 8;
+    if (prev) {  // align 8 when the estimate fits the 1 GiB budget, else align 2, else unsupported (:340-344)
+      int64_t est[2] = {0, 0};
+      const int aligns[2] = {8, 2};
+      for (int t = 0; t < 2 && !rc; t++) {
+        std::vector<float> pl;
+        rc = host_planes(near_, far_, calibs, n_cams, pars[i].plane_density, aligns[t], pl);
+        if (rc) { set_err(ctx, rc, "%s", default_message(rc)); break; }
+        const int W = (iw[0] + pars[i].scale - 1) / pars[i].scale, H = (ih[0] + pars[i].scale - 1) / pars[i].scale;
+        const size_t npx = (size_t)W * H;
+        std::vector<uint8_t> sk;
+        rc = host_skip_mask(pars[i].skip_mode, W, H, sk);
+        if (rc) { set_err(ctx, rc, "%s", default_message(rc)); break; }
+        std::vector<DevBuf> tmp;
+        uint16_t *st = nullptr, *ct = nullptr;
+        uint8_t* dsk = nullptr;
+        unsigned long long* acc = nullptr;
+        RangeResult rr{0, 0};
+        if (!rc) rc = alloc_t(ctx, tmp, npx, &st);
+        if (!rc) rc = alloc_t(ctx, tmp, npx, &ct);
+        if (!rc) rc = alloc_t(ctx, tmp, npx, &dsk);
+        if (!rc) rc = alloc_t(ctx, tmp, 1, &acc);
+        if (!rc) rc = ranges_from_previous(ctx, tmp, pl, prev, W, H, pars[i].margin, st, ct, &rr);
+        unsigned long long cost = 0;
+        if (!rc) {
+          cudaMemcpyAsync(dsk, sk.data(), npx, cudaMemcpyHostToDevice, ctx->stream);
+          cudaMemsetAsync(acc, 0, 8, ctx->stream);
+          launch_estimate_terms(ct, dsk, (int)npx, aligns[t], acc, ctx->stream);
+          cudaMemcpyAsync(&cost, acc, 8, cudaMemcpyDeviceToHost, ctx->stream);
+          if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = set_err(ctx, LUX_ERR_CUDA, "estimate failed");
+        }
+        dev_free_all(ctx, tmp);
+        if (rc) break;
+        // MemoryEstimate (DenseStereoSgm.cs:152-155)
+        int64_t maxHi = ((rr.max_hi_raw + aligns[t] - 1) / aligns[t]) * aligns[t];
+        int64_t w = W, h = H, im = 0;
+        for (int k = 0; k < n_cams; k++) im += (int64_t)ih[k] * iw[k] * 4;
+        est[t] = (int64_t)cost + w * h * 4 + 20 * (2 * w + 4) + 2 * ((4 * maxHi + 5) * (2 * w + 4) + 8 * w + 16) + im + w * h * 8;
+        if (t == 0 && est[0] < 0x40000000LL) break;
+      }
+      if (rc) break;
+      if (est[0] >= 0x40000000LL) {
+        if (est[1] >= 0x40000000LL) { rc = set_err(ctx, LUX_ERR_BUDGET, "%s", default_message(LUX_ERR_BUDGET)); break; }
+        align = 2;
+      }
+    }
+    lux_layer* L = new lux_layer();
+    rc = build_layer(ctx, n_cams, filt.data(), iw.data(), ih.data(), gray, calibs, near_, far_, pars[i], i, align, prev, keep_pass1, L);
+    if (rc) {
+      destroy_layer(L);
+      break;
+    }
+    out[i] = L;
+    prev = L;
+  }
+  dev_free_all(ctx, imgs);
+  if (rc) {
+    for (int i = 0; i < 6; i++) {
+      destroy_layer(out[i]);
+      out[i] = nullptr;
+    }
+  }
+  return rc;
+}
+
+int lux_layer_get_info(const lux_layer* L, lux_layer_info* info) {
+  if (!L || !info) return LUX_ERR_ARG;
+  info->w = L->w; info->h = L->h; info->index = L->index; info->align = L->align; info->n_planes = L->n;
+  info->min_lo = L->min_lo; info->max_hi = L->max_hi; info->tile = L->tile; info->volume = L->volume;
+  info->gpu_ms_cost = L->ms_cost; info->gpu_ms_sgm = L->ms_sgm; info->gpu_ms_wta = L->ms_wta;
+  info->sgm_kernel = L->sgm_kernel;
+  return LUX_OK;
+}
+
+static const void* field_ptr(const lux_layer* L, int32_t field, size_t* bytes) {
+  const size_t npx = (size_t)L->w * L->h;
+  switch (field) {
+    case LUX_FIELD_DEPTH: *bytes = npx * 4; return L->depth;
+    case LUX_FIELD_PLANES: *bytes = (size_t)L->n * 4; return L->planes;
+    case LUX_FIELD_SKIP: *bytes = npx; return L->skip;
+    case LUX_FIELD_START: *bytes = npx * 2; return L->start;
+    case LUX_FIELD_COUNT: *bytes = npx * 2; return L->count;
+    case LUX_FIELD_CAP: *bytes = npx * 2; return L->cap;
+    case LUX_FIELD_OFFSETS: *bytes = (npx + 1) * 8; return L->off;
+    case LUX_FIELD_AGG: *bytes = L->volume * 2; return L->agg;
+    case LUX_FIELD_AGG_PASS1: *bytes = L->volume * 2; return L->agg_pass1;
+    case LUX_FIELD_RAW: *bytes = L->volume; return L->raw;
+    case LUX_FIELD_GUIDANCE: *bytes = npx * 4; return L->guidance;
+    default: *bytes = 0; return nullptr;
+  }
+}
+
+int lux_layer_read(const lux_layer* L, int32_t field, void* dst, uint64_t bytes) {
+  if (!L || !dst) return LUX_ERR_ARG;
+  lux_sgm_ctx* ctx = L->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  size_t need = 0;
+  const void* p = field_ptr(L, field, &need);
+  if (!p) return set_err(ctx, LUX_ERR_ARG, "field %d is not available", field);
+  if (bytes != need) return set_err(ctx, LUX_ERR_ARG, "field %d holds %llu bytes, %llu given", field, (unsigned long long)need,
+                                    (unsigned long long)bytes);
+  CK(cudaMemcpyAsync(dst, p, need, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return LUX_OK;
+}
+
+const void* lux_layer_device_ptr(const lux_layer* L, int32_t field) {
+  if (!L) return nullptr;
+  size_t b;
+  return field_ptr(L, field, &b);
+}
+
+void lux_layer_destroy(lux_layer* L) {
+  if (!L) return;
+  lux_sgm_ctx* ctx = L->ctx;
+  if (ctx) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    destroy_layer(L);
+  } else {
+    delete L;
+  }
+}
+
+int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int32_t ph, int32_t prev_on_device,
+                     const lux_img_rgba8* guide, int32_t set_w, int32_t set_h, float sigma, int32_t scale, const float* prev_conf,
+                     float* out_depth, float* out_conf) {
+  if (!ctx || !prev_depth || !guide || !out_depth || pw <= 0 || ph <= 0) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  const int gw = guide->w, gh = guide->h;
+  const size_t npo = (size_t)gw * gh, npp = (size_t)pw * ph;
+  const uint8_t* dguide = nullptr;
+  float *dprev = nullptr, *dout = nullptr, *dconf = nullptr, *dpc = nullptr;
+  uint8_t* g2 = nullptr;
+  int rc = upload_image(ctx, tmp, *guide, &dguide);
+  if (!rc) {
+    if (prev_on_device) dprev = const_cast<float*>(prev_depth);
+    else if (!(rc = alloc_t(ctx, tmp, npp, &dprev)))
+      if (cudaMemcpyAsync(dprev, prev_depth, npp * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) rc = LUX_ERR_CUDA;
+  }
+  if (!rc) rc = alloc_t(ctx, tmp, npp, &g2);
+  if (!rc) rc = alloc_t(ctx, tmp, npo, &dout);
+  const bool conf = prev_conf && out_conf;
+  if (!rc && conf) {
+    rc = alloc_t(ctx, tmp, npo, &dconf);
+    if (!rc) rc = alloc_t(ctx, tmp, npp, &dpc);
+    if (!rc && cudaMemcpyAsync(dpc, prev_conf, npp * 4, prev_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                               ctx->stream) != cudaSuccess)
+      rc = LUX_ERR_CUDA;
+  }
+  if (!rc) {
+    launch_upsample(dprev, pw, ph, dguide, gw, gh, gw, sigma, ctx->d_rcp, g2, dout, conf ? dpc : nullptr, dconf, ctx->stream);
+    if (cudaMemcpyAsync(out_depth, dout, npo * 4, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) rc = LUX_ERR_CUDA;
+    if (!rc && conf && cudaMemcpyAsync(out_conf, dconf, npo * 4, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) rc = LUX_ERR_CUDA;
+    if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = LUX_ERR_CUDA;
+    if (rc) set_err(ctx, rc, "upsample failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  dev_free_all(ctx, tmp);
+  if (rc) return rc;
+  // the size check comes after the computation in the reference too (DenseUpsampleLayer.cs:43)
+  if (gw != set_w * scale || gh != set_h * scale) return set_err(ctx, LUX_ERR_UPSAMPLE_SIZE, "%s", default_message(LUX_ERR_UPSAMPLE_SIZE));
+  return LUX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,210 @@
+// Exact replay of DenseLayer.Compute's aggregation (DenseStereoSgm.cs:206-224) on the reference's own line-buffer layout.
+//
+// The reference's result depends on its traversal, not only on the SGM recurrence: sheared T-wide tiles visit the last
+// column twice per band in pass +1 (column 0 in pass -1), ragged per-pixel plane ranges spill across path blocks, reads
+// past a block see whatever the flat buffer holds there, and pass -1 starts from the state pass +1 left. This kernel
+// keeps the flat buffer (2 halves x (W+2) slots x (4·MaxHi+5) u16, plus Min/RangeS/RangeC/Pix) in global memory and runs
+// every Pixel() call of the reference in an order that gives each read the same last writer:
+//   * one CTA per band of T rows (tickets taken in order, so a band only ever waits on a running one);
+//   * tiles of a band in order; band j starts tile i once band j-1 has finished tile i+2: from tile i+3 on, a band
+//     touches no slot that tile i of the band below touches (slots within [iT-T, iT+T+2]);
+//   * inside a tile, pixel (row r, sheared offset u) runs at step u + 2r. Pixels that share or neighbour a slot (at most
+//     two columns and two rows apart) keep the reference's row-major order; pixels of one step are three or more
+//     columns apart. A revisit of the last column runs alone at step 2r.
+// Within a Pixel() call a warp handles the lanes, and the four paths run in order (a path may spill into the next).
+#include "common.cuh"
+#include "internal.h"
+
+namespace lux {
+
+struct EmuArgs {
+  int W, H, T, dir, xsw, min_lo, max_hi, slot_stride, halfL, halfM, halfR, gwN, ghN;
+  long long Llen;
+  uint16_t* L;
+  uint16_t* Min;
+  uint16_t* RangeS;
+  uint16_t* RangeC;
+  float4* Pix;
+  const uchar4* guidance;
+  const uint8_t* skip;
+  const uint16_t* start;
+  const uint16_t* count;
+  const uint16_t* cap;
+  const uint64_t* off;
+  const uint8_t* raw;
+  uint16_t* agg;
+  int p1;
+  float p2base;
+  float gw[4];
+  int* ticket;
+  int* progress;
+  int* err;
+  unsigned long long timeout_ns;
+};
+
+LUX_DEV int rd(const EmuArgs& a, long long i) {  // Rd (DenseStereoSgm.cs:324)
+  return i < 0 ? 2000 : i < a.Llen ? (int)__ldcg(a.L + i) : 0;
+}
+
+// Pixel (DenseStereoSgm.cs:234-317), one warp.
+LUX_DEV void emu_pixel(const EmuArgs& a, int x, int y, int cur, int other, int lane) {
+  const int pi = y * a.W + x, slot = x + 1;
+  const uchar4 gb = a.guidance[pi];
+  const float g[4] = {(float)gb.x, (float)gb.y, (float)gb.z, (float)gb.w};
+  if (lane == 0) __stcg(a.Pix + cur * a.halfR + slot, make_float4(g[0], g[1], g[2], g[3]));
+  const int start = a.start[pi], count = a.count[pi], cap = a.cap[pi];
+  const bool skipped = a.skip[pi] != 0;
+  const uint8_t* rawp = a.raw + a.off[pi];
+  uint16_t* aggp = a.agg + a.off[pi];
+  const int sp = __ldcg(a.RangeS + cur * a.halfR + slot), cp = __ldcg(a.RangeC + cur * a.halfR + slot);
+  for (int p = 0; p < 4; p++) {
+    const long long baseCur = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
+    {  // stale cleanup of the previously stored range (:261-263)
+      long long q0 = sp - a.min_lo, k0 = q0 < 0 ? -q0 : 0;
+      long long k1 = min((long long)cp, a.Llen - baseCur - q0);
+      for (long long k = k0 + lane; k < k1; k += 32) __stcg(a.L + baseCur + q0 + k, (uint16_t)2000);
+    }
+    __syncwarp();
+    const int ns = slot + (p == 2 ? 0 : p == 3 ? a.dir : -a.dir);
+    const int half = p == 0 ? cur : other;
+    const int minPrev = __ldcg(a.Min + half * a.halfM + ns * 4 + p);
+    const float4 pn4 = __ldcg(a.Pix + half * a.halfR + ns);
+    const float pn[4] = {pn4.x, pn4.y, pn4.z, pn4.w};
+    const int P2 = sgm_p2(g, pn, a.gw, a.p2base);
+    const int P2p = min(P2 + minPrev, 65535);
+    if (cap == 0) {
+      __syncwarp();
+      if (lane == 0) __stcg(a.Min + cur * a.halfM + slot * 4 + p, (uint16_t)0xffff);
+      __syncwarp();
+      continue;
+    }
+    const long long nb = (long long)half * a.halfL + (long long)ns * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
+    const long long q = start - a.min_lo;
+    int runMin = 0xffff;
+    for (int k = lane; k < cap; k += 32) {  // caps are multiples of 8 here (checked before the launch)
+      const long long qi = q + k;
+      const int Lm = rd(a, nb + qi - 1), L0 = rd(a, nb + qi), Lp = rd(a, nb + qi + 1);
+      const int m = min(min(min(Lm + a.p1, 65535), L0), min(min(Lp + a.p1, 65535), P2p));
+      const int rv = skipped ? (k < count ? 0 : 255) : rawp[k];
+      int lc = min(rv + m, 65535) - minPrev;
+      if (lc < 0) lc = 0;
+      const long long wi = baseCur + qi;
+      if (wi < 0 || wi >= a.Llen) atomicCAS(a.err, 0, 7);
+      else __stcg(a.L + wi, (uint16_t)lc);
+      runMin = min(runMin, lc);
+      aggp[k] = (uint16_t)min((int)aggp[k] + lc, 65535);
+    }
+    runMin = __reduce_min_sync(0xffffffffu, (unsigned)runMin);
+    __syncwarp();
+    if (lane == 0) __stcg(a.Min + cur * a.halfM + slot * 4 + p, (uint16_t)runMin);
+    __syncwarp();
+  }
+  if (lane == 0) {
+    __stcg(a.RangeS + cur * a.halfR + slot, (uint16_t)start);
+    __stcg(a.RangeC + cur * a.halfR + slot, (uint16_t)cap);
+  }
+  __syncwarp();
+}
+
+__global__ void k_sgm_emulate(const EmuArgs a) {
+  __shared__ int s_band, s_stop;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  if (tid == 0) {
+    s_band = atomicAdd(a.ticket, 1);
+    s_stop = 0;
+  }
+  __syncthreads();
+  const int j = s_band;
+  const int T = a.T;
+  if (j >= a.ghN) return;
+  for (int i = 0; i < a.gwN; i++) {
+    if (tid == 0) {
+      if (j > 0 && !wait_at_least(a.progress + (j - 1), min(i + 3, a.gwN), a.err, 11 /* LUX_ERR_TIMEOUT */, a.timeout_ns)) s_stop = 1;
+      if (*(volatile int*)a.err != 0) s_stop = 1;
+    }
+    __syncthreads();
+    if (s_stop) break;
+    for (int t = 0; t <= 3 * T - 3; t++) {
+      const int rlo = max(0, (t - T + 2) / 2), rhi = min(T - 1, t / 2);
+      for (int r = rlo + warp; r <= rhi; r += nw) {
+        const int u = t - 2 * r;
+        const int yp = j * T + r;
+        if (yp >= a.H) continue;  // yEnd (:213)
+        const int xs = min(max(i * T - r, 0), (a.xsw && a.dir > 0) ? a.W : a.W - 1);
+        const int xe = min(max(i * T + T - r, -1), a.W);
+        if (xs == xe) continue;
+        int xp;
+        if (i * T - r >= a.W) {  // the clamped row start revisits the last column
+          if (u != 0) continue;
+          xp = a.W - 1;
+        } else {
+          xp = i * T - r + u;
+          if (xp < xs || xp >= xe) continue;
+        }
+        const int x = a.dir > 0 ? xp : a.W - 1 - xp;
+        const int y = a.dir > 0 ? yp : a.H - 1 - yp;
+        const int cur = (r & 1) == 0 ? 1 : 0;
+        emu_pixel(a, x, y, cur, 1 - cur, lane);
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      __threadfence();
+      st_release(a.progress + j, i + 1);
+    }
+  }
+}
+
+size_t emu_line_buffer_elems(int W, int max_hi) { return (size_t)2 * (W + 2) * (4 * (size_t)max_hi + 5); }
+
+__global__ void k_emu_init(uint16_t* Min, uint16_t* RangeS, uint16_t* RangeC, float4* Pix, int slots, int align) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 2 * slots * 4) Min[i] = 2000;
+  if (i < 2 * slots) {
+    RangeS[i] = 0;
+    RangeC[i] = (uint16_t)align;
+    Pix[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+void emu_init_buffers(const EmuBuffers& b, int W, int max_hi, int align, int bands, cudaStream_t s) {
+  launch_fill_u16(b.L, b.Llen, 2000, s);  // AllocLineBuffers (DenseStereoSgm.cs:158-165)
+  int slots = W + 2;
+  k_emu_init<<<(2 * slots * 4 + 255) / 256, 256, 0, s>>>(b.Min, b.RangeS, b.RangeC, b.Pix, slots, align);
+  count_launches(1);
+  cudaMemsetAsync(b.ticket, 0, 2 * sizeof(int), s);
+  cudaMemsetAsync(b.progress, 0, (size_t)2 * bands * sizeof(int), s);
+}
+
+void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xsw, uint16_t p1, float p2scale, const float gw[4],
+                        const uint8_t* raw, uint16_t* agg, int* err, cudaStream_t s) {
+  EmuArgs a;
+  a.W = g.W; a.H = g.H; a.T = g.tile; a.dir = dir; a.xsw = xsw;
+  a.min_lo = g.min_lo; a.max_hi = g.max_hi;
+  a.slot_stride = 4 * g.max_hi + 5;
+  a.halfL = (g.W + 2) * a.slot_stride;
+  a.halfM = (g.W + 2) * 4;
+  a.halfR = g.W + 2;
+  a.gwN = (g.W + 2 * g.tile - 1) / g.tile;
+  a.ghN = (g.H + g.tile - 1) / g.tile;
+  a.Llen = (long long)b.Llen;
+  a.L = b.L; a.Min = b.Min; a.RangeS = b.RangeS; a.RangeC = b.RangeC; a.Pix = b.Pix;
+  a.guidance = g.guidance; a.skip = g.skip; a.start = g.start; a.count = g.count; a.cap = g.cap; a.off = g.off;
+  a.raw = raw; a.agg = agg;
+  a.p1 = p1;
+  volatile float p1f = (float)p1;
+  a.p2base = p1f * p2scale;  // (float)P1 * P2Scale (:256)
+  for (int i = 0; i < 4; i++) a.gw[i] = gw[i];
+  int pass = dir > 0 ? 0 : 1;
+  a.ticket = b.ticket + pass;
+  a.progress = b.progress + (size_t)pass * a.ghN;
+  a.err = err;
+  a.timeout_ns = kTimeoutNs;
+  int nw = g.tile / 2;
+  if (nw < 1) nw = 1;
+  if (nw > 32) nw = 32;
+  k_sgm_emulate<<<a.ghN, nw * 32, 0, s>>>(a);
+  count_launches(1);
+}
+
+}  // namespace lux

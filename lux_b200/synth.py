@@ -1,0 +1,181 @@
+"""Seeded synthetic stereo inputs for the benchmark workloads (no datasets or real captures are available offline).
+
+A workload is a rectified pair (or a multi-camera capture) expressed in the reference's own input domain: RGBA8
+"YUVA" images (grey = (Y, 128, 128, 255)) and CalibData with a pure horizontal baseline, so that plane k of the
+plane sweep is disparity k (PlaneDensity 1, a far plane at 1e30 m, near = f·B/(D-1)):
+  * texture: a 1/f-spectrum noise image, scaled to the full range of the bit depth;
+  * ground truth: six seeded piecewise-planar disparity segments (Voronoi cells) in [0, D-1];
+  * the other image: the reference warped by the disparity (nearest surface wins), holes filled by edge repeat,
+    plus N(0, sigma^2) noise; 12-bit data is mapped to bytes with (v + 8) >> 4, saturated.
+"""
+from dataclasses import dataclass
+from typing import List
+
+import numpy as np
+
+from .api import CalibData, StereoParams
+
+
+def texture(h, w, seed, max_value=255.0):
+    """1/f-spectrum texture in [0, max_value]."""
+    rng = np.random.default_rng(seed)
+    noise = rng.standard_normal((h, w)).astype(np.float32)
+    spec = np.fft.rfft2(noise)
+    fy = np.fft.fftfreq(h)[:, None]
+    fx = np.fft.rfftfreq(w)[None, :]
+    f = np.sqrt(fx * fx + fy * fy)
+    f[0, 0] = 1.0
+    spec = spec / f
+    spec[0, 0] = 0.0
+    img = np.fft.irfft2(spec, s=(h, w)).astype(np.float32)
+    lo, hi = np.percentile(img, 0.5), np.percentile(img, 99.5)
+    img = (img - lo) / max(hi - lo, 1e-6)
+    return np.clip(img, 0.0, 1.0) * max_value
+
+
+def planar_disparity(h, w, d_max, seed, segments=6):
+    """Six seeded planar segments (Voronoi cells), values clamped to [0, d_max]."""
+    rng = np.random.default_rng(seed + 7919)
+    cy = rng.uniform(0, h, segments)
+    cx = rng.uniform(0, w, segments)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    d2 = (yy[None] - cy[:, None, None]) ** 2 + (xx[None] - cx[:, None, None]) ** 2
+    lab = np.argmin(d2, axis=0)
+    disp = np.zeros((h, w), np.float32)
+    for s in range(segments):
+        base = rng.uniform(0.1, 0.9) * d_max
+        gx = rng.uniform(-0.3, 0.3) * d_max / w
+        gy = rng.uniform(-0.3, 0.3) * d_max / h
+        m = lab == s
+        disp[m] = base + gx * (xx[m] - cx[s]) + gy * (yy[m] - cy[s])
+    return np.clip(disp, 0, d_max)
+
+
+def warp_other(left, disp, seed, sigma, max_value):
+    """The other view: right(x - d) = left(x), nearest surface (largest d) wins, holes by edge repeat, + noise."""
+    h, w = left.shape
+    d = np.rint(disp).astype(np.int64)
+    xl = np.broadcast_to(np.arange(w), (h, w))
+    xr = xl - d
+    order = np.argsort(d, axis=1, kind="stable")  # ascending d: the largest d is written last and wins
+    rows = np.arange(h)[:, None]
+    xr_o = np.take_along_axis(xr, order, 1)
+    val_o = np.take_along_axis(left, order, 1)
+    ok = (xr_o >= 0) & (xr_o < w)
+    right = np.full((h, w), np.nan, np.float32)
+    rr = np.broadcast_to(rows, (h, w))[ok]
+    right[rr, xr_o[ok]] = val_o[ok]
+    # edge repeat: carry the last filled value to the right; leading holes take the first filled value
+    filled = ~np.isnan(right)
+    idx = np.where(filled, np.arange(w)[None, :], 0)
+    np.maximum.accumulate(idx, axis=1, out=idx)
+    right = np.take_along_axis(np.nan_to_num(right, nan=0.0), idx, 1)
+    first = np.argmax(filled, axis=1)
+    lead = np.arange(w)[None, :] < first[:, None]
+    right = np.where(lead, np.take_along_axis(right, first[:, None], 1), right)
+    rng = np.random.default_rng(seed + 104729)
+    right = right + rng.standard_normal((h, w)).astype(np.float32) * sigma
+    return np.clip(np.rint(right), 0, max_value)
+
+
+def to_u8(img, bits):
+    """Bytes in the reference's domain: 8-bit as is, 12-bit via (v + 8) >> 4 saturated."""
+    v = np.asarray(img).astype(np.int64)
+    if bits == 8:
+        return np.clip(v, 0, 255).astype(np.uint8)
+    return np.clip((v + 8) >> 4, 0, 255).astype(np.uint8)
+
+
+def gray_rgba(y):
+    """(Y, 128, 128, 255): a grey image as the reference's YUVA byte image."""
+    h, w = y.shape
+    out = np.empty((h, w, 4), np.uint8)
+    out[..., 0] = y
+    out[..., 1] = 128
+    out[..., 2] = 128
+    out[..., 3] = 255
+    return out
+
+
+def rectified_calibs(f, cx, cy, baseline):
+    """Reference at the origin; the other camera shifted so that a point of disparity d is sampled at x - d."""
+    K = np.array([f, 0, cx, 0, f, cy, 0, 0, 1], np.float32)
+    R = np.eye(3, dtype=np.float32).reshape(9)
+    return [CalibData(K.copy(), np.zeros(3, np.float32), R.copy()),
+            CalibData(K.copy(), np.array([-baseline, 0, 0], np.float32), R.copy())]
+
+
+@dataclass
+class PairWorkload:
+    images: List[np.ndarray]      # RGBA8 per camera (camera 0 = reference)
+    gray: List[int]
+    calibs: List[CalibData]
+    near: float
+    far: float
+    params: StereoParams
+    disparity: np.ndarray         # ground truth (reference grid)
+    d: int
+
+    @property
+    def de(self):
+        h, w = self.images[0].shape[:2]
+        return w * h * self.d
+
+
+def rectified_pair(w, h, d, seed=0, bits=8, noise_sigma=2.0, tile=64, f=1000.0, baseline=100.0):
+    """One rectified grey pair with planes == integer disparities 0..d-1 (d a multiple of 8)."""
+    maxv = 255.0 if bits == 8 else 4095.0
+    left = np.rint(texture(h, w, seed, maxv))
+    disp = planar_disparity(h, w, d - 1, seed)
+    right = warp_other(left, disp, seed, noise_sigma, maxv)
+    left = np.clip(left + np.random.default_rng(seed + 15485863).standard_normal((h, w)) * noise_sigma, 0, maxv)
+    imgs = [gray_rgba(to_u8(np.rint(left), bits)), gray_rgba(to_u8(right, bits))]
+    near = np.float32(f * baseline / (d - 1))
+    params = StereoParams(scale=1, tile=tile, skip_mode=0, plane_density=1.0)
+    return PairWorkload(imgs, [1, 1], rectified_calibs(f, w / 2.0, h / 2.0, baseline), float(near), 1e30, params, disp, d)
+
+
+@dataclass
+class CaptureWorkload:
+    images: List[np.ndarray]
+    gray: List[int]
+    calibs: List[CalibData]
+    near: float
+    far: float
+    inv_depth: np.ndarray
+
+
+def capture(w, h, n_cams, seed=0, f=None, baseline_mm=(8.0, 40.0), near=200.0, far=640000.0, colour=True):
+    """A multi-camera capture in the L16 convention: reference camera 0 plus translated cameras (R = I), colour YUVA
+    textures, a scene of planar patches at 0.4-6 m. Camera k's image is the reference resampled by the parallax
+    f·t/Z (a backward warp on the reference grid)."""
+    rng = np.random.default_rng(seed)
+    f = f if f is not None else 0.75 * w
+    z_inv = 1.0 / np.clip(planar_disparity(h, w, 1.0, seed) * 5600.0 + 400.0, 400.0, 6000.0)  # 1/mm
+    chans = [texture(h, w, seed * 7 + c, 255.0) for c in range(3)]
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    imgs, cal = [], []
+    K = np.array([f, 0, w / 2.0, 0, f, h / 2.0, 0, 0, 1], np.float32)
+    R = np.eye(3, dtype=np.float32).reshape(9)
+    for k in range(n_cams):
+        if k == 0:
+            t = np.zeros(3, np.float32)
+        else:
+            ang = rng.uniform(0, 2 * np.pi)
+            b = rng.uniform(*baseline_mm)
+            t = np.array([b * np.cos(ang), b * np.sin(ang), 0.0], np.float32)
+        # camera k sees the reference point at x + f·t/Z: sample the reference at x - f·t·invZ
+        sx = np.clip(np.rint(xx - f * t[0] * z_inv), 0, w - 1).astype(np.int64)
+        sy = np.clip(np.rint(yy - f * t[1] * z_inv), 0, h - 1).astype(np.int64)
+        img = np.empty((h, w, 4), np.uint8)
+        for c in range(3):
+            v = chans[c][sy, sx] + rng.standard_normal((h, w)) * 1.5
+            img[..., c] = np.clip(np.rint(v), 0, 255)
+        if not colour:
+            img[..., 1] = 128
+            img[..., 2] = 128
+        img[..., 3] = 255
+        imgs.append(img)
+        cal.append(CalibData(K.copy(), (-t).astype(np.float32), R.copy()))
+    gray = [0 if colour else 1] * n_cams
+    return CaptureWorkload(imgs, gray, cal, near, far, z_inv)

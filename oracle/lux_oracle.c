@@ -1,0 +1,1107 @@
+/* CPU oracle for the dense-stereo depth stage of Lux.Engine — TEST INFRASTRUCTURE ONLY (see lux_oracle.h).
+ * Parity unpinned against reference outputs (no golden vectors exist for this path; the C# reference cannot run here).
+ * Each function cites the reference file:line it restates. Build: -O2 -ffp-contract=off (no FMA, no fast-math). */
+#include "lux_oracle.h"
+#include "intel_approx_tables.h"
+
+#include <limits.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+
+/* ---------------- .NET scalar semantics ---------------- */
+static inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static inline float ffrom(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+/* (int)f in .NET 9+: truncation, saturating, NaN -> 0 */
+static inline int cs_f2i(float f) {
+  if (f != f) return 0;
+  if (f >= 2147483648.0f) return INT_MAX;
+  if (f < -2147483648.0f) return INT_MIN;
+  return (int)f;
+}
+/* Math.Max / Math.Min (float): NaN propagates, +0 > -0 */
+static inline float cs_maxf(float a, float b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  if (a == b) return signbit(a) ? b : a;
+  return a > b ? a : b;
+}
+static inline float cs_minf(float a, float b) {
+  if (a != a) return a;
+  if (b != b) return b;
+  if (a == b) return signbit(a) ? a : b;
+  return a < b ? a : b;
+}
+static inline int imin(int a, int b) { return a < b ? a : b; }
+static inline int imax(int a, int b) { return a > b ? a : b; }
+static inline int iclamp(int v, int lo, int hi) { return v < lo ? lo : v > hi ? hi : v; }
+
+/* ---------------- StereoParams (DenseStereo.cs:15-31) ---------------- */
+void lo_default_params(lo_params* p) {
+  p->margin = 1;
+  p->plane_density = 2.0f;
+  p->scale = 32;
+  p->skip_mode = 0;
+  p->p1 = 1;
+  p->p2scale = 500.0f;
+  float g = ffrom(0x3ef6384fu);
+  p->guidance[0] = g / 6.0f;
+  p->guidance[1] = g / 16.0f;
+  p->guidance[2] = g / 16.0f;
+  p->guidance[3] = 0.0f;
+  p->tile = 4;
+}
+
+void lo_l16_pyramid(lo_params out[6]) {
+  static const int scales[6] = {32, 16, 8, 4, 2, 1}, tiles[6] = {4, 8, 16, 32, 64, 64};
+  for (int i = 0; i < 6; i++) {
+    lo_default_params(&out[i]);
+    out[i].scale = scales[i];
+    out[i].tile = tiles[i];
+    out[i].skip_mode = i >= 4 ? 2 : 0;
+    out[i].plane_density = 2.0f;
+  }
+}
+
+/* ---------------- IntelApprox (IntelApprox.cs:21-45) ---------------- */
+uint32_t lo_rcp_bits(uint32_t b) {
+  uint32_t sign = b & 0x80000000u, e = (b >> 23) & 0xff, m = b & 0x7fffff;
+  if (e == 0xff) return m != 0 ? (b | 0x400000u) : sign;
+  if (e == 0) return sign | 0x7f800000u;
+  uint32_t r = lux_rcp_table[m >> 11];
+  int re = (int)((r >> 23) & 0xff) - ((int)e - 127);
+  if (re <= 0) return sign;
+  return sign | ((uint32_t)re << 23) | (r & 0x7fffff);
+}
+
+uint32_t lo_rsqrt_bits(uint32_t b) {
+  uint32_t sign = b & 0x80000000u, e = (b >> 23) & 0xff, m = b & 0x7fffff;
+  if (e == 0xff && m != 0) return b | 0x400000u;
+  if (e == 0) return sign | 0x7f800000u;
+  if (sign != 0) return 0xffc00000u;
+  if (e == 0xff) return 0;
+  int k = (int)e - 127;
+  uint32_t r;
+  int re;
+  if ((k & 1) == 0) { r = lux_rsqrt_table_e127[m >> 11]; re = (int)((r >> 23) & 0xff) - k / 2; }
+  else { r = lux_rsqrt_table_e128[m >> 11]; re = (int)((r >> 23) & 0xff) - (k - 1) / 2; }
+  if (re <= 0) return 0;
+  return ((uint32_t)re << 23) | (r & 0x7fffff);
+}
+
+float lo_rcp(float x) { return ffrom(lo_rcp_bits(fbits(x))); }
+static float lo_rsqrt_raw(float x) { return ffrom(lo_rsqrt_bits(fbits(x))); }
+
+/* Homography.Sqrt (Homography.cs:18) */
+float lo_homography_sqrt(float x) {
+  float r = lo_rsqrt_raw(x);
+  float A = x * r, B = A * (-0.5f), C = A * r, D = C + (-3.0f), s = D * B;
+  return x == 0.0f ? 0.0f : s;
+}
+
+/* RcpNr (DenseStereo.cs:37-38): rcp + one Newton step */
+static float rcp_nr(float a) {
+  float x0 = lo_rcp(a);
+  float t = a * x0;
+  t = 1.0f - t;
+  t = x0 * t;
+  return x0 + t;
+}
+
+/* ---------------- Mt19937 (FundamentalMatrixFilter.cs:8-30) ---------------- */
+void lo_mt_seed(lo_mt19937* m, uint32_t seed) {
+  m->mt[0] = seed;
+  for (int i = 1; i < 624; i++) m->mt[i] = (uint32_t)(1812433253u * (m->mt[i - 1] ^ (m->mt[i - 1] >> 30)) + (uint32_t)i);
+  m->idx = 624;
+}
+
+uint32_t lo_mt_next(lo_mt19937* m) {
+  if (m->idx >= 624) {
+    for (int i = 0; i < 624; i++) {
+      uint32_t y = (m->mt[i] & 0x80000000u) | (m->mt[(i + 1) % 624] & 0x7fffffffu);
+      m->mt[i] = m->mt[(i + 397) % 624] ^ (y >> 1) ^ ((y & 1u) != 0 ? 0x9908b0dfu : 0u);
+    }
+    m->idx = 0;
+  }
+  uint32_t r = m->mt[m->idx++];
+  r ^= r >> 11;
+  r ^= (r << 7) & 0x9d2c5680u;
+  r ^= (r << 15) & 0xefc60000u;
+  r ^= r >> 18;
+  return r;
+}
+
+/* ---------------- Mat4D (ViewTransform.cs:86-133), double ---------------- */
+static void mat4_mul(const double* a, const double* b, double* o) {
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++)
+      o[4 * i + j] = ((a[4 * i + 3] * b[12 + j] + a[4 * i + 2] * b[8 + j]) + (a[4 * i + 1] * b[4 + j] + a[4 * i] * b[j]));
+}
+
+static void mat4_inverse(const double* m, double* o) {
+  double m00 = m[0], m01 = m[1], m02 = m[2], m03 = m[3], m10 = m[4], m11 = m[5], m12 = m[6], m13 = m[7];
+  double m20 = m[8], m21 = m[9], m22 = m[10], m23 = m[11], m30 = m[12], m31 = m[13], m32 = m[14], m33 = m[15];
+  double adj[16];
+  adj[0] = (m11 * (m22 * m33 - m23 * m32)) + ((m12 * (m23 * m31 - m33 * m21)) + (m13 * (m32 * m21 - m31 * m22)));
+  adj[1] = (m01 * (m23 * m32 - m22 * m33)) + ((m02 * (m33 * m21 - m23 * m31)) + (m03 * (m31 * m22 - m32 * m21)));
+  adj[2] = (((m02 * m13 - m12 * m03) * m31) + ((m12 * m01) * m33 + (m11 * m03) * m32)) - ((m01 * m13) * m32 + (m11 * m02) * m33);
+  adj[3] = ((m23 * (m11 * m02 - m12 * m01)) + (m21 * (m12 * m03 - m02 * m13))) + (m22 * (m01 * m13 - m11 * m03));
+  adj[4] = ((m12 * (m33 * m20 - m23 * m30)) + (m13 * (m22 * m30 - m32 * m20))) + (m10 * (m23 * m32 - m22 * m33));
+  adj[5] = (m00 * (m22 * m33 - m23 * m32)) + ((m02 * (m23 * m30 - m33 * m20)) + (m03 * (m32 * m20 - m22 * m30)));
+  adj[6] = (m33 * (m02 * m10 - m00 * m12)) + ((m30 * (m12 * m03 - m02 * m13)) + (m32 * (m00 * m13 - m03 * m10)));
+  adj[7] = (((m02 * m13 - m12 * m03) * m20) + ((m03 * m10) * m22 + (m00 * m12) * m23)) - (m23 * (m02 * m10) + (m00 * m13) * m22);
+  adj[8] = (m11 * (m23 * m30 - m33 * m20)) + ((m13 * (m31 * m20 - m21 * m30)) + (m10 * (m33 * m21 - m23 * m31)));
+  adj[9] = (m00 * (m23 * m31 - m33 * m21)) + (((m33 * m20 - m23 * m30) * m01) + (m03 * (m21 * m30 - m31 * m20)));
+  adj[10] = (((m01 * m13 - m11 * m03) * m30) + ((m00 * m11) * m33 + (m03 * m10) * m31)) - ((m00 * m13) * m31 + m33 * (m01 * m10));
+  adj[11] = (m23 * (m01 * m10 - m00 * m11)) + ((m20 * (m11 * m03 - m01 * m13)) + (m21 * (m00 * m13 - m03 * m10)));
+  adj[12] = (m11 * (m32 * m20 - m22 * m30)) + ((m12 * (m21 * m30 - m31 * m20)) + (m10 * (m31 * m22 - m32 * m21)));
+  adj[13] = (m00 * (m32 * m21 - m31 * m22)) + (((m22 * m30 - m32 * m20) * m01) + (m02 * (m31 * m20 - m21 * m30)));
+  adj[14] = (m32 * (m01 * m10 - m00 * m11)) + (((m11 * m02 - m12 * m01) * m30) + (m31 * (m00 * m12 - m02 * m10)));
+  adj[15] = (((m12 * m01 - m11 * m02) * m20) + ((m02 * m10) * m21 + (m00 * m11) * m22)) - ((m01 * m10) * m22 + (m00 * m12) * m21);
+  double det = ((adj[12] * m03 + m02 * adj[8]) + (adj[4] * m01 + m00 * adj[0]));
+  double rd = 1.0 / det;
+  for (int k = 0; k < 16; k++) o[k] = adj[k] * rd;
+}
+
+static void kd(const lo_calib* c, double* k) {
+  memset(k, 0, 16 * sizeof(double));
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) k[4 * i + j] = c->K[3 * i + j];
+  k[15] = 1.0;
+}
+static void ed(const lo_calib* c, double* e) {
+  memset(e, 0, 16 * sizeof(double));
+  for (int i = 0; i < 3; i++) {
+    for (int j = 0; j < 3; j++) e[4 * i + j] = c->R[3 * i + j];
+    e[4 * i + 3] = c->T[i];
+  }
+  e[15] = 1.0;
+}
+
+void lo_flow_matrix(const lo_calib* a, const lo_calib* b, float out[16]) {
+  double ka[16], ea[16], kb[16], eb[16], p1[16], p2[16], inv[16], M[16];
+  kd(b, kb); ed(b, eb); mat4_mul(kb, eb, p1);
+  kd(a, ka); ed(a, ea); mat4_mul(ka, ea, p2);
+  mat4_inverse(p2, inv);
+  mat4_mul(p1, inv, M);
+  for (int c = 0; c < 4; c++)
+    for (int r = 0; r < 4; r++) out[4 * c + r] = (float)M[4 * r + c];
+}
+
+/* ---------------- Planes (DenseStereo.cs:41-88) ---------------- */
+int lo_planes(float near_, float far_, const lo_calib* calibs, int ncams, float density, int align, float* planes, int* n_out) {
+  if (!(near_ < far_)) return LO_ERR_NEAR_FAR;
+  if (!(near_ > 0.0f && far_ > 0.0f)) return LO_ERR_NONPOSITIVE;
+  if (align <= 0 || ncams <= 0) return LO_ERR_ARG;
+  float (*C)[3] = (float (*)[3])malloc(sizeof(float[3]) * (size_t)ncams);
+  if (!C) return LO_ERR_ALLOC;
+  for (int k = 0; k < ncams; k++) {
+    const float *R = calibs[k].R, *t = calibs[k].T;
+    C[k][0] = (t[0] * R[0] + t[1] * R[3]) + t[2] * R[6];
+    C[k][1] = (t[0] * R[1] + t[1] * R[4]) + t[2] * R[7];
+    C[k][2] = (t[0] * R[2] + t[1] * R[5]) + t[2] * R[8];
+  }
+  float B = 0.0f;
+  for (int k = 0; k < ncams; k++) {
+    float dx = C[0][0] - C[k][0], dy = C[0][1] - C[k][1], dz = C[0][2] - C[k][2];
+    float d2 = dz * dz + (dx * dx + dy * dy);
+    float d = lo_homography_sqrt(d2);
+    if (!(d <= B)) B = d;
+  }
+  free(C);
+  float x1_0 = rcp_nr(near_), x1_1 = rcp_nr(far_);
+  float inv = x1_0 - x1_1;
+  int n = cs_f2i(((inv * density) * B) * calibs[0].K[0]);
+  if (n > 0x1000) n = 0x1000;
+  if (n <= 0) return LO_ERR_BASELINE;
+  n = ((n + align - 1) / align) * align;
+  float step = (x1_0 - x1_1) / (float)(n - 1), bas = x1_1;
+  if (n - 1 <= 7) {
+    float v = bas;
+    for (int i = 0; i < n - 1; i++) { planes[i] = 1.0f / v; v += step; }
+  } else {
+    int m = (n - 1) & ~7;
+    float v4[4], d4 = 4.0f * step;
+    for (int l = 0; l < 4; l++) v4[l] = step * (float)l + bas;
+    for (int i = 0; i < m; i += 8) {
+      float hi[4];
+      for (int l = 0; l < 4; l++) hi[l] = v4[l] + d4;
+      for (int l = 0; l < 4; l++) { planes[i + l] = rcp_nr(v4[l]); planes[i + 4 + l] = rcp_nr(hi[l]); }
+      for (int l = 0; l < 4; l++) v4[l] = hi[l] + d4;
+    }
+    float v = (float)m * step + bas;
+    for (int i = m; i < n - 1; i++) { planes[i] = 1.0f / v; v += step; }
+  }
+  planes[n - 1] = near_;
+  *n_out = n;
+  return LO_OK;
+}
+
+/* ---------------- BoxFilter3 (DenseStereo.cs:93-159) ---------------- */
+static inline uint8_t sat_u8_rne(float v) {
+  /* cvtps2dq (RNE; NaN/overflow -> INT_MIN) -> packssdw -> packuswb */
+  int q;
+  if (v != v || v >= 2147483648.0f || v < -2147483648.0f) q = INT_MIN;
+  else q = (int)rintf(v);
+  if (q < 0) return 0;
+  if (q > 255) return 255;
+  return (uint8_t)q;
+}
+
+void lo_box_filter3(const uint8_t* src, int W, int H, uint8_t* dst) {
+  if (W < 2) { lo_box_filter3_scalar(src, W, H, dst); return; }
+  /* row sums of three taps (RowSums3, :126-135), then the sum of up to three rows */
+  uint16_t* sums = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)W * 4 * 3);
+  for (int y = 0; y < H; y++) {
+    int y0 = imax(y - 1, 0), y1 = imin(y + 1, H - 1);
+    int rows = y1 - y0 + 1;
+    for (int k = 0; k < rows; k++) {
+      const uint8_t* row = src + (size_t)(y0 + k) * W * 4;
+      uint16_t* s = sums + (size_t)k * W * 4;
+      int last = (W - 1) * 4;
+      for (int c = 0; c < 4; c++) {
+        s[c] = (uint16_t)(row[c] + row[4 + c]);
+        s[last + c] = (uint16_t)(row[last - 4 + c] + row[last + c]);
+      }
+      for (int i = 4; i < last; i++) s[i] = (uint16_t)(row[i - 4] + row[i] + row[i + 4]);
+    }
+    float invEdge = 1.0f / ((float)2 * (float)rows), invInner = 1.0f / ((float)3 * (float)rows);
+    for (int x = 0; x < W; x++)
+      for (int c = 0; c < 4; c++) {
+        int sum = 0;
+        for (int k = 0; k < rows; k++) sum += sums[(size_t)k * W * 4 + x * 4 + c];
+        float v = (float)sum * ((x == 0 || x == W - 1) ? invEdge : invInner);
+        dst[((size_t)y * W + x) * 4 + c] = sat_u8_rne(v);
+      }
+  }
+  free(sums);
+}
+
+void lo_box_filter3_scalar(const uint8_t* src, int W, int H, uint8_t* dst) {
+  for (int y = 0; y < H; y++) {
+    int y0 = imax(y - 1, 0), y1 = imin(y + 1, H - 1);
+    int rows = y1 - y0 + 1;
+    for (int x = 0; x < W; x++) {
+      int x0 = imax(x - 1, 0), x1 = imin(x + 1, W - 1);
+      int cols = x1 - x0 + 1;
+      float inv = 1.0f / ((float)cols * (float)rows);
+      for (int c = 0; c < 4; c++) {
+        int sum = 0;
+        for (int yy = y0; yy <= y1; yy++)
+          for (int xx = x0; xx <= x1; xx++) sum += src[((size_t)yy * W + xx) * 4 + c];
+        float v = (float)sum * inv;
+        int r = cs_f2i(rintf(v));
+        dst[((size_t)y * W + x) * 4 + c] = (uint8_t)iclamp(r, 0, 255);
+      }
+    }
+  }
+}
+
+/* ---------------- Guidance (DenseStereo.cs:163-177) ---------------- */
+void lo_guidance(const uint8_t* img0, int W0, int H0, int w, int h, int scale, uint8_t* g) {
+  if (W0 == w && H0 == h) { memcpy(g, img0, (size_t)w * h * 4); return; }
+  int half = (scale + (scale >> 31)) >> 1;
+  for (int y = 0; y < h; y++) {
+    int sy = imin(scale * y + half, H0 - 1);
+    for (int x = 0; x < w; x++) {
+      int sx = imin(scale * x + half, W0 - 1);
+      memcpy(g + ((size_t)y * w + x) * 4, img0 + ((size_t)sy * W0 + sx) * 4, 4);
+    }
+  }
+}
+
+/* ---------------- MatchingCost (DenseStereo.cs:217-373) ---------------- */
+static const uint8_t kCaps[4] = {2, 6, 6, 0}; /* CostContext.Caps, DenseStereo.cs:187 */
+
+static inline uint8_t pavgb(uint8_t a, uint8_t b) { return (uint8_t)((a + b + 1) >> 1); }
+
+/* the per-(camera, plane) projection shared by both forms (DenseStereo.cs:254-266, :319-331) */
+static inline void project(const float* Wm, float xf, float yf, float z, float* fx, float* fy) {
+  float xz = (xf * z) * 1.0f, yz = (yf * z) * 1.0f;
+  float px = ((z * Wm[8] + Wm[12]) + xz * Wm[0]) + yz * Wm[4];
+  float py = ((z * Wm[9] + Wm[13]) + xz * Wm[1]) + yz * Wm[5];
+  float pz = ((z * Wm[10] + Wm[14]) + xz * Wm[2]) + yz * Wm[6];
+  float inv = 1.0f / pz;
+  *fx = px * inv + 0.25f;
+  *fy = py * inv + 0.25f;
+}
+
+static void ref_block(const lo_costctx* c, int x, int y, uint8_t rb[3][16]) {
+  memset(rb, 0, 48);
+  for (int r = -1; r <= 1; r++) {
+    int yy = iclamp(y + r, 0, c->h - 1);
+    for (int cc = -1; cc <= 1; cc++) {
+      int xx = iclamp(x + cc, 0, c->w - 1);
+      memcpy(&rb[r + 1][(cc + 1) * 4], c->ref + ((size_t)yy * c->w + xx) * 4, 4);
+    }
+  }
+}
+
+/* the block cost of one target position: the vector form's byte lanes (DenseStereo.cs:276-287) */
+static int block_cost_vec(const uint8_t* img, int iw, int ix, int iy, int hx, int hy, const uint8_t rb[3][16], const uint16_t* wq) {
+  uint8_t a[4][16];
+  const uint8_t* t = img + ((size_t)(iy - 1) * iw + (ix - 1)) * 4;
+  for (int q = 0; q < 4; q++) memcpy(a[q], t + (size_t)q * iw * 4, 16);
+  uint8_t r[3][16];
+  for (int q = 0; q < 3; q++)
+    for (int b = 0; b < 16; b++) r[q][b] = hy ? pavgb(a[q][b], a[q + 1][b]) : a[q][b];
+  if (hx)
+    for (int q = 0; q < 3; q++) {
+      uint8_t nx[16];
+      for (int b = 0; b < 16; b++) nx[b] = r[q][(b < 12 ? b + 4 : b)]; /* NextPixel: pixels (1,2,3,3) */
+      for (int b = 0; b < 16; b++) r[q][b] = pavgb(r[q][b], nx[b]);
+    }
+  uint8_t rowSum[16];
+  for (int b = 0; b < 16; b++) {
+    int s = 0;
+    for (int q = 0; q < 3; q++) {
+      int hi = r[q][b] > rb[q][b] ? r[q][b] : rb[q][b], lo = r[q][b] > rb[q][b] ? rb[q][b] : r[q][b];
+      int d = (uint8_t)(hi - lo);
+      s += d < kCaps[b & 3] ? d : kCaps[b & 3];
+    }
+    rowSum[b] = (uint8_t)s; /* byte lanes: at most 3·28 */
+  }
+  uint32_t e0, e1, e2;
+  memcpy(&e0, rowSum, 4); memcpy(&e1, rowSum + 4, 4); memcpy(&e2, rowSum + 8, 4);
+  uint32_t s = e0 + e1 + e2;
+  int S0 = (int)(s & 0xff), S1 = (int)((s >> 8) & 0xff), S2 = (int)((s >> 16) & 0xff), S3 = (int)(s >> 24);
+  int cY = (S0 * wq[0] + 16) >> 5, cU = (S1 * wq[1] + 16) >> 5, cV = (S2 * wq[2] + 16) >> 5, cA = (S3 * wq[3] + 16) >> 5;
+  int ck = (cY + cU) + (cV + cA);
+  float cf = cs_minf((float)ck, 65535.0f);
+  return cs_f2i(cf);
+}
+
+int lo_matching_cost(const lo_costctx* c, int x, int y, int start, int count, uint16_t* cost) {
+  if (start < 0 || count < 0 || start + count > c->n_planes) return lo_matching_cost_scalar(c, x, y, start, count, cost);
+  memset(cost, 0, sizeof(uint16_t) * (size_t)count);
+  uint8_t rb[3][16];
+  ref_block(c, x, y, rb);
+  float xf = (float)x, yf = (float)y;
+  for (int k = 0; k < c->n_others; k++) {
+    const uint8_t* img = c->others[k];
+    const float* Wm = c->warps[k];
+    const uint16_t* wq = c->wq[k];
+    int iw = c->ow[k], ih = c->oh[k];
+    int x0 = 1, y0 = 1, x1 = iw - 2, y1 = ih - 2;
+    int lix = INT_MIN, liy = 0, lhx = 0, lhy = 0, lastCost = 0, haveLast = 0;
+    for (int d = 0; d < count; d++) {
+      float fx, fy;
+      project(Wm, xf, yf, c->planes[start + d], &fx, &fy);
+      int ix, iy, hx, hy;
+      if (d == 0) {
+        float cx = cs_minf(cs_maxf(fx, (float)x0), (float)(x1 - 1)), cy = cs_minf(cs_maxf(fy, (float)y0), (float)(y1 - 1));
+        ix = cs_f2i(cx); iy = cs_f2i(cy); hx = cs_f2i(cx + cx) & 1; hy = cs_f2i(cy + cy) & 1;
+        if (ix < x0 || ix >= x1 || iy < y0 || iy >= y1) return lo_matching_cost_scalar(c, x, y, start, count, cost);
+      } else {
+        ix = cs_f2i(fx); iy = cs_f2i(fy); hx = cs_f2i(fx + fx) & 1; hy = cs_f2i(fy + fy) & 1;
+        if (haveLast && ix == lix && iy == liy && hx == lhx && hy == lhy) { cost[d] = (uint16_t)(cost[d] + lastCost); continue; }
+        if (ix < x0 || ix >= x1 || iy < y0 || iy >= y1) { cost[d] = (uint16_t)(cost[d] + lastCost); continue; }
+      }
+      int costK = block_cost_vec(img, iw, ix, iy, hx, hy, rb, wq);
+      cost[d] = (uint16_t)(cost[d] + costK);
+      lix = ix; liy = iy; lhx = hx; lhy = hy; lastCost = costK; haveLast = 1;
+    }
+  }
+  return LO_OK;
+}
+
+int lo_matching_cost_scalar(const lo_costctx* c, int x, int y, int start, int count, uint16_t* cost) {
+  if (start < 0 || count < 0 || start + count > c->n_planes) return LO_ERR_INDEX;
+  memset(cost, 0, sizeof(uint16_t) * (size_t)count);
+  uint8_t refBlock[3 * 12];
+  for (int r = -1; r <= 1; r++) {
+    int yy = iclamp(y + r, 0, c->h - 1);
+    for (int cc = -1; cc <= 1; cc++) {
+      int xx = iclamp(x + cc, 0, c->w - 1);
+      for (int ch = 0; ch < 4; ch++) refBlock[(r + 1) * 12 + (cc + 1) * 4 + ch] = c->ref[((size_t)yy * c->w + xx) * 4 + ch];
+    }
+  }
+  for (int k = 0; k < c->n_others; k++) {
+    const uint8_t* img = c->others[k];
+    const float* Wm = c->warps[k];
+    const uint16_t* wq = c->wq[k];
+    int iw = c->ow[k], ih = c->oh[k];
+    int x0 = 1, y0 = 1, x1 = iw - 2, y1 = ih - 2;
+    int lix = INT_MIN, liy = 0, lhx = 0, lhy = 0, lastCost = 0, haveLast = 0;
+    for (int d = 0; d < count; d++) {
+      float fx, fy;
+      project(Wm, (float)x, (float)y, c->planes[start + d], &fx, &fy);
+      int ix, iy, hx, hy;
+      if (d == 0) {
+        float cx = cs_minf(cs_maxf(fx, (float)x0), (float)(x1 - 1)), cy = cs_minf(cs_maxf(fy, (float)y0), (float)(y1 - 1));
+        ix = cs_f2i(cx); iy = cs_f2i(cy); hx = cs_f2i(cx + cx) & 1; hy = cs_f2i(cy + cy) & 1;
+      } else {
+        ix = cs_f2i(fx); iy = cs_f2i(fy); hx = cs_f2i(fx + fx) & 1; hy = cs_f2i(fy + fy) & 1;
+        if (haveLast && ix == lix && iy == liy && hx == lhx && hy == lhy) { cost[d] = (uint16_t)(cost[d] + lastCost); continue; }
+        if (ix < x0 || ix >= x1 || iy < y0 || iy >= y1) { cost[d] = (uint16_t)(cost[d] + lastCost); continue; }
+      }
+      uint8_t T[64];
+      for (int q = 0; q < 4; q++) {
+        int yy = iy - 1 + q;
+        for (int pI = 0; pI < 4; pI++) {
+          int xx = ix - 1 + pI;
+          if (yy < 0 || yy >= ih || xx < 0 || xx >= iw) return LO_ERR_INDEX;
+          for (int ch = 0; ch < 4; ch++) T[q * 16 + pI * 4 + ch] = img[((size_t)yy * iw + xx) * 4 + ch];
+        }
+      }
+      int A[8] = {0}, Bw[8] = {0};
+      for (int q = 0; q < 3; q++) {
+        uint8_t row[16];
+        for (int b = 0; b < 16; b++) row[b] = hy ? pavgb(T[q * 16 + b], T[(q + 1) * 16 + b]) : T[q * 16 + b];
+        if (hx) {
+          for (int b = 0; b < 12; b++) row[b] = pavgb(row[b], row[b + 4]);
+          for (int b = 12; b < 16; b++) row[b] = pavgb(row[b], 0);
+        }
+        for (int b = 0; b < 16; b++) {
+          int rbv = b < 12 ? refBlock[q * 12 + b] : 0;
+          int diff = imax(row[b], rbv) - imin(row[b], rbv);
+          int dd = imin(diff, (int)kCaps[b & 3]);
+          if (b < 8) A[b] = imin(A[b] + dd, 65535); else Bw[b - 8] = imin(Bw[b - 8] + dd, 65535);
+        }
+      }
+      int S[4];
+      for (int ch = 0; ch < 4; ch++) {
+        int s0 = imin(A[ch] + Bw[ch], 65535), s1 = imin(A[4 + ch] + 0, 65535);
+        S[ch] = imin(s0 + s1, 65535);
+      }
+      int cY = (S[0] * wq[0] + 16) >> 5, cU = (S[1] * wq[1] + 16) >> 5, cV = (S[2] * wq[2] + 16) >> 5, cA = (S[3] * wq[3] + 16) >> 5;
+      int ck = (cY + cU) + (cV + cA);
+      float cf = cs_minf((float)ck, 65535.0f);
+      int costK = cs_f2i(cf);
+      cost[d] = (uint16_t)(cost[d] + costK);
+      lix = ix; liy = iy; lhx = hx; lhy = hy; lastCost = costK; haveLast = 1;
+    }
+  }
+  return LO_OK;
+}
+
+void lo_normalise(const uint16_t* cost, int count, int cap, int n_others, uint8_t* raw) {
+  float f = ffrom(0x3d17b426u) / (float)n_others;
+  for (int d = 0; d < count; d++) raw[d] = (uint8_t)cs_f2i((float)cost[d] * f);
+  for (int d = count; d < cap; d++) raw[d] = 255;
+}
+
+/* ---------------- SkipMask (DenseStereoSgm.cs:65-87) ---------------- */
+int lo_skip_mask(int mode, int w, int h, uint8_t* m) {
+  memset(m, 0, (size_t)w * h);
+  if (mode == 0) return LO_OK;
+  if (mode != 2) return LO_ERR_SKIPMODE;
+  memset(m, 0xff, (size_t)w * h);
+  int nx = w / 64 + (64 < 2 * (w % 64) ? 1 : 0), ny = h / 64 + (64 < 2 * (h % 64) ? 1 : 0);
+  if (nx < 1) nx = 1;
+  if (ny < 1) ny = 1;
+  lo_mt19937 mt;
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      int x0 = 64 * i, x1 = imin(w, x0 + 64 * (i == nx - 1 ? 2 : 1)), y0 = 64 * j, y1 = imin(h, y0 + 64 * (j == ny - 1 ? 2 : 1));
+      lo_mt_seed(&mt, 5489u);
+      for (int y = y0; y < y1; y += 2)
+        for (int x = x0; x < x1; x += 2) {
+          int dy = (int)(lo_mt_next(&mt) & 1), dx = (int)(lo_mt_next(&mt) & 1);
+          int yy = y + dy, xx = x + dx;
+          if (xx >= 0 && xx < w && yy >= 0 && yy < h) m[(size_t)yy * w + xx] = 0;
+        }
+    }
+  return LO_OK;
+}
+
+/* ---------------- RangeFromPrevious (DenseStereoSgm.cs:91-140) ---------------- */
+static int range_from_previous(lo_layer* L, const lo_layer* prev) {
+  int n = L->n_planes, pw = prev->w, ph = prev->h;
+  float* b = (float*)malloc(sizeof(float) * (size_t)n);
+  uint16_t* idx = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)pw * ph);
+  uint16_t *hmin = (uint16_t*)malloc(2 * (size_t)pw * ph), *hmax = (uint16_t*)malloc(2 * (size_t)pw * ph);
+  uint16_t *vmin = (uint16_t*)malloc(2 * (size_t)pw * ph), *vmax = (uint16_t*)malloc(2 * (size_t)pw * ph);
+  if (!b || !idx || !hmin || !hmax || !vmin || !vmax) { free(b); free(idx); free(hmin); free(hmax); free(vmin); free(vmax); return LO_ERR_ALLOC; }
+  for (int i = 0; i < n - 1; i++) b[i] = (lo_rcp(L->planes[i + 1]) + lo_rcp(L->planes[i])) * 0.5f;
+  b[n - 1] = 3.40282347e+38f;
+  for (int i = 0; i < pw * ph; i++) {
+    float v = lo_rcp(prev->depth[i]);
+    int c = 0;
+    while (c < n && b[c] <= v) c++;
+    idx[i] = (uint16_t)c;
+  }
+  for (int y = 0; y < ph; y++)
+    for (int x = 0; x < pw; x++) {
+      uint16_t mn = 0xffff, mx = 0;
+      for (int k = -1; k <= 2; k++) {
+        int xx = iclamp(x + k, 0, pw - 1);
+        if (prev->skip[y * pw + xx] > 0) continue; /* valid = computed pixels only */
+        uint16_t v = idx[y * pw + xx];
+        if (v < mn) mn = v;
+        if (v > mx) mx = v;
+      }
+      hmin[y * pw + x] = mn; hmax[y * pw + x] = mx;
+    }
+  for (int y = 0; y < ph; y++)
+    for (int x = 0; x < pw; x++) {
+      uint16_t mn = 0xffff, mx = 0;
+      for (int k = -1; k <= 2; k++) {
+        int yy = iclamp(y + k, 0, ph - 1);
+        uint16_t a = hmin[yy * pw + x], c = hmax[yy * pw + x];
+        if (a < mn) mn = a;
+        if (c > mx) mx = c;
+      }
+      vmin[y * pw + x] = mn; vmax[y * pw + x] = mx;
+    }
+  float fy = (float)(ph - 1) / (float)(L->h - 1), fx = (float)(pw - 1) / (float)(L->w - 1);
+  int maxHi = 0, minLo = INT_MAX;
+  for (int y = 0; y < L->h; y++) {
+    int py = cs_f2i((float)y * fy);
+    for (int x = 0; x < L->w; x++) {
+      int px = cs_f2i((float)x * fx);
+      if (py < 0 || py >= ph || px < 0 || px >= pw) { free(b); free(idx); free(hmin); free(hmax); free(vmin); free(vmax); return LO_ERR_INDEX; }
+      int lo = imax(0, vmin[py * pw + px] - L->p.margin), hi = imin(n - 1, vmax[py * pw + px] + 1);
+      int i = y * L->w + x;
+      L->start[i] = (uint16_t)lo;
+      L->count[i] = (uint16_t)(hi - lo);
+      maxHi = imax(maxHi, hi & 0xffff);
+      minLo = imin(minLo, lo & 0xffff);
+    }
+  }
+  L->max_hi = maxHi;
+  L->min_lo = minLo;
+  free(b); free(idx); free(hmin); free(hmax); free(vmin); free(vmax);
+  return LO_OK;
+}
+
+/* ---------------- DenseLayer.Init (DenseStereoSgm.cs:34-62) ---------------- */
+int lo_layer_init(lo_layer* L, const lo_params* p, int index, int n_cams, const uint8_t* const* images, const int* iw, const int* ih,
+                  const uint8_t* gray, const lo_calib* calibs, float near_, float far_, int align, const lo_layer* prev) {
+  memset(L, 0, sizeof(*L));
+  L->p = *p;
+  L->index = index;
+  L->align = align;
+  L->w = (iw[0] + p->scale - 1) / p->scale;
+  L->h = (ih[0] + p->scale - 1) / p->scale;
+  L->planes = (float*)malloc(sizeof(float) * (4096 + (size_t)align + 8));
+  int rc = lo_planes(near_, far_, calibs, n_cams, p->plane_density, align, L->planes, &L->n_planes);
+  if (rc) return rc;
+  int w = L->w, h = L->h, n = L->n_planes;
+  size_t npx = (size_t)w * h;
+  L->guidance = (uint8_t*)malloc(npx * 4);
+  lo_guidance(images[0], iw[0], ih[0], w, h, p->scale, L->guidance);
+  L->skip = (uint8_t*)malloc(npx);
+  rc = lo_skip_mask(p->skip_mode, w, h, L->skip);
+  if (rc) return rc;
+  L->start = (uint16_t*)calloc(npx, 2);
+  L->count = (uint16_t*)calloc(npx, 2);
+  L->cap = (uint16_t*)calloc(npx, 2);
+  if (!prev) {
+    for (size_t i = 0; i < npx; i++) { L->start[i] = 0; L->count[i] = (uint16_t)n; L->cap[i] = (uint16_t)n; }
+    L->min_lo = 0;
+    L->max_hi = ((n + align - 1) / align) * align;
+  } else {
+    rc = range_from_previous(L, prev);
+    if (rc) return rc;
+    L->max_hi = ((L->max_hi + align - 1) / align) * align;
+  }
+  L->off = (uint64_t*)malloc(sizeof(uint64_t) * (npx + 1));
+  uint64_t tot = 0;
+  for (size_t i = 0; i < npx; i++) {
+    int cap = ((L->count[i] + align - 1) / align) * align;
+    L->cap[i] = (uint16_t)cap;
+    L->off[i] = tot;
+    tot += (uint64_t)cap;
+  }
+  L->off[npx] = tot;
+  L->agg = (uint16_t*)calloc(tot + 1, 2);
+  L->raw = (uint8_t*)calloc(tot + 1, 1);
+  L->n_cams = n_cams;
+  L->images = images; L->iw = iw; L->ih = ih;
+  L->warps = (float (*)[16])malloc(sizeof(float[16]) * (size_t)(n_cams > 1 ? n_cams - 1 : 1));
+  L->wq = (uint16_t (*)[4])malloc(sizeof(uint16_t[4]) * (size_t)(n_cams > 1 ? n_cams - 1 : 1));
+  for (int k = 1; k < n_cams; k++) {
+    lo_flow_matrix(&calibs[0], &calibs[k], L->warps[k - 1]);
+    static const uint16_t wg[4] = {12240, 0, 0, 0}, wc[4] = {8160, 680, 680, 0};
+    memcpy(L->wq[k - 1], gray[k] ? wg : wc, sizeof(wg));
+  }
+  if (!L->planes || !L->guidance || !L->skip || !L->start || !L->agg || !L->raw) return LO_ERR_ALLOC;
+  return LO_OK;
+}
+
+void lo_layer_free(lo_layer* L) {
+  free(L->planes); free(L->guidance); free(L->skip); free(L->start); free(L->count); free(L->cap); free(L->off);
+  free(L->agg); free(L->agg_pass1); free(L->raw); free(L->depth); free(L->warps); free(L->wq);
+  memset(L, 0, sizeof(*L));
+}
+
+/* ---------------- MemoryEstimate (DenseStereoSgm.cs:144-156) ---------------- */
+int lo_memory_estimate(const lo_params* p, int n_cams, const int* iw, const int* ih, const lo_calib* calibs, float near_, float far_,
+                       int align, const lo_layer* prev, int64_t* out) {
+  lo_layer L;
+  memset(&L, 0, sizeof(L));
+  L.p = *p;
+  L.align = align;
+  L.w = (iw[0] + p->scale - 1) / p->scale;
+  L.h = (ih[0] + p->scale - 1) / p->scale;
+  float planes[4096 + 16];
+  L.planes = planes;
+  int rc = lo_planes(near_, far_, calibs, n_cams, p->plane_density, align, planes, &L.n_planes);
+  if (rc) return rc;
+  size_t npx = (size_t)L.w * L.h;
+  uint8_t* skip = (uint8_t*)malloc(npx);
+  rc = lo_skip_mask(p->skip_mode, L.w, L.h, skip);
+  if (rc) { free(skip); return rc; }
+  L.start = (uint16_t*)calloc(npx, 2);
+  L.count = (uint16_t*)calloc(npx, 2);
+  rc = range_from_previous(&L, prev);
+  if (rc) { free(skip); free(L.start); free(L.count); return rc; }
+  int64_t maxHi = ((L.max_hi + align - 1) / align) * align;
+  int64_t cost = 0;
+  for (size_t i = 0; i < npx; i++) {
+    int cap = ((L.count[i] + align - 1) / align) * align;
+    cost += 8 + (int64_t)cap * (skip[i] == 0 ? 3 : 2);
+  }
+  int64_t w = L.w, h = L.h, imgs = 0;
+  for (int k = 0; k < n_cams; k++) imgs += (int64_t)ih[k] * iw[k] * 4;
+  *out = cost + w * h * 4 + 20 * (2 * w + 4) + 2 * ((4LL * maxHi + 5) * (2 * w + 4) + 8 * w + 16) + imgs + w * h * 8;
+  free(skip); free(L.start); free(L.count);
+  return LO_OK;
+}
+
+/* ---------------- DenseLayer.Compute / Pixel (DenseStereoSgm.cs:158-324) ---------------- */
+typedef struct {
+  lo_layer* L;
+  uint16_t* Lb; size_t Llen;   /* _L */
+  uint16_t* Min;               /* _Min */
+  uint16_t *RangeS, *RangeC;   /* _RangeS, _RangeC */
+  float (*Pix)[4];             /* _Pix */
+  int slotStride, halfL, halfM, halfR;
+  uint8_t* rawTmp;             /* the shared scratch `raw` of Compute (n + 8 bytes) */
+  int err;
+} sgm_state;
+
+static inline int lidx(const sgm_state* s, int half, int slot, int path) {
+  return half * s->halfL + slot * s->slotStride + 1 + path * (s->L->max_hi + 1);
+}
+/* Rd (DenseStereoSgm.cs:324): before the buffer 2000, past its end 0 */
+static inline int rd(const sgm_state* s, long i) { return i < 0 ? 2000 : (size_t)i < s->Llen ? s->Lb[i] : 0; }
+
+static void pixel(sgm_state* s, int x, int y, int dir, int cur, int other) {
+  lo_layer* L = s->L;
+  int W = L->w;
+  int pi = y * W + x, slot = x + 1;
+  const uint8_t* gb = L->guidance + (size_t)pi * 4;
+  float g[4] = {(float)gb[0], (float)gb[1], (float)gb[2], (float)gb[3]};
+  memcpy(s->Pix[cur * s->halfR + slot], g, sizeof(g));
+  int start = L->start[pi], count = L->count[pi], cap = L->cap[pi];
+  uint8_t* raw = s->rawTmp;
+  if (L->skip[pi] != 0) {
+    memset(raw, 0, (size_t)cap);
+    for (int k = count; k < cap; k++) raw[k] = 255;
+  } else {
+    memcpy(raw, L->raw + L->off[pi], (size_t)cap); /* the stored costs (prepass == pass-1 costs, :176-180) */
+  }
+  int sp = s->RangeS[cur * s->halfR + slot], cp = s->RangeC[cur * s->halfR + slot];
+  uint16_t* agg = L->agg + L->off[pi];
+  int P1 = L->p.p1;
+  float p2Base = (float)L->p.p1 * L->p.p2scale;
+  const float* gw = L->p.guidance;
+  const float E3 = ffrom(0x3d9fcb52u), E2 = ffrom(0x3e677e26u), E1 = ffrom(0x3f322226u), E0 = ffrom(0x3f7ffb19u);
+  for (int p = 0; p < 4; p++) {
+    int baseCur = lidx(s, cur, slot, p);
+    {
+      long q0 = sp - L->min_lo, k0 = q0 < 0 ? -q0 : 0;
+      long k1 = cp < (long)s->Llen - baseCur - q0 ? cp : (long)s->Llen - baseCur - q0;
+      for (long k = k0; k < k1; k++) s->Lb[baseCur + q0 + k] = 2000;
+    }
+    int ns = slot + (p == 2 ? 0 : p == 3 ? dir : -dir);
+    int half = p == 0 ? cur : other;
+    int minPrev = s->Min[half * s->halfM + ns * 4 + p];
+    const float* pn = s->Pix[half * s->halfR + ns];
+    float d0 = (g[0] - pn[0]) * gw[0], d1 = (g[1] - pn[1]) * gw[1], d2 = (g[2] - pn[2]) * gw[2];
+    float S = (fabsf(d0) + fabsf(d2)) + fabsf(d1);
+    float e = cs_maxf(cs_minf(-S, 128.0f), -126.0f);
+    int ei = cs_f2i(e) + (e < 0.0f ? -1 : 0);
+    float f = e - (float)ei;
+    float poly = ((E3 * f + E2) * f + E1) * f + E0;
+    float E = ffrom(fbits(poly) + ((uint32_t)ei << 23));
+    int P2 = cs_f2i(p2Base * E);
+    int P2p = imin(P2 + minPrev, 65535);
+    if (cap == 0) { s->Min[cur * s->halfM + slot * 4 + p] = 0xffff; continue; }
+    int nb = lidx(s, half, ns, p);
+    int runMin = 0xffff;
+    int q = start - L->min_lo;
+    /* the scalar form: every read through Rd, lanes in order (DenseStereoSgm.cs:300-313); it equals the 8-lane form
+       whenever that one applies (:280-299) */
+    for (int b = 0; b < cap; b += 8)
+      for (int l = 0; l < 8; l++) {
+        long qi = (long)q + b + l;
+        int Lm = rd(s, nb + qi - 1), Lp = rd(s, nb + qi + 1), L0 = rd(s, nb + qi);
+        int m = imin(imin(imin(Lm + P1, 65535), L0), imin(imin(Lp + P1, 65535), P2p));
+        int lc = imin(raw[b + l] + m, 65535) - minPrev;
+        if (lc < 0) lc = 0;
+        long wi = baseCur + qi;
+        if (wi < 0 || (size_t)wi >= s->Llen) { s->err = LO_ERR_INDEX; return; }
+        s->Lb[wi] = (uint16_t)lc;
+        if (lc < runMin) runMin = lc;
+        if (b + l >= cap) { s->err = LO_ERR_INDEX; return; } /* agg[b + l] past the pixel's cap */
+        agg[b + l] = (uint16_t)imin(agg[b + l] + lc, 65535);
+      }
+    s->Min[cur * s->halfM + slot * 4 + p] = (uint16_t)runMin;
+  }
+  s->RangeS[cur * s->halfR + slot] = (uint16_t)start;
+  s->RangeC[cur * s->halfR + slot] = (uint16_t)cap;
+}
+
+/* raw costs of every computed pixel, rows in parallel on `threads` workers (DenseStereoSgm.cs:186-205); pass 1 then reads
+   them like pass 2 does, which the reference states gives the same values and aggregation order (:176-180) */
+typedef struct {
+  lo_layer* L;
+  lo_costctx c;
+  int next_row;
+  int err;
+  pthread_mutex_t mu;
+} raw_job;
+
+static void* raw_worker(void* arg) {
+  raw_job* j = (raw_job*)arg;
+  lo_layer* L = j->L;
+  int W = L->w, H = L->h, W0 = L->iw[0], H0 = L->ih[0], sc = L->p.scale, half = (sc + (sc >> 31)) >> 1;
+  uint16_t* cost = (uint16_t*)malloc(sizeof(uint16_t) * ((size_t)L->n_planes + 8));
+  uint8_t* raw = (uint8_t*)malloc((size_t)L->n_planes + 8 + 65536);
+  for (;;) {
+    pthread_mutex_lock(&j->mu);
+    int y = j->next_row++;
+    pthread_mutex_unlock(&j->mu);
+    if (y >= H) break;
+    for (int x = 0; x < W; x++) {
+      int pi = y * W + x;
+      if (L->skip[pi] != 0) continue;
+      int start = L->start[pi], count = L->count[pi], cap = L->cap[pi];
+      int xImg = imin(sc * x + half, W0 - 1), yImg = imin(sc * y + half, H0 - 1);
+      int rc = lo_matching_cost(&j->c, xImg, yImg, start, count, cost);
+      if (rc) {
+        pthread_mutex_lock(&j->mu);
+        j->err = rc;
+        pthread_mutex_unlock(&j->mu);
+        continue;
+      }
+      lo_normalise(cost, count, cap, j->c.n_others, raw);
+      memcpy(L->raw + L->off[pi], raw, (size_t)cap);
+    }
+  }
+  free(cost);
+  free(raw);
+  return NULL;
+}
+
+static void compute_raw(lo_layer* L, int* err) {
+  raw_job j;
+  memset(&j, 0, sizeof(j));
+  j.L = L;
+  j.c.ref = L->images[0]; j.c.w = L->iw[0]; j.c.h = L->ih[0];
+  j.c.n_others = L->n_cams - 1;
+  j.c.others = L->images + 1; j.c.ow = L->iw + 1; j.c.oh = L->ih + 1;
+  j.c.warps = (const float (*)[16])L->warps; j.c.wq = (const uint16_t (*)[4])L->wq;
+  j.c.planes = L->planes; j.c.n_planes = L->n_planes;
+  pthread_mutex_init(&j.mu, NULL);
+  int nt = L->threads > 1 ? L->threads : 1;
+  if (nt == 1) {
+    raw_worker(&j);
+  } else {
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)nt);
+    for (int t = 0; t < nt; t++) pthread_create(&th[t], NULL, raw_worker, &j);
+    for (int t = 0; t < nt; t++) pthread_join(th[t], NULL);
+    free(th);
+  }
+  pthread_mutex_destroy(&j.mu);
+  if (j.err) *err = j.err;
+}
+
+int lo_layer_compute(lo_layer* L) {
+  int err = 0;
+  compute_raw(L, &err);
+  if (err) return err;
+  sgm_state s;
+  memset(&s, 0, sizeof(s));
+  s.L = L;
+  int W = L->w, H = L->h, T = L->p.tile;
+  int maxCnt = L->max_hi;
+  s.slotStride = 4 * maxCnt + 5;
+  int slots = W + 2;
+  s.halfL = slots * s.slotStride;
+  s.Llen = (size_t)2 * s.halfL;
+  s.Lb = (uint16_t*)malloc(sizeof(uint16_t) * s.Llen);
+  for (size_t i = 0; i < s.Llen; i++) s.Lb[i] = 2000;
+  s.halfM = slots * 4;
+  s.Min = (uint16_t*)malloc(sizeof(uint16_t) * 2 * (size_t)s.halfM);
+  for (int i = 0; i < 2 * s.halfM; i++) s.Min[i] = 2000;
+  s.halfR = slots;
+  s.RangeS = (uint16_t*)calloc(2 * (size_t)slots, 2);
+  s.RangeC = (uint16_t*)malloc(sizeof(uint16_t) * 2 * (size_t)slots);
+  for (int i = 0; i < 2 * slots; i++) s.RangeC[i] = (uint16_t)L->align;
+  s.Pix = (float (*)[4])calloc(2 * (size_t)slots, sizeof(float[4]));
+  s.rawTmp = (uint8_t*)calloc((size_t)L->n_planes + 8 + 65536, 1);
+  static const int dirs[2] = {1, -1};
+  for (int di = 0; di < 2 && !s.err; di++) {
+    int dir = dirs[di];
+    int gwN = (W + T + T - 1) / T, ghN = (H + T - 1) / T;
+    for (int j = 0; j < ghN && !s.err; j++)
+      for (int i = 0; i < gwN && !s.err; i++) {
+        int x0 = dir > 0 ? i * T : W - 1 - i * T, y0 = dir > 0 ? j * T : H - 1 - j * T;
+        int yEnd = iclamp(y0 + dir * T, -1, H);
+        for (int r = 0;; r++) {
+          int y = y0 + dir * r;
+          if (y == yEnd) break;
+          int xs = iclamp(x0 - dir * r, 0, (L->xsw && dir > 0) ? W : W - 1), xe = iclamp(x0 + dir * (T - r), -1, W);
+          if (xs == xe) continue;
+          int cur = (r & 1) == 0 ? 1 : 0, other = 1 - cur;
+          for (int x = xs; x != xe && !s.err; x += dir) pixel(&s, x, y, dir, cur, other);
+        }
+      }
+    if (dir > 0 && L->keep_pass1) {
+      L->agg_pass1 = (uint16_t*)malloc(sizeof(uint16_t) * (L->off[(size_t)W * H] + 1));
+      memcpy(L->agg_pass1, L->agg, sizeof(uint16_t) * L->off[(size_t)W * H]);
+    }
+  }
+  free(s.Lb); free(s.Min); free(s.RangeS); free(s.RangeC); free(s.Pix); free(s.rawTmp);
+  if (s.err) return s.err;
+  /* WTA (DenseStereoSgm.cs:225-231) */
+  L->depth = (float*)malloc(sizeof(float) * (size_t)W * H);
+  for (size_t i = 0; i < (size_t)W * H; i++) {
+    const uint16_t* agg = L->agg + L->off[i];
+    int cnt = L->count[i];
+    uint16_t best = 0xffff;
+    int arg = 0;
+    for (int k = 0; k < cnt; k++)
+      if (agg[k] < best) { best = agg[k]; arg = k; }
+    int pl = (uint16_t)(L->start[i] + arg);
+    if (pl >= L->n_planes) return LO_ERR_INDEX;
+    L->depth[i] = L->planes[pl];
+  }
+  return LO_OK;
+}
+
+/* ---------------- DenseStereoPyramid.Run (DenseStereoSgm.cs:331-353) ---------------- */
+int lo_pyramid_run(int n_cams, const uint8_t* const* images, const int* iw, const int* ih, const uint8_t* gray,
+                   const lo_calib* calibs, float near_, float far_, int threads, int keep_pass1, lo_layer layers[6]) {
+  lo_params pars[6];
+  lo_l16_pyramid(pars);
+  uint8_t** filtered = (uint8_t**)calloc((size_t)n_cams, sizeof(uint8_t*));
+  for (int k = 0; k < n_cams; k++) {
+    filtered[k] = (uint8_t*)malloc((size_t)iw[k] * ih[k] * 4);
+    lo_box_filter3(images[k], iw[k], ih[k], filtered[k]);
+  }
+  memset(layers, 0, sizeof(lo_layer) * 6);
+  const lo_layer* prev = NULL;
+  int rc = LO_OK;
+  for (int i = 0; i < 6; i++) {
+    int align = 8;
+    if (prev) {
+      int64_t est8, est2;
+      rc = lo_memory_estimate(&pars[i], n_cams, iw, ih, calibs, near_, far_, 8, prev, &est8);
+      if (rc) break;
+      if (est8 >= 0x40000000LL) {
+        rc = lo_memory_estimate(&pars[i], n_cams, iw, ih, calibs, near_, far_, 2, prev, &est2);
+        if (rc) break;
+        if (est2 >= 0x40000000LL) { rc = LO_ERR_BUDGET; break; }
+        align = 2;
+      }
+    }
+    rc = lo_layer_init(&layers[i], &pars[i], i, n_cams, (const uint8_t* const*)filtered, iw, ih, gray, calibs, near_, far_, align, prev);
+    if (rc) break;
+    layers[i].threads = threads;
+    layers[i].keep_pass1 = keep_pass1;
+    rc = lo_layer_compute(&layers[i]);
+    if (rc) break;
+    prev = &layers[i];
+  }
+  /* the filtered images are owned by the layers' lifetime in the reference; here the caller receives copies */
+  for (int i = 0; i < 6; i++) { layers[i].images = NULL; layers[i].iw = NULL; layers[i].ih = NULL; }
+  for (int k = 0; k < n_cams; k++) free(filtered[k]);
+  free(filtered);
+  return rc;
+}
+
+/* ---------------- DenseUpsampleLayer (DenseUpsampleLayer.cs:35-218) ---------------- */
+static float cubic_tap(float x) {
+  const float sixth = ffrom(0x3e2aaaabu);
+  float x2 = x * x, x3 = x2 * x;
+  if (x < 1.0f) { float a = x3 * 9.0f; float b = x2 * (-15.0f); b = b + 6.0f; b = b + a; return b * sixth; }
+  if (x < 2.0f) { float a = x3 * (-3.0f); float b = x2 * 15.0f; float c = x * (-24.0f); c = c + 12.0f; c = c + b; c = c + a; return c * sixth; }
+  return 0.0f;
+}
+
+void lo_image_shift(const uint8_t* src, int W, int H, int stride, float sx, float sy, uint8_t* dst) {
+  int ix = cs_f2i(floorf(sx)), iy = cs_f2i(floorf(sy));
+  float tx = sx - (float)ix, ty = sy - (float)iy;
+  float kx[4] = {cubic_tap(tx + 1.0f), cubic_tap(tx), cubic_tap(1.0f - tx), cubic_tap(2.0f - tx)};
+  float ky[4] = {cubic_tap(ty + 1.0f), cubic_tap(ty), cubic_tap(1.0f - ty), cubic_tap(2.0f - ty)};
+  float* rowBuf = (float*)malloc(sizeof(float) * ((size_t)W + 4) * 4);
+  for (int y = 0; y < H; y++) {
+    int r0 = y + iy - 1;
+    int rows[4];
+    for (int i = 0; i < 4; i++) { int ry = r0 + i; rows[i] = ry < 0 ? 0 : ry >= H ? H - 1 : ry; }
+    for (int c = -2; c < W + 2; c++) {
+      int cx = c < 0 ? 0 : c >= W ? W - 1 : c;
+      int ob = (c + 2) * 4;
+      for (int ch = 0; ch < 4; ch++) {
+        float acc = (float)src[((size_t)rows[0] * stride + cx) * 4 + ch] * ky[0];
+        for (int i = 1; i < 4; i++) {
+          float t = (float)src[((size_t)rows[i] * stride + cx) * 4 + ch] * ky[i];
+          acc = t + acc;
+        }
+        rowBuf[ob + ch] = acc;
+      }
+    }
+    for (int x = 0; x < W; x++) {
+      int b = (x + ix - 1 + 2) * 4;
+      for (int ch = 0; ch < 4; ch++) {
+        float v0 = rowBuf[b + ch], v1 = rowBuf[b + 4 + ch], v2 = rowBuf[b + 8 + ch], v3 = rowBuf[b + 12 + ch];
+        float p3 = v3 * kx[3], p2 = v2 * kx[2], p1 = v1 * kx[1], p0 = v0 * kx[0];
+        float s = (p3 + p2) + (p1 + p0);
+        int q = cs_f2i(rintf(s));
+        dst[((size_t)y * W + x) * 4 + ch] = (uint8_t)(q < 0 ? 0 : q > 255 ? 255 : q);
+      }
+    }
+  }
+  free(rowBuf);
+}
+
+void lo_nearest_resize(const uint8_t* src, int sw, int sh, int sstride, int W, int H, uint8_t* dst) {
+  memset(dst, 0, (size_t)W * H * 4);
+  if (W > 0 && H > 0) {
+    int stepY = (int)((double)sh * 65536.0 / (double)H);
+    int stepX = (int)((double)sw * 65536.0 / (double)W);
+    int yAcc = 0;
+    for (int y = 0; y < H; y++) {
+      int sy = yAcc >> 16, xAcc = 0;
+      for (int x = 0; x < W; x++) {
+        int sx = xAcc >> 16;
+        memcpy(dst + ((size_t)y * W + x) * 4, src + ((size_t)sy * sstride + sx) * 4, 4);
+        xAcc += stepX;
+      }
+      yAcc += stepY;
+    }
+  }
+}
+
+void lo_inverse_depth(const float* src, size_t n, float* dst) {
+  for (size_t i = 0; i < n; i++) dst[i] = lo_rcp(src[i]);
+}
+
+static inline float exp2_fast(float t) {
+  const float C1 = ffrom(0x3d9fcb52u), C2 = ffrom(0x3e677e26u), C3 = ffrom(0x3f322226u), C4 = ffrom(0x3f7ffb19u);
+  t = t < 128.0f ? t : 128.0f;
+  t = t > -126.0f ? t : -126.0f;
+  int n = cs_f2i(t) + ((int32_t)fbits(t) >> 31);
+  float f = t - (float)n;
+  float p = ((f * C1 + C2) * f + C3) * f + C4;
+  return ffrom(fbits(p) + ((uint32_t)n << 23));
+}
+
+static inline float spatial_w(float f, int i) {
+  float d = fabsf(f - (float)(i * 2));
+  d = d < 1.0f ? d : 1.0f;
+  return cs_f2i(d) == 0 ? 1.0f : ffrom(0x3eaaaaabu);
+}
+
+void lo_bilateral_upsample(const float* lo_, int lw, int lh, const uint8_t* guide, int W, int H, int gstride, const uint8_t* g2,
+                           float sigma, float* outp) {
+  float k = 0.5f / (sigma * sigma);
+  const float eps = ffrom(0x322bcc77u);
+  int wm1 = lw - 1, hm1 = lh - 1;
+  for (int y = 0; y < H; y++) {
+    int iy0 = (y - 1) / 2;
+    float fy = (float)y + (-0.5f);
+    for (int x = 0; x < W; x++) {
+      const uint8_t* o = guide + ((size_t)y * gstride + x) * 4;
+      float hr = o[0], hg = o[1], hb = o[2];
+      int ix0 = (x - 1) / 2;
+      float fx = (float)x + (-0.5f);
+      int ibx = ix0 < 0 ? 0 : ix0;
+      if (ibx > wm1) ibx = wm1;
+      float wx0 = spatial_w(fx, ibx);
+      int ix1 = ix0 + 1;
+      if (ix1 < 0) ix1 = 0;
+      if (ix1 > wm1) ix1 = wm1;
+      float wx1 = spatial_w(fx, ix1);
+      float accV = 0.0f, accS = 0.0f;
+      for (int j = 0; j < 2; j++) {
+        int iy = iy0 + j;
+        if (iy < 0) iy = 0;
+        if (iy > hm1) iy = hm1;
+        float wy = spatial_w(fy, iy);
+        int lrow = iy * lw;
+        const uint8_t* q = g2 + ((size_t)iy * lw + ibx) * 4;
+        float d0 = hr - (float)q[0], d1 = hg - (float)q[1], d2 = hb - (float)q[2];
+        float s = d1 * d1 + (d2 * d2 + d0 * d0);
+        float t = -(s * k);
+        float w0 = (exp2_fast(t) + eps) * (wy * wx0);
+        q = g2 + ((size_t)iy * lw + ix1) * 4;
+        d0 = hr - (float)q[0]; d1 = hg - (float)q[1]; d2 = hb - (float)q[2];
+        s = d1 * d1 + (d2 * d2 + d0 * d0);
+        t = -(s * k);
+        float w1 = (exp2_fast(t) + eps) * (wy * wx1);
+        float v0 = lo_[lrow + ibx] * w0, v1 = lo_[lrow + ix1] * w1;
+        accV = v1 + (v0 + accV);
+        accS = w1 + (w0 + accS);
+      }
+      outp[(size_t)y * W + x] = accV / accS;
+    }
+  }
+}
+
+int lo_upsample(const float* prev_depth, int pw, int ph, const uint8_t* guide, int gw, int gh, int gstride, int set_w, int set_h,
+                float sigma, int scale, const float* prev_conf, float* out_depth, float* out_conf) {
+  uint8_t* shifted = (uint8_t*)malloc((size_t)gw * gh * 4);
+  uint8_t* g2 = (uint8_t*)malloc((size_t)pw * ph * 4 + 4);
+  float* inv = (float*)malloc(sizeof(float) * (size_t)pw * ph + 4);
+  float* u = (float*)malloc(sizeof(float) * (size_t)gw * gh);
+  lo_image_shift(guide, gw, gh, gstride, 0.5f, 0.5f, shifted);
+  lo_nearest_resize(shifted, gw, gh, gw, pw, ph, g2);
+  lo_inverse_depth(prev_depth, (size_t)pw * ph, inv);
+  lo_bilateral_upsample(inv, pw, ph, guide, gw, gh, gstride, g2, sigma, u);
+  lo_inverse_depth(u, (size_t)gw * gh, out_depth);
+  int rc = LO_OK;
+  if (gw != set_w * scale || gh != set_h * scale) rc = LO_ERR_UPSAMPLE_SIZE;
+  else if (prev_conf && pw > 0 && ph > 0 && out_conf) lo_bilateral_upsample(prev_conf, pw, ph, guide, gw, gh, gstride, g2, sigma, out_conf);
+  free(shifted); free(g2); free(inv); free(u);
+  return rc;
+}
+
+/* ---------------- traversal replay (DenseStereoSgm.cs:206-224) ---------------- */
+long lo_traversal_trace(int W, int H, int T, int xsw, int* ev, long max_events) {
+  int slots = W + 2;
+  long* last = (long*)malloc(sizeof(long) * 2 * (size_t)slots);
+  for (int i = 0; i < 2 * slots; i++) last[i] = -1;
+  uint8_t* seen = (uint8_t*)calloc((size_t)W * H, 1);
+  long n = 0;
+  static const int dirs[2] = {1, -1};
+  for (int di = 0; di < 2; di++) {
+    int dir = dirs[di];
+    memset(seen, 0, (size_t)W * H);
+    int gwN = (W + T + T - 1) / T, ghN = (H + T - 1) / T;
+    for (int j = 0; j < ghN; j++)
+      for (int i = 0; i < gwN; i++) {
+        int x0 = dir > 0 ? i * T : W - 1 - i * T, y0 = dir > 0 ? j * T : H - 1 - j * T;
+        int yEnd = iclamp(y0 + dir * T, -1, H);
+        for (int r = 0;; r++) {
+          int y = y0 + dir * r;
+          if (y == yEnd) break;
+          int xs = iclamp(x0 - dir * r, 0, (xsw && dir > 0) ? W : W - 1), xe = iclamp(x0 + dir * (T - r), -1, W);
+          if (xs == xe) continue;
+          int cur = (r & 1) == 0 ? 1 : 0, other = 1 - cur;
+          for (int x = xs; x != xe; x += dir) {
+            if (n >= max_events) { free(last); free(seen); return -1; }
+            int slot = x + 1;
+            int* e = ev + 9 * n;
+            e[0] = dir; e[1] = x; e[2] = y; e[3] = r; e[4] = seen[(size_t)y * W + x] ? 1 : 0;
+            seen[(size_t)y * W + x] = 1;
+            for (int p = 0; p < 4; p++) {
+              int ns = slot + (p == 2 ? 0 : p == 3 ? dir : -dir);
+              int half = p == 0 ? cur : other;
+              e[5 + p] = (int)last[half * slots + ns];
+            }
+            last[cur * slots + slot] = n;
+            n++;
+          }
+        }
+      }
+  }
+  free(last); free(seen);
+  return n;
+}

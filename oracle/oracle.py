@@ -1,0 +1,246 @@
+"""ctypes wrapper of the CPU oracle (oracle/lux_oracle.c) — TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker / baseline; never by the
+product path. Parity unpinned against reference outputs (see lux_oracle.h).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liblux_oracle.so")
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+class LoParams(ctypes.Structure):
+    _fields_ = [("margin", ctypes.c_int), ("plane_density", ctypes.c_float), ("scale", ctypes.c_int), ("skip_mode", ctypes.c_int),
+                ("p1", ctypes.c_uint16), ("p2scale", ctypes.c_float), ("guidance", ctypes.c_float * 4), ("tile", ctypes.c_int)]
+
+
+class LoCalib(ctypes.Structure):
+    _fields_ = [("K", ctypes.c_float * 9), ("T", ctypes.c_float * 3), ("R", ctypes.c_float * 9)]
+
+
+class LoLayer(ctypes.Structure):
+    _fields_ = [("p", LoParams), ("index", ctypes.c_int), ("align", ctypes.c_int), ("w", ctypes.c_int), ("h", ctypes.c_int),
+                ("n_planes", ctypes.c_int), ("min_lo", ctypes.c_int), ("max_hi", ctypes.c_int),
+                ("planes", ctypes.POINTER(ctypes.c_float)), ("guidance", ctypes.POINTER(ctypes.c_uint8)),
+                ("skip", ctypes.POINTER(ctypes.c_uint8)), ("start", ctypes.POINTER(ctypes.c_uint16)),
+                ("count", ctypes.POINTER(ctypes.c_uint16)), ("cap", ctypes.POINTER(ctypes.c_uint16)),
+                ("off", ctypes.POINTER(ctypes.c_uint64)), ("agg", ctypes.POINTER(ctypes.c_uint16)),
+                ("agg_pass1", ctypes.POINTER(ctypes.c_uint16)), ("raw", ctypes.POINTER(ctypes.c_uint8)),
+                ("depth", ctypes.POINTER(ctypes.c_float)),
+                ("n_cams", ctypes.c_int), ("images", ctypes.c_void_p), ("iw", ctypes.c_void_p), ("ih", ctypes.c_void_p),
+                ("warps", ctypes.c_void_p), ("wq", ctypes.c_void_p),
+                ("threads", ctypes.c_int), ("keep_pass1", ctypes.c_int), ("xsw", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        l = ctypes.CDLL(LIB)
+        l.lo_planes.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.POINTER(LoCalib), ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)]
+        l.lo_box_filter3.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        l.lo_box_filter3_scalar.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        l.lo_layer_init.argtypes = [ctypes.POINTER(LoLayer), ctypes.POINTER(LoParams), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(LoCalib), ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_int, ctypes.POINTER(LoLayer)]
+        l.lo_layer_compute.argtypes = [ctypes.POINTER(LoLayer)]
+        l.lo_layer_free.argtypes = [ctypes.POINTER(LoLayer)]
+        l.lo_pyramid_run.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.POINTER(LoCalib), ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(LoLayer)]
+        l.lo_upsample.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p]
+        l.lo_traversal_trace.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_long]
+        l.lo_traversal_trace.restype = ctypes.c_long
+        l.lo_rcp_bits.argtypes = [ctypes.c_uint32]
+        l.lo_rcp_bits.restype = ctypes.c_uint32
+        l.lo_rsqrt_bits.argtypes = [ctypes.c_uint32]
+        l.lo_rsqrt_bits.restype = ctypes.c_uint32
+        l.lo_mt_seed.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        l.lo_mt_next.argtypes = [ctypes.c_void_p]
+        l.lo_mt_next.restype = ctypes.c_uint32
+        l.lo_skip_mask.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        l.lo_flow_matrix.argtypes = [ctypes.POINTER(LoCalib), ctypes.POINTER(LoCalib), ctypes.POINTER(ctypes.c_float)]
+        l.lo_default_params.argtypes = [ctypes.POINTER(LoParams)]
+        l.lo_l16_pyramid.argtypes = [ctypes.POINTER(LoParams)]
+        _lib = l
+    return _lib
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code, where):
+        super().__init__(f"oracle error {code} in {where}")
+        self.code = code
+
+
+def _calibs(calibs):
+    arr = (LoCalib * len(calibs))()
+    for i, c in enumerate(calibs):
+        for j, v in enumerate(np.asarray(c.K, np.float32).reshape(9)):
+            arr[i].K[j] = float(v)
+        for j, v in enumerate(np.asarray(c.T, np.float32).reshape(3)):
+            arr[i].T[j] = float(v)
+        for j, v in enumerate(np.asarray(c.R, np.float32).reshape(9)):
+            arr[i].R[j] = float(v)
+    return arr
+
+
+def params_c(p):
+    lp = LoParams()
+    lp.margin, lp.plane_density, lp.scale, lp.skip_mode = p.margin, p.plane_density, p.scale, p.skip_mode
+    lp.p1, lp.p2scale, lp.tile = p.p1, p.p2scale, p.tile
+    for i in range(4):
+        lp.guidance[i] = float(p.guidance[i])
+    return lp
+
+
+def planes(near, far, calibs, density, align):
+    out = (ctypes.c_float * (4096 + align + 16))()
+    n = ctypes.c_int()
+    rc = lib().lo_planes(near, far, _calibs(calibs), len(calibs), density, align, out, ctypes.byref(n))
+    if rc:
+        raise OracleError(rc, "planes")
+    return np.frombuffer(out, np.float32, n.value).copy()
+
+
+def box_filter3(img, scalar=False):
+    a = np.ascontiguousarray(img, np.uint8)
+    h, w, _ = a.shape
+    out = np.empty_like(a)
+    (lib().lo_box_filter3_scalar if scalar else lib().lo_box_filter3)(a.ctypes.data, w, h, out.ctypes.data)
+    return out
+
+
+def _arr(ptr, dtype, n):
+    if n == 0 or not ptr:
+        return np.zeros(0, dtype)
+    return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
+
+
+def _extract(L):
+    w, h = L.w, L.h
+    npx = w * h
+    vol = int(np.ctypeslib.as_array(L.off, shape=(npx + 1,))[npx])
+    return {
+        "W": w, "H": h, "n_planes": L.n_planes, "MinLo": L.min_lo, "MaxHi": L.max_hi, "Align": L.align,
+        "Planes": _arr(L.planes, np.float32, L.n_planes),
+        "Guidance": _arr(L.guidance, np.uint8, npx * 4).reshape(h, w, 4),
+        "Skip": _arr(L.skip, np.uint8, npx).reshape(h, w),
+        "Start": _arr(L.start, np.uint16, npx).reshape(h, w),
+        "Count": _arr(L.count, np.uint16, npx).reshape(h, w),
+        "Cap": _arr(L.cap, np.uint16, npx).reshape(h, w),
+        "Offsets": _arr(L.off, np.uint64, npx + 1),
+        "Agg": _arr(L.agg, np.uint16, vol),
+        "AggPass1": _arr(L.agg_pass1, np.uint16, vol) if L.agg_pass1 else None,
+        "Raw": _arr(L.raw, np.uint8, vol),
+        "Depth": _arr(L.depth, np.float32, npx).reshape(h, w) if L.depth else None,
+    }
+
+
+def _images(images):
+    imgs = [np.ascontiguousarray(im, np.uint8) for im in images]
+    ptrs = (ctypes.c_void_p * len(imgs))(*[im.ctypes.data for im in imgs])
+    iw = (ctypes.c_int * len(imgs))(*[im.shape[1] for im in imgs])
+    ih = (ctypes.c_int * len(imgs))(*[im.shape[0] for im in imgs])
+    return imgs, ptrs, iw, ih
+
+
+def layer(filtered, gray, calibs, near, far, params, index=0, align=8, prev=None, keep_pass1=False, threads=1, xsw=False):
+    """DenseLayer.Init + Compute on box-filtered images. prev: a dict from a previous call (needs its Depth and Skip)."""
+    imgs, ptrs, iw, ih = _images(filtered)
+    g = np.ascontiguousarray(np.asarray(gray, np.uint8))
+    cc = _calibs(calibs)
+    L = LoLayer()
+    prevL = None
+    if prev is not None:
+        prevL = LoLayer()
+        prevL.w, prevL.h = prev["W"], prev["H"]
+        pd = np.ascontiguousarray(prev["Depth"], np.float32)
+        ps = np.ascontiguousarray(prev["Skip"], np.uint8)
+        prevL.depth = pd.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        prevL.skip = ps.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+    lp = params_c(params)
+    rc = lib().lo_layer_init(ctypes.byref(L), ctypes.byref(lp), index, len(imgs), ptrs, iw, ih, g.ctypes.data, cc, near, far, align,
+                             ctypes.byref(prevL) if prevL is not None else None)
+    try:
+        if rc:
+            raise OracleError(rc, "layer_init")
+        L.threads, L.keep_pass1, L.xsw = threads, 1 if keep_pass1 else 0, 1 if xsw else 0
+        rc = lib().lo_layer_compute(ctypes.byref(L))
+        if rc:
+            raise OracleError(rc, "layer_compute")
+        return _extract(L)
+    finally:
+        lib().lo_layer_free(ctypes.byref(L))
+
+
+def pyramid(images, gray, calibs, near, far, threads=1, keep_pass1=False):
+    """DenseStereoPyramid.Run on the raw camera images: six layer dicts."""
+    imgs, ptrs, iw, ih = _images(images)
+    g = np.ascontiguousarray(np.asarray(gray, np.uint8))
+    cc = _calibs(calibs)
+    Ls = (LoLayer * 6)()
+    rc = lib().lo_pyramid_run(len(imgs), ptrs, iw, ih, g.ctypes.data, cc, near, far, threads, 1 if keep_pass1 else 0, Ls)
+    try:
+        if rc:
+            raise OracleError(rc, "pyramid")
+        return [_extract(Ls[i]) for i in range(6)]
+    finally:
+        for i in range(6):
+            lib().lo_layer_free(ctypes.byref(Ls[i]))
+
+
+def upsample(prev_depth, pw, ph, guide, set_w, set_h, sigma=12.0, scale=2, prev_conf=None):
+    g = np.ascontiguousarray(guide, np.uint8)
+    gh, gw, _ = g.shape
+    pd = np.ascontiguousarray(np.asarray(prev_depth, np.float32).reshape(-1))
+    out = np.empty(gw * gh, np.float32)
+    conf = None
+    if prev_conf is not None:
+        pc = np.ascontiguousarray(np.asarray(prev_conf, np.float32).reshape(-1))
+        conf = np.empty(gw * gh, np.float32)
+    rc = lib().lo_upsample(pd.ctypes.data, pw, ph, g.ctypes.data, gw, gh, gw, set_w, set_h, sigma, scale,
+                           pc.ctypes.data if prev_conf is not None else None, out.ctypes.data,
+                           conf.ctypes.data if conf is not None else None)
+    if rc:
+        raise OracleError(rc, "upsample")
+    return out.reshape(gh, gw), (conf.reshape(gh, gw) if conf is not None else None)
+
+
+def traversal_trace(w, h, tile, xsw=False):
+    """Per Pixel() call of the reference traversal: (dir, x, y, r, is_revisit, src0..src3) as an (n, 9) int array."""
+    cap = 2 * w * h * 2 + 64
+    buf = np.empty(cap * 9, np.int32)
+    n = lib().lo_traversal_trace(w, h, tile, 1 if xsw else 0, buf.ctypes.data, cap)
+    if n < 0:
+        raise OracleError(-1, "traversal_trace")
+    return buf[: n * 9].reshape(n, 9).copy()
+
+
+def skip_mask(mode, w, h):
+    out = np.empty(w * h, np.uint8)
+    rc = lib().lo_skip_mask(mode, w, h, out.ctypes.data)
+    if rc:
+        raise OracleError(rc, "skip_mask")
+    return out.reshape(h, w)
+
+
+def mt19937_stream(seed, n):
+    st = ctypes.create_string_buffer(624 * 4 + 16)
+    lib().lo_mt_seed(st, seed)
+    return np.array([lib().lo_mt_next(st) for _ in range(n)], np.uint32)

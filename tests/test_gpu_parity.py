@@ -1,0 +1,114 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle, bit for bit (integer stages) and within 1e-5
+relative (the float upsample; it is checked for exact equality as well)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from lux_b200 import api
+    return api.Context(0)
+
+
+def _filtered(oracle, images):
+    return [oracle.box_filter3(im) for im in images]
+
+
+@pytest.mark.parametrize("h,w", [(1, 1), (2, 2), (3, 7), (41, 67), (480, 640)])
+def test_box_filter(ctx, oracle, h, w):
+    from lux_b200 import api
+    img = np.random.default_rng(h + w).integers(0, 256, (h, w, 4), dtype=np.uint8)
+    assert np.array_equal(api.DenseStereo.box_filter3(img, ctx=ctx), oracle.box_filter3(img))
+
+
+def _compare_layer(gl, ol, tag):
+    assert (gl.W, gl.H, gl.n_planes, gl.MinLo, gl.MaxHi) == (ol["W"], ol["H"], ol["n_planes"], ol["MinLo"], ol["MaxHi"]), tag
+    assert np.array_equal(gl.Planes, ol["Planes"]), tag
+    assert np.array_equal(gl.Start, ol["Start"]) and np.array_equal(gl.Count, ol["Count"]), tag
+    assert np.array_equal(gl.Cap, ol["Cap"]) and np.array_equal(gl.Skip, ol["Skip"]), tag
+    assert np.array_equal(gl.Offsets, ol["Offsets"]), tag
+    assert np.array_equal(gl.Guidance, ol["Guidance"]), tag
+    comp = (ol["Skip"].reshape(-1) == 0)
+    off, cap = ol["Offsets"][:-1], ol["Cap"].reshape(-1).astype(np.int64)
+    mask = np.repeat(comp, cap)
+    assert np.array_equal(gl.Raw[mask], ol["Raw"][mask]), tag + " raw"
+    if ol["AggPass1"] is not None:
+        assert np.array_equal(gl.AggPass1, ol["AggPass1"]), tag + " agg pass1"
+    assert np.array_equal(gl.Agg, ol["Agg"]), tag + " agg"
+    assert np.array_equal(gl.Depth.view(np.uint32), ol["Depth"].view(np.uint32)), tag + " depth"
+
+
+@pytest.mark.parametrize("w,h,d,tile", [(48, 40, 16, 8), (65, 49, 16, 4), (160, 120, 32, 16), (257, 93, 64, 64), (100, 77, 24, 8)])
+def test_uniform_layer_bit_exact(ctx, oracle, w, h, d, tile):
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(w, h, d, seed=w + h, tile=tile)
+    filt = _filtered(oracle, wl.images)
+    ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, ctx=ctx)
+    try:
+        _compare_layer(gl, ol, f"{w}x{h} D{d} T{tile}")
+    finally:
+        gl.close()
+
+
+def test_multicamera_colour_layer_bit_exact(ctx, oracle):
+    """Three colour cameras, translated in x and y: the general projection with half-pixel resampling."""
+    from lux_b200 import api, synth
+    cap = synth.capture(120, 90, 3, seed=11, f=90.0, baseline_mm=(20.0, 60.0))
+    filt = _filtered(oracle, cap.images)
+    p = api.StereoParams(scale=1, tile=8, skip_mode=0, plane_density=2.0)
+    ol = oracle.layer(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True, ctx=ctx)
+    try:
+        _compare_layer(gl, ol, "3cam")
+    finally:
+        gl.close()
+
+
+def test_pyramid_bit_exact(ctx, oracle):
+    """DenseStereoPyramid.Run: six L16 layers (ragged ranges, skip masks, align choice) against the oracle."""
+    from lux_b200 import api, synth
+    cap = synth.capture(416, 312, 3, seed=5, f=330.0)
+    ol = oracle.pyramid(cap.images, cap.gray, cap.calibs, cap.near, cap.far, keep_pass1=True)
+    gls = api.DenseStereoPyramid.run(cap.images, cap.gray, cap.calibs, cap.near, cap.far, keep_pass1=True, ctx=ctx)
+    try:
+        for i in range(6):
+            _compare_layer(gls[i], ol[i], f"L{i}")
+    finally:
+        for g in gls:
+            g.close()
+
+
+@pytest.mark.parametrize("pw,ph", [(52, 39), (208, 156)])
+def test_upsample(ctx, oracle, pw, ph):
+    from lux_b200 import api
+    rng = np.random.default_rng(pw)
+    depth = rng.uniform(300.0, 6000.0, (ph, pw)).astype(np.float32)
+    guide = rng.integers(0, 256, (2 * ph, 2 * pw, 4), dtype=np.uint8)
+    conf = rng.uniform(0, 1, (ph, pw)).astype(np.float32)
+    od, oc = oracle.upsample(depth, pw, ph, guide, pw, ph, prev_conf=conf)
+    r = api.DenseUpsampleLayer.run(depth, pw, ph, guide, pw, ph, prev_confidence=conf, ctx=ctx)
+    rel = np.abs(r.Depth - od) / np.abs(od)
+    assert rel.max() <= 1e-5
+    assert np.array_equal(r.Depth.view(np.uint32), od.view(np.uint32))
+    assert np.array_equal(r.Confidence.view(np.uint32), oc.view(np.uint32))
+
+
+def test_upsample_size_error(ctx):
+    from lux_b200 import api
+    depth = np.ones((10, 12), np.float32) * 1000
+    guide = np.zeros((20, 24, 4), np.uint8)
+    with pytest.raises(api.InvalidOperationError):
+        api.DenseUpsampleLayer.run(depth, 12, 10, guide, 13, 10, ctx=ctx)
+
+
+def test_layer_errors(ctx):
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(32, 24, 16, seed=1, tile=8)
+    with pytest.raises(api.InvalidOperationError):
+        api.DenseLayer.compute(wl.images, wl.gray, wl.calibs, 500.0, 100.0, wl.params, ctx=ctx)
+    bad = api.StereoParams(scale=1, tile=8, skip_mode=3, plane_density=1.0)
+    with pytest.raises(api.NotSupportedError):
+        api.DenseLayer.compute(wl.images, wl.gray, wl.calibs, wl.near, wl.far, bad, ctx=ctx)
