@@ -85,20 +85,31 @@ int lux_sgm_planes(float near_, float far_, const lux_calib* calibs, int32_t n_c
 /* DenseStereo.BoxFilter3 (DenseStereo.cs:93-123) of one image; dst is host memory of w*h*4 bytes (dense). */
 int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst);
 
+/* flags of lux_sgm_layer / lux_sgm_pyramid */
+#define LUX_LAYER_KEEP_PASS1 1   /* keep the aggregates after pass +1 (DenseLayer.KeepPass1) */
+#define LUX_LAYER_KEEP_AGG 2     /* keep the final aggregates (DenseLayer.Agg); the depth never needs them */
+#define LUX_LAYER_PREFILTER 4    /* images are unfiltered: apply DenseStereo.BoxFilter3 on the device first */
+#define LUX_LAYER_FORCE_REPLAY 8 /* aggregate with the exact traversal replay even where the fast uniform kernel applies */
+
 /* DenseLayer.Init + DenseLayer.Compute (DenseStereoSgm.cs:34-62, 181-232): one pyramid layer on the GPU.
- * images: n_cams camera images (camera 0 = reference), box-FILTERED already unless prefilter != 0, which applies
- * DenseStereo.BoxFilter3 to each on the device first (as DenseStereoPyramid.Run does, DenseStereoSgm.cs:335);
- * gray[k] selects the grey cost weights; prev = the previous layer (NULL for a first layer: every pixel searches all
- * planes). keep_pass1 keeps the aggregates after pass +1. The layer object owns its device state until
- * lux_layer_destroy. */
+ * images: n_cams camera images (camera 0 = reference), box-FILTERED already unless LUX_LAYER_PREFILTER (as
+ * DenseStereoPyramid.Run filters them, DenseStereoSgm.cs:335); gray[k] selects the grey cost weights; prev = the
+ * previous layer (NULL for a first layer: every pixel searches all planes). The layer object owns its device state
+ * until lux_layer_destroy. */
 int lux_sgm_layer(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
                   float near_, float far_, const lux_stereo_params* params, int32_t index, int32_t align, const lux_layer* prev,
-                  int32_t keep_pass1, int32_t prefilter, lux_layer** out);
+                  int32_t flags, lux_layer** out);
 
 /* DenseStereoPyramid.Run (DenseStereoSgm.cs:331-353): box filter, six L16 layers with the 1 GiB align-8/align-2 choice.
- * out receives six layer objects. */
+ * flags: LUX_LAYER_KEEP_PASS1 / KEEP_AGG / FORCE_REPLAY apply to every layer. out receives six layer objects. */
 int lux_sgm_pyramid(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
-                    float near_, float far_, int32_t keep_pass1, lux_layer* out[6]);
+                    float near_, float far_, int32_t flags, lux_layer* out[6]);
+
+/* Diagnostic (host only): the revisit schedule the fast uniform kernel replays for a w×h layer with tile T, one pass
+ * (second_pass = pass -1), as 7 int32 per row: flags, batch_first, batch_count, src0, src1, src2, extra
+ * (see lux_b200/csrc/revisit_schedule.h), then end_first and end_count: out holds 7*h + 2 int32. *y_b receives
+ * pass +1's last odd row. */
+int lux_sgm_revisit_schedule(int32_t w, int32_t h, int32_t tile, int32_t second_pass, int32_t* out, int32_t* y_b);
 
 /* Layer facts (DenseLayer fields). */
 typedef struct {

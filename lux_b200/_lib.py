@@ -18,6 +18,8 @@ ERRORS = {
 FIELD_DEPTH, FIELD_PLANES, FIELD_SKIP, FIELD_START, FIELD_COUNT, FIELD_CAP = 0, 1, 2, 3, 4, 5
 FIELD_OFFSETS, FIELD_AGG, FIELD_AGG_PASS1, FIELD_RAW, FIELD_GUIDANCE = 6, 7, 8, 9, 10
 
+LAYER_KEEP_PASS1, LAYER_KEEP_AGG, LAYER_PREFILTER, LAYER_FORCE_REPLAY = 1, 2, 4, 8
+
 
 class Img(ctypes.Structure):
     _fields_ = [("data", ctypes.c_void_p), ("w", ctypes.c_int32), ("h", ctypes.c_int32), ("stride", ctypes.c_int32),
@@ -49,6 +51,8 @@ SIGNATURES = [
     ("lux_sgm_sync", ctypes.c_int, [ctypes.c_void_p]),
     ("lux_sgm_kernel_launches", ctypes.c_uint64, []),
     ("lux_sgm_stream", ctypes.c_void_p, [ctypes.c_void_p]),
+    ("lux_sgm_revisit_schedule", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("lux_sgm_default_params", None, [ctypes.POINTER(Params)]),
     ("lux_sgm_l16_pyramid", None, [ctypes.POINTER(Params)]),
     ("lux_sgm_planes", ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.POINTER(Calib), ctypes.c_int32, ctypes.c_float,
@@ -56,7 +60,7 @@ SIGNATURES = [
     ("lux_sgm_box_filter3", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Img), ctypes.c_void_p]),
     ("lux_sgm_layer", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Img), ctypes.c_void_p, ctypes.POINTER(Calib),
                                      ctypes.c_float, ctypes.c_float, ctypes.POINTER(Params), ctypes.c_int32, ctypes.c_int32,
-                                     ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+                                     ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     ("lux_sgm_pyramid", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Img), ctypes.c_void_p, ctypes.POINTER(Calib),
                                        ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     ("lux_layer_get_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LayerInfo)]),

@@ -145,6 +145,22 @@ class Context:
 _default_ctx = None
 
 
+def _flags(keep_pass1, keep_agg, prefilter, force_replay):
+    return ((L.LAYER_KEEP_PASS1 if keep_pass1 else 0) | (L.LAYER_KEEP_AGG if keep_agg else 0) |
+            (L.LAYER_PREFILTER if prefilter else 0) | (L.LAYER_FORCE_REPLAY if force_replay else 0))
+
+
+def revisit_schedule(w, h, tile, second_pass):
+    """The revisit schedule of the fast uniform kernel (diagnostic): (h, 7) int32 rows, pass +1's last odd row, and the
+    (first, count) of the revisits the last row runs after its own visit."""
+    out = np.zeros(7 * h + 2, np.int32)
+    yb = ctypes.c_int32()
+    rc = L.load().lux_sgm_revisit_schedule(w, h, tile, 1 if second_pass else 0, out.ctypes.data, ctypes.byref(yb))
+    if rc:
+        _raise(rc, "lux_sgm_revisit_schedule failed")
+    return out[: 7 * h].reshape(h, 7), yb.value, (int(out[7 * h]), int(out[7 * h + 1]))
+
+
 def kernel_launches() -> int:
     """Kernels the CUDA library has launched in this process."""
     return int(L.load().lux_sgm_kernel_launches())
@@ -197,9 +213,12 @@ class DenseLayer:
 
     @staticmethod
     def compute(images, gray, calibs, near, far, params: StereoParams, index=0, align=8, prev: Optional["DenseLayer"] = None,
-                keep_pass1=False, prefilter=False, ctx: Optional[Context] = None) -> "DenseLayer":
+                keep_pass1=False, prefilter=False, keep_agg=False, force_replay=False,
+                ctx: Optional[Context] = None) -> "DenseLayer":
         """DenseLayer.Init + Compute (DenseStereoSgm.cs:34-62, 181-232). images: RGBA8 (camera 0 = reference), box-filtered
-        already unless prefilter=True (then BoxFilter3 runs on the GPU first, as DenseStereoPyramid.Run does)."""
+        already unless prefilter=True (then BoxFilter3 runs on the GPU first, as DenseStereoPyramid.Run does).
+        keep_pass1 / keep_agg keep DenseLayer.AggPass1 / Agg readable (the depth needs neither); force_replay aggregates
+        with the exact traversal replay kernel even where the fast uniform kernel applies."""
         ctx = ctx or default_context()
         arr = (L.Img * len(images))()
         keep = []
@@ -212,8 +231,8 @@ class DenseLayer:
         p = params.to_c()
         out = ctypes.c_void_p()
         rc = ctx.lib.lux_sgm_layer(ctx.handle, len(images), arr, g.ctypes.data, cc, near, far, ctypes.byref(p), index, align,
-                                   prev.handle if prev is not None else None, 1 if keep_pass1 else 0, 1 if prefilter else 0,
-                                   ctypes.byref(out))
+                                   prev.handle if prev is not None else None,
+                                   _flags(keep_pass1, keep_agg, prefilter, force_replay), ctypes.byref(out))
         ctx.check(rc)
         return DenseLayer(ctx, out)
 
@@ -284,7 +303,8 @@ class DenseLayer:
 
 class DenseStereoPyramid:
     @staticmethod
-    def run(images, gray, calibs, near=200.0, far=640000.0, keep_pass1=False, ctx: Optional[Context] = None) -> List[DenseLayer]:
+    def run(images, gray, calibs, near=200.0, far=640000.0, keep_pass1=False, keep_agg=False, force_replay=False,
+            ctx: Optional[Context] = None) -> List[DenseLayer]:
         """DenseStereoPyramid.Run (DenseStereoSgm.cs:331-353): the raw (unfiltered) camera images in, six layers out."""
         ctx = ctx or default_context()
         arr = (L.Img * len(images))()
@@ -296,7 +316,8 @@ class DenseStereoPyramid:
         g = np.ascontiguousarray(np.asarray(gray, dtype=np.uint8))
         cc = _calibs_c(calibs)
         outs = (ctypes.c_void_p * 6)()
-        ctx.check(ctx.lib.lux_sgm_pyramid(ctx.handle, len(images), arr, g.ctypes.data, cc, near, far, 1 if keep_pass1 else 0, outs))
+        ctx.check(ctx.lib.lux_sgm_pyramid(ctx.handle, len(images), arr, g.ctypes.data, cc, near, far,
+                                          _flags(keep_pass1, keep_agg, False, force_replay), outs))
         return [DenseLayer(ctx, ctypes.c_void_p(outs[i])) for i in range(6)]
 
 

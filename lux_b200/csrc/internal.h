@@ -88,9 +88,11 @@ struct UniformBuffers {
   void* events;         // host-built revisit schedule
 };
 size_t uniform_supported_planes();
-bool uniform_fast_supported(int W, int H, int n_planes, int tile);
+bool uniform_fast_supported(int W, int H, int n_planes, int tile, uint16_t p1, float p2scale);
 size_t uniform_scratch_bytes(int W, int H, int n_planes, int tile);
+// Both passes, WTA into depth. agg holds pass +1's aggregates afterwards, and the final ones when keep_agg.
 int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
-                    uint16_t* agg_pass1, float* depth, void* scratch, size_t scratch_bytes, int* err, cudaStream_t s);
+                    uint16_t* agg_pass1, float* depth, int keep_agg, void* scratch, size_t scratch_bytes, int* err,
+                    cudaStream_t s);
 
 }  // namespace lux

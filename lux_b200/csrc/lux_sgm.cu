@@ -13,6 +13,7 @@
 #include "../../include/lux_sgm.h"
 #include "host_geom.h"
 #include "internal.h"
+#include "revisit_schedule.h"
 
 using namespace lux;
 
@@ -39,6 +40,7 @@ struct lux_layer {
   uint64_t volume = 0;
   float ms_cost = 0.f, ms_sgm = 0.f, ms_wta = 0.f;
   int sgm_kernel = 0;
+  bool agg_final = false;  // agg holds the final aggregates (always for the replay kernel, on request for the fast one)
   std::vector<float> planes_h;
   float* planes = nullptr;
   uchar4* guidance = nullptr;
@@ -200,7 +202,7 @@ int ranges_from_previous(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, const std::
 
 int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const int* iw, const int* ih, const uint8_t* gray,
                 const lux_calib* calibs, float near_, float far_, const lux_stereo_params& p, int index, int align, const lux_layer* prev,
-                int keep_pass1, lux_layer* L) {
+                int flags, lux_layer* L) {
   int rc;
   if (p.scale <= 0) return set_err(ctx, LUX_ERR_ARG, "scale must be positive");
   if (p.tile < 2) return set_err(ctx, LUX_ERR_UNSUPPORTED, "tile %d: the GPU traversal needs a tile of at least 2", p.tile);
@@ -262,7 +264,7 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   if ((rc = alloc_t(ctx, B, L->volume + 8, &L->raw))) return rc;
   CK(cudaMemsetAsync(L->agg, 0, (L->volume + 8) * 2, s));
   if (!uniform) CK(cudaMemsetAsync(L->raw, 0, L->volume + 8, s));
-  if (keep_pass1) {
+  if (flags & LUX_LAYER_KEEP_PASS1) {
     if ((rc = alloc_t(ctx, B, L->volume + 8, &L->agg_pass1))) return rc;
   }
   LayerGeom g;
@@ -294,6 +296,26 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   launch_cost(ca, g, L->raw, ctx->d_err, s);
   // aggregation: two passes over the sheared tiles, then WTA
   CK(cudaEventRecord(ctx->ev[1], s));
+  const int xsw = 0;  // LUX_SGM_XSW unset: the reference default (DenseStereoSgm.cs:31)
+  if (uniform && !(flags & LUX_LAYER_FORCE_REPLAY) && uniform_fast_supported(W, H, L->n, p.tile, p.p1, p.p2scale)) {
+    void* scr = nullptr;
+    const size_t sb = uniform_scratch_bytes(W, H, L->n, p.tile);
+    if ((rc = dev_alloc(ctx, tmp, sb, &scr))) return rc;
+    rc = run_sgm_uniform(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth,
+                         (flags & LUX_LAYER_KEEP_AGG) ? 1 : 0, scr, sb, ctx->d_err, s);
+    if (rc) return set_err(ctx, LUX_ERR_CUDA, "uniform aggregation launch failed (%d)", rc);
+    CK(cudaEventRecord(ctx->ev[2], s));
+    CK(cudaEventRecord(ctx->ev[3], s));
+    L->sgm_kernel = 1;
+    L->agg_final = (flags & LUX_LAYER_KEEP_AGG) != 0;
+    CK(cudaGetLastError());
+    if ((rc = take_device_error(ctx))) return rc;
+    CK(cudaEventElapsedTime(&L->ms_cost, ctx->ev[0], ctx->ev[1]));
+    CK(cudaEventElapsedTime(&L->ms_sgm, ctx->ev[1], ctx->ev[2]));
+    L->ms_wta = 0.f;  // fused into pass -1
+    return LUX_OK;
+  }
+  L->agg_final = true;
   const int bands = (H + p.tile - 1) / p.tile;
   EmuBuffers eb;
   eb.Llen = emu_line_buffer_elems(W, L->max_hi);
@@ -305,9 +327,8 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   if ((rc = alloc_t(ctx, tmp, 2, &eb.ticket))) return rc;
   if ((rc = alloc_t(ctx, tmp, (size_t)2 * bands, &eb.progress))) return rc;
   emu_init_buffers(eb, W, L->max_hi, align, bands, s);
-  const int xsw = 0;  // LUX_SGM_XSW unset: the reference default
   launch_sgm_emulate(g, eb, +1, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, ctx->d_err, s);
-  if (keep_pass1) CK(cudaMemcpyAsync(L->agg_pass1, L->agg, (L->volume + 8) * 2, cudaMemcpyDeviceToDevice, s));
+  if (L->agg_pass1) CK(cudaMemcpyAsync(L->agg_pass1, L->agg, (L->volume + 8) * 2, cudaMemcpyDeviceToDevice, s));
   launch_sgm_emulate(g, eb, -1, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, ctx->d_err, s);
   CK(cudaEventRecord(ctx->ev[2], s));
   launch_wta(g, L->agg, L->depth, ctx->d_err, s);
@@ -376,6 +397,19 @@ uint64_t lux_sgm_kernel_launches(void) { return lux::kernel_launches(); }
 
 void* lux_sgm_stream(lux_sgm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+int lux_sgm_revisit_schedule(int32_t w, int32_t h, int32_t tile, int32_t second_pass, int32_t* out, int32_t* y_b) {
+  if (w <= 0 || h <= 0 || tile <= 0 || !out) return LUX_ERR_ARG;
+  RevisitSchedule sch;
+  build_revisit_schedule(w, h, tile, second_pass != 0, sch);
+  const std::vector<int>* cols[7] = {&sch.flags, &sch.batch_first, &sch.batch_count, &sch.src0, &sch.src1, &sch.src2, &sch.extra};
+  for (int y = 0; y < h; y++)
+    for (int k = 0; k < 7; k++) out[(size_t)y * 7 + k] = (*cols[k])[y];
+  out[(size_t)h * 7] = sch.end_first;
+  out[(size_t)h * 7 + 1] = sch.end_count;
+  if (y_b) *y_b = sch.y_b;
+  return LUX_OK;
+}
+
 int lux_sgm_sync(lux_sgm_ctx* ctx) {
   if (!ctx) return LUX_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
@@ -430,7 +464,7 @@ int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst
 
 int lux_sgm_layer(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
                   float near_, float far_, const lux_stereo_params* params, int32_t index, int32_t align, const lux_layer* prev,
-                  int32_t keep_pass1, int32_t prefilter, lux_layer** out) {
+                  int32_t flags, lux_layer** out) {
   if (!ctx || !images || !calibs || !params || !out || n_cams <= 0) return LUX_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
@@ -446,7 +480,7 @@ int lux_sgm_layer(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images,
     rc = upload_image(ctx, imgs, images[k], &dimg[k]);
     iw[k] = images[k].w;
     ih[k] = images[k].h;
-    if (!rc && prefilter) {  // DenseStereo.BoxFilter3 on the device
+    if (!rc && (flags & LUX_LAYER_PREFILTER)) {  // DenseStereo.BoxFilter3 on the device
       uint8_t* f = nullptr;
       rc = alloc_t(ctx, imgs, (size_t)iw[k] * ih[k] * 4, &f);
       if (!rc) launch_box_filter3(dimg[k], iw[k], ih[k], iw[k], f, ctx->stream);
@@ -454,7 +488,7 @@ int lux_sgm_layer(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images,
     }
   }
   if (!rc) rc = build_layer(ctx, n_cams, dimg.data(), iw.data(), ih.data(), gray, calibs, near_, far_, *params, index, align, prev,
-                            keep_pass1, L);
+                            flags, L);
   dev_free_all(ctx, imgs);
   if (rc) {
     destroy_layer(L);
@@ -465,7 +499,7 @@ int lux_sgm_layer(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images,
 }
 
 int lux_sgm_pyramid(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
-                    float near_, float far_, int32_t keep_pass1, lux_layer* out[6]) {
+                    float near_, float far_, int32_t flags, lux_layer* out[6]) {
   if (!ctx || !images || !calibs || !out || n_cams <= 0) return LUX_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   cudaSetDevice(ctx->device);
@@ -536,7 +570,7 @@ int lux_sgm_pyramid(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* image
       }
     }
     lux_layer* L = new lux_layer();
-    rc = build_layer(ctx, n_cams, filt.data(), iw.data(), ih.data(), gray, calibs, near_, far_, pars[i], i, align, prev, keep_pass1, L);
+    rc = build_layer(ctx, n_cams, filt.data(), iw.data(), ih.data(), gray, calibs, near_, far_, pars[i], i, align, prev, flags & ~LUX_LAYER_PREFILTER, L);
     if (rc) {
       destroy_layer(L);
       break;
@@ -573,7 +607,7 @@ static const void* field_ptr(const lux_layer* L, int32_t field, size_t* bytes) {
     case LUX_FIELD_COUNT: *bytes = npx * 2; return L->count;
     case LUX_FIELD_CAP: *bytes = npx * 2; return L->cap;
     case LUX_FIELD_OFFSETS: *bytes = (npx + 1) * 8; return L->off;
-    case LUX_FIELD_AGG: *bytes = L->volume * 2; return L->agg;
+    case LUX_FIELD_AGG: *bytes = L->volume * 2; return L->agg_final ? L->agg : nullptr;
     case LUX_FIELD_AGG_PASS1: *bytes = L->volume * 2; return L->agg_pass1;
     case LUX_FIELD_RAW: *bytes = L->volume; return L->raw;
     case LUX_FIELD_GUIDANCE: *bytes = npx * 4; return L->guidance;
@@ -632,7 +666,7 @@ int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int3
     else if (!(rc = alloc_t(ctx, tmp, npp, &dprev)))
       if (cudaMemcpyAsync(dprev, prev_depth, npp * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) rc = LUX_ERR_CUDA;
   }
-  if (!rc) rc = alloc_t(ctx, tmp, npp, &g2);
+  if (!rc) rc = alloc_t(ctx, tmp, npp * 4, &g2);  // RGBA8 at the previous layer's size
   if (!rc) rc = alloc_t(ctx, tmp, npo, &dout);
   const bool conf = prev_conf && out_conf;
   if (!rc && conf) {

@@ -1,6 +1,620 @@
-// Fast aggregation of a uniform layer: placeholder until the band kernel lands; the emulator covers every layer.
+// Fast aggregation of a uniform layer (every pixel searches planes [0, n), the first layer of a pyramid and every
+// plain pair): bit-exact with the reference's traversal (DenseStereoSgm.cs:181-324) through revisit_schedule.h.
+//
+// Shape: a CTA owns R consecutive rows of a pass (mirrored coordinates in pass -1), one warp per row, and walks the
+// row in lockstep: at step s warp w handles pixel x = s - 2w, so the row above always finished x+1 one step earlier.
+// All four paths of a pixel are fused, so each pass reads the raw volume once and touches the aggregates once:
+//   pass +1: agg = Σ paths;  pass -1: agg += Σ paths, then WTA (and the aggregates are stored only when kept).
+// A lane owns LPT consecutive planes as LPT/2 packed u16 pairs: min.u16x2 for the four-way minimum, byte permutes for
+// the d±1 neighbours, one shuffle per side across lanes, and redux.sync for the running minimum. The row above hands
+// paths 1-3 over through a 4-slot shared-memory ring; the first warp of a CTA reads the CTA above's last row from a
+// global band buffer, gated by that CTA's progress counter (bounded waits, tickets taken in order).
+//
+// Exactness without saturation: with P2 <= p2base <= 1744 every stored L is at most 255 + 1744 < 2000 (the value of a
+// never-written word), the running minimum is at most 2000, and every candidate of the four-way minimum is at least
+// the previous minimum, so raw + m - minPrev never leaves [0, 65535] and 16 path contributions never exceed 65535.
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
 #include "internal.h"
+#include "revisit_schedule.h"
+
 namespace lux {
-size_t uniform_supported_planes() { return 0; }
-bool uniform_fast_supported(int, int, int, int) { return false; }
+
+constexpr int kRows = 8;       // rows (warps) per CTA
+constexpr int kBandBufs = 4;   // band buffers in rotation
+constexpr uint32_t kInit2 = 0x07d007d0u;  // 2000 | 2000
+
+LUX_DEV uint32_t vmin2(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("min.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+LUX_DEV uint32_t pair_of(uint32_t lo_src_hi, uint32_t hi_src_lo) { return __byte_perm(lo_src_hi, hi_src_lo, 0x5432); }
+LUX_DEV uint32_t dup16(uint32_t v) { return __byte_perm(v, 0, 0x1010); }
+
+struct UniArgs {
+  int W, H, n, T, dir, nCB;
+  const uint8_t* raw;
+  uint16_t* agg;
+  float* depth;
+  const float* planes;
+  const uchar4* guidance;
+  int p1;
+  float p2base;
+  float gw[4];
+  uint16_t* bnd;      // [kBandBufs][W][3][Dp]
+  uint16_t* bnd_min;  // [kBandBufs][W][3]
+  int* progress;      // [nCB]
+  int* ticket;
+  uint16_t* edge;     // [W][3][Dp] pass +1's final half-0 row, unmirrored x (paths 1, 2, 3)
+  uint16_t* edge_min; // [W][3]
+  int y_b;            // its row, -1 = none
+  int edge_write, edge_read;
+  uint16_t* cs;       // [H][5][Dp] column states (rows of the pass)
+  uint16_t* cs_min;   // [H][5]
+  const int* flags;
+  const int* batch_first;
+  const int* batch_count;
+  const int* src0;
+  const int* src1;
+  const int* src2;
+  const int* extra;
+  int end_first, end_count;
+  int keep_agg, wta;
+  int* err;
+  unsigned long long timeout_ns;
+};
+
+template <int LPT>
+struct V {
+  uint32_t r[LPT / 2];
+};
+
+template <int LPT>
+LUX_DEV void vload(V<LPT>& v, const uint16_t* p, int lane) {
+  const uint32_t* q = reinterpret_cast<const uint32_t*>(p + lane * LPT);
+  if constexpr (LPT == 8) {
+    uint4 t = __ldcg(reinterpret_cast<const uint4*>(q));
+    v.r[0] = t.x; v.r[1] = t.y; v.r[2] = t.z; v.r[3] = t.w;
+  } else if constexpr (LPT == 4) {
+    uint2 t = __ldcg(reinterpret_cast<const uint2*>(q));
+    v.r[0] = t.x; v.r[1] = t.y;
+  } else {
+    v.r[0] = __ldcg(q);
+  }
+}
+template <int LPT>
+LUX_DEV void vstore(const V<LPT>& v, uint16_t* p, int lane) {
+  uint32_t* q = reinterpret_cast<uint32_t*>(p + lane * LPT);
+  if constexpr (LPT == 8) __stcg(reinterpret_cast<uint4*>(q), make_uint4(v.r[0], v.r[1], v.r[2], v.r[3]));
+  else if constexpr (LPT == 4) __stcg(reinterpret_cast<uint2*>(q), make_uint2(v.r[0], v.r[1]));
+  else __stcg(q, v.r[0]);
+}
+template <int LPT>
+LUX_DEV void vload_s(V<LPT>& v, const uint16_t* p, int lane) {  // shared memory
+  const uint32_t* q = reinterpret_cast<const uint32_t*>(p + lane * LPT);
+#pragma unroll
+  for (int i = 0; i < LPT / 2; i++) v.r[i] = q[i];
+}
+template <int LPT>
+LUX_DEV void vstore_s(const V<LPT>& v, uint16_t* p, int lane) {
+  uint32_t* q = reinterpret_cast<uint32_t*>(p + lane * LPT);
+#pragma unroll
+  for (int i = 0; i < LPT / 2; i++) q[i] = v.r[i];
+}
+template <int LPT>
+LUX_DEV void vinit(V<LPT>& v) {
+#pragma unroll
+  for (int i = 0; i < LPT / 2; i++) v.r[i] = kInit2;
+}
+
+// One path step (DenseStereoSgm.cs:276-313) for a lane's planes. nb: the neighbour's L (2000 past the plane range),
+// mp: its minimum, p2p: min(P2 + mp, 65535). Returns the new L; adds lc to acc; folds lc into rmin.
+template <int LPT>
+LUX_DEV void path_step(const V<LPT>& nb, uint32_t mp, uint32_t p2p, uint32_t p1x2, const V<LPT>& raw2, bool active, int lane,
+                       V<LPT>& out, V<LPT>& acc, uint32_t& rmin) {
+  constexpr int NR = LPT / 2;
+  uint32_t prev = __shfl_up_sync(0xffffffffu, nb.r[NR - 1], 1);
+  uint32_t next = __shfl_down_sync(0xffffffffu, nb.r[0], 1);
+  if (lane == 0) prev = kInit2;    // plane -1: the word before the block holds 2000
+  if (lane == 31) next = kInit2;   // plane n (or a padding lane): 2000
+  const uint32_t mp2 = dup16(mp), p2x2 = dup16(p2p);
+  uint32_t lm[NR + 1];
+  lm[0] = pair_of(prev, nb.r[0]);
+#pragma unroll
+  for (int i = 1; i < NR; i++) lm[i] = pair_of(nb.r[i - 1], nb.r[i]);
+  lm[NR] = pair_of(nb.r[NR - 1], next);
+#pragma unroll
+  for (int i = 0; i < NR; i++) {
+    uint32_t t = vmin2(lm[i], lm[i + 1]) + p1x2;       // min(L[d-1], L[d+1]) + P1
+    t = vmin2(vmin2(t, nb.r[i]), p2x2);                 // with L[d] and P2 + minPrev
+    uint32_t lc = t + raw2.r[i] - mp2;                   // raw + m - minPrev, each half in [0, 2000)
+    lc = active ? lc : kInit2;                           // padding lanes keep 2000
+    out.r[i] = lc;
+    rmin = vmin2(rmin, lc);
+    acc.r[i] += lc;
+  }
+}
+
+template <int LPT>
+LUX_DEV uint32_t warp_min(uint32_t rmin) {  // min over both halves and all lanes
+  uint32_t m = min(rmin & 0xffffu, rmin >> 16);
+  return __reduce_min_sync(0xffffffffu, m);
+}
+
+LUX_DEV float4 pix_of(const UniArgs& a, int xm, int ym) {  // guidance at a pixel given in pass coordinates
+  const int x = a.dir > 0 ? xm : a.W - 1 - xm, y = a.dir > 0 ? ym : a.H - 1 - ym;
+  const uchar4 g = __ldg(a.guidance + (size_t)y * a.W + x);
+  return make_float4(g.x, g.y, g.z, g.w);
+}
+LUX_DEV float4 pix_edge(const UniArgs& a, int xu) {  // guidance of pass +1's row y_b at unmirrored x
+  const uchar4 g = __ldg(a.guidance + (size_t)a.y_b * a.W + xu);
+  return make_float4(g.x, g.y, g.z, g.w);
+}
+LUX_DEV int p2_of(const UniArgs& a, float4 g, float4 n) {
+  const float gg[4] = {g.x, g.y, g.z, g.w}, nn[4] = {n.x, n.y, n.z, n.w};
+  return sgm_p2(gg, nn, a.gw, a.p2base);
+}
+
+// A neighbour state: L vector, minimum and guidance.
+template <int LPT>
+struct Src {
+  V<LPT> L;
+  uint32_t mn;
+  float4 pix;
+};
+
+template <int LPT>
+LUX_DEV float4 pick_pix(const Src<LPT> (&s)[4], int lane) {  // lanes 0..3 take their path's neighbour guidance
+  return lane == 0 ? s[0].pix : lane == 1 ? s[1].pix : lane == 2 ? s[2].pix : s[3].pix;
+}
+
+template <int LPT>
+LUX_DEV void src_init(Src<LPT>& s) {
+  vinit(s.L);
+  s.mn = 2000;
+  s.pix = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+__host__ __device__ constexpr int Dp_of(int LPT) { return 32 * LPT; }
+
+// The edge state (pass +1's final line buffer at row y_b) of path p (1..3) at unmirrored x.
+template <int LPT>
+LUX_DEV void src_edge(const UniArgs& a, Src<LPT>& s, int xu, int p, int lane) {
+  if (a.y_b < 0 || xu < 0 || xu >= a.W) { src_init(s); return; }
+  constexpr int Dp = Dp_of(LPT);
+  vload<LPT>(s.L, a.edge + ((size_t)xu * 3 + (p - 1)) * Dp, lane);
+  s.mn = __ldcg(a.edge_min + (size_t)xu * 3 + (p - 1));
+  s.pix = pix_edge(a, xu);
+}
+// A column state of the revisit machinery.
+template <int LPT>
+LUX_DEV void src_cs(const UniArgs& a, Src<LPT>& s, int row, int slot, int xm, int lane) {
+  constexpr int Dp = Dp_of(LPT);
+  vload<LPT>(s.L, a.cs + ((size_t)row * 5 + slot) * Dp, lane);
+  s.mn = __ldcg(a.cs_min + (size_t)row * 5 + slot);
+  s.pix = pix_of(a, xm, row);
+}
+template <int LPT>
+LUX_DEV void cs_put(const UniArgs& a, const V<LPT>& L, uint32_t mn, int row, int slot, int lane) {
+  constexpr int Dp = Dp_of(LPT);
+  vstore<LPT>(L, a.cs + ((size_t)row * 5 + slot) * Dp, lane);
+  if (lane == 0) __stcg(a.cs_min + (size_t)row * 5 + slot, (uint16_t)mn);
+}
+
+template <int LPT>
+LUX_DEV void load_raw(const UniArgs& a, int xm, int ym, V<LPT>& raw2, bool active, int lane) {
+  const int x = a.dir > 0 ? xm : a.W - 1 - xm, y = a.dir > 0 ? ym : a.H - 1 - ym;
+  const uint8_t* p = a.raw + ((size_t)y * a.W + x) * a.n + lane * LPT;
+  if (!active) {
+#pragma unroll
+    for (int i = 0; i < LPT / 2; i++) raw2.r[i] = 0;
+    return;
+  }
+  if constexpr (LPT == 8) {
+    uint2 b = __ldcs(reinterpret_cast<const uint2*>(p));
+    raw2.r[0] = __byte_perm(b.x, 0, 0x4140); raw2.r[1] = __byte_perm(b.x, 0, 0x4342);
+    raw2.r[2] = __byte_perm(b.y, 0, 0x4140); raw2.r[3] = __byte_perm(b.y, 0, 0x4342);
+  } else if constexpr (LPT == 4) {
+    uint32_t b = __ldcs(reinterpret_cast<const unsigned int*>(p));
+    raw2.r[0] = __byte_perm(b, 0, 0x4140); raw2.r[1] = __byte_perm(b, 0, 0x4342);
+  } else {
+    uint32_t b = __ldcs(reinterpret_cast<const unsigned short*>(p));
+    raw2.r[0] = __byte_perm(b, 0, 0x4140);
+  }
+}
+
+template <int LPT>
+LUX_DEV uint16_t* agg_ptr(const UniArgs& a, int xm, int ym, int lane) {
+  const int x = a.dir > 0 ? xm : a.W - 1 - xm, y = a.dir > 0 ? ym : a.H - 1 - ym;
+  return a.agg + ((size_t)y * a.W + x) * a.n + lane * LPT;
+}
+template <int LPT>
+LUX_DEV void agg_load(const uint16_t* p, V<LPT>& v, bool active) {
+  if (!active) {
+#pragma unroll
+    for (int i = 0; i < LPT / 2; i++) v.r[i] = 0;
+    return;
+  }
+  if constexpr (LPT == 8) {
+    uint4 t = __ldcs(reinterpret_cast<const uint4*>(p));
+    v.r[0] = t.x; v.r[1] = t.y; v.r[2] = t.z; v.r[3] = t.w;
+  } else if constexpr (LPT == 4) {
+    uint2 t = __ldcs(reinterpret_cast<const uint2*>(p));
+    v.r[0] = t.x; v.r[1] = t.y;
+  } else {
+    v.r[0] = __ldcs(reinterpret_cast<const unsigned int*>(p));
+  }
+}
+template <int LPT>
+LUX_DEV void agg_store(uint16_t* p, const V<LPT>& v, bool active) {
+  if (!active) return;
+  if constexpr (LPT == 8) __stcs(reinterpret_cast<uint4*>(p), make_uint4(v.r[0], v.r[1], v.r[2], v.r[3]));
+  else if constexpr (LPT == 4) __stcs(reinterpret_cast<uint2*>(p), make_uint2(v.r[0], v.r[1]));
+  else __stcs(reinterpret_cast<unsigned int*>(p), v.r[0]);
+}
+
+// First minimum of the lane's planes, then over the warp (DenseStereoSgm.cs:228-230): key = value·4096 + plane.
+template <int LPT>
+LUX_DEV int wta_arg(const V<LPT>& agg, bool active, int lane) {
+  uint32_t best = 0xffffu, arg = 0xfffu;
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < LPT / 2; i++) {
+      uint32_t lo = agg.r[i] & 0xffffu, hi = agg.r[i] >> 16;
+      if (lo < best) { best = lo; arg = lane * LPT + 2 * i; }
+      if (hi < best) { best = hi; arg = lane * LPT + 2 * i + 1; }
+    }
+  }
+  uint32_t key = __reduce_min_sync(0xffffffffu, (best << 12) | arg);
+  return key >= (0xffffu << 12) ? 0 : (int)(key & 0xfffu);
+}
+
+// A revisit R(c, y) (DenseStereoSgm.cs:234-317 replayed at the last column), run by one warp.
+template <int LPT>
+LUX_DEV void run_revisit(const UniArgs& a, int y, int lane, bool active) {
+  const int c = a.W - 1;
+  Src<LPT> s[4];
+  const int e[3] = {a.src0[y], a.src1[y], a.src2[y]};
+  const int xsrc[3] = {c - 1, c - 1, c};
+#pragma unroll
+  for (int p = 0; p < 3; p++) {
+    const int kind = src_kind(e[p]), row = src_row(e[p]);
+    if (kind == kSrcInit) src_init(s[p]);
+    else if (kind == kSrcEdge) src_edge<LPT>(a, s[p], a.dir > 0 ? xsrc[p] : a.W - 1 - xsrc[p], p, lane);
+    else src_cs<LPT>(a, s[p], row, kind - kSrcCs, xsrc[p], lane);
+  }
+  src_init(s[3]);
+  const float4 g = pix_of(a, c, y);
+  int p2 = 0;
+  if (lane < 4) p2 = p2_of(a, g, pick_pix<LPT>(s, lane));
+  V<LPT> raw2, acc, out[4];
+  load_raw<LPT>(a, c, y, raw2, active, lane);
+#pragma unroll
+  for (int i = 0; i < LPT / 2; i++) acc.r[i] = 0;
+  const uint32_t p1x2 = dup16((uint32_t)a.p1);
+  uint32_t mins[4];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    const int P2 = __shfl_sync(0xffffffffu, p2, p);
+    const uint32_t p2p = (uint32_t)min(P2 + (int)s[p].mn, 65535);
+    uint32_t rmin = 0xffffffffu;
+    path_step<LPT>(s[p].L, s[p].mn, p2p, p1x2, raw2, active, lane, out[p], acc, rmin);
+    mins[p] = warp_min<LPT>(rmin);
+  }
+  uint16_t* ap = agg_ptr<LPT>(a, c, y, lane);  // the revisit adds its four paths once more (:311)
+  V<LPT> old;
+  agg_load<LPT>(ap, old, active);
+#pragma unroll
+  for (int i = 0; i < LPT / 2; i++) old.r[i] += acc.r[i];
+  agg_store<LPT>(ap, old, active);
+  cs_put<LPT>(a, out[1], mins[1], y, 3, lane);
+  cs_put<LPT>(a, out[2], mins[2], y, 4, lane);
+  if (a.edge_write && (a.extra[y] & 1)) {  // R(y_b) is what pass -1 will read at the last column
+    constexpr int Dp = Dp_of(LPT);
+    vstore<LPT>(out[1], a.edge + ((size_t)c * 3 + 0) * Dp, lane);
+    vstore<LPT>(out[2], a.edge + ((size_t)c * 3 + 1) * Dp, lane);
+    if (lane == 0) {
+      __stcg(a.edge_min + (size_t)c * 3 + 0, (uint16_t)mins[1]);
+      __stcg(a.edge_min + (size_t)c * 3 + 1, (uint16_t)mins[2]);
+    }
+  }
+  __syncwarp();
+}
+
+template <int LPT>
+constexpr size_t ring_bytes() {
+  return (size_t)kRows * 4 * 3 * Dp_of(LPT) * 2 + (size_t)kRows * 4 * 3 * 2;
+}
+
+template <int LPT>
+__global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
+  constexpr int NR = LPT / 2, Dp = Dp_of(LPT);
+  extern __shared__ __align__(16) uint16_t smem_ring[];
+  // ring[w][slot][path][Dp]: row w's paths 1..3 at pixel x with slot x & 3, read by row w + 1
+  auto ring = [&](int w_, int slot, int p) { return smem_ring + (((size_t)w_ * 4 + slot) * 3 + p) * Dp; };
+  uint16_t* ring_min = smem_ring + (size_t)kRows * 4 * 3 * Dp;
+  auto rmin_at = [&](int w_, int slot, int p) -> uint16_t& { return ring_min[((size_t)w_ * 4 + slot) * 3 + p]; };
+  __shared__ int s_cb, s_stop;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid == 0) {
+    s_cb = atomicAdd(a.ticket, 1);
+    s_stop = 0;
+  }
+  __syncthreads();
+  const int cb = s_cb;
+  const int y = cb * kRows + w;  // row of the pass
+  const bool row_ok = y < a.H;
+  const bool active = lane * LPT < a.n;
+  const int c = a.W - 1;
+  const uint32_t p1x2 = dup16((uint32_t)a.p1);
+  uint16_t* bnd_up = a.bnd + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3 * Dp;
+  uint16_t* bnd_up_min = a.bnd_min + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3;
+  uint16_t* bnd_me = a.bnd + (size_t)(cb % kBandBufs) * a.W * 3 * Dp;
+  uint16_t* bnd_me_min = a.bnd_min + (size_t)(cb % kBandBufs) * a.W * 3;
+  int seen = 0;  // progress of the CTA above, as last read
+  V<LPT> L0;     // path 0 state (the pixel to the left)
+  uint32_t m0 = 2000;
+  vinit(L0);
+  float4 g_left = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int flags = row_ok ? a.flags[y] : 0;
+  const int nsteps = a.W + 2 * (kRows - 1);
+  for (int s = 0; s < nsteps; s++) {
+    const int x = s - 2 * w;
+    if (row_ok && x >= 0 && x < a.W) {
+      // ---- the row above: paths 1, 2, 3 read pixels x-1, x, x+1 of row y-1 ----
+      if (w == 0 && cb > 0) {
+        const int need = min(a.W, x + 2);
+        if (seen < need) {
+          if (lane == 0) {
+            if (!wait_at_least(a.progress + (cb - 1), need, a.err, 11, a.timeout_ns)) s_stop = 1;
+            seen = ld_acquire(a.progress + (cb - 1));
+          }
+          seen = __shfl_sync(0xffffffffu, seen, 0);
+          __syncwarp();
+        }
+      }
+      // ---- revisits that the reference runs before this visit (they may produce this visit's path-2 input) ----
+      if (x == c) {
+        const int cnt = a.batch_count[y], first = a.batch_first[y];
+        for (int k = 0; k < cnt; k++) run_revisit<LPT>(a, first + k, lane, active);
+      }
+      Src<LPT> nb[4];
+      nb[0].L = L0;
+      nb[0].mn = m0;
+      nb[0].pix = g_left;
+#pragma unroll
+      for (int p = 1; p < 4; p++) {
+        const int xn = x + (p == 1 ? -1 : p == 2 ? 0 : 1);
+        if (xn < 0 || xn >= a.W) { src_init(nb[p]); continue; }
+        if (w > 0) {
+          vload_s<LPT>(nb[p].L, ring(w - 1, xn & 3, p - 1), lane);
+          nb[p].mn = rmin_at(w - 1, xn & 3, p - 1);
+          nb[p].pix = pix_of(a, xn, y - 1);
+        } else if (cb > 0) {
+          vload<LPT>(nb[p].L, bnd_up + ((size_t)xn * 3 + (p - 1)) * Dp, lane);
+          nb[p].mn = __ldcg(bnd_up_min + (size_t)xn * 3 + (p - 1));
+          nb[p].pix = pix_of(a, xn, y - 1);
+        } else if (a.edge_read) {
+          src_edge<LPT>(a, nb[p], a.dir > 0 ? xn : a.W - 1 - xn, p, lane);
+        } else {
+          src_init(nb[p]);
+        }
+      }
+      if (x == c && (flags & 1)) src_cs<LPT>(a, nb[2], y - 1, 4, c, lane);  // N(c).p2 reads R(c, y-1)
+      // ---- the four paths ----
+      const float4 g = pix_of(a, x, y);
+      int p2 = 0;
+      if (lane < 4) p2 = p2_of(a, g, pick_pix<LPT>(nb, lane));
+      V<LPT> raw2, acc, out[4];
+      load_raw<LPT>(a, x, y, raw2, active, lane);
+      uint16_t* ap = agg_ptr<LPT>(a, x, y, lane);
+      if (a.dir > 0) {
+#pragma unroll
+        for (int i = 0; i < NR; i++) acc.r[i] = 0;
+      } else {
+        agg_load<LPT>(ap, acc, active);
+      }
+      uint32_t mins[4];
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        const int P2 = __shfl_sync(0xffffffffu, p2, p);
+        const uint32_t p2p = (uint32_t)min(P2 + (int)nb[p].mn, 65535);
+        uint32_t rmin = 0xffffffffu;
+        path_step<LPT>(nb[p].L, nb[p].mn, p2p, p1x2, raw2, active, lane, out[p], acc, rmin);
+        mins[p] = warp_min<LPT>(rmin);
+      }
+      if (a.dir > 0 || a.keep_agg || x == c) agg_store<LPT>(ap, acc, active);
+      if (a.wta && x != c) {
+        const int arg = wta_arg<LPT>(acc, active, lane);
+        if (lane == 0) a.depth[(size_t)(a.H - 1 - y) * a.W + (a.W - 1 - x)] = __ldg(a.planes + arg);
+      }
+      // ---- hand-over ----
+      L0 = out[0];
+      m0 = mins[0];
+      g_left = g;
+      if (w < kRows - 1) {
+#pragma unroll
+        for (int p = 1; p < 4; p++) {
+          vstore_s<LPT>(out[p], ring(w, x & 3, p - 1), lane);
+          if (lane == 0) rmin_at(w, x & 3, p - 1) = (uint16_t)mins[p];
+        }
+      } else {
+#pragma unroll
+        for (int p = 1; p < 4; p++) {
+          vstore<LPT>(out[p], bnd_me + ((size_t)x * 3 + (p - 1)) * Dp, lane);
+          if (lane == 0) __stcg(bnd_me_min + (size_t)x * 3 + (p - 1), (uint16_t)mins[p]);
+        }
+      }
+      if (x == c - 1) {
+        cs_put<LPT>(a, out[0], mins[0], y, 0, lane);
+        cs_put<LPT>(a, out[1], mins[1], y, 1, lane);
+      }
+      if (x == c) cs_put<LPT>(a, out[2], mins[2], y, 2, lane);
+      if (a.edge_write && y == a.y_b) {
+#pragma unroll
+        for (int p = 1; p < 4; p++) {
+          vstore<LPT>(out[p], a.edge + ((size_t)x * 3 + (p - 1)) * Dp, lane);
+          if (lane == 0) __stcg(a.edge_min + (size_t)x * 3 + (p - 1), (uint16_t)mins[p]);
+        }
+      }
+      if (x == c && y == a.H - 1) {  // the last band's revisits when no later visit of the column follows them
+        for (int k = 0; k < a.end_count; k++) run_revisit<LPT>(a, a.end_first + k, lane, active);
+      }
+    }
+    // ---- publish the last row's progress to the CTA below (every 8 pixels and at the end) ----
+    if (w == kRows - 1) {
+      const int x = s - 2 * w;
+      const bool last_row_ok = row_ok || y >= a.H;
+      if (last_row_ok && x >= 0 && x < a.W && (((x & 7) == 7) || x == a.W - 1)) {
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) st_release(a.progress + cb, x + 1);
+      }
+    }
+    __syncthreads();
+    if (s_stop) break;
+  }
+  // rows past the image end still publish completion
+  if (tid == 0) {
+    __threadfence();
+    st_release(a.progress + cb, a.W);
+  }
+}
+
+// WTA of the last column of pass -1 (its aggregates are final only after the revisits).
+__global__ void k_wta_column(const uint16_t* __restrict__ agg, int W, int H, int n, int col, const float* __restrict__ planes,
+                             float* __restrict__ depth) {
+  const int y = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (y >= H) return;
+  const uint16_t* p = agg + ((size_t)y * W + col) * n;
+  int best = 0xffff, arg = 0x7fffffff;
+  for (int k = lane; k < n; k += 32) {
+    int v = p[k];
+    if (v < best) { best = v; arg = k; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    int ob = __shfl_xor_sync(0xffffffffu, best, o), oa = __shfl_xor_sync(0xffffffffu, arg, o);
+    if (ob < best || (ob == best && oa < arg)) { best = ob; arg = oa; }
+  }
+  if (lane == 0) depth[(size_t)y * W + col] = planes[arg == 0x7fffffff ? 0 : arg];
+}
+
+size_t uniform_supported_planes() { return 256; }
+
+static int lpt_for(int n) { return n <= 64 ? 2 : n <= 128 ? 4 : 8; }
+
+bool uniform_fast_supported(int W, int H, int n, int tile, uint16_t p1, float p2scale) {
+  if (n <= 0 || n > 256 || (n & 7) != 0) return false;
+  if ((tile & 1) != 0 || tile < 2) return false;  // a row's half of the line buffer is its parity only for even tiles
+  if (W < 3 || H < 2) return false;
+  volatile float p1f = (float)p1;
+  const float p2base = p1f * p2scale;
+  if (!(p2scale >= 0.0f) || !(p2base <= 1744.0f) || p1 > 60000) return false;  // the no-saturation bound above
+  return true;
+}
+
+struct UniScratchLayout {
+  size_t bnd, bnd_min, progress, edge, edge_min, cs, cs_min, sched, total;
+};
+
+static UniScratchLayout layout_of(int W, int H, int n) {
+  const size_t Dp = 32 * (size_t)lpt_for(n);
+  const int nCB = (H + kRows - 1) / kRows;
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  UniScratchLayout L;
+  size_t o = 0;
+  L.bnd = o; o += al((size_t)kBandBufs * W * 3 * Dp * 2);
+  L.bnd_min = o; o += al((size_t)kBandBufs * W * 3 * 2);
+  L.progress = o; o += al((size_t)(nCB + 2) * 4 * 2);
+  L.edge = o; o += al((size_t)W * 3 * Dp * 2);
+  L.edge_min = o; o += al((size_t)W * 3 * 2);
+  L.cs = o; o += al((size_t)H * 5 * Dp * 2);
+  L.cs_min = o; o += al((size_t)H * 5 * 2);
+  L.sched = o; o += al((size_t)2 * 7 * H * 4);
+  L.total = o;
+  return L;
+}
+
+size_t uniform_scratch_bytes(int W, int H, int n, int tile) {
+  (void)tile;
+  return layout_of(W, H, n).total;
+}
+
+template <int LPT>
+static void launch_pass(const UniArgs& a, cudaStream_t s) {
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_sgm_uniform<LPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring_bytes<LPT>());
+    configured = true;
+  }
+  k_sgm_uniform<LPT><<<a.nCB, kRows * 32, ring_bytes<LPT>(), s>>>(a);
+  count_launches(1);
+}
+
+int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
+                    uint16_t* agg_pass1, float* depth, int keep_agg, void* scratch, size_t scratch_bytes, int* err,
+                    cudaStream_t s) {
+  if (xsw) return 12;  // LUX_SGM_XSW changes the traversal; the replay kernel covers it
+  const int W = g.W, H = g.H, n = g.n_planes, T = g.tile;
+  const UniScratchLayout L = layout_of(W, H, n);
+  if (scratch_bytes < L.total) return 9;
+  char* base = static_cast<char*>(scratch);
+  // host schedules of both passes, uploaded together
+  RevisitSchedule sch[2];
+  std::vector<int> host((size_t)2 * 7 * H);
+  for (int pass = 0; pass < 2; pass++) {
+    build_revisit_schedule(W, H, T, pass == 1, sch[pass]);
+    int* h = host.data() + (size_t)pass * 7 * H;
+    const std::vector<int>* cols[7] = {&sch[pass].flags, &sch[pass].batch_first, &sch[pass].batch_count, &sch[pass].src0,
+                                       &sch[pass].src1, &sch[pass].src2, &sch[pass].extra};
+    for (int k = 0; k < 7; k++) std::memcpy(h + (size_t)k * H, cols[k]->data(), (size_t)H * 4);
+  }
+  int* dsched = reinterpret_cast<int*>(base + L.sched);
+  if (cudaMemcpyAsync(dsched, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return 10;
+  const int nCB = (H + kRows - 1) / kRows;
+  int* progress = reinterpret_cast<int*>(base + L.progress);
+  cudaMemsetAsync(progress, 0, (size_t)(nCB + 2) * 4 * 2, s);
+  UniArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.W = W; a.H = H; a.n = n; a.T = T; a.nCB = nCB;
+  a.raw = raw; a.agg = agg; a.depth = depth; a.planes = g.planes; a.guidance = g.guidance;
+  a.p1 = p1;
+  volatile float p1f = (float)p1;
+  a.p2base = p1f * p2scale;
+  for (int i = 0; i < 4; i++) a.gw[i] = gw[i];
+  a.bnd = reinterpret_cast<uint16_t*>(base + L.bnd);
+  a.bnd_min = reinterpret_cast<uint16_t*>(base + L.bnd_min);
+  a.edge = reinterpret_cast<uint16_t*>(base + L.edge);
+  a.edge_min = reinterpret_cast<uint16_t*>(base + L.edge_min);
+  a.cs = reinterpret_cast<uint16_t*>(base + L.cs);
+  a.cs_min = reinterpret_cast<uint16_t*>(base + L.cs_min);
+  a.y_b = sch[0].y_b;
+  a.err = err;
+  a.timeout_ns = kTimeoutNs;
+  a.keep_agg = keep_agg;
+  const int lpt = lpt_for(n);
+  for (int pass = 0; pass < 2; pass++) {
+    const int* h = dsched + (size_t)pass * 7 * H;
+    a.flags = h; a.batch_first = h + H; a.batch_count = h + 2 * H; a.src0 = h + 3 * H; a.src1 = h + 4 * H; a.src2 = h + 5 * H;
+    a.extra = h + 6 * H;
+    a.end_first = sch[pass].end_first;
+    a.end_count = sch[pass].end_count;
+    a.dir = pass == 0 ? 1 : -1;
+    a.progress = progress + (size_t)pass * (nCB + 2);
+    a.ticket = progress + (size_t)pass * (nCB + 2) + nCB;
+    a.edge_write = pass == 0;
+    a.edge_read = pass == 1;
+    a.wta = pass == 1;
+    if (lpt == 2) launch_pass<2>(a, s);
+    else if (lpt == 4) launch_pass<4>(a, s);
+    else launch_pass<8>(a, s);
+    if (pass == 0 && agg_pass1) cudaMemcpyAsync(agg_pass1, agg, (size_t)W * H * n * 2, cudaMemcpyDeviceToDevice, s);
+  }
+  k_wta_column<<<(H * 32 + 255) / 256, 256, 0, s>>>(agg, W, H, n, 0, g.planes, depth);
+  count_launches(1);
+  return 0;
+}
+
 }  // namespace lux

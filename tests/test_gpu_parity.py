@@ -40,15 +40,40 @@ def _compare_layer(gl, ol, tag):
     assert np.array_equal(gl.Depth.view(np.uint32), ol["Depth"].view(np.uint32)), tag + " depth"
 
 
-@pytest.mark.parametrize("w,h,d,tile", [(48, 40, 16, 8), (65, 49, 16, 4), (160, 120, 32, 16), (257, 93, 64, 64), (100, 77, 24, 8)])
-def test_uniform_layer_bit_exact(ctx, oracle, w, h, d, tile):
+# (W, H, D, T): K = T - ((W-1) mod T) revisit rows per band takes the values 1, T and in between; D covers the 2-, 4- and
+# 8-plane lane widths with and without padding lanes; H covers partial last bands and partial last CTA bands.
+UNIFORM_CASES = [(48, 40, 16, 8), (65, 49, 16, 4), (160, 120, 32, 16), (257, 93, 64, 64), (100, 77, 24, 8), (130, 70, 96, 16),
+                 (200, 35, 136, 8), (71, 66, 256, 64), (33, 17, 40, 2), (64, 9, 192, 32)]
+
+
+@pytest.mark.parametrize("kernel", ["fast", "replay"])
+@pytest.mark.parametrize("w,h,d,tile", UNIFORM_CASES)
+def test_uniform_layer_bit_exact(ctx, oracle, w, h, d, tile, kernel):
     from lux_b200 import api, synth
     wl = synth.rectified_pair(w, h, d, seed=w + h, tile=tile)
     filt = _filtered(oracle, wl.images)
     ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True)
-    gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, ctx=ctx)
+    gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, keep_agg=True,
+                                force_replay=(kernel == "replay"), ctx=ctx)
     try:
-        _compare_layer(gl, ol, f"{w}x{h} D{d} T{tile}")
+        assert gl.sgm_kernel == (1 if kernel == "fast" else 0)
+        _compare_layer(gl, ol, f"{w}x{h} D{d} T{tile} {kernel}")
+    finally:
+        gl.close()
+
+
+def test_uniform_fast_depth_without_kept_aggregates(ctx, oracle):
+    """The production form (no Agg kept, WTA fused into pass -1) gives the same depth."""
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(300, 170, 64, seed=9, tile=64)
+    filt = _filtered(oracle, wl.images)
+    ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params)
+    gl = api.DenseLayer.compute(wl.images, wl.gray, wl.calibs, wl.near, wl.far, wl.params, prefilter=True, ctx=ctx)
+    try:
+        assert gl.sgm_kernel == 1
+        assert np.array_equal(gl.Depth.view(np.uint32), ol["Depth"].view(np.uint32))
+        with pytest.raises(api.LuxError):
+            gl.Agg
     finally:
         gl.close()
 
@@ -60,7 +85,7 @@ def test_multicamera_colour_layer_bit_exact(ctx, oracle):
     filt = _filtered(oracle, cap.images)
     p = api.StereoParams(scale=1, tile=8, skip_mode=0, plane_density=2.0)
     ol = oracle.layer(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True)
-    gl = api.DenseLayer.compute(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True, ctx=ctx)
+    gl = api.DenseLayer.compute(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True, keep_agg=True, ctx=ctx)
     try:
         _compare_layer(gl, ol, "3cam")
     finally:
@@ -72,7 +97,7 @@ def test_pyramid_bit_exact(ctx, oracle):
     from lux_b200 import api, synth
     cap = synth.capture(416, 312, 3, seed=5, f=330.0)
     ol = oracle.pyramid(cap.images, cap.gray, cap.calibs, cap.near, cap.far, keep_pass1=True)
-    gls = api.DenseStereoPyramid.run(cap.images, cap.gray, cap.calibs, cap.near, cap.far, keep_pass1=True, ctx=ctx)
+    gls = api.DenseStereoPyramid.run(cap.images, cap.gray, cap.calibs, cap.near, cap.far, keep_pass1=True, keep_agg=True, ctx=ctx)
     try:
         for i in range(6):
             _compare_layer(gls[i], ol[i], f"L{i}")
