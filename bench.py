@@ -28,7 +28,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-W_, H_, D_, TILE, BITS = 4160, 3120, 256, 64, 12
+WORKLOADS = {  # name: (W, H, D, tile, bits, description)
+    "pair13mp": (4160, 3120, 256, 64, 12, "plain 13 MP pair 4160x3120 u16 12-bit -> u8, D=256, 8 paths, tile 64, P1 1, P2 500 adaptive"),
+    "pair1mp": (1040, 780, 64, 64, 8, "plain pair 1040x780 u8, D=64, 8 paths, tile 64, P1 1, P2 500 adaptive"),
+    "preview": (520, 390, 32, 64, 8, "preview pair 520x390 u8, D=32, 8 paths, tile 64"),
+}
+W_, H_, D_, TILE, BITS, DESC = WORKLOADS["pair13mp"]
 METRIC = "SGM MDE/s (W·H·D per second), 13 MP pair 4160x3120 D=256, bit-exact"
 BYTES_PER_DE_AGG = 8  # raw read x2 (2) + pass-1 agg write (2) + pass-2 agg read (2) + write (2)
 
@@ -41,7 +46,12 @@ def args_():
     p.add_argument("--impl", default="lux", choices=["lux", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-rows", type=int, default=130, help="rows of the CPU sample strip")
-    return p.parse_args()
+    p.add_argument("--workload", default="pair13mp", choices=sorted(WORKLOADS),
+                   help="pair13mp is the benchmark; the smaller pairs are for profiling captures")
+    a = p.parse_args()
+    global W_, H_, D_, TILE, BITS, DESC
+    W_, H_, D_, TILE, BITS, DESC = WORKLOADS[a.workload]
+    return a
 
 
 def peaks():
@@ -135,12 +145,12 @@ def run_reference(a):
         tot_de += de
         tot_t += dt
     value = tot_de / tot_t / 1e6
-    sample = f"{W_}x{a.cpu_rows} row strip of the 4160x3120 D=256 pair per step (oracle port: box filter, cost on {threads} threads, serial SGM, WTA)"
+    sample = f"{W_}x{a.cpu_rows} row strip of the {W_}x{H_} D={D_} pair per step (oracle port: box filter, cost on {threads} threads, serial SGM, WTA)"
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "MDE/s", "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": tot_t / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8/u16", "data": "synthetic",
-        "config": {"workload": "plain 13 MP pair 4160x3120 u16 12-bit, D=256, 8 paths, tile 64", "sample_rows": a.cpu_rows},
+        "config": {"workload": DESC, "sample_rows": a.cpu_rows},
         "cpu_baseline": {"value": value, "unit": "MDE/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "MDE/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -220,7 +230,7 @@ def run_lux(a):
         "metric": METRIC, "value": value, "unit": "MDE/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_v / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8 cost / u16 aggregation", "data": "synthetic (seeded 1/f texture, planar disparity, warped view)",
-        "config": {"workload": "plain 13 MP pair 4160x3120 u16 12-bit -> u8, D=256, 8 paths, tile 64, P1 1, P2 500 adaptive",
+        "config": {"workload": DESC,
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (3.3 GB cost volume, 6.6 GB aggregates)",
                    "stages_ms": {"cost": cost_ms, "sgm_2_passes": sgm_ms, "wta": wta_ms},
                    "sgm_kernel": "uniform-fast" if inf_v and inf_v[0][3] == 1 else "exact-replay"},

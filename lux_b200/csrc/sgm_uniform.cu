@@ -328,6 +328,68 @@ constexpr size_t ring_bytes() {
   return (size_t)kRows * 4 * 3 * Dp_of(LPT) * 2 + (size_t)kRows * 4 * 3 * 2;
 }
 
+// Raw bytes of a lane's planes as loaded (8, 4 or 2 bytes), unpacked to u16 pairs when used.
+template <int LPT>
+struct RawB {
+  uint32_t r[LPT >= 8 ? 2 : 1];
+};
+template <int LPT>
+LUX_DEV void raw_fetch(const UniArgs& a, int xm, int ym, RawB<LPT>& b, bool active, int lane) {
+  const int x = a.dir > 0 ? xm : a.W - 1 - xm, y = a.dir > 0 ? ym : a.H - 1 - ym;
+  const uint8_t* p = a.raw + ((size_t)y * a.W + x) * a.n + lane * LPT;
+  if (!active) { b.r[0] = 0; if constexpr (LPT >= 8) b.r[1] = 0; return; }
+  if constexpr (LPT == 8) {
+    uint2 t = __ldcs(reinterpret_cast<const uint2*>(p));
+    b.r[0] = t.x; b.r[1] = t.y;
+  } else if constexpr (LPT == 4) {
+    b.r[0] = __ldcs(reinterpret_cast<const unsigned int*>(p));
+  } else {
+    b.r[0] = __ldcs(reinterpret_cast<const unsigned short*>(p));
+  }
+}
+template <int LPT>
+LUX_DEV void raw_unpack(const RawB<LPT>& b, V<LPT>& raw2) {
+  raw2.r[0] = __byte_perm(b.r[0], 0, 0x4140);
+  if constexpr (LPT >= 4) raw2.r[1] = __byte_perm(b.r[0], 0, 0x4342);
+  if constexpr (LPT == 8) {
+    raw2.r[2] = __byte_perm(b.r[1], 0, 0x4140);
+    raw2.r[3] = __byte_perm(b.r[1], 0, 0x4342);
+  }
+}
+
+// Guidance of the path-p neighbour of pixel (xq, yq) of the pass: margins and never-written slots give 0; the row above
+// the first row is pass +1's row y_b in pass -1 (its final line buffer) and never written in pass +1.
+LUX_DEV float4 neighbour_pix(const UniArgs& a, int p, int xq, int yq) {
+  const int xn = xq + (p == 0 || p == 1 ? -1 : p == 2 ? 0 : 1);
+  const int yn = p == 0 ? yq : yq - 1;
+  if (xn < 0 || xn >= a.W) return make_float4(0.f, 0.f, 0.f, 0.f);
+  if (yn < 0) {
+    if (!a.edge_read || a.y_b < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
+    return pix_edge(a, a.dir > 0 ? xn : a.W - 1 - xn);
+  }
+  return pix_of(a, xn, yn);
+}
+
+template <int LPT>
+LUX_DEV void up_fetch(const UniArgs& a, const uint16_t* bnd_up, const uint16_t* bnd_up_min, int cb, int xq, Src<LPT> (&u)[3],
+                      int lane) {
+  constexpr int Dp = Dp_of(LPT);
+#pragma unroll
+  for (int p = 1; p < 4; p++) {
+    const int xn = xq + (p == 1 ? -1 : p == 2 ? 0 : 1);
+    Src<LPT>& d = u[p - 1];
+    if (xn < 0 || xn >= a.W) { src_init(d); continue; }
+    if (cb > 0) {
+      vload<LPT>(d.L, bnd_up + ((size_t)xn * 3 + (p - 1)) * Dp, lane);
+      d.mn = __ldcg(bnd_up_min + (size_t)xn * 3 + (p - 1));
+    } else if (a.edge_read) {
+      src_edge<LPT>(a, d, a.dir > 0 ? xn : a.W - 1 - xn, p, lane);
+    } else {
+      src_init(d);
+    }
+  }
+}
+
 template <int LPT>
 __global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
   constexpr int NR = LPT / 2, Dp = Dp_of(LPT);
@@ -349,91 +411,112 @@ __global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
   const bool active = lane * LPT < a.n;
   const int c = a.W - 1;
   const uint32_t p1x2 = dup16((uint32_t)a.p1);
-  uint16_t* bnd_up = a.bnd + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3 * Dp;
-  uint16_t* bnd_up_min = a.bnd_min + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3;
+  const uint16_t* bnd_up = a.bnd + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3 * Dp;
+  const uint16_t* bnd_up_min = a.bnd_min + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3;
   uint16_t* bnd_me = a.bnd + (size_t)(cb % kBandBufs) * a.W * 3 * Dp;
   uint16_t* bnd_me_min = a.bnd_min + (size_t)(cb % kBandBufs) * a.W * 3;
   int seen = 0;  // progress of the CTA above, as last read
-  V<LPT> L0;     // path 0 state (the pixel to the left)
-  uint32_t m0 = 2000;
-  vinit(L0);
-  float4 g_left = make_float4(0.f, 0.f, 0.f, 0.f);
+  Src<LPT> left;  // path 0: the pixel to the left
+  src_init(left);
+  Src<LPT> up[3];  // warp 0: paths 1..3 of the pixel at hand, fetched one step ahead
+  RawB<LPT> raw_q[2];  // raw bytes of x+1, x+2 (a two-deep prefetch)
+  V<LPT> agg_q[2];     // pass -1: pass +1's aggregates of x+1, x+2
+  int p2_cur = 0;      // lanes 0..3: P2 of path `lane` for the pixel at hand
   const int flags = row_ok ? a.flags[y] : 0;
   const int nsteps = a.W + 2 * (kRows - 1);
+  // waits until the CTA above has published `need` pixels of its last row (bounded)
+  auto wait_up = [&](int need) {
+    if (seen < need) {
+      if (lane == 0) {
+        if (!wait_at_least(a.progress + (cb - 1), need, a.err, 11, a.timeout_ns)) s_stop = 1;
+        seen = ld_acquire(a.progress + (cb - 1));
+      }
+      seen = __shfl_sync(0xffffffffu, seen, 0);
+      __syncwarp();
+    }
+  };
   for (int s = 0; s < nsteps; s++) {
     const int x = s - 2 * w;
     if (row_ok && x >= 0 && x < a.W) {
-      // ---- the row above: paths 1, 2, 3 read pixels x-1, x, x+1 of row y-1 ----
-      if (w == 0 && cb > 0) {
-        const int need = min(a.W, x + 2);
-        if (seen < need) {
-          if (lane == 0) {
-            if (!wait_at_least(a.progress + (cb - 1), need, a.err, 11, a.timeout_ns)) s_stop = 1;
-            seen = ld_acquire(a.progress + (cb - 1));
-          }
-          seen = __shfl_sync(0xffffffffu, seen, 0);
-          __syncwarp();
+      if (x == 0) {  // prologue: the row's first pixels
+        raw_fetch<LPT>(a, 0, y, raw_q[0], active, lane);
+        if (a.dir < 0) agg_load<LPT>(agg_ptr<LPT>(a, 0, y, lane), agg_q[0], active);
+        if (a.W > 1) {
+          raw_fetch<LPT>(a, 1, y, raw_q[1], active, lane);
+          if (a.dir < 0) agg_load<LPT>(agg_ptr<LPT>(a, 1, y, lane), agg_q[1], active);
         }
+        if (lane < 4) p2_cur = p2_of(a, pix_of(a, 0, y), neighbour_pix(a, lane, 0, y));
+        if (w == 0) {
+          if (cb > 0) wait_up(min(a.W, 2));
+          up_fetch<LPT>(a, bnd_up, bnd_up_min, cb, 0, up, lane);
+        }
+      }
+      // ---- prefetch for the pixels ahead: raw and aggregates of x+2, the row above of x+1, guidance of x+1 ----
+      RawB<LPT> raw_n;
+      V<LPT> agg_n;
+      const bool have2 = x + 2 < a.W;
+      if (have2) {
+        raw_fetch<LPT>(a, x + 2, y, raw_n, active, lane);
+        if (a.dir < 0) agg_load<LPT>(agg_ptr<LPT>(a, x + 2, y, lane), agg_n, active);
+      }
+      Src<LPT> up_n[3];
+      if (w == 0 && x + 1 < a.W) {
+        if (cb > 0) wait_up(min(a.W, x + 3));
+        up_fetch<LPT>(a, bnd_up, bnd_up_min, cb, x + 1, up_n, lane);
+      }
+      float4 g_n = make_float4(0.f, 0.f, 0.f, 0.f), pn_n = g_n;
+      if (lane < 4 && x + 1 < a.W) {
+        g_n = pix_of(a, x + 1, y);
+        pn_n = neighbour_pix(a, lane, x + 1, y);
       }
       // ---- revisits that the reference runs before this visit (they may produce this visit's path-2 input) ----
       if (x == c) {
         const int cnt = a.batch_count[y], first = a.batch_first[y];
         for (int k = 0; k < cnt; k++) run_revisit<LPT>(a, first + k, lane, active);
       }
+      // ---- neighbour states: paths 1, 2, 3 read pixels x-1, x, x+1 of row y-1 ----
       Src<LPT> nb[4];
-      nb[0].L = L0;
-      nb[0].mn = m0;
-      nb[0].pix = g_left;
+      nb[0] = left;
+      if (w > 0) {
 #pragma unroll
-      for (int p = 1; p < 4; p++) {
-        const int xn = x + (p == 1 ? -1 : p == 2 ? 0 : 1);
-        if (xn < 0 || xn >= a.W) { src_init(nb[p]); continue; }
-        if (w > 0) {
+        for (int p = 1; p < 4; p++) {
+          const int xn = x + (p == 1 ? -1 : p == 2 ? 0 : 1);
+          if (xn < 0 || xn >= a.W) { src_init(nb[p]); continue; }
           vload_s<LPT>(nb[p].L, ring(w - 1, xn & 3, p - 1), lane);
           nb[p].mn = rmin_at(w - 1, xn & 3, p - 1);
-          nb[p].pix = pix_of(a, xn, y - 1);
-        } else if (cb > 0) {
-          vload<LPT>(nb[p].L, bnd_up + ((size_t)xn * 3 + (p - 1)) * Dp, lane);
-          nb[p].mn = __ldcg(bnd_up_min + (size_t)xn * 3 + (p - 1));
-          nb[p].pix = pix_of(a, xn, y - 1);
-        } else if (a.edge_read) {
-          src_edge<LPT>(a, nb[p], a.dir > 0 ? xn : a.W - 1 - xn, p, lane);
-        } else {
-          src_init(nb[p]);
         }
+      } else {
+#pragma unroll
+        for (int p = 1; p < 4; p++) nb[p] = up[p - 1];
       }
       if (x == c && (flags & 1)) src_cs<LPT>(a, nb[2], y - 1, 4, c, lane);  // N(c).p2 reads R(c, y-1)
       // ---- the four paths ----
-      const float4 g = pix_of(a, x, y);
-      int p2 = 0;
-      if (lane < 4) p2 = p2_of(a, g, pick_pix<LPT>(nb, lane));
       V<LPT> raw2, acc, out[4];
-      load_raw<LPT>(a, x, y, raw2, active, lane);
-      uint16_t* ap = agg_ptr<LPT>(a, x, y, lane);
+      raw_unpack<LPT>(raw_q[0], raw2);
       if (a.dir > 0) {
 #pragma unroll
         for (int i = 0; i < NR; i++) acc.r[i] = 0;
       } else {
-        agg_load<LPT>(ap, acc, active);
+        acc = agg_q[0];
       }
       uint32_t mins[4];
 #pragma unroll
       for (int p = 0; p < 4; p++) {
-        const int P2 = __shfl_sync(0xffffffffu, p2, p);
+        const int P2 = __shfl_sync(0xffffffffu, p2_cur, p);
         const uint32_t p2p = (uint32_t)min(P2 + (int)nb[p].mn, 65535);
         uint32_t rmin = 0xffffffffu;
         path_step<LPT>(nb[p].L, nb[p].mn, p2p, p1x2, raw2, active, lane, out[p], acc, rmin);
         mins[p] = warp_min<LPT>(rmin);
       }
+      uint16_t* ap = agg_ptr<LPT>(a, x, y, lane);
       if (a.dir > 0 || a.keep_agg || x == c) agg_store<LPT>(ap, acc, active);
       if (a.wta && x != c) {
         const int arg = wta_arg<LPT>(acc, active, lane);
         if (lane == 0) a.depth[(size_t)(a.H - 1 - y) * a.W + (a.W - 1 - x)] = __ldg(a.planes + arg);
       }
       // ---- hand-over ----
-      L0 = out[0];
-      m0 = mins[0];
-      g_left = g;
+      left.L = out[0];
+      left.mn = mins[0];
       if (w < kRows - 1) {
 #pragma unroll
         for (int p = 1; p < 4; p++) {
@@ -462,12 +545,26 @@ __global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
       if (x == c && y == a.H - 1) {  // the last band's revisits when no later visit of the column follows them
         for (int k = 0; k < a.end_count; k++) run_revisit<LPT>(a, a.end_first + k, lane, active);
       }
+      // ---- rotate the prefetch queues; P2 of the next pixel ----
+      if (x + 1 < a.W) {
+        if (lane < 4) p2_cur = p2_of(a, g_n, pn_n);
+        left.pix = pix_of(a, x, y);
+        raw_q[0] = raw_q[1];
+        agg_q[0] = agg_q[1];
+        if (have2) {
+          raw_q[1] = raw_n;
+          agg_q[1] = agg_n;
+        }
+        if (w == 0) {
+#pragma unroll
+          for (int p = 0; p < 3; p++) up[p] = up_n[p];
+        }
+      }
     }
-    // ---- publish the last row's progress to the CTA below (every 8 pixels and at the end) ----
+    // ---- publish the last row's progress to the CTA below (every 4 pixels and at the end) ----
     if (w == kRows - 1) {
       const int x = s - 2 * w;
-      const bool last_row_ok = row_ok || y >= a.H;
-      if (last_row_ok && x >= 0 && x < a.W && (((x & 7) == 7) || x == a.W - 1)) {
+      if (x >= 0 && x < a.W && (((x & 3) == 3) || x == a.W - 1)) {
         __threadfence();
         __syncwarp();
         if (lane == 0) st_release(a.progress + cb, x + 1);
