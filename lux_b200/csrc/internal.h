@@ -61,7 +61,9 @@ void launch_upsample(const float* prev, int pw, int ph, const uint8_t* guide, in
                      cudaStream_t s);
 
 // cost.cu
-void launch_cost(const CostArgs& a, const LayerGeom& g, uint8_t* raw, int* err, cudaStream_t s);
+// zt: per other camera and plane, the plane-only projection terms (z·W[8] + W[12], z·W[9] + W[13], z·W[10] + W[14]),
+// each product and sum rounded to float, as (3 floats) × n_planes × n_others.
+void launch_cost(const CostArgs& a, const LayerGeom& g, const float* zt, uint8_t* raw, int* err, cudaStream_t s);
 
 // sgm_emulate.cu: the exact replay of the reference's sheared-tile traversal on its line-buffer layout (any layer)
 struct EmuBuffers {

@@ -292,8 +292,21 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
     ca.norm = f / nf;
   }
   ca.scale = p.scale;
+  // the plane-only projection terms of every camera (DenseStereo.cs:257-259: (z·W2 + W3), one rounding per op)
+  std::vector<float> zt_h((size_t)ca.n_others * L->n * 3);
+  for (int k = 0; k < ca.n_others; k++)
+    for (int i = 0; i < L->n; i++) {
+      const float z = L->planes_h[i];
+      for (int r = 0; r < 3; r++) {
+        volatile float prod = z * ca.warp[k][8 + r];
+        zt_h[((size_t)k * L->n + i) * 3 + r] = prod + ca.warp[k][12 + r];
+      }
+    }
+  float* zt = nullptr;
+  if ((rc = alloc_t(ctx, tmp, zt_h.size(), &zt))) return rc;
+  CK(cudaMemcpyAsync(zt, zt_h.data(), zt_h.size() * 4, cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(ctx->ev[0], s));
-  launch_cost(ca, g, L->raw, ctx->d_err, s);
+  launch_cost(ca, g, zt, L->raw, ctx->d_err, s);
   // aggregation: two passes over the sheared tiles, then WTA
   CK(cudaEventRecord(ctx->ev[1], s));
   const int xsw = 0;  // LUX_SGM_XSW unset: the reference default (DenseStereoSgm.cs:31)

@@ -61,6 +61,7 @@ struct UniArgs {
   const int* src1;
   const int* src2;
   const int* extra;
+  const uint2* p2t;   // [H][W] P2 of paths 0..3 per pixel of the pass
   int end_first, end_count;
   int keep_agg, wta;
   int* err;
@@ -390,8 +391,20 @@ LUX_DEV void up_fetch(const UniArgs& a, const uint16_t* bnd_up, const uint16_t* 
   }
 }
 
-template <int LPT>
-__global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
+// The four P2 values of every pixel of a pass (DenseStereoSgm.cs:266-273): they depend only on the guidance image (and
+// at the first row of pass -1 on pass +1's row y_b), so they are computed once per pass, packed as u16 (P2 <= 1744).
+__global__ void k_p2_table(const UniArgs a, uint2* __restrict__ p2t) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= a.W) return;
+  const float4 g = pix_of(a, x, y);
+  uint32_t v[4];
+#pragma unroll
+  for (int p = 0; p < 4; p++) v[p] = (uint32_t)p2_of(a, g, neighbour_pix(a, p, x, y));
+  p2t[(size_t)y * a.W + x] = make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
+}
+
+template <int LPT, bool FULL>
+__global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) {
   constexpr int NR = LPT / 2, Dp = Dp_of(LPT);
   extern __shared__ __align__(16) uint16_t smem_ring[];
   // ring[w][slot][path][Dp]: row w's paths 1..3 at pixel x with slot x & 3, read by row w + 1
@@ -408,22 +421,39 @@ __global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
   const int cb = s_cb;
   const int y = cb * kRows + w;  // row of the pass
   const bool row_ok = y < a.H;
-  const bool active = lane * LPT < a.n;
+  const bool active = FULL || lane * LPT < a.n;
   const int c = a.W - 1;
   const uint32_t p1x2 = dup16((uint32_t)a.p1);
   const uint16_t* bnd_up = a.bnd + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3 * Dp;
   const uint16_t* bnd_up_min = a.bnd_min + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3;
   uint16_t* bnd_me = a.bnd + (size_t)(cb % kBandBufs) * a.W * 3 * Dp;
   uint16_t* bnd_me_min = a.bnd_min + (size_t)(cb % kBandBufs) * a.W * 3;
+  // the row in memory: x of the pass maps to column x0 + xs·x
+  const int yu = a.dir > 0 ? y : a.H - 1 - y;
+  const long long x0 = a.dir > 0 ? 0 : a.W - 1, xs = a.dir > 0 ? 1 : -1;
+  const uint8_t* raw_row = a.raw + ((size_t)(row_ok ? yu : 0) * a.W) * a.n + lane * LPT;
+  uint16_t* agg_row = a.agg + ((size_t)(row_ok ? yu : 0) * a.W) * a.n + lane * LPT;
+  const uint2* p2_row = a.p2t + (size_t)(row_ok ? y : 0) * a.W;
+  float* depth_row = a.depth + (size_t)(row_ok ? yu : 0) * a.W;
   int seen = 0;  // progress of the CTA above, as last read
   Src<LPT> left;  // path 0: the pixel to the left
   src_init(left);
   Src<LPT> up[3];  // warp 0: paths 1..3 of the pixel at hand, fetched one step ahead
   RawB<LPT> raw_q[2];  // raw bytes of x+1, x+2 (a two-deep prefetch)
   V<LPT> agg_q[2];     // pass -1: pass +1's aggregates of x+1, x+2
-  int p2_cur = 0;      // lanes 0..3: P2 of path `lane` for the pixel at hand
+  uint2 p2_q[2];       // P2 of x+1, x+2
   const int flags = row_ok ? a.flags[y] : 0;
   const int nsteps = a.W + 2 * (kRows - 1);
+  auto fetch_px = [&](int xq, RawB<LPT>& rb, V<LPT>& ag, uint2& p2) {
+    const long long col = x0 + xs * xq;
+    const uint8_t* rp = raw_row + col * a.n;
+    if (!active) { rb.r[0] = 0; if constexpr (LPT >= 8) rb.r[1] = 0; }
+    else if constexpr (LPT == 8) { uint2 t = __ldcs(reinterpret_cast<const uint2*>(rp)); rb.r[0] = t.x; rb.r[1] = t.y; }
+    else if constexpr (LPT == 4) rb.r[0] = __ldcs(reinterpret_cast<const unsigned int*>(rp));
+    else rb.r[0] = __ldcs(reinterpret_cast<const unsigned short*>(rp));
+    if (a.dir < 0) agg_load<LPT>(agg_row + col * a.n, ag, active);
+    p2 = __ldg(p2_row + xq);
+  };
   // waits until the CTA above has published `need` pixels of its last row (bounded)
   auto wait_up = [&](int need) {
     if (seen < need) {
@@ -435,39 +465,28 @@ __global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
       __syncwarp();
     }
   };
+  uint2 p2_cur = make_uint2(0, 0);
   for (int s = 0; s < nsteps; s++) {
     const int x = s - 2 * w;
     if (row_ok && x >= 0 && x < a.W) {
       if (x == 0) {  // prologue: the row's first pixels
-        raw_fetch<LPT>(a, 0, y, raw_q[0], active, lane);
-        if (a.dir < 0) agg_load<LPT>(agg_ptr<LPT>(a, 0, y, lane), agg_q[0], active);
-        if (a.W > 1) {
-          raw_fetch<LPT>(a, 1, y, raw_q[1], active, lane);
-          if (a.dir < 0) agg_load<LPT>(agg_ptr<LPT>(a, 1, y, lane), agg_q[1], active);
-        }
-        if (lane < 4) p2_cur = p2_of(a, pix_of(a, 0, y), neighbour_pix(a, lane, 0, y));
+        fetch_px(0, raw_q[0], agg_q[0], p2_q[0]);
+        fetch_px(1, raw_q[1], agg_q[1], p2_q[1]);
         if (w == 0) {
           if (cb > 0) wait_up(min(a.W, 2));
           up_fetch<LPT>(a, bnd_up, bnd_up_min, cb, 0, up, lane);
         }
       }
-      // ---- prefetch for the pixels ahead: raw and aggregates of x+2, the row above of x+1, guidance of x+1 ----
+      // ---- prefetch for the pixels ahead: x+2 from memory, the row above of x+1 ----
       RawB<LPT> raw_n;
       V<LPT> agg_n;
+      uint2 p2_n;
       const bool have2 = x + 2 < a.W;
-      if (have2) {
-        raw_fetch<LPT>(a, x + 2, y, raw_n, active, lane);
-        if (a.dir < 0) agg_load<LPT>(agg_ptr<LPT>(a, x + 2, y, lane), agg_n, active);
-      }
+      if (have2) fetch_px(x + 2, raw_n, agg_n, p2_n);
       Src<LPT> up_n[3];
       if (w == 0 && x + 1 < a.W) {
         if (cb > 0) wait_up(min(a.W, x + 3));
         up_fetch<LPT>(a, bnd_up, bnd_up_min, cb, x + 1, up_n, lane);
-      }
-      float4 g_n = make_float4(0.f, 0.f, 0.f, 0.f), pn_n = g_n;
-      if (lane < 4 && x + 1 < a.W) {
-        g_n = pix_of(a, x + 1, y);
-        pn_n = neighbour_pix(a, lane, x + 1, y);
       }
       // ---- revisits that the reference runs before this visit (they may produce this visit's path-2 input) ----
       if (x == c) {
@@ -491,6 +510,7 @@ __global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
       }
       if (x == c && (flags & 1)) src_cs<LPT>(a, nb[2], y - 1, 4, c, lane);  // N(c).p2 reads R(c, y-1)
       // ---- the four paths ----
+      p2_cur = p2_q[0];
       V<LPT> raw2, acc, out[4];
       raw_unpack<LPT>(raw_q[0], raw2);
       if (a.dir > 0) {
@@ -502,17 +522,17 @@ __global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
       uint32_t mins[4];
 #pragma unroll
       for (int p = 0; p < 4; p++) {
-        const int P2 = __shfl_sync(0xffffffffu, p2_cur, p);
-        const uint32_t p2p = (uint32_t)min(P2 + (int)nb[p].mn, 65535);
+        const uint32_t P2 = ((p < 2 ? p2_cur.x : p2_cur.y) >> ((p & 1) * 16)) & 0xffffu;
+        const uint32_t p2p = min(P2 + nb[p].mn, 65535u);
         uint32_t rmin = 0xffffffffu;
         path_step<LPT>(nb[p].L, nb[p].mn, p2p, p1x2, raw2, active, lane, out[p], acc, rmin);
         mins[p] = warp_min<LPT>(rmin);
       }
-      uint16_t* ap = agg_ptr<LPT>(a, x, y, lane);
-      if (a.dir > 0 || a.keep_agg || x == c) agg_store<LPT>(ap, acc, active);
+      const long long colx = x0 + xs * x;
+      if (a.dir > 0 || a.keep_agg || x == c) agg_store<LPT>(agg_row + colx * a.n, acc, active);
       if (a.wta && x != c) {
         const int arg = wta_arg<LPT>(acc, active, lane);
-        if (lane == 0) a.depth[(size_t)(a.H - 1 - y) * a.W + (a.W - 1 - x)] = __ldg(a.planes + arg);
+        if (lane == 0) depth_row[colx] = __ldg(a.planes + arg);
       }
       // ---- hand-over ----
       left.L = out[0];
@@ -530,11 +550,14 @@ __global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
           if (lane == 0) __stcg(bnd_me_min + (size_t)x * 3 + (p - 1), (uint16_t)mins[p]);
         }
       }
-      if (x == c - 1) {
-        cs_put<LPT>(a, out[0], mins[0], y, 0, lane);
-        cs_put<LPT>(a, out[1], mins[1], y, 1, lane);
+      if (x >= c - 1) {
+        if (x == c - 1) {
+          cs_put<LPT>(a, out[0], mins[0], y, 0, lane);
+          cs_put<LPT>(a, out[1], mins[1], y, 1, lane);
+        } else {
+          cs_put<LPT>(a, out[2], mins[2], y, 2, lane);
+        }
       }
-      if (x == c) cs_put<LPT>(a, out[2], mins[2], y, 2, lane);
       if (a.edge_write && y == a.y_b) {
 #pragma unroll
         for (int p = 1; p < 4; p++) {
@@ -545,20 +568,18 @@ __global__ void __launch_bounds__(kRows * 32) k_sgm_uniform(const UniArgs a) {
       if (x == c && y == a.H - 1) {  // the last band's revisits when no later visit of the column follows them
         for (int k = 0; k < a.end_count; k++) run_revisit<LPT>(a, a.end_first + k, lane, active);
       }
-      // ---- rotate the prefetch queues; P2 of the next pixel ----
-      if (x + 1 < a.W) {
-        if (lane < 4) p2_cur = p2_of(a, g_n, pn_n);
-        left.pix = pix_of(a, x, y);
-        raw_q[0] = raw_q[1];
-        agg_q[0] = agg_q[1];
-        if (have2) {
-          raw_q[1] = raw_n;
-          agg_q[1] = agg_n;
-        }
-        if (w == 0) {
+      // ---- rotate the prefetch queues ----
+      raw_q[0] = raw_q[1];
+      agg_q[0] = agg_q[1];
+      p2_q[0] = p2_q[1];
+      if (have2) {
+        raw_q[1] = raw_n;
+        agg_q[1] = agg_n;
+        p2_q[1] = p2_n;
+      }
+      if (w == 0 && x + 1 < a.W) {
 #pragma unroll
-          for (int p = 0; p < 3; p++) up[p] = up_n[p];
-        }
+        for (int p = 0; p < 3; p++) up[p] = up_n[p];
       }
     }
     // ---- publish the last row's progress to the CTA below (every 4 pixels and at the end) ----
@@ -613,7 +634,7 @@ bool uniform_fast_supported(int W, int H, int n, int tile, uint16_t p1, float p2
 }
 
 struct UniScratchLayout {
-  size_t bnd, bnd_min, progress, edge, edge_min, cs, cs_min, sched, total;
+  size_t bnd, bnd_min, progress, edge, edge_min, cs, cs_min, sched, p2t, total;
 };
 
 static UniScratchLayout layout_of(int W, int H, int n) {
@@ -630,6 +651,7 @@ static UniScratchLayout layout_of(int W, int H, int n) {
   L.cs = o; o += al((size_t)H * 5 * Dp * 2);
   L.cs_min = o; o += al((size_t)H * 5 * 2);
   L.sched = o; o += al((size_t)2 * 7 * H * 4);
+  L.p2t = o; o += al((size_t)W * H * 8);
   L.total = o;
   return L;
 }
@@ -639,15 +661,20 @@ size_t uniform_scratch_bytes(int W, int H, int n, int tile) {
   return layout_of(W, H, n).total;
 }
 
-template <int LPT>
-static void launch_pass(const UniArgs& a, cudaStream_t s) {
+template <int LPT, bool FULL>
+static void launch_pass_t(const UniArgs& a, cudaStream_t s) {
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(k_sgm_uniform<LPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring_bytes<LPT>());
+    cudaFuncSetAttribute(k_sgm_uniform<LPT, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring_bytes<LPT>());
     configured = true;
   }
-  k_sgm_uniform<LPT><<<a.nCB, kRows * 32, ring_bytes<LPT>(), s>>>(a);
+  k_sgm_uniform<LPT, FULL><<<a.nCB, kRows * 32, ring_bytes<LPT>(), s>>>(a);
   count_launches(1);
+}
+template <int LPT>
+static void launch_pass(const UniArgs& a, cudaStream_t s) {
+  if (a.n == 32 * LPT) launch_pass_t<LPT, true>(a, s);
+  else launch_pass_t<LPT, false>(a, s);
 }
 
 int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
@@ -704,6 +731,9 @@ int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, con
     a.edge_write = pass == 0;
     a.edge_read = pass == 1;
     a.wta = pass == 1;
+    a.p2t = reinterpret_cast<const uint2*>(base + L.p2t);
+    k_p2_table<<<dim3((W + 127) / 128, H), 128, 0, s>>>(a, reinterpret_cast<uint2*>(base + L.p2t));
+    count_launches(1);
     if (lpt == 2) launch_pass<2>(a, s);
     else if (lpt == 4) launch_pass<4>(a, s);
     else launch_pass<8>(a, s);
