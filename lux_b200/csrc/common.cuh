@@ -76,6 +76,27 @@ LUX_DEV int ld_acquire(const int* p) {
   return v;
 }
 LUX_DEV void st_release(int* p, int v) { asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
+// CTA-scope acquire / release on shared memory: the hand-over between warps of one block.
+LUX_DEV int ld_acquire_cta(const int* p) {
+  int v;
+  asm volatile("ld.acquire.cta.shared.s32 %0, [%1];" : "=r"(v) : "r"((unsigned)__cvta_generic_to_shared(p)) : "memory");
+  return v;
+}
+LUX_DEV void st_release_cta(int* p, int v) {
+  asm volatile("st.release.cta.shared.s32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "r"(v) : "memory");
+}
+// Waits (bounded) until the shared counter *p >= target. Returns false on timeout or when *stop is set.
+LUX_DEV bool wait_shared_at_least(const int* p, int target, const volatile int* stop, uint64_t timeout_ns) {
+  if (ld_acquire_cta(p) >= target) return true;
+  const uint64_t t0 = global_ns();
+  for (unsigned it = 0;; it++) {
+    if (ld_acquire_cta(p) >= target) return true;
+    if ((it & 63) == 63) {
+      if (*stop) return false;
+      if (global_ns() - t0 > timeout_ns) return false;
+    }
+  }
+}
 
 // Waits until *flag >= target; on timeout sets *err = code and returns false. Spins are bounded by wall time.
 LUX_DEV bool wait_at_least(const int* flag, int target, int* err, int code, uint64_t timeout_ns) {

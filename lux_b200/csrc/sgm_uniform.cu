@@ -24,6 +24,7 @@ namespace lux {
 
 constexpr int kRows = 8;       // rows (warps) per CTA
 constexpr int kBandBufs = 4;   // band buffers in rotation
+constexpr int kRing = 8;       // slots of the hand-over ring between neighbouring rows of a block
 constexpr uint32_t kInit2 = 0x07d007d0u;  // 2000 | 2000
 
 LUX_DEV uint32_t vmin2(uint32_t a, uint32_t b) {
@@ -325,8 +326,8 @@ LUX_DEV void run_revisit(const UniArgs& a, int y, int lane, bool active) {
 }
 
 template <int LPT>
-constexpr size_t ring_bytes() {
-  return (size_t)kRows * 4 * 3 * Dp_of(LPT) * 2 + (size_t)kRows * 4 * 3 * 2;
+constexpr size_t ring_bytes() {  // the ring, its minima, padding, and one progress counter per row
+  return (size_t)kRows * kRing * 3 * Dp_of(LPT) * 2 + (size_t)kRows * kRing * 3 * 2 + 16 + (size_t)kRows * 4 + 16;
 }
 
 // Raw bytes of a lane's planes as loaded (8, 4 or 2 bytes), unpacked to u16 pairs when used.
@@ -407,20 +408,24 @@ template <int LPT, bool FULL>
 __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) {
   constexpr int NR = LPT / 2, Dp = Dp_of(LPT);
   extern __shared__ __align__(16) uint16_t smem_ring[];
-  // ring[w][slot][path][Dp]: row w's paths 1..3 at pixel x with slot x & 3, read by row w + 1
-  auto ring = [&](int w_, int slot, int p) { return smem_ring + (((size_t)w_ * 4 + slot) * 3 + p) * Dp; };
-  uint16_t* ring_min = smem_ring + (size_t)kRows * 4 * 3 * Dp;
-  auto rmin_at = [&](int w_, int slot, int p) -> uint16_t& { return ring_min[((size_t)w_ * 4 + slot) * 3 + p]; };
-  __shared__ int s_cb, s_stop;
+  // ring[w][slot][path][Dp]: row w's paths 1..3 at pixel x in slot x % kRing, read by row w + 1
+  auto ring = [&](int w_, int slot, int p) { return smem_ring + (((size_t)w_ * kRing + slot) * 3 + p) * Dp; };
+  uint16_t* ring_min = smem_ring + (size_t)kRows * kRing * 3 * Dp;
+  auto rmin_at = [&](int w_, int slot, int p) -> uint16_t& { return ring_min[((size_t)w_ * kRing + slot) * 3 + p]; };
+  int* prog = reinterpret_cast<int*>(ring_min + (size_t)kRows * kRing * 3 + 8);  // pixels finished per row (warp)
+  __shared__ int s_cb;
+  __shared__ volatile int s_stop;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   if (tid == 0) {
     s_cb = atomicAdd(a.ticket, 1);
     s_stop = 0;
   }
+  if (tid < kRows) prog[tid] = 0;
   __syncthreads();
   const int cb = s_cb;
   const int y = cb * kRows + w;  // row of the pass
   const bool row_ok = y < a.H;
+  const bool has_below = w + 1 < kRows && y + 1 < a.H;  // a row of this block reads this row's ring
   const bool active = FULL || lane * LPT < a.n;
   const int c = a.W - 1;
   const uint32_t p1x2 = dup16((uint32_t)a.p1);
@@ -435,15 +440,14 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
   uint16_t* agg_row = a.agg + ((size_t)(row_ok ? yu : 0) * a.W) * a.n + lane * LPT;
   const uint2* p2_row = a.p2t + (size_t)(row_ok ? y : 0) * a.W;
   float* depth_row = a.depth + (size_t)(row_ok ? yu : 0) * a.W;
-  int seen = 0;  // progress of the CTA above, as last read
+  int seen = 0;  // warp 0: progress of the block above, as last read
   Src<LPT> left;  // path 0: the pixel to the left
   src_init(left);
-  Src<LPT> up[3];  // warp 0: paths 1..3 of the pixel at hand, fetched one step ahead
+  Src<LPT> up[3];  // warp 0: paths 1..3 of the pixel at hand, fetched one pixel ahead
   RawB<LPT> raw_q[2];  // raw bytes of x+1, x+2 (a two-deep prefetch)
   V<LPT> agg_q[2];     // pass -1: pass +1's aggregates of x+1, x+2
   uint2 p2_q[2];       // P2 of x+1, x+2
   const int flags = row_ok ? a.flags[y] : 0;
-  const int nsteps = a.W + 2 * (kRows - 1);
   auto fetch_px = [&](int xq, RawB<LPT>& rb, V<LPT>& ag, uint2& p2) {
     const long long col = x0 + xs * xq;
     const uint8_t* rp = raw_row + col * a.n;
@@ -454,7 +458,7 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
     if (a.dir < 0) agg_load<LPT>(agg_row + col * a.n, ag, active);
     p2 = __ldg(p2_row + xq);
   };
-  // waits until the CTA above has published `need` pixels of its last row (bounded)
+  // warp 0: waits until the block above has published `need` pixels of its last row (bounded)
   auto wait_up = [&](int need) {
     if (seen < need) {
       if (lane == 0) {
@@ -465,18 +469,26 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
       __syncwarp();
     }
   };
-  uint2 p2_cur = make_uint2(0, 0);
-  for (int s = 0; s < nsteps; s++) {
-    const int x = s - 2 * w;
-    if (row_ok && x >= 0 && x < a.W) {
-      if (x == 0) {  // prologue: the row's first pixels
-        fetch_px(0, raw_q[0], agg_q[0], p2_q[0]);
-        fetch_px(1, raw_q[1], agg_q[1], p2_q[1]);
-        if (w == 0) {
-          if (cb > 0) wait_up(min(a.W, 2));
-          up_fetch<LPT>(a, bnd_up, bnd_up_min, cb, 0, up, lane);
-        }
-      }
+  // waits on a neighbouring row of this block; a timeout stops the whole block
+  auto wait_row = [&](int row, int need) {
+    if (lane == 0 && !wait_shared_at_least(prog + row, need, &s_stop, a.timeout_ns)) {
+      atomicCAS(a.err, 0, 11);
+      s_stop = 1;
+    }
+    __syncwarp();
+  };
+  if (row_ok) {
+    fetch_px(0, raw_q[0], agg_q[0], p2_q[0]);
+    fetch_px(1, raw_q[1], agg_q[1], p2_q[1]);
+    if (w == 0) {
+      if (cb > 0) wait_up(min(a.W, 2));
+      up_fetch<LPT>(a, bnd_up, bnd_up_min, cb, 0, up, lane);
+    }
+    for (int x = 0; x < a.W; x++) {
+      // ---- hand-over in: the row above finished x+1; the row below is done with the ring slot this pixel reuses ----
+      if (w > 0) wait_row(w - 1, min(a.W, x + 2));
+      if (has_below && x >= kRing - 1) wait_row(w + 1, x - kRing + 2);
+      if (s_stop) break;
       // ---- prefetch for the pixels ahead: x+2 from memory, the row above of x+1 ----
       RawB<LPT> raw_n;
       V<LPT> agg_n;
@@ -501,8 +513,9 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
         for (int p = 1; p < 4; p++) {
           const int xn = x + (p == 1 ? -1 : p == 2 ? 0 : 1);
           if (xn < 0 || xn >= a.W) { src_init(nb[p]); continue; }
-          vload_s<LPT>(nb[p].L, ring(w - 1, xn & 3, p - 1), lane);
-          nb[p].mn = rmin_at(w - 1, xn & 3, p - 1);
+          const int sl = xn & (kRing - 1);
+          vload_s<LPT>(nb[p].L, ring(w - 1, sl, p - 1), lane);
+          nb[p].mn = rmin_at(w - 1, sl, p - 1);
         }
       } else {
 #pragma unroll
@@ -510,7 +523,7 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
       }
       if (x == c && (flags & 1)) src_cs<LPT>(a, nb[2], y - 1, 4, c, lane);  // N(c).p2 reads R(c, y-1)
       // ---- the four paths ----
-      p2_cur = p2_q[0];
+      const uint2 p2_cur = p2_q[0];
       V<LPT> raw2, acc, out[4];
       raw_unpack<LPT>(raw_q[0], raw2);
       if (a.dir > 0) {
@@ -534,14 +547,15 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
         const int arg = wta_arg<LPT>(acc, active, lane);
         if (lane == 0) depth_row[colx] = __ldg(a.planes + arg);
       }
-      // ---- hand-over ----
+      // ---- hand-over out ----
       left.L = out[0];
       left.mn = mins[0];
       if (w < kRows - 1) {
+        const int sl = x & (kRing - 1);
 #pragma unroll
         for (int p = 1; p < 4; p++) {
-          vstore_s<LPT>(out[p], ring(w, x & 3, p - 1), lane);
-          if (lane == 0) rmin_at(w, x & 3, p - 1) = (uint16_t)mins[p];
+          vstore_s<LPT>(out[p], ring(w, sl, p - 1), lane);
+          if (lane == 0) rmin_at(w, sl, p - 1) = (uint16_t)mins[p];
         }
       } else {
 #pragma unroll
@@ -568,6 +582,14 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
       if (x == c && y == a.H - 1) {  // the last band's revisits when no later visit of the column follows them
         for (int k = 0; k < a.end_count; k++) run_revisit<LPT>(a, a.end_first + k, lane, active);
       }
+      __syncwarp();
+      if (w < kRows - 1) {
+        if (lane == 0) st_release_cta(prog + w, x + 1);
+      } else if (((x & 3) == 3) || x == a.W - 1) {  // the block below reads the last row from global memory
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) st_release(a.progress + cb, x + 1);
+      }
       // ---- rotate the prefetch queues ----
       raw_q[0] = raw_q[1];
       agg_q[0] = agg_q[1];
@@ -582,22 +604,15 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
         for (int p = 0; p < 3; p++) up[p] = up_n[p];
       }
     }
-    // ---- publish the last row's progress to the CTA below (every 4 pixels and at the end) ----
-    if (w == kRows - 1) {
-      const int x = s - 2 * w;
-      if (x >= 0 && x < a.W && (((x & 3) == 3) || x == a.W - 1)) {
-        __threadfence();
-        __syncwarp();
-        if (lane == 0) st_release(a.progress + cb, x + 1);
-      }
-    }
-    __syncthreads();
-    if (s_stop) break;
   }
-  // rows past the image end still publish completion
-  if (tid == 0) {
-    __threadfence();
-    st_release(a.progress + cb, a.W);
+  // rows that stopped early or do not exist still release their neighbours
+  __syncwarp();
+  if (lane == 0) {
+    if (w < kRows - 1) st_release_cta(prog + w, a.W);
+    else {
+      __threadfence();
+      st_release(a.progress + cb, a.W);
+    }
   }
 }
 
