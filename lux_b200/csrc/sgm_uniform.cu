@@ -583,9 +583,8 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
         for (int k = 0; k < a.end_count; k++) run_revisit<LPT>(a, a.end_first + k, lane, active);
       }
       __syncwarp();
-      if (w < kRows - 1) {
-        if (lane == 0) st_release_cta(prog + w, x + 1);
-      } else if (((x & 3) == 3) || x == a.W - 1) {  // the block below reads the last row from global memory
+      if (lane == 0) st_release_cta(prog + w, x + 1);  // the row above waits on it before reusing a ring slot
+      if (w == kRows - 1 && (((x & 3) == 3) || x == a.W - 1)) {  // the block below reads the last row from global memory
         __threadfence();
         __syncwarp();
         if (lane == 0) st_release(a.progress + cb, x + 1);
@@ -608,8 +607,8 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
   // rows that stopped early or do not exist still release their neighbours
   __syncwarp();
   if (lane == 0) {
-    if (w < kRows - 1) st_release_cta(prog + w, a.W);
-    else {
+    st_release_cta(prog + w, a.W);
+    if (w == kRows - 1) {
       __threadfence();
       st_release(a.progress + cb, a.W);
     }
