@@ -22,7 +22,8 @@
 
 namespace lux {
 
-constexpr int kRows = 8;       // rows (warps) per CTA
+constexpr int kRows = 6;       // rows of the recurrence per block (one warp each)
+constexpr int kWarps = kRows + 2;  // plus the loader and the publisher warps
 constexpr int kBandBufs = 4;   // band buffers in rotation
 constexpr int kRing = 8;       // slots of the hand-over ring between neighbouring rows of a block
 constexpr uint32_t kInit2 = 0x07d007d0u;  // 2000 | 2000
@@ -144,6 +145,44 @@ template <int LPT>
 LUX_DEV uint32_t warp_min(uint32_t rmin) {  // min over both halves and all lanes
   uint32_t m = min(rmin & 0xffffu, rmin >> 16);
   return __reduce_min_sync(0xffffffffu, m);
+}
+
+// The four paths of one pixel, written path-parallel so the independent chains interleave: all neighbour shuffles
+// first, then the min/add chains, then the four warp minima. nb[p]/mp[p]: neighbour L and minimum of path p; p2[p]: P2.
+template <int LPT, bool FULL>
+LUX_DEV void four_paths(const V<LPT> (&nb)[4], const uint32_t (&mp)[4], const uint32_t (&p2)[4], uint32_t p1x2, const V<LPT>& raw2,
+                        bool active, int lane, V<LPT> (&out)[4], V<LPT>& acc, uint32_t (&mins)[4]) {
+  constexpr int NR = LPT / 2;
+  uint32_t prev[4], next[4];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    prev[p] = __shfl_up_sync(0xffffffffu, nb[p].r[NR - 1], 1);
+    next[p] = __shfl_down_sync(0xffffffffu, nb[p].r[0], 1);
+  }
+  uint32_t rmin[4];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    if (lane == 0) prev[p] = kInit2;   // plane -1: the word before the block holds 2000
+    if (lane == 31) next[p] = kInit2;  // plane n (or a padding lane): 2000
+    rmin[p] = 0xffffffffu;
+  }
+#pragma unroll
+  for (int i = 0; i < NR; i++) {
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const uint32_t lm = pair_of(i == 0 ? prev[p] : nb[p].r[i - 1], nb[p].r[i]);       // L[d-1]
+      const uint32_t lp = pair_of(nb[p].r[i], i == NR - 1 ? next[p] : nb[p].r[i + 1]);  // L[d+1]
+      uint32_t t = vmin2(lm, lp) + p1x2;
+      t = vmin2(vmin2(t, nb[p].r[i]), dup16(min(p2[p] + mp[p], 65535u)));
+      uint32_t lc = t + raw2.r[i] - dup16(mp[p]);  // raw + m - minPrev, each half in [0, 2000)
+      if (!FULL) lc = active ? lc : kInit2;          // padding lanes keep 2000
+      out[p].r[i] = lc;
+      rmin[p] = vmin2(rmin[p], lc);
+      acc.r[i] += lc;
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 4; p++) mins[p] = warp_min<LPT>(rmin[p]);
 }
 
 LUX_DEV float4 pix_of(const UniArgs& a, int xm, int ym) {  // guidance at a pixel given in pass coordinates
@@ -325,9 +364,11 @@ LUX_DEV void run_revisit(const UniArgs& a, int y, int lane, bool active) {
   __syncwarp();
 }
 
+// Shared memory of a block: kRows + 1 hand-over rings (ring kRows is the row above the block, filled by the loader warp),
+// their minima, and the progress counters: rows 0..kRows-1, the loader (kRows), the publisher (kRows + 1).
 template <int LPT>
-constexpr size_t ring_bytes() {  // the ring, its minima, padding, and one progress counter per row
-  return (size_t)kRows * kRing * 3 * Dp_of(LPT) * 2 + (size_t)kRows * kRing * 3 * 2 + 16 + (size_t)kRows * 4 + 16;
+constexpr size_t ring_bytes() {
+  return (size_t)(kRows + 1) * kRing * 3 * Dp_of(LPT) * 2 + (size_t)(kRows + 1) * kRing * 3 * 2 + 16 + (size_t)(kRows + 2) * 4 + 16;
 }
 
 // Raw bytes of a lane's planes as loaded (8, 4 or 2 bytes), unpacked to u16 pairs when used.
@@ -335,20 +376,6 @@ template <int LPT>
 struct RawB {
   uint32_t r[LPT >= 8 ? 2 : 1];
 };
-template <int LPT>
-LUX_DEV void raw_fetch(const UniArgs& a, int xm, int ym, RawB<LPT>& b, bool active, int lane) {
-  const int x = a.dir > 0 ? xm : a.W - 1 - xm, y = a.dir > 0 ? ym : a.H - 1 - ym;
-  const uint8_t* p = a.raw + ((size_t)y * a.W + x) * a.n + lane * LPT;
-  if (!active) { b.r[0] = 0; if constexpr (LPT >= 8) b.r[1] = 0; return; }
-  if constexpr (LPT == 8) {
-    uint2 t = __ldcs(reinterpret_cast<const uint2*>(p));
-    b.r[0] = t.x; b.r[1] = t.y;
-  } else if constexpr (LPT == 4) {
-    b.r[0] = __ldcs(reinterpret_cast<const unsigned int*>(p));
-  } else {
-    b.r[0] = __ldcs(reinterpret_cast<const unsigned short*>(p));
-  }
-}
 template <int LPT>
 LUX_DEV void raw_unpack(const RawB<LPT>& b, V<LPT>& raw2) {
   raw2.r[0] = __byte_perm(b.r[0], 0, 0x4140);
@@ -372,26 +399,6 @@ LUX_DEV float4 neighbour_pix(const UniArgs& a, int p, int xq, int yq) {
   return pix_of(a, xn, yn);
 }
 
-template <int LPT>
-LUX_DEV void up_fetch(const UniArgs& a, const uint16_t* bnd_up, const uint16_t* bnd_up_min, int cb, int xq, Src<LPT> (&u)[3],
-                      int lane) {
-  constexpr int Dp = Dp_of(LPT);
-#pragma unroll
-  for (int p = 1; p < 4; p++) {
-    const int xn = xq + (p == 1 ? -1 : p == 2 ? 0 : 1);
-    Src<LPT>& d = u[p - 1];
-    if (xn < 0 || xn >= a.W) { src_init(d); continue; }
-    if (cb > 0) {
-      vload<LPT>(d.L, bnd_up + ((size_t)xn * 3 + (p - 1)) * Dp, lane);
-      d.mn = __ldcg(bnd_up_min + (size_t)xn * 3 + (p - 1));
-    } else if (a.edge_read) {
-      src_edge<LPT>(a, d, a.dir > 0 ? xn : a.W - 1 - xn, p, lane);
-    } else {
-      src_init(d);
-    }
-  }
-}
-
 // The four P2 values of every pixel of a pass (DenseStereoSgm.cs:266-273): they depend only on the guidance image (and
 // at the first row of pass -1 on pass +1's row y_b), so they are computed once per pass, packed as u16 (P2 <= 1744).
 __global__ void k_p2_table(const UniArgs a, uint2* __restrict__ p2t) {
@@ -404,15 +411,36 @@ __global__ void k_p2_table(const UniArgs a, uint2* __restrict__ p2t) {
   p2t[(size_t)y * a.W + x] = make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
 }
 
+// The row above a block, pixel by pixel, as the block's first row reads it: the last row of the block above (from the
+// global band buffer), pass +1's final line buffer at the first row of pass -1, or never-written slots.
+template <int LPT>
+LUX_DEV void row_above(const UniArgs& a, const uint16_t* bnd_up, const uint16_t* bnd_up_min, int cb, int x, Src<LPT> (&u)[3], int lane) {
+  constexpr int Dp = Dp_of(LPT);
+#pragma unroll
+  for (int p = 1; p < 4; p++) {
+    if (cb > 0) {
+      vload<LPT>(u[p - 1].L, bnd_up + ((size_t)x * 3 + (p - 1)) * Dp, lane);
+      u[p - 1].mn = __ldcg(bnd_up_min + (size_t)x * 3 + (p - 1));
+    } else if (a.edge_read) {
+      src_edge<LPT>(a, u[p - 1], a.dir > 0 ? x : a.W - 1 - x, p, lane);
+    } else {
+      src_init(u[p - 1]);
+    }
+  }
+}
+
+// Warps 0..kRows-1 run the recurrence of one row each; warp kRows (loader) brings the row above the block into ring
+// kRows; warp kRows+1 (publisher) copies the block's last row to the global band buffer for the block below. A row
+// waits only on its neighbours (shared-memory acquire/release), so the global latencies of the block boundary stay
+// off the rows' own critical path.
 template <int LPT, bool FULL>
-__global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) {
-  constexpr int NR = LPT / 2, Dp = Dp_of(LPT);
+__global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a) {
+  constexpr int NR = LPT / 2, Dp = Dp_of(LPT), kBatch = 4;
   extern __shared__ __align__(16) uint16_t smem_ring[];
-  // ring[w][slot][path][Dp]: row w's paths 1..3 at pixel x in slot x % kRing, read by row w + 1
-  auto ring = [&](int w_, int slot, int p) { return smem_ring + (((size_t)w_ * kRing + slot) * 3 + p) * Dp; };
-  uint16_t* ring_min = smem_ring + (size_t)kRows * kRing * 3 * Dp;
-  auto rmin_at = [&](int w_, int slot, int p) -> uint16_t& { return ring_min[((size_t)w_ * kRing + slot) * 3 + p]; };
-  int* prog = reinterpret_cast<int*>(ring_min + (size_t)kRows * kRing * 3 + 8);  // pixels finished per row (warp)
+  auto ring = [&](int set, int slot, int p) { return smem_ring + (((size_t)set * kRing + slot) * 3 + p) * Dp; };
+  uint16_t* ring_min = smem_ring + (size_t)(kRows + 1) * kRing * 3 * Dp;
+  auto rmin_at = [&](int set, int slot, int p) -> uint16_t& { return ring_min[((size_t)set * kRing + slot) * 3 + p]; };
+  int* prog = reinterpret_cast<int*>(ring_min + (size_t)(kRows + 1) * kRing * 3 + 8);
   __shared__ int s_cb;
   __shared__ volatile int s_stop;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -420,33 +448,106 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
     s_cb = atomicAdd(a.ticket, 1);
     s_stop = 0;
   }
-  if (tid < kRows) prog[tid] = 0;
+  if (tid < kRows + 2) prog[tid] = 0;
   __syncthreads();
   const int cb = s_cb;
-  const int y = cb * kRows + w;  // row of the pass
-  const bool row_ok = y < a.H;
-  const bool has_below = w + 1 < kRows && y + 1 < a.H;  // a row of this block reads this row's ring
+  const int y0 = cb * kRows;
+  const bool below_exists = y0 + kRows < a.H;  // a block below reads this block's last row
   const bool active = FULL || lane * LPT < a.n;
-  const int c = a.W - 1;
-  const uint32_t p1x2 = dup16((uint32_t)a.p1);
   const uint16_t* bnd_up = a.bnd + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3 * Dp;
   const uint16_t* bnd_up_min = a.bnd_min + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3;
   uint16_t* bnd_me = a.bnd + (size_t)(cb % kBandBufs) * a.W * 3 * Dp;
   uint16_t* bnd_me_min = a.bnd_min + (size_t)(cb % kBandBufs) * a.W * 3;
-  // the row in memory: x of the pass maps to column x0 + xs·x
+  // waits (bounded) on a progress counter of this block; a timeout stops the block
+  auto wait_ctr = [&](int ctr, int need) {
+    if (lane == 0 && !wait_shared_at_least(prog + ctr, need, &s_stop, a.timeout_ns)) {
+      atomicCAS(a.err, 0, 11);
+      s_stop = 1;
+    }
+    __syncwarp();
+  };
+
+  if (w == kRows) {
+    // ---------------- loader: the row above the block into ring kRows ----------------
+    if (y0 < a.H) {
+      for (int xb = 0; xb < a.W && !s_stop; xb += kBatch) {
+        const int xe = min(a.W, xb + kBatch);
+        if (xe - 1 >= kRing - 1) wait_ctr(0, xe - kRing + 1);  // row 0 is done with these slots
+        if (cb > 0 && lane == 0 && !wait_at_least(a.progress + (cb - 1), xe, a.err, 11, a.timeout_ns)) s_stop = 1;
+        __syncwarp();
+        Src<LPT> u[kBatch][3];
+#pragma unroll
+        for (int k = 0; k < kBatch; k++)
+          if (xb + k < xe) row_above<LPT>(a, bnd_up, bnd_up_min, cb, xb + k, u[k], lane);
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) {
+          if (xb + k >= xe) break;
+          const int sl = (xb + k) & (kRing - 1);
+#pragma unroll
+          for (int p = 0; p < 3; p++) {
+            vstore_s<LPT>(u[k][p].L, ring(kRows, sl, p), lane);
+            if (lane == 0) rmin_at(kRows, sl, p) = (uint16_t)u[k][p].mn;
+          }
+        }
+        __syncwarp();
+        if (lane == 0) st_release_cta(prog + kRows, xe);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) st_release_cta(prog + kRows, a.W);
+    return;
+  }
+  if (w == kRows + 1) {
+    // ---------------- publisher: the block's last row into the global band buffer ----------------
+    if (below_exists) {
+      for (int xb = 0; xb < a.W && !s_stop; xb += kBatch) {
+        const int xe = min(a.W, xb + kBatch);
+        wait_ctr(kRows - 1, xe);
+        for (int x = xb; x < xe; x++) {
+          const int sl = x & (kRing - 1);
+#pragma unroll
+          for (int p = 0; p < 3; p++) {
+            V<LPT> v;
+            vload_s<LPT>(v, ring(kRows - 1, sl, p), lane);
+            vstore<LPT>(v, bnd_me + ((size_t)x * 3 + p) * Dp, lane);
+            if (lane == 0) __stcg(bnd_me_min + (size_t)x * 3 + p, rmin_at(kRows - 1, sl, p));
+          }
+        }
+        __syncwarp();
+        if (lane == 0) st_release_cta(prog + kRows + 1, xe);  // the ring slots are free again
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) st_release(a.progress + cb, xe);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      st_release_cta(prog + kRows + 1, a.W);
+      __threadfence();
+      st_release(a.progress + cb, a.W);
+    }
+    return;
+  }
+
+  // ---------------- a row of the recurrence ----------------
+  const int y = y0 + w;  // row of the pass
+  const bool row_ok = y < a.H;
+  const int up_set = w == 0 ? kRows : w - 1;            // the ring (and counter) holding the row above
+  const int cons_ctr = w + 1 < kRows ? w + 1 : kRows + 1;  // who reads this row's ring
+  const bool has_consumer = y + 1 < a.H;
+  const int c = a.W - 1;
+  const uint32_t p1x2 = dup16((uint32_t)a.p1);
   const int yu = a.dir > 0 ? y : a.H - 1 - y;
   const long long x0 = a.dir > 0 ? 0 : a.W - 1, xs = a.dir > 0 ? 1 : -1;
   const uint8_t* raw_row = a.raw + ((size_t)(row_ok ? yu : 0) * a.W) * a.n + lane * LPT;
   uint16_t* agg_row = a.agg + ((size_t)(row_ok ? yu : 0) * a.W) * a.n + lane * LPT;
   const uint2* p2_row = a.p2t + (size_t)(row_ok ? y : 0) * a.W;
   float* depth_row = a.depth + (size_t)(row_ok ? yu : 0) * a.W;
-  int seen = 0;  // warp 0: progress of the block above, as last read
   Src<LPT> left;  // path 0: the pixel to the left
   src_init(left);
-  Src<LPT> up[3];  // warp 0: paths 1..3 of the pixel at hand, fetched one pixel ahead
-  RawB<LPT> raw_q[2];  // raw bytes of x+1, x+2 (a two-deep prefetch)
-  V<LPT> agg_q[2];     // pass -1: pass +1's aggregates of x+1, x+2
-  uint2 p2_q[2];       // P2 of x+1, x+2
+  RawB<LPT> raw_q[2];  // raw bytes of x, x+1 (a two-deep prefetch)
+  V<LPT> agg_q[2];     // pass -1: pass +1's aggregates of x, x+1
+  uint2 p2_q[2];       // P2 of x, x+1
   const int flags = row_ok ? a.flags[y] : 0;
   auto fetch_px = [&](int xq, RawB<LPT>& rb, V<LPT>& ag, uint2& p2) {
     const long long col = x0 + xs * xq;
@@ -458,72 +559,41 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
     if (a.dir < 0) agg_load<LPT>(agg_row + col * a.n, ag, active);
     p2 = __ldg(p2_row + xq);
   };
-  // warp 0: waits until the block above has published `need` pixels of its last row (bounded)
-  auto wait_up = [&](int need) {
-    if (seen < need) {
-      if (lane == 0) {
-        if (!wait_at_least(a.progress + (cb - 1), need, a.err, 11, a.timeout_ns)) s_stop = 1;
-        seen = ld_acquire(a.progress + (cb - 1));
-      }
-      seen = __shfl_sync(0xffffffffu, seen, 0);
-      __syncwarp();
-    }
-  };
-  // waits on a neighbouring row of this block; a timeout stops the whole block
-  auto wait_row = [&](int row, int need) {
-    if (lane == 0 && !wait_shared_at_least(prog + row, need, &s_stop, a.timeout_ns)) {
-      atomicCAS(a.err, 0, 11);
-      s_stop = 1;
-    }
-    __syncwarp();
-  };
   if (row_ok) {
     fetch_px(0, raw_q[0], agg_q[0], p2_q[0]);
     fetch_px(1, raw_q[1], agg_q[1], p2_q[1]);
-    if (w == 0) {
-      if (cb > 0) wait_up(min(a.W, 2));
-      up_fetch<LPT>(a, bnd_up, bnd_up_min, cb, 0, up, lane);
-    }
     for (int x = 0; x < a.W; x++) {
-      // ---- hand-over in: the row above finished x+1; the row below is done with the ring slot this pixel reuses ----
-      if (w > 0) wait_row(w - 1, min(a.W, x + 2));
-      if (has_below && x >= kRing - 1) wait_row(w + 1, x - kRing + 2);
+      // ---- hand-over in: the row above finished x+1; the next row is done with the ring slot this pixel reuses ----
+      wait_ctr(up_set, min(a.W, x + 2));
+      if (has_consumer && x >= kRing - 1) wait_ctr(cons_ctr, x - kRing + 2);
       if (s_stop) break;
-      // ---- prefetch for the pixels ahead: x+2 from memory, the row above of x+1 ----
-      RawB<LPT> raw_n;
-      V<LPT> agg_n;
-      uint2 p2_n;
-      const bool have2 = x + 2 < a.W;
-      if (have2) fetch_px(x + 2, raw_n, agg_n, p2_n);
-      Src<LPT> up_n[3];
-      if (w == 0 && x + 1 < a.W) {
-        if (cb > 0) wait_up(min(a.W, x + 3));
-        up_fetch<LPT>(a, bnd_up, bnd_up_min, cb, x + 1, up_n, lane);
-      }
       // ---- revisits that the reference runs before this visit (they may produce this visit's path-2 input) ----
       if (x == c) {
         const int cnt = a.batch_count[y], first = a.batch_first[y];
         for (int k = 0; k < cnt; k++) run_revisit<LPT>(a, first + k, lane, active);
       }
       // ---- neighbour states: paths 1, 2, 3 read pixels x-1, x, x+1 of row y-1 ----
-      Src<LPT> nb[4];
-      nb[0] = left;
-      if (w > 0) {
+      V<LPT> nbL[4];
+      uint32_t mp[4];
+      nbL[0] = left.L;
+      mp[0] = left.mn;
 #pragma unroll
-        for (int p = 1; p < 4; p++) {
-          const int xn = x + (p == 1 ? -1 : p == 2 ? 0 : 1);
-          if (xn < 0 || xn >= a.W) { src_init(nb[p]); continue; }
-          const int sl = xn & (kRing - 1);
-          vload_s<LPT>(nb[p].L, ring(w - 1, sl, p - 1), lane);
-          nb[p].mn = rmin_at(w - 1, sl, p - 1);
-        }
-      } else {
-#pragma unroll
-        for (int p = 1; p < 4; p++) nb[p] = up[p - 1];
+      for (int p = 1; p < 4; p++) {
+        const int xn = x + (p == 1 ? -1 : p == 2 ? 0 : 1);
+        if (xn < 0 || xn >= a.W) { vinit(nbL[p]); mp[p] = 2000; continue; }
+        const int sl = xn & (kRing - 1);
+        vload_s<LPT>(nbL[p], ring(up_set, sl, p - 1), lane);
+        mp[p] = rmin_at(up_set, sl, p - 1);
       }
-      if (x == c && (flags & 1)) src_cs<LPT>(a, nb[2], y - 1, 4, c, lane);  // N(c).p2 reads R(c, y-1)
+      if (x == c && (flags & 1)) {  // N(c).p2 reads R(c, y-1)
+        Src<LPT> r;
+        src_cs<LPT>(a, r, y - 1, 4, c, lane);
+        nbL[2] = r.L;
+        mp[2] = r.mn;
+      }
       // ---- the four paths ----
-      const uint2 p2_cur = p2_q[0];
+      const uint2 p2v = p2_q[0];
+      const uint32_t p2[4] = {p2v.x & 0xffffu, p2v.x >> 16, p2v.y & 0xffffu, p2v.y >> 16};
       V<LPT> raw2, acc, out[4];
       raw_unpack<LPT>(raw_q[0], raw2);
       if (a.dir > 0) {
@@ -533,44 +603,30 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
         acc = agg_q[0];
       }
       uint32_t mins[4];
+      four_paths<LPT, FULL>(nbL, mp, p2, p1x2, raw2, active, lane, out, acc, mins);
+      // ---- hand-over out: the ring first, then the release; global stores after it ----
+      const int sl = x & (kRing - 1);
 #pragma unroll
-      for (int p = 0; p < 4; p++) {
-        const uint32_t P2 = ((p < 2 ? p2_cur.x : p2_cur.y) >> ((p & 1) * 16)) & 0xffffu;
-        const uint32_t p2p = min(P2 + nb[p].mn, 65535u);
-        uint32_t rmin = 0xffffffffu;
-        path_step<LPT>(nb[p].L, nb[p].mn, p2p, p1x2, raw2, active, lane, out[p], acc, rmin);
-        mins[p] = warp_min<LPT>(rmin);
+      for (int p = 1; p < 4; p++) {
+        vstore_s<LPT>(out[p], ring(w, sl, p - 1), lane);
+        if (lane == 0) rmin_at(w, sl, p - 1) = (uint16_t)mins[p];
       }
       const long long colx = x0 + xs * x;
-      if (a.dir > 0 || a.keep_agg || x == c) agg_store<LPT>(agg_row + colx * a.n, acc, active);
-      if (a.wta && x != c) {
-        const int arg = wta_arg<LPT>(acc, active, lane);
-        if (lane == 0) depth_row[colx] = __ldg(a.planes + arg);
-      }
-      // ---- hand-over out ----
-      left.L = out[0];
-      left.mn = mins[0];
-      if (w < kRows - 1) {
-        const int sl = x & (kRing - 1);
-#pragma unroll
-        for (int p = 1; p < 4; p++) {
-          vstore_s<LPT>(out[p], ring(w, sl, p - 1), lane);
-          if (lane == 0) rmin_at(w, sl, p - 1) = (uint16_t)mins[p];
-        }
-      } else {
-#pragma unroll
-        for (int p = 1; p < 4; p++) {
-          vstore<LPT>(out[p], bnd_me + ((size_t)x * 3 + (p - 1)) * Dp, lane);
-          if (lane == 0) __stcg(bnd_me_min + (size_t)x * 3 + (p - 1), (uint16_t)mins[p]);
-        }
-      }
-      if (x >= c - 1) {
+      if (x >= c - 1) {  // what later revisits of this block read must be stored before the release
         if (x == c - 1) {
           cs_put<LPT>(a, out[0], mins[0], y, 0, lane);
           cs_put<LPT>(a, out[1], mins[1], y, 1, lane);
         } else {
           cs_put<LPT>(a, out[2], mins[2], y, 2, lane);
+          agg_store<LPT>(agg_row + colx * a.n, acc, active);
         }
+      }
+      __syncwarp();
+      if (lane == 0) st_release_cta(prog + w, x + 1);
+      if (x != c && (a.dir > 0 || a.keep_agg)) agg_store<LPT>(agg_row + colx * a.n, acc, active);
+      if (a.wta && x != c) {
+        const int arg = wta_arg<LPT>(acc, active, lane);
+        if (lane == 0) depth_row[colx] = __ldg(a.planes + arg);
       }
       if (a.edge_write && y == a.y_b) {
 #pragma unroll
@@ -582,37 +638,17 @@ __global__ void __launch_bounds__(kRows * 32, 2) k_sgm_uniform(const UniArgs a) 
       if (x == c && y == a.H - 1) {  // the last band's revisits when no later visit of the column follows them
         for (int k = 0; k < a.end_count; k++) run_revisit<LPT>(a, a.end_first + k, lane, active);
       }
-      __syncwarp();
-      if (lane == 0) st_release_cta(prog + w, x + 1);  // the row above waits on it before reusing a ring slot
-      if (w == kRows - 1 && (((x & 3) == 3) || x == a.W - 1)) {  // the block below reads the last row from global memory
-        __threadfence();
-        __syncwarp();
-        if (lane == 0) st_release(a.progress + cb, x + 1);
-      }
-      // ---- rotate the prefetch queues ----
+      left.L = out[0];
+      left.mn = mins[0];
+      // ---- rotate the prefetch queue and fetch x+2 ----
       raw_q[0] = raw_q[1];
       agg_q[0] = agg_q[1];
       p2_q[0] = p2_q[1];
-      if (have2) {
-        raw_q[1] = raw_n;
-        agg_q[1] = agg_n;
-        p2_q[1] = p2_n;
-      }
-      if (w == 0 && x + 1 < a.W) {
-#pragma unroll
-        for (int p = 0; p < 3; p++) up[p] = up_n[p];
-      }
+      if (x + 2 < a.W) fetch_px(x + 2, raw_q[1], agg_q[1], p2_q[1]);
     }
   }
-  // rows that stopped early or do not exist still release their neighbours
   __syncwarp();
-  if (lane == 0) {
-    st_release_cta(prog + w, a.W);
-    if (w == kRows - 1) {
-      __threadfence();
-      st_release(a.progress + cb, a.W);
-    }
-  }
+  if (lane == 0) st_release_cta(prog + w, a.W);  // rows that stopped early or do not exist release their neighbours
 }
 
 // WTA of the last column of pass -1 (its aggregates are final only after the revisits).
@@ -682,7 +718,7 @@ static void launch_pass_t(const UniArgs& a, cudaStream_t s) {
     cudaFuncSetAttribute(k_sgm_uniform<LPT, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring_bytes<LPT>());
     configured = true;
   }
-  k_sgm_uniform<LPT, FULL><<<a.nCB, kRows * 32, ring_bytes<LPT>(), s>>>(a);
+  k_sgm_uniform<LPT, FULL><<<a.nCB, kWarps * 32, ring_bytes<LPT>(), s>>>(a);
   count_launches(1);
 }
 template <int LPT>
