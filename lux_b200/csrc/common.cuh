@@ -90,6 +90,7 @@ LUX_DEV bool wait_shared_at_least(const int* p, int target, const volatile int* 
   if (ld_acquire_cta(p) >= target) return true;
   const uint64_t t0 = global_ns();
   for (unsigned it = 0;; it++) {
+    __nanosleep(16);  // leave the issue slots to the warps that have work
     if (ld_acquire_cta(p) >= target) return true;
     if ((it & 63) == 63) {
       if (*stop) return false;

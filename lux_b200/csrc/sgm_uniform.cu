@@ -435,7 +435,7 @@ LUX_DEV void row_above(const UniArgs& a, const uint16_t* bnd_up, const uint16_t*
 // off the rows' own critical path.
 template <int LPT, bool FULL>
 __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a) {
-  constexpr int NR = LPT / 2, Dp = Dp_of(LPT), kBatch = 4;
+  constexpr int NR = LPT / 2, Dp = Dp_of(LPT), kBatch = 2;
   extern __shared__ __align__(16) uint16_t smem_ring[];
   auto ring = [&](int set, int slot, int p) { return smem_ring + (((size_t)set * kRing + slot) * 3 + p) * Dp; };
   uint16_t* ring_min = smem_ring + (size_t)(kRows + 1) * kRing * 3 * Dp;
@@ -458,9 +458,14 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
   const uint16_t* bnd_up_min = a.bnd_min + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3;
   uint16_t* bnd_me = a.bnd + (size_t)(cb % kBandBufs) * a.W * 3 * Dp;
   uint16_t* bnd_me_min = a.bnd_min + (size_t)(cb % kBandBufs) * a.W * 3;
-  // waits (bounded) on a progress counter of this block; a timeout stops the block
+  // waits (bounded) on a progress counter of this block; a timeout stops the block. The first check is one broadcast
+  // load for the whole warp, so the common case takes no divergent branch.
   auto wait_ctr = [&](int ctr, int need) {
-    if (lane == 0 && !wait_shared_at_least(prog + ctr, need, &s_stop, a.timeout_ns)) {
+    if (ld_acquire_cta(prog + ctr) >= need) return;
+    int ok = 1;
+    if (lane == 0) ok = wait_shared_at_least(prog + ctr, need, &s_stop, a.timeout_ns) ? 1 : 0;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    if (!ok && lane == 0) {
       atomicCAS(a.err, 0, 11);
       s_stop = 1;
     }
@@ -490,7 +495,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
           }
         }
         __syncwarp();
-        if (lane == 0) st_release_cta(prog + kRows, xe);
+        st_release_cta(prog + kRows, xe);
       }
     }
     __syncwarp();
@@ -514,10 +519,10 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
           }
         }
         __syncwarp();
-        if (lane == 0) st_release_cta(prog + kRows + 1, xe);  // the ring slots are free again
+        st_release_cta(prog + kRows + 1, xe);  // the ring slots are free again
         __threadfence();
         __syncwarp();
-        if (lane == 0) st_release(a.progress + cb, xe);
+        st_release(a.progress + cb, xe);
       }
     }
     __syncwarp();
@@ -622,7 +627,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
         }
       }
       __syncwarp();
-      if (lane == 0) st_release_cta(prog + w, x + 1);
+      st_release_cta(prog + w, x + 1);
       if (x != c && (a.dir > 0 || a.keep_agg)) agg_store<LPT>(agg_row + colx * a.n, acc, active);
       if (a.wta && x != c) {
         const int arg = wta_arg<LPT>(acc, active, lane);
