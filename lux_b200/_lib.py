@@ -70,6 +70,9 @@ SIGNATURES = [
     ("lux_sgm_upsample", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.POINTER(Img), ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_int32,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("lux_sgm_upsample_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                                ctypes.POINTER(Img), ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+                                                ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
 ]
 
 _lib = None

@@ -704,3 +704,60 @@ int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int3
 }
 
 }  // extern "C"
+
+// ---------------- allocation-free upsample ----------------
+namespace {
+
+// The resampled guidance (RGBA8 at the previous layer's size) of lux_sgm_upsample_noalloc lives in module-static device
+// memory, so that call allocates nothing. Every byte of it that the bilateral pass reads is written earlier in the same
+// call (k_shift_resize covers all pw·ph pixels), so nothing has to start at zero.
+constexpr size_t kNoAllocMaxPixels = LUX_UPSAMPLE_NOALLOC_MAX_PIXELS;
+static __device__ __align__(256) uint8_t g_upsample_scratch[kNoAllocMaxPixels * 4];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+void* g_scratch_ptr[kMaxDevices] = {};
+
+// The array's address on `device`, looked up once per device; the caller has made `device` current.
+int upsample_scratch(int device, uint8_t** out) {
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (device < 0 || device >= kMaxDevices) return LUX_ERR_ARG;
+  if (!g_scratch_ptr[device]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_upsample_scratch) != cudaSuccess || !p) return LUX_ERR_CUDA;
+    g_scratch_ptr[device] = p;
+  }
+  *out = static_cast<uint8_t*>(g_scratch_ptr[device]);
+  return LUX_OK;
+}
+
+}  // namespace
+
+extern "C" int lux_sgm_upsample_noalloc(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int32_t ph, const lux_img_rgba8* guide,
+                                        int32_t set_w, int32_t set_h, float sigma, int32_t scale, const float* prev_conf,
+                                        float* out_depth, float* out_conf) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!prev_depth || !guide || !out_depth || pw <= 0 || ph <= 0)
+    return set_err(ctx, LUX_ERR_ARG, "upsample_noalloc: null pointer or non-positive previous size");
+  if (!guide->data || !guide->on_device || guide->w <= 0 || guide->h <= 0 || guide->stride < guide->w)
+    return set_err(ctx, LUX_ERR_ARG, "upsample_noalloc: the guide must be a device image (on_device != 0, w, h > 0, stride >= w)");
+  const unsigned long long npp = (unsigned long long)pw * (unsigned long long)ph;
+  if (npp > kNoAllocMaxPixels)
+    return set_err(ctx, LUX_ERR_ARG, "upsample_noalloc: pw*ph = %llu exceeds the static scratch of %llu pixels", npp,
+                   (unsigned long long)kNoAllocMaxPixels);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, LUX_ERR_CUDA, "upsample_noalloc: cudaSetDevice failed");
+  uint8_t* g2 = nullptr;
+  int rc = upsample_scratch(ctx->device, &g2);
+  if (rc) return set_err(ctx, rc, "upsample_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(cudaGetLastError()));
+  const bool conf = prev_conf && out_conf;
+  launch_upsample(prev_depth, pw, ph, guide->data, guide->w, guide->h, guide->stride, sigma, ctx->d_rcp, g2, out_depth,
+                  conf ? prev_conf : nullptr, conf ? out_conf : nullptr, ctx->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return set_err(ctx, LUX_ERR_CUDA, "upsample_noalloc failed: %s", cudaGetErrorString(e));
+  // the size check comes after the computation in the reference too (DenseUpsampleLayer.cs:43)
+  if (guide->w != set_w * scale || guide->h != set_h * scale)
+    return set_err(ctx, LUX_ERR_UPSAMPLE_SIZE, "%s", default_message(LUX_ERR_UPSAMPLE_SIZE));
+  return LUX_OK;
+}
