@@ -99,6 +99,43 @@ LUX_DEV bool wait_shared_at_least(const int* p, int target, const volatile int* 
   }
 }
 
+// Shared-memory mbarriers: the hand-over between warps of one block. arrive releases (CTA scope) what the arriving
+// thread and, through a preceding __syncwarp, its warp wrote; a successful try_wait acquires it. A thread in try_wait is
+// suspended by the hardware until the phase completes or a time limit passes, so waiting warps take no issue slots.
+LUX_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+LUX_DEV void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+LUX_DEV void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// true once the phase of parity `parity` has completed
+LUX_DEV bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for a phase: gives up when *stop is set or after timeout_ns (then sets *err = 11 and *stop).
+LUX_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* stop, int* err, uint64_t timeout_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (unsigned it = 0;; it++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 7) == 7) {
+      if (*stop) return false;
+      if (global_ns() - t0 > timeout_ns) {
+        atomicCAS(err, 0, 11);
+        *stop = 1;
+        return false;
+      }
+    }
+  }
+}
+
 // Waits until *flag >= target; on timeout sets *err = code and returns false. Spins are bounded by wall time.
 LUX_DEV bool wait_at_least(const int* flag, int target, int* err, int code, uint64_t timeout_ns) {
   if (ld_acquire(flag) >= target) return true;

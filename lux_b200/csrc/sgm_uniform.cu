@@ -1,14 +1,18 @@
 // Fast aggregation of a uniform layer (every pixel searches planes [0, n), the first layer of a pyramid and every
 // plain pair): bit-exact with the reference's traversal (DenseStereoSgm.cs:181-324) through revisit_schedule.h.
 //
-// Shape: a CTA owns R consecutive rows of a pass (mirrored coordinates in pass -1), one warp per row, and walks the
-// row in lockstep: at step s warp w handles pixel x = s - 2w, so the row above always finished x+1 one step earlier.
-// All four paths of a pixel are fused, so each pass reads the raw volume once and touches the aggregates once:
-//   pass +1: agg = Σ paths;  pass -1: agg += Σ paths, then WTA (and the aggregates are stored only when kept).
+// Shape: a CTA owns kRows consecutive rows of a pass (mirrored coordinates in pass -1), one warp per row. Row y handles
+// pixel x once row y-1 has finished x+1, so the rows of a block run as a wavefront two pixels apart. All four paths of
+// a pixel are fused, so each pass reads the raw volume once and touches the aggregates once:
+//   pass +1: agg = sum of paths;  pass -1: agg += sum of paths, then WTA (the aggregates are stored only when kept).
 // A lane owns LPT consecutive planes as LPT/2 packed u16 pairs: min.u16x2 for the four-way minimum, byte permutes for
-// the d±1 neighbours, one shuffle per side across lanes, and redux.sync for the running minimum. The row above hands
-// paths 1-3 over through a 4-slot shared-memory ring; the first warp of a CTA reads the CTA above's last row from a
-// global band buffer, gated by that CTA's progress counter (bounded waits, tickets taken in order).
+// the d±1 neighbours, one shuffle per side across lanes, and redux.sync for the running minimum.
+// Hand-over: each row writes its path states 1-3 into a kRing-slot shared-memory ring; the row below waits on the
+// slot's full mbarrier and frees it through its empty mbarrier (waiting warps are suspended by the hardware, not
+// spinning). A loader warp fills the ring of the row above the block from a global band buffer, gated by the previous
+// block's progress counter; a publisher warp copies the block's last row out and releases its own counter every
+// kPublish pixels. Blocks take tickets in order, so a block only ever waits on a block that is already running; every
+// wait is bounded and a timeout stops the block with error 11.
 //
 // Exactness without saturation: with P2 <= p2base <= 1744 every stored L is at most 255 + 1744 < 2000 (the value of a
 // never-written word), the running minimum is at most 2000, and every candidate of the four-way minimum is at least
@@ -22,10 +26,11 @@
 
 namespace lux {
 
-constexpr int kRows = 6;       // rows of the recurrence per block (one warp each)
+constexpr int kRows = 14;      // rows of the recurrence per block (one warp each)
 constexpr int kWarps = kRows + 2;  // plus the loader and the publisher warps
 constexpr int kBandBufs = 4;   // band buffers in rotation
 constexpr int kRing = 8;       // slots of the hand-over ring between neighbouring rows of a block
+constexpr int kPublish = 4;    // the publisher releases the global band progress every kPublish pixels
 constexpr uint32_t kInit2 = 0x07d007d0u;  // 2000 | 2000
 
 LUX_DEV uint32_t vmin2(uint32_t a, uint32_t b) {
@@ -365,10 +370,11 @@ LUX_DEV void run_revisit(const UniArgs& a, int y, int lane, bool active) {
 }
 
 // Shared memory of a block: kRows + 1 hand-over rings (ring kRows is the row above the block, filled by the loader warp),
-// their minima, and the progress counters: rows 0..kRows-1, the loader (kRows), the publisher (kRows + 1).
+// their minima, and a full and an empty mbarrier per ring slot.
 template <int LPT>
 constexpr size_t ring_bytes() {
-  return (size_t)(kRows + 1) * kRing * 3 * Dp_of(LPT) * 2 + (size_t)(kRows + 1) * kRing * 3 * 2 + 16 + (size_t)(kRows + 2) * 4 + 16;
+  return (size_t)(kRows + 1) * kRing * 3 * Dp_of(LPT) * 2 + (size_t)(kRows + 1) * kRing * 3 * 2 + 16 +
+         (size_t)2 * (kRows + 1) * kRing * 8;
 }
 
 // Raw bytes of a lane's planes as loaded (8, 4 or 2 bytes), unpacked to u16 pairs when used.
@@ -434,13 +440,16 @@ LUX_DEV void row_above(const UniArgs& a, const uint16_t* bnd_up, const uint16_t*
 // waits only on its neighbours (shared-memory acquire/release), so the global latencies of the block boundary stay
 // off the rows' own critical path.
 template <int LPT, bool FULL>
-__global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a) {
+__global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a) {
   constexpr int NR = LPT / 2, Dp = Dp_of(LPT), kBatch = 2;
   extern __shared__ __align__(16) uint16_t smem_ring[];
   auto ring = [&](int set, int slot, int p) { return smem_ring + (((size_t)set * kRing + slot) * 3 + p) * Dp; };
   uint16_t* ring_min = smem_ring + (size_t)(kRows + 1) * kRing * 3 * Dp;
   auto rmin_at = [&](int set, int slot, int p) -> uint16_t& { return ring_min[((size_t)set * kRing + slot) * 3 + p]; };
-  int* prog = reinterpret_cast<int*>(ring_min + (size_t)(kRows + 1) * kRing * 3 + 8);
+  // full(set, slot): the producer of ring `set` filled the slot; empty(set, slot): its consumer is done with it
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring_min + (size_t)(kRows + 1) * kRing * 3 + 8);
+  auto full = [&](int set, int slot) { return bars + set * kRing + slot; };
+  auto empty = [&](int set, int slot) { return bars + (kRows + 1) * kRing + set * kRing + slot; };
   __shared__ int s_cb;
   __shared__ volatile int s_stop;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -448,7 +457,7 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
     s_cb = atomicAdd(a.ticket, 1);
     s_stop = 0;
   }
-  if (tid < kRows + 2) prog[tid] = 0;
+  if (tid < 2 * (kRows + 1) * kRing) mbar_init(bars + tid, 1);
   __syncthreads();
   const int cb = s_cb;
   const int y0 = cb * kRows;
@@ -458,18 +467,14 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
   const uint16_t* bnd_up_min = a.bnd_min + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3;
   uint16_t* bnd_me = a.bnd + (size_t)(cb % kBandBufs) * a.W * 3 * Dp;
   uint16_t* bnd_me_min = a.bnd_min + (size_t)(cb % kBandBufs) * a.W * 3;
-  // waits (bounded) on a progress counter of this block; a timeout stops the block. The first check is one broadcast
-  // load for the whole warp, so the common case takes no divergent branch.
-  auto wait_ctr = [&](int ctr, int need) {
-    if (ld_acquire_cta(prog + ctr) >= need) return;
-    int ok = 1;
-    if (lane == 0) ok = wait_shared_at_least(prog + ctr, need, &s_stop, a.timeout_ns) ? 1 : 0;
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (!ok && lane == 0) {
-      atomicCAS(a.err, 0, 11);
-      s_stop = 1;
-    }
-    __syncwarp();
+  // Slot x & (kRing - 1) of a ring holds pixel x; it completes phase x / kRing of its full barrier when filled and,
+  // once the consumer is done with it, phase x / kRing of its empty barrier. Waits are bounded: a timeout stops the
+  // block (error 11) and every other wait of the block then gives up.
+  auto wait_filled = [&](int set, int x) {  // pixel x of ring `set` is there
+    return mbar_wait(full(set, x & (kRing - 1)), (uint32_t)(x / kRing) & 1u, &s_stop, a.err, a.timeout_ns);
+  };
+  auto wait_free = [&](int set, int x) {  // the slot of pixel x no longer holds pixel x - kRing for the consumer
+    return x < kRing || mbar_wait(empty(set, x & (kRing - 1)), (uint32_t)(x / kRing - 1) & 1u, &s_stop, a.err, a.timeout_ns);
   };
 
   if (w == kRows) {
@@ -477,9 +482,12 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
     if (y0 < a.H) {
       for (int xb = 0; xb < a.W && !s_stop; xb += kBatch) {
         const int xe = min(a.W, xb + kBatch);
-        if (xe - 1 >= kRing - 1) wait_ctr(0, xe - kRing + 1);  // row 0 is done with these slots
+        bool ok = true;
+        for (int x = xb; x < xe && ok; x++) ok = wait_free(kRows, x);  // row 0 is done with these slots
+        if (!ok) break;
         if (cb > 0 && lane == 0 && !wait_at_least(a.progress + (cb - 1), xe, a.err, 11, a.timeout_ns)) s_stop = 1;
         __syncwarp();
+        if (s_stop) break;
         Src<LPT> u[kBatch][3];
 #pragma unroll
         for (int k = 0; k < kBatch; k++)
@@ -495,50 +503,39 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
           }
         }
         __syncwarp();
-        st_release_cta(prog + kRows, xe);
+        if (lane == 0)
+          for (int x = xb; x < xe; x++) mbar_arrive(full(kRows, x & (kRing - 1)));
       }
     }
-    __syncwarp();
-    if (lane == 0) st_release_cta(prog + kRows, a.W);
     return;
   }
   if (w == kRows + 1) {
     // ---------------- publisher: the block's last row into the global band buffer ----------------
     if (below_exists) {
-      for (int xb = 0; xb < a.W && !s_stop; xb += kBatch) {
-        const int xe = min(a.W, xb + kBatch);
-        wait_ctr(kRows - 1, xe);
-        for (int x = xb; x < xe; x++) {
-          const int sl = x & (kRing - 1);
+      for (int x = 0; x < a.W; x++) {
+        if (!wait_filled(kRows - 1, x)) break;
+        const int sl = x & (kRing - 1);
 #pragma unroll
-          for (int p = 0; p < 3; p++) {
-            V<LPT> v;
-            vload_s<LPT>(v, ring(kRows - 1, sl, p), lane);
-            vstore<LPT>(v, bnd_me + ((size_t)x * 3 + p) * Dp, lane);
-            if (lane == 0) __stcg(bnd_me_min + (size_t)x * 3 + p, rmin_at(kRows - 1, sl, p));
-          }
+        for (int p = 0; p < 3; p++) {
+          V<LPT> v;
+          vload_s<LPT>(v, ring(kRows - 1, sl, p), lane);
+          vstore<LPT>(v, bnd_me + ((size_t)x * 3 + p) * Dp, lane);
+          if (lane == 0) __stcg(bnd_me_min + (size_t)x * 3 + p, rmin_at(kRows - 1, sl, p));
         }
         __syncwarp();
-        st_release_cta(prog + kRows + 1, xe);  // the ring slots are free again
-        __threadfence();
-        __syncwarp();
-        st_release(a.progress + cb, xe);
+        if (lane == 0) mbar_arrive(empty(kRows - 1, x & (kRing - 1)));  // the ring slot is free again
+        if ((x + 1) % kPublish == 0) st_release(a.progress + cb, x + 1);  // the next block's loader polls this
       }
     }
     __syncwarp();
-    if (lane == 0) {
-      st_release_cta(prog + kRows + 1, a.W);
-      __threadfence();
-      st_release(a.progress + cb, a.W);
-    }
+    if (lane == 0) st_release(a.progress + cb, a.W);
     return;
   }
 
   // ---------------- a row of the recurrence ----------------
   const int y = y0 + w;  // row of the pass
   const bool row_ok = y < a.H;
-  const int up_set = w == 0 ? kRows : w - 1;            // the ring (and counter) holding the row above
-  const int cons_ctr = w + 1 < kRows ? w + 1 : kRows + 1;  // who reads this row's ring
+  const int up_set = w == 0 ? kRows : w - 1;  // the ring holding the row above
   const bool has_consumer = y + 1 < a.H;
   const int c = a.W - 1;
   const uint32_t p1x2 = dup16((uint32_t)a.p1);
@@ -569,9 +566,8 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
     fetch_px(1, raw_q[1], agg_q[1], p2_q[1]);
     for (int x = 0; x < a.W; x++) {
       // ---- hand-over in: the row above finished x+1; the next row is done with the ring slot this pixel reuses ----
-      wait_ctr(up_set, min(a.W, x + 2));
-      if (has_consumer && x >= kRing - 1) wait_ctr(cons_ctr, x - kRing + 2);
-      if (s_stop) break;
+      if (x + 1 < a.W && !wait_filled(up_set, x + 1)) break;
+      if (has_consumer && !wait_free(w, x)) break;
       // ---- revisits that the reference runs before this visit (they may produce this visit's path-2 input) ----
       if (x == c) {
         const int cnt = a.batch_count[y], first = a.batch_first[y];
@@ -627,7 +623,10 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
         }
       }
       __syncwarp();
-      st_release_cta(prog + w, x + 1);
+      if (lane == 0) {
+        mbar_arrive(full(w, sl));                                    // pixel x is in the ring
+        if (x >= 1) mbar_arrive(empty(up_set, (x - 1) & (kRing - 1)));  // the row above's pixel x-1 is no longer read
+      }
       if (x != c && (a.dir > 0 || a.keep_agg)) agg_store<LPT>(agg_row + colx * a.n, acc, active);
       if (a.wta && x != c) {
         const int arg = wta_arg<LPT>(acc, active, lane);
@@ -652,8 +651,6 @@ __global__ void __launch_bounds__(kWarps * 32, 2) k_sgm_uniform(const UniArgs a)
       if (x + 2 < a.W) fetch_px(x + 2, raw_q[1], agg_q[1], p2_q[1]);
     }
   }
-  __syncwarp();
-  if (lane == 0) st_release_cta(prog + w, a.W);  // rows that stopped early or do not exist release their neighbours
 }
 
 // WTA of the last column of pass -1 (its aggregates are final only after the revisits).
