@@ -18,6 +18,7 @@
 // never-written word), the running minimum is at most 2000, and every candidate of the four-way minimum is at least
 // the previous minimum, so raw + m - minPrev never leaves [0, 65535] and 16 path contributions never exceed 65535.
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -439,7 +440,7 @@ LUX_DEV void row_above(const UniArgs& a, const uint16_t* bnd_up, const uint16_t*
 // kRows; warp kRows+1 (publisher) copies the block's last row to the global band buffer for the block below. A row
 // waits only on its neighbours (shared-memory acquire/release), so the global latencies of the block boundary stay
 // off the rows' own critical path.
-template <int LPT, bool FULL>
+template <int LPT, bool FULL, bool PASS2>
 __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a) {
   constexpr int NR = LPT / 2, Dp = Dp_of(LPT), kBatch = 2;
   extern __shared__ __align__(16) uint16_t smem_ring[];
@@ -452,7 +453,10 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
   auto empty = [&](int set, int slot) { return bars + (kRows + 1) * kRing + set * kRing + slot; };
   __shared__ int s_cb;
   __shared__ volatile int s_stop;
+  __shared__ float s_planes[256];  // the WTA's plane depths (pass -1)
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (PASS2)
+    for (int i = tid; i < a.n; i += blockDim.x) s_planes[i] = a.planes[i];
   if (tid == 0) {
     s_cb = atomicAdd(a.ticket, 1);
     s_stop = 0;
@@ -534,122 +538,161 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
 
   // ---------------- a row of the recurrence ----------------
   const int y = y0 + w;  // row of the pass
-  const bool row_ok = y < a.H;
+  if (y >= a.H) return;
   const int up_set = w == 0 ? kRows : w - 1;  // the ring holding the row above
   const bool has_consumer = y + 1 < a.H;
   const int c = a.W - 1;
   const uint32_t p1x2 = dup16((uint32_t)a.p1);
-  const int yu = a.dir > 0 ? y : a.H - 1 - y;
-  const long long x0 = a.dir > 0 ? 0 : a.W - 1, xs = a.dir > 0 ? 1 : -1;
-  const uint8_t* raw_row = a.raw + ((size_t)(row_ok ? yu : 0) * a.W) * a.n + lane * LPT;
-  uint16_t* agg_row = a.agg + ((size_t)(row_ok ? yu : 0) * a.W) * a.n + lane * LPT;
-  const uint2* p2_row = a.p2t + (size_t)(row_ok ? y : 0) * a.W;
-  float* depth_row = a.depth + (size_t)(row_ok ? yu : 0) * a.W;
+  const int yu = PASS2 ? a.H - 1 - y : y;
+  // pixel x of the pass is column x0 + xs·x of the image
+  const long long x0 = PASS2 ? a.W - 1 : 0, xs = PASS2 ? -1 : 1;
+  const uint8_t* raw_row = a.raw + (size_t)yu * a.W * a.n + lane * LPT;
+  uint16_t* agg_row = a.agg + (size_t)yu * a.W * a.n + lane * LPT;
+  const uint2* p2_row = a.p2t + (size_t)y * a.W;
+  float* depth_row = a.depth + (size_t)yu * a.W;
+  const int flags = a.flags[y];
+  const bool edge_row = !PASS2 && y == a.y_b;  // pass +1's row y_b is what pass -1 reads above its first row
   Src<LPT> left;  // path 0: the pixel to the left
   src_init(left);
-  RawB<LPT> raw_q[2];  // raw bytes of x, x+1 (a two-deep prefetch)
-  V<LPT> agg_q[2];     // pass -1: pass +1's aggregates of x, x+1
-  uint2 p2_q[2];       // P2 of x, x+1
-  const int flags = row_ok ? a.flags[y] : 0;
-  auto fetch_px = [&](int xq, RawB<LPT>& rb, V<LPT>& ag, uint2& p2) {
+  struct Queued {  // what a pixel reads from HBM, fetched two pixels ahead
+    RawB<LPT> raw;
+    V<LPT> agg;  // pass -1: pass +1's aggregates
+    uint2 p2;
+  };
+  auto fetch = [&](int xq, Queued& q) {
     const long long col = x0 + xs * xq;
     const uint8_t* rp = raw_row + col * a.n;
-    if (!active) { rb.r[0] = 0; if constexpr (LPT >= 8) rb.r[1] = 0; }
-    else if constexpr (LPT == 8) { uint2 t = __ldcs(reinterpret_cast<const uint2*>(rp)); rb.r[0] = t.x; rb.r[1] = t.y; }
-    else if constexpr (LPT == 4) rb.r[0] = __ldcs(reinterpret_cast<const unsigned int*>(rp));
-    else rb.r[0] = __ldcs(reinterpret_cast<const unsigned short*>(rp));
-    if (a.dir < 0) agg_load<LPT>(agg_row + col * a.n, ag, active);
-    p2 = __ldg(p2_row + xq);
+    if (!active) {
+      q.raw.r[0] = 0;
+      if constexpr (LPT >= 8) q.raw.r[1] = 0;
+    } else if constexpr (LPT == 8) {
+      const uint2 t = __ldcs(reinterpret_cast<const uint2*>(rp));
+      q.raw.r[0] = t.x;
+      q.raw.r[1] = t.y;
+    } else if constexpr (LPT == 4) {
+      q.raw.r[0] = __ldcs(reinterpret_cast<const unsigned int*>(rp));
+    } else {
+      q.raw.r[0] = __ldcs(reinterpret_cast<const unsigned short*>(rp));
+    }
+    if constexpr (PASS2) agg_load<LPT>(agg_row + col * a.n, q.agg, active);
+    q.p2 = __ldg(p2_row + xq);
   };
-  if (row_ok) {
-    fetch_px(0, raw_q[0], agg_q[0], p2_q[0]);
-    fetch_px(1, raw_q[1], agg_q[1], p2_q[1]);
-    for (int x = 0; x < a.W; x++) {
-      // ---- hand-over in: the row above finished x+1; the next row is done with the ring slot this pixel reuses ----
-      if (x + 1 < a.W && !wait_filled(up_set, x + 1)) break;
-      if (has_consumer && !wait_free(w, x)) break;
-      // ---- revisits that the reference runs before this visit (they may produce this visit's path-2 input) ----
-      if (x == c) {
-        const int cnt = a.batch_count[y], first = a.batch_first[y];
-        for (int k = 0; k < cnt; k++) run_revisit<LPT>(a, first + k, lane, active);
-      }
-      // ---- neighbour states: paths 1, 2, 3 read pixels x-1, x, x+1 of row y-1 ----
-      V<LPT> nbL[4];
-      uint32_t mp[4];
-      nbL[0] = left.L;
-      mp[0] = left.mn;
+  // One visit N(x, y). KIND: 0 the first column, 1 a column with both neighbours and no revisit business, 2 the column
+  // c-1 (its path states 0 and 1 are kept for the revisits), 3 the last column c (revisits, the special path-2 read).
+  auto pixel = [&](int x, Queued& q, auto kind) -> bool {
+    constexpr int KIND = decltype(kind)::value;
+    // ---- hand-over in: the row above finished x+1; the next row is done with the ring slot this pixel reuses ----
+    if constexpr (KIND != 3) {
+      if (!wait_filled(up_set, x + 1)) return false;
+    }
+    if (has_consumer && !wait_free(w, x)) return false;
+    // ---- revisits that the reference runs before this visit (they may produce this visit's path-2 input) ----
+    if constexpr (KIND == 3) {
+      const int cnt = a.batch_count[y], first = a.batch_first[y];
+      for (int k = 0; k < cnt; k++) run_revisit<LPT>(a, first + k, lane, active);
+    }
+    // ---- neighbour states: path 0 the pixel to the left, paths 1, 2, 3 pixels x-1, x, x+1 of row y-1 ----
+    V<LPT> nbL[4];
+    uint32_t mp[4];
+    nbL[0] = left.L;
+    mp[0] = left.mn;
 #pragma unroll
-      for (int p = 1; p < 4; p++) {
-        const int xn = x + (p == 1 ? -1 : p == 2 ? 0 : 1);
-        if (xn < 0 || xn >= a.W) { vinit(nbL[p]); mp[p] = 2000; continue; }
-        const int sl = xn & (kRing - 1);
-        vload_s<LPT>(nbL[p], ring(up_set, sl, p - 1), lane);
-        mp[p] = rmin_at(up_set, sl, p - 1);
+    for (int p = 1; p < 4; p++) {
+      if ((KIND == 0 && p == 1) || (KIND == 3 && p == 3)) {  // outside the image: a never-written slot
+        vinit(nbL[p]);
+        mp[p] = 2000;
+        continue;
       }
-      if (x == c && (flags & 1)) {  // N(c).p2 reads R(c, y-1)
+      const int sl = (x + p - 2) & (kRing - 1);
+      vload_s<LPT>(nbL[p], ring(up_set, sl, p - 1), lane);
+      mp[p] = rmin_at(up_set, sl, p - 1);
+    }
+    if constexpr (KIND == 3) {
+      if (flags & 1) {  // N(c).p2 reads R(c, y-1)
         Src<LPT> r;
         src_cs<LPT>(a, r, y - 1, 4, c, lane);
         nbL[2] = r.L;
         mp[2] = r.mn;
       }
-      // ---- the four paths ----
-      const uint2 p2v = p2_q[0];
-      const uint32_t p2[4] = {p2v.x & 0xffffu, p2v.x >> 16, p2v.y & 0xffffu, p2v.y >> 16};
-      V<LPT> raw2, acc, out[4];
-      raw_unpack<LPT>(raw_q[0], raw2);
-      if (a.dir > 0) {
+    }
+    // ---- the four paths ----
+    const uint32_t p2[4] = {q.p2.x & 0xffffu, q.p2.x >> 16, q.p2.y & 0xffffu, q.p2.y >> 16};
+    V<LPT> raw2, acc, out[4];
+    raw_unpack<LPT>(q.raw, raw2);
+    if constexpr (PASS2) {
+      acc = q.agg;
+    } else {
 #pragma unroll
-        for (int i = 0; i < NR; i++) acc.r[i] = 0;
-      } else {
-        acc = agg_q[0];
+      for (int i = 0; i < NR; i++) acc.r[i] = 0;
+    }
+    uint32_t mins[4];
+    four_paths<LPT, FULL>(nbL, mp, p2, p1x2, raw2, active, lane, out, acc, mins);
+    // ---- hand-over out: the ring first, then the release; global stores after it ----
+    const int sl = x & (kRing - 1);
+#pragma unroll
+    for (int p = 1; p < 4; p++) {
+      vstore_s<LPT>(out[p], ring(w, sl, p - 1), lane);
+      if (lane == 0) rmin_at(w, sl, p - 1) = (uint16_t)mins[p];
+    }
+    uint16_t* ap = agg_row + (x0 + xs * x) * a.n;
+    if constexpr (KIND == 2) {  // what later revisits of this block read is stored before the release
+      cs_put<LPT>(a, out[0], mins[0], y, 0, lane);
+      cs_put<LPT>(a, out[1], mins[1], y, 1, lane);
+    }
+    if constexpr (KIND == 3) {
+      cs_put<LPT>(a, out[2], mins[2], y, 2, lane);
+      agg_store<LPT>(ap, acc, active);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      mbar_arrive(full(w, sl));                                                          // pixel x is in the ring
+      if constexpr (KIND != 0) mbar_arrive(empty(up_set, (x - 1) & (kRing - 1)));  // the row above's x-1 is done
+    }
+    if constexpr (KIND != 3) {
+      if (!PASS2 || a.keep_agg) agg_store<LPT>(ap, acc, active);
+      if constexpr (PASS2) {  // WTA; the last column waits for its revisits (k_wta_column)
+        const int arg = wta_arg<LPT>(acc, active, lane);
+        if (lane == 0) depth_row[x0 + xs * x] = s_planes[arg];
       }
-      uint32_t mins[4];
-      four_paths<LPT, FULL>(nbL, mp, p2, p1x2, raw2, active, lane, out, acc, mins);
-      // ---- hand-over out: the ring first, then the release; global stores after it ----
-      const int sl = x & (kRing - 1);
+    }
+    if (edge_row) {
 #pragma unroll
       for (int p = 1; p < 4; p++) {
-        vstore_s<LPT>(out[p], ring(w, sl, p - 1), lane);
-        if (lane == 0) rmin_at(w, sl, p - 1) = (uint16_t)mins[p];
+        vstore<LPT>(out[p], a.edge + ((size_t)x * 3 + (p - 1)) * Dp, lane);
+        if (lane == 0) __stcg(a.edge_min + (size_t)x * 3 + (p - 1), (uint16_t)mins[p]);
       }
-      const long long colx = x0 + xs * x;
-      if (x >= c - 1) {  // what later revisits of this block read must be stored before the release
-        if (x == c - 1) {
-          cs_put<LPT>(a, out[0], mins[0], y, 0, lane);
-          cs_put<LPT>(a, out[1], mins[1], y, 1, lane);
-        } else {
-          cs_put<LPT>(a, out[2], mins[2], y, 2, lane);
-          agg_store<LPT>(agg_row + colx * a.n, acc, active);
-        }
-      }
-      __syncwarp();
-      if (lane == 0) {
-        mbar_arrive(full(w, sl));                                    // pixel x is in the ring
-        if (x >= 1) mbar_arrive(empty(up_set, (x - 1) & (kRing - 1)));  // the row above's pixel x-1 is no longer read
-      }
-      if (x != c && (a.dir > 0 || a.keep_agg)) agg_store<LPT>(agg_row + colx * a.n, acc, active);
-      if (a.wta && x != c) {
-        const int arg = wta_arg<LPT>(acc, active, lane);
-        if (lane == 0) depth_row[colx] = __ldg(a.planes + arg);
-      }
-      if (a.edge_write && y == a.y_b) {
-#pragma unroll
-        for (int p = 1; p < 4; p++) {
-          vstore<LPT>(out[p], a.edge + ((size_t)x * 3 + (p - 1)) * Dp, lane);
-          if (lane == 0) __stcg(a.edge_min + (size_t)x * 3 + (p - 1), (uint16_t)mins[p]);
-        }
-      }
-      if (x == c && y == a.H - 1) {  // the last band's revisits when no later visit of the column follows them
-        for (int k = 0; k < a.end_count; k++) run_revisit<LPT>(a, a.end_first + k, lane, active);
-      }
-      left.L = out[0];
-      left.mn = mins[0];
-      // ---- rotate the prefetch queue and fetch x+2 ----
-      raw_q[0] = raw_q[1];
-      agg_q[0] = agg_q[1];
-      p2_q[0] = p2_q[1];
-      if (x + 2 < a.W) fetch_px(x + 2, raw_q[1], agg_q[1], p2_q[1]);
     }
+    if constexpr (KIND == 3) {
+      if (y == a.H - 1)  // the last band's revisits when no later visit of the column follows them
+        for (int k = 0; k < a.end_count; k++) run_revisit<LPT>(a, a.end_first + k, lane, active);
+    }
+    left.L = out[0];
+    left.mn = mins[0];
+    if constexpr (KIND <= 1) fetch(x + 2, q);  // x + 2 <= c
+    return true;
+  };
+  using K0 = std::integral_constant<int, 0>;
+  using K1 = std::integral_constant<int, 1>;
+  using K2 = std::integral_constant<int, 2>;
+  using K3 = std::integral_constant<int, 3>;
+  // Pixel x reads queue entry x & 1, so the two-deep prefetch needs no register moves.
+  Queued q0, q1;
+  fetch(0, q0);
+  fetch(1, q1);
+  if (!pixel(0, q0, K0{})) return;
+  int x = 1;
+  for (; x + 1 <= c - 2; x += 2) {
+    if (!pixel(x, q1, K1{})) return;
+    if (!pixel(x + 1, q0, K1{})) return;
+  }
+  if (x <= c - 2) {
+    if (!pixel(x, q1, K1{})) return;
+    x++;
+  }
+  if (x & 1) {
+    if (pixel(c - 1, q1, K2{})) pixel(c, q0, K3{});
+  } else {
+    if (pixel(c - 1, q0, K2{})) pixel(c, q1, K3{});
   }
 }
 
@@ -713,20 +756,26 @@ size_t uniform_scratch_bytes(int W, int H, int n, int tile) {
   return layout_of(W, H, n).total;
 }
 
-template <int LPT, bool FULL>
+template <int LPT, bool FULL, bool PASS2>
 static void launch_pass_t(const UniArgs& a, cudaStream_t s) {
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(k_sgm_uniform<LPT, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring_bytes<LPT>());
+    cudaFuncSetAttribute(k_sgm_uniform<LPT, FULL, PASS2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring_bytes<LPT>());
     configured = true;
   }
-  k_sgm_uniform<LPT, FULL><<<a.nCB, kWarps * 32, ring_bytes<LPT>(), s>>>(a);
+  k_sgm_uniform<LPT, FULL, PASS2><<<a.nCB, kWarps * 32, ring_bytes<LPT>(), s>>>(a);
   count_launches(1);
 }
 template <int LPT>
 static void launch_pass(const UniArgs& a, cudaStream_t s) {
-  if (a.n == 32 * LPT) launch_pass_t<LPT, true>(a, s);
-  else launch_pass_t<LPT, false>(a, s);
+  const bool full = a.n == 32 * LPT;
+  if (a.dir > 0) {
+    if (full) launch_pass_t<LPT, true, false>(a, s);
+    else launch_pass_t<LPT, false, false>(a, s);
+  } else {
+    if (full) launch_pass_t<LPT, true, true>(a, s);
+    else launch_pass_t<LPT, false, true>(a, s);
+  }
 }
 
 int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
