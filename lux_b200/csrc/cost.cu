@@ -2,14 +2,17 @@
 //
 // One warp per reference pixel, lanes over planes. Per other camera and plane: the projection through the flow matrix
 // (no FMA, IEEE 1/pz; the plane-only terms z·W2 + W3 come from a per-layer table), the half-pixel `pavgb` resampling
-// of a 4x4 target block, capped |diff| of the 3x3 blocks, the fixed-point channel weights, and a u16 wrap-sum over
+// of the target block, capped |diff| of the 3x3 blocks, the fixed-point channel weights, and a u16 wrap-sum over
 // cameras. A plane whose position repeats or leaves the valid rect reuses the last computed cost (:273-274): the warp
 // finds that plane with a ballot and carries it across chunks of 32 planes.
 //
-// Byte arithmetic: a grey camera (weights {12240, 0, 0, 0}) only ever contributes its Y channel, so its block cost is
-// nine scalar byte differences. A colour camera splits each RGBA word into two u16x2 lanes (Y|V and U|A) and uses
-// min/max.u16x2 for |a-b| and the caps. Both are exact restatements of the byte-lane sums of the reference (each
-// channel sum is at most 9·6, so nothing carries between lanes).
+// Half-pixel phases: the resampled block value at (x, y) with fractions (hx, hy) is pavgb over rows first, then over
+// columns, of the 2x2 neighbourhood at (x, y) (:248-253); it depends on (x, y, hx, hy) only, so k_phase_* writes the four
+// phase images of every other camera once per layer and a plane's 3x3 block is three row loads with no averaging:
+//   grey camera (weights {12240, 0, 0, 0}, only Y contributes): one u32 per pixel and phase holding the Y bytes of
+//     columns x..x+3, so a block row is one aligned load; |t - r| capped at 2 in u16x2 lanes (min/max.u16x2);
+//   colour camera: the RGBA word per pixel and phase; even bytes (Y, V) and odd bytes (U, A) as u16x2 lanes.
+// Both are exact restatements of the reference's byte-lane sums (each channel sum is at most 9·6).
 #include "common.cuh"
 #include "internal.h"
 
@@ -25,60 +28,73 @@ LUX_DEV uint32_t vmax2c(uint32_t a, uint32_t b) {
   asm("max.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
   return d;
 }
-LUX_DEV int yb(uint32_t w) { return (int)(w & 0xffu); }
-LUX_DEV int avg_u8(int a, int b) { return (a + b + 1) >> 1; }  // pavgb on one byte
-// pavgb on the u16x2 lanes of byte values
-LUX_DEV uint32_t avg_u16x2(uint32_t a, uint32_t b) { return ((a + b + 0x00010001u) >> 1) & 0x00ff00ffu; }
+LUX_DEV uint32_t absdiff2(uint32_t a, uint32_t b) { return vmax2c(a, b) - vmin2c(a, b); }  // per u16 lane, no borrow
+LUX_DEV int avg_u8(int a, int b) { return (a + b + 1) >> 1; }                 // pavgb on one byte
 
-// Grey camera: S0 = Σ min(|t - r|, 2) over the 3x3 block of Y values (rows averaged first, then pixels).
-template <int HX, int HY>
-LUX_DEV int grey_block(const uint32_t* __restrict__ base, int iw, const int (&ry)[3][3]) {
-  int s = 0;
-#pragma unroll
-  for (int q = 0; q < 3; q++) {
-    int row[4];
-#pragma unroll
-    for (int p = 0; p < 3 + HX; p++) {
-      int v = yb(__ldg(base + (size_t)q * iw + p));
-      if (HY) v = avg_u8(v, yb(__ldg(base + (size_t)(q + 1) * iw + p)));
-      row[p] = v;
-    }
-#pragma unroll
-    for (int p = 0; p < 3; p++) {
-      const int v = HX ? avg_u8(row[p], row[p + 1]) : row[p];
-      s += min(abs(v - ry[q][p]), 2);
-    }
+// The phase-h value (h = 2·hy + hx) of byte channel `ch` at (x, y): rows averaged first, then columns. Only positions
+// whose 2x2 neighbourhood lies in the image are ever read by the cost; the others are clamped.
+LUX_DEV int phase_byte(const uint8_t* img, int iw, int ih, int x, int y, int h, int ch) {
+  const int x1 = min(x + 1, iw - 1), y1 = min(y + 1, ih - 1);
+  auto at = [&](int xx, int yy) { return (int)img[((size_t)yy * iw + xx) * 4 + ch]; };
+  int a = at(x, y), b = at(x1, y);
+  if (h & 2) {
+    a = avg_u8(a, at(x, y1));
+    b = avg_u8(b, at(x1, y1));
   }
-  return (s * 12240 + 16) >> 5;
+  return (h & 1) ? avg_u8(a, b) : a;
 }
 
-// Colour camera: even bytes (Y, V) and odd bytes (U, A) as u16 pairs.
-template <int HX, int HY>
-LUX_DEV int colour_block(const uint32_t* __restrict__ base, int iw, const uint32_t (&re)[3][3], const uint32_t (&ro)[3][3],
-                         const uint16_t (&wq)[4]) {
-  const uint32_t capE = 0x00060002u, capO = 0x00000006u;  // {Y:2, V:6} and {U:6, A:0}
+// Grey: out[h][y][x] = Y bytes of phase h at columns x, x+1, x+2, x+3 (little-endian).
+__global__ void k_phase_grey(const uint8_t* __restrict__ img, int iw, int ih, uint32_t* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= iw) return;
+#pragma unroll
+  for (int h = 0; h < 4; h++) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) v |= (uint32_t)phase_byte(img, iw, ih, min(x + j, iw - 1), y, h, 0) << (8 * j);
+    out[((size_t)h * ih + y) * iw + x] = v;
+  }
+}
+// Colour: out[h][y][x] = the RGBA word of phase h.
+__global__ void k_phase_colour(const uint8_t* __restrict__ img, int iw, int ih, uint32_t* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= iw) return;
+#pragma unroll
+  for (int h = 0; h < 4; h++) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int ch = 0; ch < 4; ch++) v |= (uint32_t)phase_byte(img, iw, ih, x, y, h, ch) << (8 * ch);
+    out[((size_t)h * ih + y) * iw + x] = v;
+  }
+}
+
+// Grey block: S0 = Σ min(|t - r|, 2) over the 3x3 Y block; row q of the target is one word (bytes t0..t2 used, the
+// fourth lane's cap is 0). re/ro: the reference row's even bytes (r0 | r2 << 16) and odd byte (r1).
+LUX_DEV int grey_cost(const uint32_t* __restrict__ q, int iw, const uint32_t (&re)[3], const uint32_t (&ro)[3]) {
+  uint32_t s = 0;
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const uint32_t t = __ldg(q + (size_t)r * iw);
+    const uint32_t te = __byte_perm(t, 0, 0x4240), to = __byte_perm(t, 0, 0x4341);
+    s += vmin2c(absdiff2(te, re[r]), 0x00020002u) + vmin2c(absdiff2(to, ro[r]), 0x00000002u);
+  }
+  const int S0 = (int)((s & 0xffffu) + (s >> 16));
+  return (S0 * 12240 + 16) >> 5;
+}
+
+// Colour block: even bytes (Y, V) and odd bytes (U, A) as u16 pairs, caps {Y:2, V:6} and {U:6, A:0}.
+LUX_DEV int colour_cost(const uint32_t* __restrict__ q, int iw, const uint32_t (&re)[3][3], const uint32_t (&ro)[3][3],
+                        const uint16_t (&wq)[4]) {
+  const uint32_t capE = 0x00060002u, capO = 0x00000006u;
   uint32_t se = 0, so = 0;
 #pragma unroll
-  for (int q = 0; q < 3; q++) {
-    uint32_t e[4], o[4];
-#pragma unroll
-    for (int p = 0; p < 3 + HX; p++) {
-      uint32_t w = __ldg(base + (size_t)q * iw + p);
-      uint32_t ev = w & 0x00ff00ffu, od = (w >> 8) & 0x00ff00ffu;
-      if (HY) {
-        uint32_t w2 = __ldg(base + (size_t)(q + 1) * iw + p);
-        ev = avg_u16x2(ev, w2 & 0x00ff00ffu);
-        od = avg_u16x2(od, (w2 >> 8) & 0x00ff00ffu);
-      }
-      e[p] = ev;
-      o[p] = od;
-    }
+  for (int r = 0; r < 3; r++) {
 #pragma unroll
     for (int p = 0; p < 3; p++) {
-      const uint32_t ve = HX ? avg_u16x2(e[p], e[p + 1]) : e[p];
-      const uint32_t vo = HX ? avg_u16x2(o[p], o[p + 1]) : o[p];
-      se += vmin2c(vmax2c(ve, re[q][p]) - vmin2c(ve, re[q][p]), capE);
-      so += vmin2c(vmax2c(vo, ro[q][p]) - vmin2c(vo, ro[q][p]), capO);
+      const uint32_t w = __ldg(q + (size_t)r * iw + p);
+      se += vmin2c(absdiff2(w & 0x00ff00ffu, re[r][p]), capE);
+      so += vmin2c(absdiff2((w >> 8) & 0x00ff00ffu, ro[r][p]), capO);
     }
   }
   const int S0 = se & 0xffff, S2 = se >> 16, S1 = so & 0xffff, S3 = so >> 16;
@@ -87,8 +103,8 @@ LUX_DEV int colour_block(const uint32_t* __restrict__ base, int iw, const uint32
 }
 
 template <bool GREY>
-__global__ void __launch_bounds__(256) k_cost(const CostArgs a, const LayerGeom g, const float* __restrict__ zt, uint8_t* __restrict__ raw,
-                                              int* err) {
+__global__ void __launch_bounds__(256) k_cost(const CostArgs a, const LayerGeom g, const float4* __restrict__ zt,
+                                              uint8_t* __restrict__ raw, int* err) {
   __shared__ int s_carry[8][kMaxCams];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -97,7 +113,12 @@ __global__ void __launch_bounds__(256) k_cost(const CostArgs a, const LayerGeom 
   const int half = (a.scale + (a.scale >> 31)) >> 1;
   const uint32_t* ref = reinterpret_cast<const uint32_t*>(a.ref);
   for (int pi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; pi < npx; pi += nwarps) {
-    if (g.skip[pi]) continue;
+    if (g.skip[pi]) {  // skipped pixels aggregate raw 0 and 255 past their count (DenseStereoSgm.cs:242)
+      uint8_t* out = raw + g.off[pi];
+      const int count = g.count[pi], cap = g.cap[pi];
+      for (int d = lane; d < cap; d += 32) out[d] = d < count ? 0 : 255;
+      continue;
+    }
     const int x = pi % g.W, y = pi / g.W;
     const int xImg = min(a.scale * x + half, a.rw - 1), yImg = min(a.scale * y + half, a.rh - 1);
     const int start = g.start[pi], count = g.count[pi], cap = g.cap[pi];
@@ -106,18 +127,21 @@ __global__ void __launch_bounds__(256) k_cost(const CostArgs a, const LayerGeom 
       if (lane == 0) atomicCAS(err, 0, 7);
       continue;
     }
-    int ry[3][3];
-    uint32_t re[3][3], ro[3][3];
+    // the reference 3x3 block, rows/columns clamped to the image
+    uint32_t ge[3], go[3], re[3][3], ro[3][3];
 #pragma unroll
-    for (int r = 0; r < 3; r++) {  // the reference 3x3 block, rows/columns clamped to the image
+    for (int r = 0; r < 3; r++) {
       const int yy = min(max(yImg + r - 1, 0), a.rh - 1);
+      uint32_t yb[3];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const uint32_t w = __ldg(ref + (size_t)yy * a.rw + min(max(xImg + c - 1, 0), a.rw - 1));
-        ry[r][c] = yb(w);
+        yb[c] = w & 0xffu;
         re[r][c] = w & 0x00ff00ffu;
         ro[r][c] = (w >> 8) & 0x00ff00ffu;
       }
+      ge[r] = yb[0] | (yb[2] << 16);
+      go[r] = yb[1];
     }
     const float xf = (float)xImg, yf = (float)yImg;
     for (int c0 = 0; c0 < count; c0 += 32) {
@@ -126,43 +150,36 @@ __global__ void __launch_bounds__(256) k_cost(const CostArgs a, const LayerGeom 
       const int pl = valid ? start + d : start;
       const float z = __ldg(g.planes + pl);
       const int last = min(31, count - 1 - c0);
+      const float xz = __fmul_rn(xf, z), yz = __fmul_rn(yf, z);  // (x·z)·1.0f: the product by one is exact
       uint32_t acc = 0;
       for (int k = 0; k < a.n_others; k++) {
         const float* Wm = a.warp[k];
         const int iw = a.ow[k], ih = a.oh[k];
         const int x0 = 1, y0 = 1, x1 = iw - 2, y1 = ih - 2;
         // p = ((z·W2 + W3) + xz·W0) + yz·W1 (:255-259), the first term from the table; then 1/pz and the +0.25 bias
-        const float* zk = zt + ((size_t)k * n + pl) * 3;
-        const float xz = __fmul_rn(xf, z), yz = __fmul_rn(yf, z);  // (x·z)·1.0f: the product by one is exact
-        const float px = __fadd_rn(__fadd_rn(__ldg(zk + 0), __fmul_rn(xz, Wm[0])), __fmul_rn(yz, Wm[4]));
-        const float py = __fadd_rn(__fadd_rn(__ldg(zk + 1), __fmul_rn(xz, Wm[1])), __fmul_rn(yz, Wm[5]));
-        const float pz = __fadd_rn(__fadd_rn(__ldg(zk + 2), __fmul_rn(xz, Wm[2])), __fmul_rn(yz, Wm[6]));
-        const float inv = __fdiv_rn(1.0f, pz);
-        const float fx = __fadd_rn(__fmul_rn(px, inv), 0.25f), fy = __fadd_rn(__fmul_rn(py, inv), 0.25f);
-        int ix, iy, hx, hy;
-        bool inb;
+        const float4 zk = __ldg(zt + (size_t)k * n + pl);
+        const float px = __fadd_rn(__fadd_rn(zk.x, __fmul_rn(xz, Wm[0])), __fmul_rn(yz, Wm[4]));
+        const float py = __fadd_rn(__fadd_rn(zk.y, __fmul_rn(xz, Wm[1])), __fmul_rn(yz, Wm[5]));
+        const float pz = __fadd_rn(__fadd_rn(zk.z, __fmul_rn(xz, Wm[2])), __fmul_rn(yz, Wm[6]));
+        const float inv = __frcp_rn(pz);  // the correctly rounded 1/pz, as the reference's division
+        float fx = __fadd_rn(__fmul_rn(px, inv), 0.25f), fy = __fadd_rn(__fmul_rn(py, inv), 0.25f);
         if (d == 0) {  // the first plane is clamped into the rect (:263-269)
-          const float cx = cs_minf(cs_maxf(fx, (float)x0), (float)(x1 - 1)), cy = cs_minf(cs_maxf(fy, (float)y0), (float)(y1 - 1));
-          ix = f2i(cx); iy = f2i(cy); hx = f2i(__fadd_rn(cx, cx)) & 1; hy = f2i(__fadd_rn(cy, cy)) & 1;
-          inb = true;
-          if (ix < x0 || ix >= x1 || iy < y0 || iy >= y1) {  // the scalar fallback of the reference would read out of the image
-            atomicCAS(err, 0, 7);
-            inb = false;
-          }
-        } else {
-          ix = f2i(fx); iy = f2i(fy); hx = f2i(__fadd_rn(fx, fx)) & 1; hy = f2i(__fadd_rn(fy, fy)) & 1;
-          inb = valid && !(ix < x0 || ix >= x1 || iy < y0 || iy >= y1);
+          fx = cs_minf(cs_maxf(fx, (float)x0), (float)(x1 - 1));
+          fy = cs_minf(cs_maxf(fy, (float)y0), (float)(y1 - 1));
+        }
+        // (int)(2f) gives the integer part (>> 1) and the half-pixel bit (& 1) wherever the position can be in the rect
+        // (f >= 1); elsewhere both forms fall outside it
+        const int tx = f2i(__fadd_rn(fx, fx)), ty = f2i(__fadd_rn(fy, fy));
+        const int ix = tx >> 1, iy = ty >> 1, h = ((ty & 1) << 1) | (tx & 1);
+        bool inb = valid && !(ix < x0 || ix >= x1 || iy < y0 || iy >= y1);
+        if (d == 0 && !inb) {  // the scalar fallback of the reference would read out of the image
+          atomicCAS(err, 0, 7);
         }
         int costK = 0;
         if (inb) {
-          const uint32_t* base = reinterpret_cast<const uint32_t*>(a.other[k]) + (size_t)(iy - 1) * iw + (ix - 1);
-          if (GREY) {
-            costK = hx ? (hy ? grey_block<1, 1>(base, iw, ry) : grey_block<1, 0>(base, iw, ry))
-                       : (hy ? grey_block<0, 1>(base, iw, ry) : grey_block<0, 0>(base, iw, ry));
-          } else {
-            costK = hx ? (hy ? colour_block<1, 1>(base, iw, re, ro, a.wq[k]) : colour_block<1, 0>(base, iw, re, ro, a.wq[k]))
-                       : (hy ? colour_block<0, 1>(base, iw, re, ro, a.wq[k]) : colour_block<0, 0>(base, iw, re, ro, a.wq[k]));
-          }
+          const uint32_t* q = a.phase[k] + ((size_t)h * ih + (iy - 1)) * iw + (ix - 1);
+          if (GREY) costK = grey_cost(q, iw, ge, go);
+          else costK = colour_cost(q, iw, re, ro, a.wq[k]);
         }
         const uint32_t m = __ballot_sync(0xffffffffu, inb);
         const uint32_t below = m & ((1u << lane) - 1u);
@@ -182,15 +199,141 @@ __global__ void __launch_bounds__(256) k_cost(const CostArgs a, const LayerGeom 
   }
 }
 
-void launch_cost(const CostArgs& a, const LayerGeom& g, const float* zt, uint8_t* raw, int* err, cudaStream_t s) {
-  const int npx = g.W * g.H;
-  int blocks = (npx + 7) / 8;
-  if (blocks > 148 * 64) blocks = 148 * 64;
-  bool grey = true;
+// Uniform layers (every pixel searches planes [0, n), cap n, n % 8 == 0): lanes over 32 neighbouring pixels of a row,
+// each lane walking its pixel's planes in order like the reference's loop, so the last computed cost of a camera
+// (:273-274) is a register, the plane terms are the same for the whole warp, and the camera constants stay in
+// registers. Eight planes of u8 costs go out per 8-byte store. Skipped pixels get raw 0 (DenseStereoSgm.cs:242).
+template <bool GREY, int NK>
+__global__ void __launch_bounds__(256) k_cost_rows(const CostArgs a, const LayerGeom g, const float4* __restrict__ zt,
+                                                   uint8_t* __restrict__ raw, int* err) {
+  const int lane = threadIdx.x & 31;
+  const int tiles_x = (g.W + 31) >> 5;
+  const int ntiles = tiles_x * g.H;
+  const int n = g.n_planes;
+  const int half = (a.scale + (a.scale >> 31)) >> 1;
+  const uint32_t* ref = reinterpret_cast<const uint32_t*>(a.ref);
+  // camera constants
+  float w0[NK], w1[NK], w2[NK], w4[NK], w5[NK], w6[NK];
+  int iwk[NK], ihk[NK];
+#pragma unroll
+  for (int k = 0; k < NK; k++) {
+    w0[k] = a.warp[k][0]; w1[k] = a.warp[k][1]; w2[k] = a.warp[k][2];
+    w4[k] = a.warp[k][4]; w5[k] = a.warp[k][5]; w6[k] = a.warp[k][6];
+    iwk[k] = a.ow[k]; ihk[k] = a.oh[k];
+  }
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += (gridDim.x * blockDim.x) >> 5) {
+    const int y = t / tiles_x, x = ((t - y * tiles_x) << 5) + lane;
+    if (x >= g.W) continue;
+    const size_t pi = (size_t)y * g.W + x;
+    uint8_t* out = raw + pi * n;
+    if (g.skip[pi]) {
+      for (int d = 0; d < n; d += 8) *reinterpret_cast<uint2*>(out + d) = make_uint2(0u, 0u);
+      continue;
+    }
+    const int xImg = min(a.scale * x + half, a.rw - 1), yImg = min(a.scale * y + half, a.rh - 1);
+    uint32_t ge[3], go[3], re[3][3], ro[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {  // the reference 3x3 block, rows/columns clamped to the image
+      const int yy = min(max(yImg + r - 1, 0), a.rh - 1);
+      uint32_t yb[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const uint32_t w = __ldg(ref + (size_t)yy * a.rw + min(max(xImg + c - 1, 0), a.rw - 1));
+        yb[c] = w & 0xffu;
+        re[r][c] = w & 0x00ff00ffu;
+        ro[r][c] = (w >> 8) & 0x00ff00ffu;
+      }
+      ge[r] = yb[0] | (yb[2] << 16);
+      go[r] = yb[1];
+    }
+    const float xf = (float)xImg, yf = (float)yImg;
+    int last[NK];
+#pragma unroll
+    for (int k = 0; k < NK; k++) last[k] = 0;
+    uint32_t pk0 = 0, pk1 = 0;
+    for (int d = 0; d < n; d++) {
+      const float z = __ldg(g.planes + d);
+      const float xz = __fmul_rn(xf, z), yz = __fmul_rn(yf, z);
+      uint32_t acc = 0;
+#pragma unroll
+      for (int k = 0; k < NK; k++) {
+        const float4 zk = __ldg(zt + (size_t)k * n + d);
+        const float px = __fadd_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0[k])), __fmul_rn(yz, w4[k]));
+        const float py = __fadd_rn(__fadd_rn(zk.y, __fmul_rn(xz, w1[k])), __fmul_rn(yz, w5[k]));
+        const float pz = __fadd_rn(__fadd_rn(zk.z, __fmul_rn(xz, w2[k])), __fmul_rn(yz, w6[k]));
+        const float inv = __frcp_rn(pz);
+        float fx = __fadd_rn(__fmul_rn(px, inv), 0.25f), fy = __fadd_rn(__fmul_rn(py, inv), 0.25f);
+        const int x1 = iwk[k] - 2, y1 = ihk[k] - 2;
+        if (d == 0) {  // the first plane is clamped into the rect (:263-269)
+          fx = cs_minf(cs_maxf(fx, 1.0f), (float)(x1 - 1));
+          fy = cs_minf(cs_maxf(fy, 1.0f), (float)(y1 - 1));
+        }
+        const int tx = f2i(__fadd_rn(fx, fx)), ty = f2i(__fadd_rn(fy, fy));
+        const int ix = tx >> 1, iy = ty >> 1;
+        if (ix >= 1 && ix < x1 && iy >= 1 && iy < y1) {
+          const int h = ((ty & 1) << 1) | (tx & 1);
+          const uint32_t* q = a.phase[k] + ((size_t)h * ihk[k] + (iy - 1)) * iwk[k] + (ix - 1);
+          last[k] = GREY ? grey_cost(q, iwk[k], ge, go) : colour_cost(q, iwk[k], re, ro, a.wq[k]);
+        } else if (d == 0) {  // the scalar fallback of the reference would read out of the image
+          atomicCAS(err, 0, 7);
+        }
+        acc += (uint32_t)last[k];
+      }
+      const uint32_t b = (uint32_t)f2i(__fmul_rn((float)(acc & 0xffffu), a.norm)) & 0xffu;  // Normalise (:378-379)
+      const int sh = (d & 3) * 8;
+      if (d & 4) pk1 |= b << sh;
+      else pk0 |= b << sh;
+      if ((d & 7) == 7) {
+        *reinterpret_cast<uint2*>(out + (d - 7)) = make_uint2(pk0, pk1);
+        pk0 = pk1 = 0;
+      }
+    }
+  }
+}
+
+bool cost_all_grey(const CostArgs& a) {
   for (int k = 0; k < a.n_others; k++)
-    if (!(a.wq[k][0] == 12240 && a.wq[k][1] == 0 && a.wq[k][2] == 0 && a.wq[k][3] == 0)) grey = false;
-  if (grey) k_cost<true><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);
-  else k_cost<false><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);
+    if (!(a.wq[k][0] == 12240 && a.wq[k][1] == 0 && a.wq[k][2] == 0 && a.wq[k][3] == 0)) return false;
+  return true;
+}
+
+void launch_phases(const CostArgs& a, cudaStream_t s) {
+  const bool grey = cost_all_grey(a);
+  for (int k = 0; k < a.n_others; k++) {
+    dim3 grid((a.ow[k] + 127) / 128, a.oh[k]);
+    uint32_t* out = const_cast<uint32_t*>(a.phase[k]);
+    if (grey) k_phase_grey<<<grid, 128, 0, s>>>(a.other[k], a.ow[k], a.oh[k], out);
+    else k_phase_colour<<<grid, 128, 0, s>>>(a.other[k], a.ow[k], a.oh[k], out);
+    count_launches(1);
+  }
+}
+
+template <bool GREY>
+static void launch_rows(int nk, int blocks, const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t* raw, int* err,
+                        cudaStream_t s) {
+  switch (nk) {
+    case 1: k_cost_rows<GREY, 1><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
+    case 2: k_cost_rows<GREY, 2><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
+    case 3: k_cost_rows<GREY, 3><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
+    default: k_cost_rows<GREY, 4><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
+  }
+}
+
+void launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t* raw, int* err, cudaStream_t s) {
+  const int npx = g.W * g.H;
+  const bool grey = cost_all_grey(a);
+  if (g.uniform && g.n_planes % 8 == 0 && a.n_others >= 1 && a.n_others <= 4) {
+    const int tiles = ((g.W + 31) / 32) * g.H;
+    int blocks = (tiles + 7) / 8;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (grey) launch_rows<true>(a.n_others, blocks, a, g, zt, raw, err, s);
+    else launch_rows<false>(a.n_others, blocks, a, g, zt, raw, err, s);
+  } else {
+    int blocks = (npx + 7) / 8;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (grey) k_cost<true><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);
+    else k_cost<false><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);
+  }
   count_launches(1);
 }
 

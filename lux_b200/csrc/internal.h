@@ -31,6 +31,7 @@ struct CostArgs {
   const uint8_t* ref; int rw, rh;  // box-filtered reference image (dense RGBA8)
   int n_others;
   const uint8_t* other[kMaxCams];
+  const uint32_t* phase[kMaxCams];  // per other camera: its four half-pixel phase images ([4][oh][ow] u32, k_phase_*)
   int ow[kMaxCams], oh[kMaxCams];
   float warp[kMaxCams][16];
   uint16_t wq[kMaxCams][4];
@@ -61,9 +62,12 @@ void launch_upsample(const float* prev, int pw, int ph, const uint8_t* guide, in
                      cudaStream_t s);
 
 // cost.cu
-// zt: per other camera and plane, the plane-only projection terms (z·W[8] + W[12], z·W[9] + W[13], z·W[10] + W[14]),
-// each product and sum rounded to float, as (3 floats) × n_planes × n_others.
-void launch_cost(const CostArgs& a, const LayerGeom& g, const float* zt, uint8_t* raw, int* err, cudaStream_t s);
+// The phase images of every other camera into a.phase (4·ow·oh u32 each); then the cost volume.
+// zt: per other camera and plane, the plane-only projection terms (z·W[8] + W[12], z·W[9] + W[13], z·W[10] + W[14], 0),
+// each product and sum rounded to float, as float4 × n_planes × n_others.
+bool cost_all_grey(const CostArgs& a);
+void launch_phases(const CostArgs& a, cudaStream_t s);
+void launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t* raw, int* err, cudaStream_t s);
 
 // sgm_emulate.cu: the exact replay of the reference's sheared-tile traversal on its line-buffer layout (any layer)
 struct EmuBuffers {

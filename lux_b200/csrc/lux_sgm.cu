@@ -262,7 +262,9 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   }
   if ((rc = alloc_t(ctx, B, L->volume + 8, &L->agg))) return rc;
   if ((rc = alloc_t(ctx, B, L->volume + 8, &L->raw))) return rc;
-  CK(cudaMemsetAsync(L->agg, 0, (L->volume + 8) * 2, s));
+  // the fast uniform aggregation writes every aggregate before it reads one; the replay accumulates into zeros
+  const bool fast = uniform && !(flags & LUX_LAYER_FORCE_REPLAY) && uniform_fast_supported(W, H, L->n, p.tile, p.p1, p.p2scale);
+  if (!fast) CK(cudaMemsetAsync(L->agg, 0, (L->volume + 8) * 2, s));
   if (!uniform) CK(cudaMemsetAsync(L->raw, 0, L->volume + 8, s));
   if (flags & LUX_LAYER_KEEP_PASS1) {
     if ((rc = alloc_t(ctx, B, L->volume + 8, &L->agg_pass1))) return rc;
@@ -293,24 +295,30 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   }
   ca.scale = p.scale;
   // the plane-only projection terms of every camera (DenseStereo.cs:257-259: (z·W2 + W3), one rounding per op)
-  std::vector<float> zt_h((size_t)ca.n_others * L->n * 3);
+  std::vector<float> zt_h((size_t)ca.n_others * L->n * 4, 0.0f);
   for (int k = 0; k < ca.n_others; k++)
     for (int i = 0; i < L->n; i++) {
       const float z = L->planes_h[i];
       for (int r = 0; r < 3; r++) {
         volatile float prod = z * ca.warp[k][8 + r];
-        zt_h[((size_t)k * L->n + i) * 3 + r] = prod + ca.warp[k][12 + r];
+        zt_h[((size_t)k * L->n + i) * 4 + r] = prod + ca.warp[k][12 + r];
       }
     }
-  float* zt = nullptr;
-  if ((rc = alloc_t(ctx, tmp, zt_h.size(), &zt))) return rc;
+  float4* zt = nullptr;
+  if ((rc = alloc_t(ctx, tmp, zt_h.size() / 4, &zt))) return rc;
   CK(cudaMemcpyAsync(zt, zt_h.data(), zt_h.size() * 4, cudaMemcpyHostToDevice, s));
+  for (int k = 0; k < ca.n_others; k++) {  // the half-pixel phase images of the other cameras
+    uint32_t* ph = nullptr;
+    if ((rc = alloc_t(ctx, tmp, (size_t)4 * ca.ow[k] * ca.oh[k], &ph))) return rc;
+    ca.phase[k] = ph;
+  }
   CK(cudaEventRecord(ctx->ev[0], s));
+  launch_phases(ca, s);
   launch_cost(ca, g, zt, L->raw, ctx->d_err, s);
   // aggregation: two passes over the sheared tiles, then WTA
   CK(cudaEventRecord(ctx->ev[1], s));
   const int xsw = 0;  // LUX_SGM_XSW unset: the reference default (DenseStereoSgm.cs:31)
-  if (uniform && !(flags & LUX_LAYER_FORCE_REPLAY) && uniform_fast_supported(W, H, L->n, p.tile, p.p1, p.p2scale)) {
+  if (fast) {
     void* scr = nullptr;
     const size_t sb = uniform_scratch_bytes(W, H, L->n, p.tile);
     if ((rc = dev_alloc(ctx, tmp, sb, &scr))) return rc;

@@ -92,6 +92,39 @@ def test_multicamera_colour_layer_bit_exact(ctx, oracle):
         gl.close()
 
 
+@pytest.mark.parametrize("kernel", ["fast", "replay"])
+def test_uniform_layer_with_skip_mask(ctx, oracle, kernel):
+    """A first layer with SkipMode 2: skipped pixels aggregate raw 0 (DenseStereoSgm.cs:242)."""
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(150, 96, 32, seed=21, tile=16)
+    p = api.StereoParams(**{**wl.params.__dict__, "skip_mode": 2})
+    filt = _filtered(oracle, wl.images)
+    ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, p, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, p, keep_pass1=True, keep_agg=True,
+                                force_replay=(kernel == "replay"), ctx=ctx)
+    try:
+        assert gl.Skip.any()
+        assert gl.sgm_kernel == (1 if kernel == "fast" else 0)
+        _compare_layer(gl, ol, f"skip {kernel}")
+    finally:
+        gl.close()
+
+
+@pytest.mark.parametrize("n_cams,colour", [(4, False), (6, True), (6, False)])
+def test_multicamera_layers_bit_exact(ctx, oracle, n_cams, colour):
+    """Grey and colour layers with 3 and 5 other cameras (the per-camera cost paths, beyond four cameras too)."""
+    from lux_b200 import api, synth
+    cap = synth.capture(96, 72, n_cams, seed=30 + n_cams, f=72.0, baseline_mm=(15.0, 50.0), colour=colour)
+    filt = _filtered(oracle, cap.images)
+    p = api.StereoParams(scale=1, tile=8, skip_mode=0, plane_density=2.0)
+    ol = oracle.layer(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True, keep_agg=True, ctx=ctx)
+    try:
+        _compare_layer(gl, ol, f"{n_cams}cam colour={colour}")
+    finally:
+        gl.close()
+
+
 def test_pyramid_bit_exact(ctx, oracle):
     """DenseStereoPyramid.Run: six L16 layers (ragged ranges, skip masks, align choice) against the oracle."""
     from lux_b200 import api, synth
