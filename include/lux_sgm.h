@@ -156,14 +156,18 @@ int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int3
                      const lux_img_rgba8* guide, int32_t set_w, int32_t set_h, float sigma, int32_t scale,
                      const float* prev_conf, float* out_depth, float* out_conf);
 
-/* No reference counterpart: lux_sgm_upsample without any device allocation, for callers that keep every buffer on the GPU.
+/* No counterpart in the reference. lux_sgm_upsample without any device allocation, for hosts that cannot let this
+ * library allocate GPU memory: a process whose HBM is already reserved by another allocator (an inference server or a
+ * framework's caching pool holding nearly all of it), where a cudaMalloc here would fail or fragment that pool, and a
+ * serving loop that must not pay the implicit device synchronisation of cudaMalloc / cudaFree on every request.
  * prev_depth (and prev_conf) are device arrays of pw×ph floats, guide a device image (on_device != 0, stride >= w), out_depth
- * (and out_conf) device arrays of guide.w×guide.h floats; results equal lux_sgm_upsample's. The resampled guidance
- * (pw·ph RGBA8 pixels) goes to a static device array of LUX_UPSAMPLE_NOALLOC_MAX_PIXELS pixels (16 MiB); a larger pw·ph
- * returns LUX_ERR_ARG. Nothing in that array has to start at zero. The first call on a device looks the array up
- * (cudaGetSymbolAddress, with the context's device current): make it before any stream capture. Calls that overlap in
- * time on one device (through different contexts) share the array and race: serialise them. Returns after the context's
- * stream has finished the work. */
+ * (and out_conf) device arrays of guide.w×guide.h floats; results equal lux_sgm_upsample's. The one scratch buffer, the
+ * resampled guidance (pw·ph RGBA8 pixels), is a static device array of LUX_UPSAMPLE_NOALLOC_MAX_PIXELS pixels (16 MiB)
+ * that every GPU which loads this library holds until the process exits; a larger pw·ph returns LUX_ERR_ARG. Each call
+ * writes every byte of it that it reads, so nothing has to start at zero. The first call on a device looks the array up
+ * (cudaGetSymbolAddress, with the context's device current): make that first call before any stream capture. All calls
+ * share the array and it keeps the last call's contents, so calls that overlap in time on one device (through different
+ * contexts) race: serialise them. Returns after the context's stream has finished the work. */
 #define LUX_UPSAMPLE_NOALLOC_MAX_PIXELS (4u << 20)
 int lux_sgm_upsample_noalloc(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int32_t ph, const lux_img_rgba8* guide,
                              int32_t set_w, int32_t set_h, float sigma, int32_t scale, const float* prev_conf,

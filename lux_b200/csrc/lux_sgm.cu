@@ -717,8 +717,11 @@ int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int3
 namespace {
 
 // The resampled guidance (RGBA8 at the previous layer's size) of lux_sgm_upsample_noalloc lives in module-static device
-// memory, so that call allocates nothing. Every byte of it that the bilateral pass reads is written earlier in the same
-// call (k_shift_resize covers all pw·ph pixels), so nothing has to start at zero.
+// memory, so that call allocates nothing: it serves hosts whose GPU memory belongs to another allocator, or whose
+// request loop must not synchronise on cudaMalloc / cudaFree. Every GPU that loads the library holds these 16 MiB until
+// exit. Every byte the bilateral pass reads is written earlier in the same call (k_shift_resize covers all pw·ph
+// pixels), so nothing has to start at zero. Host code must not pass the array's name to a kernel (on the host it is
+// only a stand-in for the symbol): upsample_scratch() looks up its device address.
 constexpr size_t kNoAllocMaxPixels = LUX_UPSAMPLE_NOALLOC_MAX_PIXELS;
 static __device__ __align__(256) uint8_t g_upsample_scratch[kNoAllocMaxPixels * 4];
 

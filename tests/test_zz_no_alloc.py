@@ -1,5 +1,7 @@
-"""lux_sgm_upsample_noalloc (the allocation-free upsample, no reference counterpart) against lux_sgm_upsample, on two calls
-in a row with different sizes, plus its size limit. The file name sorts it after the other test files."""
+"""lux_sgm_upsample_noalloc, the upsample for hosts that cannot let this library allocate GPU memory (their HBM belongs to
+another allocator, or their request loop must not synchronise on cudaMalloc / cudaFree), checked through the C ABI
+against lux_sgm_upsample on two calls in a row with different sizes, plus its size limit. It has no counterpart in the
+reference. The file name makes pytest collect it after the other test files."""
 import ctypes
 
 import numpy as np
