@@ -136,6 +136,24 @@ LUX_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* stop, int* 
   }
 }
 
+// Waits until *flag >= target and returns the value it saw (which may be larger); on timeout, or when another block
+// already failed, returns -1 (setting *err = code on timeout). Spins are bounded by wall time.
+LUX_DEV int wait_at_least_value(const int* flag, int target, int* err, int code, uint64_t timeout_ns) {
+  int v = ld_acquire(flag);
+  if (v >= target) return v;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    __nanosleep(32);
+    v = ld_acquire(flag);
+    if (v >= target) return v;
+    if (*(volatile int*)err != 0) return -1;
+    if (global_ns() - t0 > timeout_ns) {
+      atomicCAS(err, 0, code);
+      return -1;
+    }
+  }
+}
+
 // Waits until *flag >= target; on timeout sets *err = code and returns false. Spins are bounded by wall time.
 LUX_DEV bool wait_at_least(const int* flag, int target, int* err, int code, uint64_t timeout_ns) {
   if (ld_acquire(flag) >= target) return true;

@@ -31,7 +31,7 @@ constexpr int kRows = 14;      // rows of the recurrence per block (one warp eac
 constexpr int kWarps = kRows + 2;  // plus the loader and the publisher warps
 constexpr int kBandBufs = 4;   // band buffers in rotation
 constexpr int kRing = 8;       // slots of the hand-over ring between neighbouring rows of a block
-constexpr int kPublish = 4;    // the publisher releases the global band progress every kPublish pixels
+constexpr int kPublish = 8;    // the publisher releases the global band progress every kPublish pixels
 constexpr uint32_t kInit2 = 0x07d007d0u;  // 2000 | 2000
 
 LUX_DEV uint32_t vmin2(uint32_t a, uint32_t b) {
@@ -442,7 +442,7 @@ LUX_DEV void row_above(const UniArgs& a, const uint16_t* bnd_up, const uint16_t*
 // off the rows' own critical path.
 template <int LPT, bool FULL, bool PASS2>
 __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a) {
-  constexpr int NR = LPT / 2, Dp = Dp_of(LPT), kBatch = 2;
+  constexpr int NR = LPT / 2, Dp = Dp_of(LPT), kBatch = 4;
   extern __shared__ __align__(16) uint16_t smem_ring[];
   auto ring = [&](int set, int slot, int p) { return smem_ring + (((size_t)set * kRing + slot) * 3 + p) * Dp; };
   uint16_t* ring_min = smem_ring + (size_t)(kRows + 1) * kRing * 3 * Dp;
@@ -484,14 +484,25 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
   if (w == kRows) {
     // ---------------- loader: the row above the block into ring kRows ----------------
     if (y0 < a.H) {
+      // pixels of the block above known to be published: the counter is polled only when the loader has caught up with
+      // it, and then up to kBatch pixels are loaded at once, so their L2 round trips overlap
+      int avail = cb > 0 ? 0 : a.W;
       for (int xb = 0; xb < a.W && !s_stop; xb += kBatch) {
         const int xe = min(a.W, xb + kBatch);
         bool ok = true;
         for (int x = xb; x < xe && ok; x++) ok = wait_free(kRows, x);  // row 0 is done with these slots
         if (!ok) break;
-        if (cb > 0 && lane == 0 && !wait_at_least(a.progress + (cb - 1), xe, a.err, 11, a.timeout_ns)) s_stop = 1;
-        __syncwarp();
-        if (s_stop) break;
+        if (avail < xe) {
+          int v = 0;
+          if (lane == 0) v = wait_at_least_value(a.progress + (cb - 1), xe, a.err, 11, a.timeout_ns);
+          v = __shfl_sync(0xffffffffu, v, 0);
+          __syncwarp();  // lane 0's acquire orders the band-buffer reads of every lane
+          if (v < 0) {
+            s_stop = 1;
+            break;
+          }
+          avail = v;
+        }
         Src<LPT> u[kBatch][3];
 #pragma unroll
         for (int k = 0; k < kBatch; k++)
