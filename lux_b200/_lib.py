@@ -40,7 +40,8 @@ class LayerInfo(ctypes.Structure):
     _fields_ = [("w", ctypes.c_int32), ("h", ctypes.c_int32), ("index", ctypes.c_int32), ("align", ctypes.c_int32),
                 ("n_planes", ctypes.c_int32), ("min_lo", ctypes.c_int32), ("max_hi", ctypes.c_int32), ("tile", ctypes.c_int32),
                 ("volume", ctypes.c_uint64), ("gpu_ms_cost", ctypes.c_float), ("gpu_ms_sgm", ctypes.c_float),
-                ("gpu_ms_wta", ctypes.c_float), ("sgm_kernel", ctypes.c_int32)]
+                ("gpu_ms_wta", ctypes.c_float), ("sgm_kernel", ctypes.c_int32),
+                ("cost_kernel", ctypes.c_int32)]
 
 
 # every exported symbol with its signature: (name, restype, argtypes)

@@ -210,6 +210,7 @@ class DenseLayer:
         self.volume = info.volume
         self.gpu_ms_cost, self.gpu_ms_sgm, self.gpu_ms_wta = info.gpu_ms_cost, info.gpu_ms_sgm, info.gpu_ms_wta
         self.sgm_kernel = info.sgm_kernel
+        self.cost_kernel = info.cost_kernel
 
     @staticmethod
     def compute(images, gray, calibs, near, far, params: StereoParams, index=0, align=8, prev: Optional["DenseLayer"] = None,

@@ -13,6 +13,8 @@
 //     columns x..x+3, so a block row is one aligned load; |t - r| capped at 2 in u16x2 lanes (min/max.u16x2);
 //   colour camera: the RGBA word per pixel and phase; even bytes (Y, V) and odd bytes (U, A) as u16x2 lanes.
 // Both are exact restatements of the reference's byte-lane sums (each channel sum is at most 9·6).
+#include <climits>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -291,6 +293,121 @@ __global__ void __launch_bounds__(256) k_cost_rows(const CostArgs a, const Layer
   }
 }
 
+// Uniform layers of one axis-aligned camera pair (flow-matrix terms W1 = W2 = W4 = W6 = 0, as for a rectified pair; the
+// host checks them, that every plane term z·W10 + W14 is finite and non-zero and that x·z cannot overflow). Then, exactly:
+//   pz = z·W10 + W14 (adding the ±0 products changes no non-zero value), so 1/pz is a per-plane constant (zt.w);
+//   px = (z·W8 + W12) + x·z·W0, where the dropped ±0 term can only change the sign of a zero px, and a zero px gives
+//     the same fx (0.25, or NaN with an infinite 1/pz) either way;
+//   py = (z·W9 + W13) + y·z·W5 likewise, so the row and half-pixel bit of the target depend on (row, plane) only: lane j
+//     of a warp computes them for plane d0 + j and the warp shuffles them to every pixel.
+// The first plane (clamped into the rect) keeps the general projection.
+template <bool GREY>
+__global__ void __launch_bounds__(256) k_cost_axis(const CostArgs a, const LayerGeom g, const float4* __restrict__ zt,
+                                                   uint8_t* __restrict__ raw, int* err) {
+  const int lane = threadIdx.x & 31;
+  const int tiles_x = (g.W + 31) >> 5;
+  const int ntiles = tiles_x * g.H;
+  const int n = g.n_planes;
+  const int half = (a.scale + (a.scale >> 31)) >> 1;
+  const uint32_t* ref = reinterpret_cast<const uint32_t*>(a.ref);
+  const float* Wm = a.warp[0];
+  const float w0 = Wm[0], w1 = Wm[1], w2 = Wm[2], w4 = Wm[4], w5 = Wm[5], w6 = Wm[6];
+  const int iw = a.ow[0], ih = a.oh[0], x1 = iw - 2, y1 = ih - 2;
+  const uint32_t* phase = a.phase[0];
+  const int plane_stride = ih * iw;
+  constexpr int kNoRow = INT_MIN;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += (gridDim.x * blockDim.x) >> 5) {
+    const int y = t / tiles_x, xr = ((t - y * tiles_x) << 5) + lane;
+    const int x = min(xr, g.W - 1);
+    const size_t pi = (size_t)y * g.W + x;
+    uint8_t* out = raw + pi * n;
+    const bool skipped = g.skip[pi] != 0;
+    const bool live = xr < g.W && !skipped;
+    if (xr < g.W && skipped)
+      for (int d = 0; d < n; d += 8) *reinterpret_cast<uint2*>(out + d) = make_uint2(0u, 0u);
+    if (__ballot_sync(0xffffffffu, live) == 0) continue;
+    const int xImg = min(a.scale * x + half, a.rw - 1), yImg = min(a.scale * y + half, a.rh - 1);
+    uint32_t ge[3], go[3], re[3][3], ro[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {  // the reference 3x3 block, rows/columns clamped to the image
+      const int yy = min(max(yImg + r - 1, 0), a.rh - 1);
+      uint32_t yb[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const uint32_t w = __ldg(ref + (size_t)yy * a.rw + min(max(xImg + c - 1, 0), a.rw - 1));
+        yb[c] = w & 0xffu;
+        re[r][c] = w & 0x00ff00ffu;
+        ro[r][c] = (w >> 8) & 0x00ff00ffu;
+      }
+      ge[r] = yb[0] | (yb[2] << 16);
+      go[r] = yb[1];
+    }
+    const float xf = (float)xImg, yf = (float)yImg;
+    int last = 0;
+    uint32_t pk0 = 0, pk1 = 0;
+    auto put = [&](int d, uint32_t acc) {  // Normalise (:378-379) and eight planes per store
+      const uint32_t b = (uint32_t)f2i(__fmul_rn((float)(acc & 0xffffu), a.norm)) & 0xffu;
+      const int sh = (d & 3) * 8;
+      if (d & 4) pk1 |= b << sh;
+      else pk0 |= b << sh;
+      if ((d & 7) == 7) {
+        if (live) *reinterpret_cast<uint2*>(out + (d - 7)) = make_uint2(pk0, pk1);
+        pk0 = pk1 = 0;
+      }
+    };
+    {  // plane 0: the general projection, clamped into the rect (:263-269)
+      const float z = __ldg(g.planes);
+      const float xz = __fmul_rn(xf, z), yz = __fmul_rn(yf, z);
+      const float4 zk = __ldg(zt);
+      const float px = __fadd_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0)), __fmul_rn(yz, w4));
+      const float py = __fadd_rn(__fadd_rn(zk.y, __fmul_rn(xz, w1)), __fmul_rn(yz, w5));
+      const float pz = __fadd_rn(__fadd_rn(zk.z, __fmul_rn(xz, w2)), __fmul_rn(yz, w6));
+      const float inv = __frcp_rn(pz);
+      const float fx = cs_minf(cs_maxf(__fadd_rn(__fmul_rn(px, inv), 0.25f), 1.0f), (float)(x1 - 1));
+      const float fy = cs_minf(cs_maxf(__fadd_rn(__fmul_rn(py, inv), 0.25f), 1.0f), (float)(y1 - 1));
+      const int tx = f2i(__fadd_rn(fx, fx)), ty = f2i(__fadd_rn(fy, fy));
+      const int ix = tx >> 1, iy = ty >> 1;
+      if (ix >= 1 && ix < x1 && iy >= 1 && iy < y1) {
+        if (live) {
+          const uint32_t* q = phase + ((size_t)(((ty & 1) << 1) | (tx & 1)) * ih + (iy - 1)) * iw + (ix - 1);
+          last = GREY ? grey_cost(q, iw, ge, go) : colour_cost(q, iw, re, ro, a.wq[0]);
+        }
+      } else if (live) {  // the scalar fallback of the reference would read out of the image
+        atomicCAS(err, 0, 7);
+      }
+      put(0, (uint32_t)last);
+    }
+    for (int d0 = 0; d0 < n; d0 += 32) {
+      // lane j: the target row offset of plane d0 + j (or kNoRow when the row leaves the rect)
+      int rowoff;
+      {
+        const int dj = min(d0 + lane, n - 1);
+        const float4 zj = __ldg(zt + dj);
+        const float yz = __fmul_rn(yf, __ldg(g.planes + dj));
+        const float fy = __fadd_rn(__fmul_rn(__fadd_rn(zj.y, __fmul_rn(yz, w5)), zj.w), 0.25f);
+        const int ty = f2i(__fadd_rn(fy, fy)), iy = ty >> 1;
+        rowoff = (iy >= 1 && iy < y1) ? ((((ty & 1) << 1) * ih) + iy - 1) * iw - 1 : kNoRow;
+      }
+      const int jend = min(32, n - d0);
+      for (int j = (d0 == 0 ? 1 : 0); j < jend; j++) {
+        const int d = d0 + j;
+        const int ro_d = __shfl_sync(0xffffffffu, rowoff, j);
+        if (ro_d != kNoRow && live) {
+          const float4 zk = __ldg(zt + d);
+          const float xz = __fmul_rn(xf, __ldg(g.planes + d));
+          const float fx = __fadd_rn(__fmul_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0)), zk.w), 0.25f);
+          const int tx = f2i(__fadd_rn(fx, fx)), ix = tx >> 1;
+          if (ix >= 1 && ix < x1) {
+            const uint32_t* q = phase + (ro_d + (tx & 1) * plane_stride + ix);
+            last = GREY ? grey_cost(q, iw, ge, go) : colour_cost(q, iw, re, ro, a.wq[0]);
+          }
+        }
+        put(d, (uint32_t)last);
+      }
+    }
+  }
+}
+
 bool cost_all_grey(const CostArgs& a) {
   for (int k = 0; k < a.n_others; k++)
     if (!(a.wq[k][0] == 12240 && a.wq[k][1] == 0 && a.wq[k][2] == 0 && a.wq[k][3] == 0)) return false;
@@ -319,15 +436,23 @@ static void launch_rows(int nk, int blocks, const CostArgs& a, const LayerGeom& 
   }
 }
 
-void launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t* raw, int* err, cudaStream_t s) {
+int launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t* raw, int* err, cudaStream_t s) {
   const int npx = g.W * g.H;
   const bool grey = cost_all_grey(a);
+  int kind = 0;
   if (g.uniform && g.n_planes % 8 == 0 && a.n_others >= 1 && a.n_others <= 4) {
     const int tiles = ((g.W + 31) / 32) * g.H;
     int blocks = (tiles + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    if (grey) launch_rows<true>(a.n_others, blocks, a, g, zt, raw, err, s);
-    else launch_rows<false>(a.n_others, blocks, a, g, zt, raw, err, s);
+    if (a.axis) {
+      if (grey) k_cost_axis<true><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);
+      else k_cost_axis<false><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);
+      kind = 2;
+    } else {
+      if (grey) launch_rows<true>(a.n_others, blocks, a, g, zt, raw, err, s);
+      else launch_rows<false>(a.n_others, blocks, a, g, zt, raw, err, s);
+      kind = 1;
+    }
   } else {
     int blocks = (npx + 7) / 8;
     if (blocks > 148 * 64) blocks = 148 * 64;
@@ -335,6 +460,7 @@ void launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_
     else k_cost<false><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);
   }
   count_launches(1);
+  return kind;
 }
 
 }  // namespace lux

@@ -37,6 +37,7 @@ struct CostArgs {
   uint16_t wq[kMaxCams][4];
   float norm;                       // 0x3d17b426 / nOthers
   int scale;
+  int axis;                         // one other camera, axis-aligned flow matrix: zt.w holds 1/pz per plane
 };
 
 // prep.cu
@@ -67,7 +68,8 @@ void launch_upsample(const float* prev, int pw, int ph, const uint8_t* guide, in
 // each product and sum rounded to float, as float4 × n_planes × n_others.
 bool cost_all_grey(const CostArgs& a);
 void launch_phases(const CostArgs& a, cudaStream_t s);
-void launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t* raw, int* err, cudaStream_t s);
+// Returns the kernel it used: 0 per-pixel warps, 1 per-row warps (uniform layers), 2 per-row warps of an axis-aligned pair.
+int launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t* raw, int* err, cudaStream_t s);
 
 // sgm_emulate.cu: the exact replay of the reference's sheared-tile traversal on its line-buffer layout (any layer)
 struct EmuBuffers {

@@ -3,6 +3,7 @@
 // 34, 181) and DenseUpsampleLayer.Run (DenseUpsampleLayer.cs:35).
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -40,6 +41,7 @@ struct lux_layer {
   uint64_t volume = 0;
   float ms_cost = 0.f, ms_sgm = 0.f, ms_wta = 0.f;
   int sgm_kernel = 0;
+  int cost_kernel = 0;
   bool agg_final = false;  // agg holds the final aggregates (always for the replay kernel, on request for the fast one)
   std::vector<float> planes_h;
   float* planes = nullptr;
@@ -304,6 +306,26 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
         zt_h[((size_t)k * L->n + i) * 4 + r] = prod + ca.warp[k][12 + r];
       }
     }
+  // An axis-aligned pair (W1 = W2 = W4 = W6 = 0) takes the cost kernel whose 1/pz is per plane: pz is then exactly the
+  // plane term, provided it is finite and non-zero for every plane and x·z, y·z stay finite.
+  ca.axis = 0;
+  if (ca.n_others == 1 && uniform) {
+    const float* Wm = ca.warp[0];
+    bool ok = Wm[1] == 0.0f && Wm[2] == 0.0f && Wm[4] == 0.0f && Wm[6] == 0.0f;
+    double zmax = 0.0;
+    for (int i = 0; i < L->n && ok; i++) {
+      const float z = L->planes_h[i], pz = zt_h[(size_t)i * 4 + 2];
+      ok = std::isfinite(z) && std::isfinite(pz) && pz != 0.0f;
+      zmax = std::max(zmax, std::fabs((double)z));
+    }
+    if (ok && zmax * (double)std::max(iw[0], ih[0]) < 1e37) {
+      ca.axis = 1;
+      for (int i = 0; i < L->n; i++) {
+        volatile float pz = zt_h[(size_t)i * 4 + 2];
+        zt_h[(size_t)i * 4 + 3] = 1.0f / pz;  // IEEE division, as __frcp_rn
+      }
+    }
+  }
   float4* zt = nullptr;
   if ((rc = alloc_t(ctx, tmp, zt_h.size() / 4, &zt))) return rc;
   CK(cudaMemcpyAsync(zt, zt_h.data(), zt_h.size() * 4, cudaMemcpyHostToDevice, s));
@@ -314,7 +336,7 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   }
   CK(cudaEventRecord(ctx->ev[0], s));
   launch_phases(ca, s);
-  launch_cost(ca, g, zt, L->raw, ctx->d_err, s);
+  L->cost_kernel = launch_cost(ca, g, zt, L->raw, ctx->d_err, s);
   // aggregation: two passes over the sheared tiles, then WTA
   CK(cudaEventRecord(ctx->ev[1], s));
   const int xsw = 0;  // LUX_SGM_XSW unset: the reference default (DenseStereoSgm.cs:31)
@@ -615,6 +637,7 @@ int lux_layer_get_info(const lux_layer* L, lux_layer_info* info) {
   info->min_lo = L->min_lo; info->max_hi = L->max_hi; info->tile = L->tile; info->volume = L->volume;
   info->gpu_ms_cost = L->ms_cost; info->gpu_ms_sgm = L->ms_sgm; info->gpu_ms_wta = L->ms_wta;
   info->sgm_kernel = L->sgm_kernel;
+  info->cost_kernel = L->cost_kernel;
   return LUX_OK;
 }
 

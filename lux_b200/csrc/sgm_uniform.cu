@@ -179,7 +179,7 @@ LUX_DEV void four_paths(const V<LPT> (&nb)[4], const uint32_t (&mp)[4], const ui
       const uint32_t lm = pair_of(i == 0 ? prev[p] : nb[p].r[i - 1], nb[p].r[i]);       // L[d-1]
       const uint32_t lp = pair_of(nb[p].r[i], i == NR - 1 ? next[p] : nb[p].r[i + 1]);  // L[d+1]
       uint32_t t = vmin2(lm, lp) + p1x2;
-      t = vmin2(vmin2(t, nb[p].r[i]), dup16(min(p2[p] + mp[p], 65535u)));
+      t = vmin2(vmin2(t, nb[p].r[i]), dup16(p2[p] + mp[p]));  // P2 <= 1744 and minPrev <= 2000: no u16 overflow
       uint32_t lc = t + raw2.r[i] - dup16(mp[p]);  // raw + m - minPrev, each half in [0, 2000)
       if (!FULL) lc = active ? lc : kInit2;          // padding lanes keep 2000
       out[p].r[i] = lc;
@@ -555,8 +555,6 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
   const int c = a.W - 1;
   const uint32_t p1x2 = dup16((uint32_t)a.p1);
   const int yu = PASS2 ? a.H - 1 - y : y;
-  // pixel x of the pass is column x0 + xs·x of the image
-  const long long x0 = PASS2 ? a.W - 1 : 0, xs = PASS2 ? -1 : 1;
   const uint8_t* raw_row = a.raw + (size_t)yu * a.W * a.n + lane * LPT;
   uint16_t* agg_row = a.agg + (size_t)yu * a.W * a.n + lane * LPT;
   const uint2* p2_row = a.p2t + (size_t)y * a.W;
@@ -570,9 +568,11 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
     V<LPT> agg;  // pass -1: pass +1's aggregates
     uint2 p2;
   };
+  // pixel x of the pass is image column col_of(x); 32-bit offsets (W·n < 2^31) keep the addressing to a few adds
+  auto col_of = [&](int x) { return PASS2 ? c - x : x; };
   auto fetch = [&](int xq, Queued& q) {
-    const long long col = x0 + xs * xq;
-    const uint8_t* rp = raw_row + col * a.n;
+    const int off = col_of(xq) * a.n;
+    const uint8_t* rp = raw_row + off;
     if (!active) {
       q.raw.r[0] = 0;
       if constexpr (LPT >= 8) q.raw.r[1] = 0;
@@ -585,7 +585,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
     } else {
       q.raw.r[0] = __ldcs(reinterpret_cast<const unsigned short*>(rp));
     }
-    if constexpr (PASS2) agg_load<LPT>(agg_row + col * a.n, q.agg, active);
+    if constexpr (PASS2) agg_load<LPT>(agg_row + off, q.agg, active);
     q.p2 = __ldg(p2_row + xq);
   };
   // One visit N(x, y). KIND: 0 the first column, 1 a column with both neighbours and no revisit business, 2 the column
@@ -645,7 +645,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
       vstore_s<LPT>(out[p], ring(w, sl, p - 1), lane);
       if (lane == 0) rmin_at(w, sl, p - 1) = (uint16_t)mins[p];
     }
-    uint16_t* ap = agg_row + (x0 + xs * x) * a.n;
+    uint16_t* ap = agg_row + col_of(x) * a.n;
     if constexpr (KIND == 2) {  // what later revisits of this block read is stored before the release
       cs_put<LPT>(a, out[0], mins[0], y, 0, lane);
       cs_put<LPT>(a, out[1], mins[1], y, 1, lane);
@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
       if (!PASS2 || a.keep_agg) agg_store<LPT>(ap, acc, active);
       if constexpr (PASS2) {  // WTA; the last column waits for its revisits (k_wta_column)
         const int arg = wta_arg<LPT>(acc, active, lane);
-        if (lane == 0) depth_row[x0 + xs * x] = s_planes[arg];
+        if (lane == 0) depth_row[col_of(x)] = s_planes[arg];
       }
     }
     if (edge_row) {

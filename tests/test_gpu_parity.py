@@ -57,6 +57,7 @@ def test_uniform_layer_bit_exact(ctx, oracle, w, h, d, tile, kernel):
                                 force_replay=(kernel == "replay"), ctx=ctx)
     try:
         assert gl.sgm_kernel == (1 if kernel == "fast" else 0)
+        assert gl.cost_kernel == (2 if d % 8 == 0 else 0)  # a rectified pair: the axis-aligned cost kernel
         _compare_layer(gl, ol, f"{w}x{h} D{d} T{tile} {kernel}")
     finally:
         gl.close()
@@ -87,7 +88,30 @@ def test_multicamera_colour_layer_bit_exact(ctx, oracle):
     ol = oracle.layer(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True)
     gl = api.DenseLayer.compute(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True, keep_agg=True, ctx=ctx)
     try:
+        assert gl.cost_kernel == 1
         _compare_layer(gl, ol, "3cam")
+    finally:
+        gl.close()
+
+
+def test_axis_pair_colour_bit_exact(ctx, oracle):
+    """A rectified colour pair: the axis-aligned cost kernel with the colour block (the tests above are grey)."""
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(140, 90, 48, seed=41, tile=8)
+    rng = np.random.default_rng(41)
+    imgs = []
+    for im in wl.images:
+        im = im.copy()
+        im[..., 1] = np.clip(im[..., 0].astype(np.int32) // 2 + rng.integers(0, 60, im.shape[:2]), 0, 255)
+        im[..., 2] = np.clip(255 - im[..., 0].astype(np.int32) + rng.integers(0, 40, im.shape[:2]), 0, 255)
+        imgs.append(im)
+    gray = [0, 0]
+    filt = _filtered(oracle, imgs)
+    ol = oracle.layer(filt, gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, keep_agg=True, ctx=ctx)
+    try:
+        assert gl.cost_kernel == 2
+        _compare_layer(gl, ol, "axis colour")
     finally:
         gl.close()
 
@@ -120,6 +144,7 @@ def test_multicamera_layers_bit_exact(ctx, oracle, n_cams, colour):
     ol = oracle.layer(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True)
     gl = api.DenseLayer.compute(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True, keep_agg=True, ctx=ctx)
     try:
+        assert gl.cost_kernel == (1 if n_cams <= 5 else 0)
         _compare_layer(gl, ol, f"{n_cams}cam colour={colour}")
     finally:
         gl.close()
