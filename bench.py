@@ -249,10 +249,10 @@ def run_lux(a):
         "config": {"workload": DESC,
                    "parallelism": f"replicas x{world}", "l2": l2_note(),
                    "stages_ms": {"cost": cost_ms, "sgm_2_passes": sgm_ms, "wta": wta_ms},
-                   "sgm_kernel": "uniform-fast" if inf_v and inf_v[0][3] == 1 else "exact-replay"},
+                   "sgm_kernel": {0: "exact-replay", 1: "fused-wavefront", 2: "path-group-chains"}.get(inf_v[0][3] if inf_v else -1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
                      "frac": achieved / pk.get("hbm_gbs"), "traffic": TRAFFIC_PER_DE_LAUNCH * de,
-                     "kernel": "k_sgm_uniform (aggregation; per launch, 2 launches per layer)",
+                     "kernel": "SGM aggregation (per pass; 2 passes per layer)",
                      "bytes_per_de_per_launch": BYTES_PER_DE_AGG / 2,
                      "traffic_source": "ncu dram__bytes_read+write of the 2080x1560 D=256 launches, scaled by DE",
                      "peak_source": "fallback" if pk.get("fallback") else "MEASURED_PEAKS.json hbm_gbs (measured)"},

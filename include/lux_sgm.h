@@ -90,6 +90,11 @@ int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst
 #define LUX_LAYER_KEEP_AGG 2     /* keep the final aggregates (DenseLayer.Agg); the depth never needs them */
 #define LUX_LAYER_PREFILTER 4    /* images are unfiltered: apply DenseStereo.BoxFilter3 on the device first */
 #define LUX_LAYER_FORCE_REPLAY 8 /* aggregate with the exact traversal replay even where the fast uniform kernel applies */
+/* The fast uniform aggregation has two forms with the same results: the four paths fused in one wavefront (faster on
+ * small layers) and the path groups {0,1} / {2,3} as row and column chains (faster from about 2 MP). By default the
+ * library picks by size; these flags force one form (tuning and tests). */
+#define LUX_LAYER_SGM_FUSED 16
+#define LUX_LAYER_SGM_SPLIT 32
 
 /* DenseLayer.Init + DenseLayer.Compute (DenseStereoSgm.cs:34-62, 181-232): one pyramid layer on the GPU.
  * images: n_cams camera images (camera 0 = reference), box-FILTERED already unless LUX_LAYER_PREFILTER (as
@@ -118,7 +123,7 @@ typedef struct {
   float gpu_ms_cost;     /* device time of the matching-cost kernel (CUDA events on the context's stream) */
   float gpu_ms_sgm;      /* device time of the two aggregation passes */
   float gpu_ms_wta;      /* device time of the winner-take-all */
-  int32_t sgm_kernel;    /* 1 = the fast uniform-layer aggregation, 0 = the exact traversal replay */
+  int32_t sgm_kernel;    /* 0 = the exact traversal replay, 1 = fast, four paths fused, 2 = fast, path groups as chains */
   int32_t cost_kernel;   /* 0 = per-pixel warps (any layer), 1 = per-row warps (uniform layer), 2 = per-row warps of an axis-aligned pair */
 } lux_layer_info;
 int lux_layer_get_info(const lux_layer* layer, lux_layer_info* info);

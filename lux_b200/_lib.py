@@ -19,6 +19,7 @@ FIELD_DEPTH, FIELD_PLANES, FIELD_SKIP, FIELD_START, FIELD_COUNT, FIELD_CAP = 0, 
 FIELD_OFFSETS, FIELD_AGG, FIELD_AGG_PASS1, FIELD_RAW, FIELD_GUIDANCE = 6, 7, 8, 9, 10
 
 LAYER_KEEP_PASS1, LAYER_KEEP_AGG, LAYER_PREFILTER, LAYER_FORCE_REPLAY = 1, 2, 4, 8
+LAYER_SGM_FUSED, LAYER_SGM_SPLIT = 16, 32
 
 
 class Img(ctypes.Structure):

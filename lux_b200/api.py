@@ -145,9 +145,12 @@ class Context:
 _default_ctx = None
 
 
-def _flags(keep_pass1, keep_agg, prefilter, force_replay):
+def _flags(keep_pass1, keep_agg, prefilter, force_replay, sgm="auto"):
+    if sgm not in ("auto", "fused", "split"):
+        raise ValueError(f"sgm must be 'auto', 'fused' or 'split', not {sgm!r}")
     return ((L.LAYER_KEEP_PASS1 if keep_pass1 else 0) | (L.LAYER_KEEP_AGG if keep_agg else 0) |
-            (L.LAYER_PREFILTER if prefilter else 0) | (L.LAYER_FORCE_REPLAY if force_replay else 0))
+            (L.LAYER_PREFILTER if prefilter else 0) | (L.LAYER_FORCE_REPLAY if force_replay else 0) |
+            (L.LAYER_SGM_FUSED if sgm == "fused" else 0) | (L.LAYER_SGM_SPLIT if sgm == "split" else 0))
 
 
 def revisit_schedule(w, h, tile, second_pass):
@@ -214,12 +217,13 @@ class DenseLayer:
 
     @staticmethod
     def compute(images, gray, calibs, near, far, params: StereoParams, index=0, align=8, prev: Optional["DenseLayer"] = None,
-                keep_pass1=False, prefilter=False, keep_agg=False, force_replay=False,
+                keep_pass1=False, prefilter=False, keep_agg=False, force_replay=False, sgm="auto",
                 ctx: Optional[Context] = None) -> "DenseLayer":
         """DenseLayer.Init + Compute (DenseStereoSgm.cs:34-62, 181-232). images: RGBA8 (camera 0 = reference), box-filtered
         already unless prefilter=True (then BoxFilter3 runs on the GPU first, as DenseStereoPyramid.Run does).
         keep_pass1 / keep_agg keep DenseLayer.AggPass1 / Agg readable (the depth needs neither); force_replay aggregates
-        with the exact traversal replay kernel even where the fast uniform kernel applies."""
+        with the exact traversal replay kernel even where the fast uniform kernel applies; sgm picks the form of the fast
+        kernel ("fused" four-path wavefront, "split" path-group chains, "auto" by size)."""
         ctx = ctx or default_context()
         arr = (L.Img * len(images))()
         keep = []
@@ -233,7 +237,7 @@ class DenseLayer:
         out = ctypes.c_void_p()
         rc = ctx.lib.lux_sgm_layer(ctx.handle, len(images), arr, g.ctypes.data, cc, near, far, ctypes.byref(p), index, align,
                                    prev.handle if prev is not None else None,
-                                   _flags(keep_pass1, keep_agg, prefilter, force_replay), ctypes.byref(out))
+                                   _flags(keep_pass1, keep_agg, prefilter, force_replay, sgm), ctypes.byref(out))
         ctx.check(rc)
         return DenseLayer(ctx, out)
 
@@ -305,7 +309,7 @@ class DenseLayer:
 class DenseStereoPyramid:
     @staticmethod
     def run(images, gray, calibs, near=200.0, far=640000.0, keep_pass1=False, keep_agg=False, force_replay=False,
-            ctx: Optional[Context] = None) -> List[DenseLayer]:
+            sgm="auto", ctx: Optional[Context] = None) -> List[DenseLayer]:
         """DenseStereoPyramid.Run (DenseStereoSgm.cs:331-353): the raw (unfiltered) camera images in, six layers out."""
         ctx = ctx or default_context()
         arr = (L.Img * len(images))()
@@ -318,7 +322,7 @@ class DenseStereoPyramid:
         cc = _calibs_c(calibs)
         outs = (ctypes.c_void_p * 6)()
         ctx.check(ctx.lib.lux_sgm_pyramid(ctx.handle, len(images), arr, g.ctypes.data, cc, near, far,
-                                          _flags(keep_pass1, keep_agg, False, force_replay), outs))
+                                          _flags(keep_pass1, keep_agg, False, force_replay, sgm), outs))
         return [DenseLayer(ctx, ctypes.c_void_p(outs[i])) for i in range(6)]
 
 

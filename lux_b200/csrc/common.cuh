@@ -136,6 +136,20 @@ LUX_DEV bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* stop, int* 
   }
 }
 
+// Asynchronous global -> shared copies (cp.async): the data is the issuing thread's after cp.async.wait_group, and the
+// warp's after a following __syncwarp.
+LUX_DEV void cp_async8(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+LUX_DEV void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+LUX_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+LUX_DEV void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Waits until *flag >= target and returns the value it saw (which may be larger); on timeout, or when another block
 // already failed, returns -1 (setting *err = code on timeout). Spins are bounded by wall time.
 LUX_DEV int wait_at_least_value(const int* flag, int target, int* err, int code, uint64_t timeout_ns) {

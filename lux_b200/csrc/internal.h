@@ -99,6 +99,10 @@ size_t uniform_supported_planes();
 bool uniform_fast_supported(int W, int H, int n_planes, int tile, uint16_t p1, float p2scale);
 size_t uniform_scratch_bytes(int W, int H, int n_planes, int tile);
 // Both passes, WTA into depth. agg holds pass +1's aggregates afterwards, and the final ones when keep_agg.
+// sgm_split.cu: the same aggregation by path groups {0, 1} (row chains) and {2, 3} (column chains)
+size_t split_scratch_bytes(int W, int H, int n);
+int run_sgm_split(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
+                  uint16_t* agg_pass1, float* depth, int keep_agg, void* scratch, size_t scratch_bytes, int* err, cudaStream_t s);
 int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
                     uint16_t* agg_pass1, float* depth, int keep_agg, void* scratch, size_t scratch_bytes, int* err,
                     cudaStream_t s);

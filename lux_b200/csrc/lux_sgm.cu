@@ -342,14 +342,20 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   const int xsw = 0;  // LUX_SGM_XSW unset: the reference default (DenseStereoSgm.cs:31)
   if (fast) {
     void* scr = nullptr;
-    const size_t sb = uniform_scratch_bytes(W, H, L->n, p.tile);
+    // the path-group chains win from about 2 MP (their critical path is W or H steps instead of 2H + W)
+    const bool split = (flags & LUX_LAYER_SGM_SPLIT) ? true : (flags & LUX_LAYER_SGM_FUSED) ? false : (size_t)W * H >= 2000000;
+    const size_t sb = split ? split_scratch_bytes(W, H, L->n) : uniform_scratch_bytes(W, H, L->n, p.tile);
     if ((rc = dev_alloc(ctx, tmp, sb, &scr))) return rc;
-    rc = run_sgm_uniform(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth,
+    if (split)
+      rc = run_sgm_split(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth,
                          (flags & LUX_LAYER_KEEP_AGG) ? 1 : 0, scr, sb, ctx->d_err, s);
+    else
+      rc = run_sgm_uniform(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth,
+                           (flags & LUX_LAYER_KEEP_AGG) ? 1 : 0, scr, sb, ctx->d_err, s);
     if (rc) return set_err(ctx, LUX_ERR_CUDA, "uniform aggregation launch failed (%d)", rc);
     CK(cudaEventRecord(ctx->ev[2], s));
     CK(cudaEventRecord(ctx->ev[3], s));
-    L->sgm_kernel = 1;
+    L->sgm_kernel = split ? 2 : 1;
     L->agg_final = (flags & LUX_LAYER_KEEP_AGG) != 0;
     CK(cudaGetLastError());
     if ((rc = take_device_error(ctx))) return rc;

@@ -46,7 +46,14 @@ UNIFORM_CASES = [(48, 40, 16, 8), (65, 49, 16, 4), (160, 120, 32, 16), (257, 93,
                  (200, 35, 136, 8), (71, 66, 256, 64), (33, 17, 40, 2), (64, 9, 192, 32)]
 
 
-@pytest.mark.parametrize("kernel", ["fast", "replay"])
+SGM_FORMS = {"fused": 1, "split": 2, "replay": 0}  # kernel -> lux_layer_info.sgm_kernel
+
+
+def _sgm_args(kernel):
+    return dict(force_replay=True) if kernel == "replay" else dict(sgm=kernel)
+
+
+@pytest.mark.parametrize("kernel", ["fused", "split", "replay"])
 @pytest.mark.parametrize("w,h,d,tile", UNIFORM_CASES)
 def test_uniform_layer_bit_exact(ctx, oracle, w, h, d, tile, kernel):
     from lux_b200 import api, synth
@@ -54,24 +61,25 @@ def test_uniform_layer_bit_exact(ctx, oracle, w, h, d, tile, kernel):
     filt = _filtered(oracle, wl.images)
     ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True)
     gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, keep_agg=True,
-                                force_replay=(kernel == "replay"), ctx=ctx)
+                                ctx=ctx, **_sgm_args(kernel))
     try:
-        assert gl.sgm_kernel == (1 if kernel == "fast" else 0)
+        assert gl.sgm_kernel == SGM_FORMS[kernel]
         assert gl.cost_kernel == (2 if d % 8 == 0 else 0)  # a rectified pair: the axis-aligned cost kernel
         _compare_layer(gl, ol, f"{w}x{h} D{d} T{tile} {kernel}")
     finally:
         gl.close()
 
 
-def test_uniform_fast_depth_without_kept_aggregates(ctx, oracle):
-    """The production form (no Agg kept, WTA fused into pass -1) gives the same depth."""
+@pytest.mark.parametrize("kernel", ["fused", "split"])
+def test_uniform_fast_depth_without_kept_aggregates(ctx, oracle, kernel):
+    """The production form (no Agg kept, WTA fused into the last kernel of pass -1) gives the same depth."""
     from lux_b200 import api, synth
     wl = synth.rectified_pair(300, 170, 64, seed=9, tile=64)
     filt = _filtered(oracle, wl.images)
     ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params)
-    gl = api.DenseLayer.compute(wl.images, wl.gray, wl.calibs, wl.near, wl.far, wl.params, prefilter=True, ctx=ctx)
+    gl = api.DenseLayer.compute(wl.images, wl.gray, wl.calibs, wl.near, wl.far, wl.params, prefilter=True, sgm=kernel, ctx=ctx)
     try:
-        assert gl.sgm_kernel == 1
+        assert gl.sgm_kernel == SGM_FORMS[kernel]
         assert np.array_equal(gl.Depth.view(np.uint32), ol["Depth"].view(np.uint32))
         with pytest.raises(api.LuxError):
             gl.Agg
@@ -94,7 +102,8 @@ def test_multicamera_colour_layer_bit_exact(ctx, oracle):
         gl.close()
 
 
-def test_axis_pair_colour_bit_exact(ctx, oracle):
+@pytest.mark.parametrize("kernel", ["fused", "split"])
+def test_axis_pair_colour_bit_exact(ctx, oracle, kernel):
     """A rectified colour pair: the axis-aligned cost kernel with the colour block (the tests above are grey)."""
     from lux_b200 import api, synth
     wl = synth.rectified_pair(140, 90, 48, seed=41, tile=8)
@@ -108,15 +117,17 @@ def test_axis_pair_colour_bit_exact(ctx, oracle):
     gray = [0, 0]
     filt = _filtered(oracle, imgs)
     ol = oracle.layer(filt, gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True)
-    gl = api.DenseLayer.compute(filt, gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, keep_agg=True, ctx=ctx)
+    gl = api.DenseLayer.compute(filt, gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, keep_agg=True, sgm=kernel,
+                                ctx=ctx)
     try:
+        assert gl.sgm_kernel == SGM_FORMS[kernel]
         assert gl.cost_kernel == 2
         _compare_layer(gl, ol, "axis colour")
     finally:
         gl.close()
 
 
-@pytest.mark.parametrize("kernel", ["fast", "replay"])
+@pytest.mark.parametrize("kernel", ["fused", "split", "replay"])
 def test_uniform_layer_with_skip_mask(ctx, oracle, kernel):
     """A first layer with SkipMode 2: skipped pixels aggregate raw 0 (DenseStereoSgm.cs:242)."""
     from lux_b200 import api, synth
@@ -124,39 +135,45 @@ def test_uniform_layer_with_skip_mask(ctx, oracle, kernel):
     p = api.StereoParams(**{**wl.params.__dict__, "skip_mode": 2})
     filt = _filtered(oracle, wl.images)
     ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, p, keep_pass1=True)
-    gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, p, keep_pass1=True, keep_agg=True,
-                                force_replay=(kernel == "replay"), ctx=ctx)
+    gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, p, keep_pass1=True, keep_agg=True, ctx=ctx,
+                                **_sgm_args(kernel))
     try:
         assert gl.Skip.any()
-        assert gl.sgm_kernel == (1 if kernel == "fast" else 0)
+        assert gl.sgm_kernel == SGM_FORMS[kernel]
         _compare_layer(gl, ol, f"skip {kernel}")
     finally:
         gl.close()
 
 
+@pytest.mark.parametrize("kernel", ["fused", "split"])
 @pytest.mark.parametrize("n_cams,colour", [(4, False), (6, True), (6, False)])
-def test_multicamera_layers_bit_exact(ctx, oracle, n_cams, colour):
+def test_multicamera_layers_bit_exact(ctx, oracle, n_cams, colour, kernel):
     """Grey and colour layers with 3 and 5 other cameras (the per-camera cost paths, beyond four cameras too)."""
     from lux_b200 import api, synth
     cap = synth.capture(96, 72, n_cams, seed=30 + n_cams, f=72.0, baseline_mm=(15.0, 50.0), colour=colour)
     filt = _filtered(oracle, cap.images)
     p = api.StereoParams(scale=1, tile=8, skip_mode=0, plane_density=2.0)
     ol = oracle.layer(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True)
-    gl = api.DenseLayer.compute(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True, keep_agg=True, ctx=ctx)
+    gl = api.DenseLayer.compute(filt, cap.gray, cap.calibs, cap.near, cap.far, p, keep_pass1=True, keep_agg=True, sgm=kernel,
+                                ctx=ctx)
     try:
+        assert gl.sgm_kernel == SGM_FORMS[kernel]
         assert gl.cost_kernel == (1 if n_cams <= 5 else 0)
         _compare_layer(gl, ol, f"{n_cams}cam colour={colour}")
     finally:
         gl.close()
 
 
-def test_pyramid_bit_exact(ctx, oracle):
+@pytest.mark.parametrize("kernel", ["fused", "split"])
+def test_pyramid_bit_exact(ctx, oracle, kernel):
     """DenseStereoPyramid.Run: six L16 layers (ragged ranges, skip masks, align choice) against the oracle."""
     from lux_b200 import api, synth
     cap = synth.capture(416, 312, 3, seed=5, f=330.0)
     ol = oracle.pyramid(cap.images, cap.gray, cap.calibs, cap.near, cap.far, keep_pass1=True)
-    gls = api.DenseStereoPyramid.run(cap.images, cap.gray, cap.calibs, cap.near, cap.far, keep_pass1=True, keep_agg=True, ctx=ctx)
+    gls = api.DenseStereoPyramid.run(cap.images, cap.gray, cap.calibs, cap.near, cap.far, keep_pass1=True, keep_agg=True,
+                                     sgm=kernel, ctx=ctx)
     try:
+        assert gls[0].sgm_kernel == SGM_FORMS[kernel]  # the first layer is uniform; the others take the replay
         for i in range(6):
             _compare_layer(gls[i], ol[i], f"L{i}")
     finally:
