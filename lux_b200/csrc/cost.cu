@@ -9,8 +9,8 @@
 // Half-pixel phases: the resampled block value at (x, y) with fractions (hx, hy) is pavgb over rows first, then over
 // columns, of the 2x2 neighbourhood at (x, y) (:248-253); it depends on (x, y, hx, hy) only, so k_phase_* writes the four
 // phase images of every other camera once per layer and a plane's 3x3 block is three row loads with no averaging:
-//   grey camera (weights {12240, 0, 0, 0}, only Y contributes): one u32 per pixel and phase holding the Y bytes of
-//     columns x..x+3, so a block row is one aligned load; |t - r| capped at 2 in u16x2 lanes (min/max.u16x2);
+//   grey camera (weights {12240, 0, 0, 0}, only Y contributes): per pixel and phase the Y bytes of columns x, x+1, x+2
+//     as u16 pairs {x | x+2 << 16, x+1}, so a block row is one 8-byte load; |t - r| capped at 2 in u16x2 lanes;
 //   colour camera: the RGBA word per pixel and phase; even bytes (Y, V) and odd bytes (U, A) as u16x2 lanes.
 // Both are exact restatements of the reference's byte-lane sums (each channel sum is at most 9·6).
 #include <climits>
@@ -46,16 +46,15 @@ LUX_DEV int phase_byte(const uint8_t* img, int iw, int ih, int x, int y, int h, 
   return (h & 1) ? avg_u8(a, b) : a;
 }
 
-// Grey: out[h][y][x] = Y bytes of phase h at columns x, x+1, x+2, x+3 (little-endian).
-__global__ void k_phase_grey(const uint8_t* __restrict__ img, int iw, int ih, uint32_t* __restrict__ out) {
+// Grey: out[h][y][x] = the Y bytes of phase h at columns x, x+1, x+2 as u16 pairs: {x | x+2 << 16, x+1}.
+__global__ void k_phase_grey(const uint8_t* __restrict__ img, int iw, int ih, uint2* __restrict__ out) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
   if (x >= iw) return;
 #pragma unroll
   for (int h = 0; h < 4; h++) {
-    uint32_t v = 0;
-#pragma unroll
-    for (int j = 0; j < 4; j++) v |= (uint32_t)phase_byte(img, iw, ih, min(x + j, iw - 1), y, h, 0) << (8 * j);
-    out[((size_t)h * ih + y) * iw + x] = v;
+    const uint32_t p0 = phase_byte(img, iw, ih, x, y, h, 0), p1 = phase_byte(img, iw, ih, min(x + 1, iw - 1), y, h, 0),
+                   p2 = phase_byte(img, iw, ih, min(x + 2, iw - 1), y, h, 0);
+    out[((size_t)h * ih + y) * iw + x] = make_uint2(p0 | (p2 << 16), p1);
   }
 }
 // Colour: out[h][y][x] = the RGBA word of phase h.
@@ -71,17 +70,32 @@ __global__ void k_phase_colour(const uint8_t* __restrict__ img, int iw, int ih, 
   }
 }
 
-// Grey block: S0 = Σ min(|t - r|, 2) over the 3x3 Y block; row q of the target is one word (bytes t0..t2 used, the
-// fourth lane's cap is 0). re/ro: the reference row's even bytes (r0 | r2 << 16) and odd byte (r1).
-LUX_DEV int grey_cost(const uint32_t* __restrict__ q, int iw, const uint32_t (&re)[3], const uint32_t (&ro)[3]) {
+// Grey block: S0 = Σ min(|t - r|, 2) over the 3x3 Y block. Row r of the target is one 8-byte load {t0 | t2 << 16, t1}.
+// In each u16 lane max(t + (256 - r), (256 + r) - t) = 256 + |t - r|, so min(., 258) - 256 is the capped difference
+// with two adds and two min/max instead of three min/max and a subtract (the 256s are removed once, at the end); the
+// unused upper lane of the odd word is capped at 256 (a zero term).
+struct GreyRef {
+  uint32_t ea[3], eb[3], oa[3], ob[3];  // per row: 256 - r and 256 + r for the lanes {r0, r2} and {r1, 0}
+};
+LUX_DEV GreyRef grey_ref(const uint32_t (&ge)[3], const uint32_t (&go)[3]) {
+  GreyRef g;
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    g.ea[r] = 0x01000100u - ge[r];
+    g.eb[r] = 0x01000100u + ge[r];
+    g.oa[r] = 0x01000100u - go[r];
+    g.ob[r] = 0x01000100u + go[r];
+  }
+  return g;
+}
+LUX_DEV int grey_cost(const uint2* __restrict__ q, int iw, const GreyRef& g) {
   uint32_t s = 0;
 #pragma unroll
   for (int r = 0; r < 3; r++) {
-    const uint32_t t = __ldg(q + (size_t)r * iw);
-    const uint32_t te = __byte_perm(t, 0, 0x4240), to = __byte_perm(t, 0, 0x4341);
-    s += vmin2c(absdiff2(te, re[r]), 0x00020002u) + vmin2c(absdiff2(to, ro[r]), 0x00000002u);
+    const uint2 t = __ldg(q + (size_t)r * iw);
+    s += vmin2c(vmax2c(t.x + g.ea[r], g.eb[r] - t.x), 0x01020102u) + vmin2c(vmax2c(t.y + g.oa[r], g.ob[r] - t.y), 0x01000102u);
   }
-  const int S0 = (int)((s & 0xffffu) + (s >> 16));
+  const int S0 = (int)((s & 0xffffu) + (s >> 16)) - 12 * 256;
   return (S0 * 12240 + 16) >> 5;
 }
 
@@ -145,6 +159,7 @@ __global__ void __launch_bounds__(256) k_cost(const CostArgs a, const LayerGeom 
       ge[r] = yb[0] | (yb[2] << 16);
       go[r] = yb[1];
     }
+    const GreyRef gr = grey_ref(ge, go);
     const float xf = (float)xImg, yf = (float)yImg;
     for (int c0 = 0; c0 < count; c0 += 32) {
       const int d = c0 + lane;
@@ -179,9 +194,9 @@ __global__ void __launch_bounds__(256) k_cost(const CostArgs a, const LayerGeom 
         }
         int costK = 0;
         if (inb) {
-          const uint32_t* q = a.phase[k] + ((size_t)h * ih + (iy - 1)) * iw + (ix - 1);
-          if (GREY) costK = grey_cost(q, iw, ge, go);
-          else costK = colour_cost(q, iw, re, ro, a.wq[k]);
+          const size_t qi = ((size_t)h * ih + (iy - 1)) * iw + (ix - 1);
+          if (GREY) costK = grey_cost(reinterpret_cast<const uint2*>(a.phase[k]) + qi, iw, gr);
+          else costK = colour_cost(a.phase[k] + qi, iw, re, ro, a.wq[k]);
         }
         const uint32_t m = __ballot_sync(0xffffffffu, inb);
         const uint32_t below = m & ((1u << lane) - 1u);
@@ -248,6 +263,7 @@ __global__ void __launch_bounds__(256) k_cost_rows(const CostArgs a, const Layer
       ge[r] = yb[0] | (yb[2] << 16);
       go[r] = yb[1];
     }
+    const GreyRef gr = grey_ref(ge, go);
     const float xf = (float)xImg, yf = (float)yImg;
     int last[NK];
 #pragma unroll
@@ -274,8 +290,9 @@ __global__ void __launch_bounds__(256) k_cost_rows(const CostArgs a, const Layer
         const int ix = tx >> 1, iy = ty >> 1;
         if (ix >= 1 && ix < x1 && iy >= 1 && iy < y1) {
           const int h = ((ty & 1) << 1) | (tx & 1);
-          const uint32_t* q = a.phase[k] + ((size_t)h * ihk[k] + (iy - 1)) * iwk[k] + (ix - 1);
-          last[k] = GREY ? grey_cost(q, iwk[k], ge, go) : colour_cost(q, iwk[k], re, ro, a.wq[k]);
+          const size_t qi = ((size_t)h * ihk[k] + (iy - 1)) * iwk[k] + (ix - 1);
+          last[k] = GREY ? grey_cost(reinterpret_cast<const uint2*>(a.phase[k]) + qi, iwk[k], gr)
+                         : colour_cost(a.phase[k] + qi, iwk[k], re, ro, a.wq[k]);
         } else if (d == 0) {  // the scalar fallback of the reference would read out of the image
           atomicCAS(err, 0, 7);
         }
@@ -342,6 +359,7 @@ __global__ void __launch_bounds__(256) k_cost_axis(const CostArgs a, const Layer
       ge[r] = yb[0] | (yb[2] << 16);
       go[r] = yb[1];
     }
+    const GreyRef gr = grey_ref(ge, go);
     const float xf = (float)xImg, yf = (float)yImg;
     int last = 0;
     uint32_t pk0 = 0, pk1 = 0;
@@ -369,8 +387,8 @@ __global__ void __launch_bounds__(256) k_cost_axis(const CostArgs a, const Layer
       const int ix = tx >> 1, iy = ty >> 1;
       if (ix >= 1 && ix < x1 && iy >= 1 && iy < y1) {
         if (live) {
-          const uint32_t* q = phase + ((size_t)(((ty & 1) << 1) | (tx & 1)) * ih + (iy - 1)) * iw + (ix - 1);
-          last = GREY ? grey_cost(q, iw, ge, go) : colour_cost(q, iw, re, ro, a.wq[0]);
+          const size_t qi = ((size_t)(((ty & 1) << 1) | (tx & 1)) * ih + (iy - 1)) * iw + (ix - 1);
+          last = GREY ? grey_cost(reinterpret_cast<const uint2*>(phase) + qi, iw, gr) : colour_cost(phase + qi, iw, re, ro, a.wq[0]);
         }
       } else if (live) {  // the scalar fallback of the reference would read out of the image
         atomicCAS(err, 0, 7);
@@ -398,8 +416,8 @@ __global__ void __launch_bounds__(256) k_cost_axis(const CostArgs a, const Layer
           const float fx = __fadd_rn(__fmul_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0)), zk.w), 0.25f);
           const int tx = f2i(__fadd_rn(fx, fx)), ix = tx >> 1;
           if (ix >= 1 && ix < x1) {
-            const uint32_t* q = phase + (ro_d + (tx & 1) * plane_stride + ix);
-            last = GREY ? grey_cost(q, iw, ge, go) : colour_cost(q, iw, re, ro, a.wq[0]);
+            const int qi = ro_d + (tx & 1) * plane_stride + ix;
+            last = GREY ? grey_cost(reinterpret_cast<const uint2*>(phase) + qi, iw, gr) : colour_cost(phase + qi, iw, re, ro, a.wq[0]);
           }
         }
         put(d, (uint32_t)last);
@@ -419,7 +437,7 @@ void launch_phases(const CostArgs& a, cudaStream_t s) {
   for (int k = 0; k < a.n_others; k++) {
     dim3 grid((a.ow[k] + 127) / 128, a.oh[k]);
     uint32_t* out = const_cast<uint32_t*>(a.phase[k]);
-    if (grey) k_phase_grey<<<grid, 128, 0, s>>>(a.other[k], a.ow[k], a.oh[k], out);
+    if (grey) k_phase_grey<<<grid, 128, 0, s>>>(a.other[k], a.ow[k], a.oh[k], reinterpret_cast<uint2*>(out));
     else k_phase_colour<<<grid, 128, 0, s>>>(a.other[k], a.ow[k], a.oh[k], out);
     count_launches(1);
   }

@@ -31,7 +31,7 @@ struct CostArgs {
   const uint8_t* ref; int rw, rh;  // box-filtered reference image (dense RGBA8)
   int n_others;
   const uint8_t* other[kMaxCams];
-  const uint32_t* phase[kMaxCams];  // per other camera: its four half-pixel phase images ([4][oh][ow] u32, k_phase_*)
+  const uint32_t* phase[kMaxCams];  // per other camera: four half-pixel phase images, [4][oh][ow] of uint2 (grey) or u32
   int ow[kMaxCams], oh[kMaxCams];
   float warp[kMaxCams][16];
   uint16_t wq[kMaxCams][4];

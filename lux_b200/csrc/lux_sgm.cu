@@ -329,9 +329,10 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   float4* zt = nullptr;
   if ((rc = alloc_t(ctx, tmp, zt_h.size() / 4, &zt))) return rc;
   CK(cudaMemcpyAsync(zt, zt_h.data(), zt_h.size() * 4, cudaMemcpyHostToDevice, s));
+  const size_t phase_words = cost_all_grey(ca) ? 8 : 4;  // per pixel: four phases of {u16 pairs} (grey) or RGBA words
   for (int k = 0; k < ca.n_others; k++) {  // the half-pixel phase images of the other cameras
     uint32_t* ph = nullptr;
-    if ((rc = alloc_t(ctx, tmp, (size_t)4 * ca.ow[k] * ca.oh[k], &ph))) return rc;
+    if ((rc = alloc_t(ctx, tmp, phase_words * ca.ow[k] * ca.oh[k], &ph))) return rc;
     ca.phase[k] = ph;
   }
   CK(cudaEventRecord(ctx->ev[0], s));
