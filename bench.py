@@ -35,12 +35,13 @@ WORKLOADS = {  # name: (W, H, D, tile, bits, description)
     "preview": (520, 390, 32, 64, 8, "preview pair 520x390 u8, D=32, 8 paths, tile 64"),
 }
 W_, H_, D_, TILE, BITS, DESC = WORKLOADS["pair13mp"]
-# Algorithmic HBM bytes per disparity element (DE = one pixel x one plane) of the two aggregation launches, aggregates not
-# kept: pass +1 reads the u8 raw volume (1) and writes the u16 aggregates (2); pass -1 reads both again (1 + 2).
+# Algorithmic HBM bytes per disparity element (DE = one pixel x one plane) of a layer's aggregation, aggregates not kept:
+# pass +1 reads the u8 raw volume (1) and writes the u16 aggregates (2); pass -1 reads both again (1 + 2).
 BYTES_PER_DE_AGG = 6
-# DRAM bytes (read + write) per DE of one aggregation launch, from `ncu --set full` of both launches on the 2080x1560
-# D=256 pair (2.484 GB and 2.529 GB for 831 MDE); traffic grows in proportion to the DE count.
-TRAFFIC_PER_DE_LAUNCH = (2.484e9 + 2.529e9) / 2 / (2080 * 1560 * 256)
+# DRAM bytes (read + write) per DE of a layer's aggregation as built (the path-group chains: 4 launches per layer),
+# from ncu dram__bytes_read.sum + dram__bytes_write.sum on the 2080x1560 D=256 pair: 13.74 GB for 830.7 MDE. The split
+# design trades these extra bytes (agg read/written by both path groups, raw read by each) for a short critical path.
+TRAFFIC_PER_DE_LAYER = 13.74e9 / (2080 * 1560 * 256)
 
 
 def metric():
@@ -240,8 +241,8 @@ def run_lux(a):
     cost_ms = statistics.mean(x[0] for x in inf_v)
     wta_ms = statistics.mean(x[2] for x in inf_v)
     pk = peaks()
-    # per launch: the two aggregation launches each move half of the algorithmic bytes in (about) half of sgm_ms
-    achieved = (BYTES_PER_DE_AGG / 2) * de / (sgm_ms / 2 / 1e3) / 1e9
+    # per layer: the algorithmic bytes of both passes over the device time of the layer's aggregation launches
+    achieved = BYTES_PER_DE_AGG * de / (sgm_ms / 1e3) / 1e9
     out = {
         "metric": metric(), "value": value, "unit": "MDE/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_v / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -251,10 +252,10 @@ def run_lux(a):
                    "stages_ms": {"cost": cost_ms, "sgm_2_passes": sgm_ms, "wta": wta_ms},
                    "sgm_kernel": {0: "exact-replay", 1: "fused-wavefront", 2: "path-group-chains"}.get(inf_v[0][3] if inf_v else -1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
-                     "frac": achieved / pk.get("hbm_gbs"), "traffic": TRAFFIC_PER_DE_LAUNCH * de,
-                     "kernel": "SGM aggregation (per pass; 2 passes per layer)",
-                     "bytes_per_de_per_launch": BYTES_PER_DE_AGG / 2,
-                     "traffic_source": "ncu dram__bytes_read+write of the 2080x1560 D=256 launches, scaled by DE",
+                     "frac": achieved / pk.get("hbm_gbs"), "traffic": TRAFFIC_PER_DE_LAYER * de,
+                     "kernel": "SGM aggregation of one layer (both passes; 4 chain launches, or 2 fused ones below 2 MP)",
+                     "bytes_per_de": BYTES_PER_DE_AGG, "traffic_per_de": TRAFFIC_PER_DE_LAYER,
+                     "traffic_source": "ncu dram__bytes_read+write of the 2080x1560 D=256 chain launches, scaled by DE",
                      "peak_source": "fallback" if pk.get("fallback") else "MEASURED_PEAKS.json hbm_gbs (measured)"},
         "e2e": {"value": e2e, "unit": "MDE/s", "h2d_bytes_per_step": sum(im.nbytes for im in wl.images),
                 "d2h_bytes_per_step": W_ * H_ * 4},
