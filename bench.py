@@ -31,6 +31,8 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {  # name: (W, H, D, tile, bits, description)
     "pair13mp": (4160, 3120, 256, 64, 12, "plain 13 MP pair 4160x3120 u16 12-bit -> u8, D=256, 8 paths, tile 64, P1 1, P2 500 adaptive"),
     "pair3mp": (2080, 1560, 256, 64, 12, "plain 3 MP pair 2080x1560 u16 12-bit -> u8, D=256, 8 paths, tile 64, P1 1, P2 500 adaptive"),
+    "capture10": (2080, 1560, 0, 64, 0, "batched capture: 2080x1560 reference + 10 module cameras (1-6 MP crops, focal 1.0-2.7x, "
+                  "D_k in {64,96,128,192}), one layer summing all costs, grey u8"),
     "pair1mp": (1040, 780, 64, 64, 8, "plain pair 1040x780 u8, D=64, 8 paths, tile 64, P1 1, P2 500 adaptive"),
     "preview": (520, 390, 32, 64, 8, "preview pair 520x390 u8, D=32, 8 paths, tile 64"),
 }
@@ -45,6 +47,8 @@ TRAFFIC_PER_DE_LAYER = 13.74e9 / (2080 * 1560 * 256)
 
 
 def metric():
+    if BITS == 0:
+        return f"SGM MDE/s (W·H·D per second), {W_}x{H_} reference + 10 module cameras D={D_}, bit-exact"
     return f"SGM MDE/s (W·H·D per second), {W_}x{H_} pair D={D_}, bit-exact"
 
 
@@ -131,13 +135,20 @@ def l2_note():
 
 def workload(seed=0):
     from lux_b200 import synth
+    if BITS == 0:  # a batched module capture: the reference grid W_ x H_ and 10 other cameras
+        from lux_b200 import api
+        mc = synth.module_capture(W_, H_, seed=seed, tile=TILE)
+        global D_
+        D_ = len(api.DenseStereo.planes(mc.near, mc.far, mc.calibs, mc.params.plane_density, 8))  # the layer's n
+        return mc
     return synth.rectified_pair(W_, H_, D_, seed=seed, bits=BITS, tile=TILE)
 
 
 def cpu_sample(wl, rows, threads):
     """The oracle (CPU restatement) on a row strip of the workload: cost prepass on `threads` cores, serial SGM."""
     from oracle import oracle as O
-    imgs = [np.ascontiguousarray(im[:rows]) for im in wl.images]
+    # a strip of the reference image; the other cameras stay whole (their geometry is their own)
+    imgs = [np.ascontiguousarray(wl.images[0][:rows])] + [np.ascontiguousarray(im) for im in wl.images[1:]]
     t0 = time.perf_counter()
     filt = [O.box_filter3(im) for im in imgs]
     O.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, threads=threads)

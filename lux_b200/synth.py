@@ -179,3 +179,75 @@ def capture(w, h, n_cams, seed=0, f=None, baseline_mm=(8.0, 40.0), near=200.0, f
         cal.append(CalibData(K.copy(), (-t).astype(np.float32), R.copy()))
     gray = [0 if colour else 1] * n_cams
     return CaptureWorkload(imgs, gray, cal, near, far, z_inv)
+
+
+@dataclass
+class ModuleCapture(CaptureWorkload):
+    """A capture of one reference module and several others, each with its own crop, focal scale and disparity range."""
+    sizes: List[tuple]        # (w, h) per camera
+    d_per_camera: List[int]   # the disparity range each other camera spans between near and the far plane
+    params: StereoParams = None
+
+    @property
+    def de(self):
+        h, w = self.images[0].shape[:2]
+        return w * h * max(self.d_per_camera)
+
+
+def module_capture(w, h, n_others=10, seed=0, crop_mp=(1.0, 6.0), ds=(64, 96, 128, 192), near=400.0, far=1e30,
+                   size_scale=1.0, tile=64):
+    """A batched full capture: reference camera 0 (w x h, focal 0.9 w) and n_others module cameras, half "wide" (focal
+    scale 1.0-1.3) and half "tele" (2.2-2.7), each with a crop uniform in crop_mp megapixels (4:3, times size_scale in
+    area) and a disparity range D_k drawn from ds, realised by its baseline B_k = D_k·near/f_k in a random direction
+    (R = I). Grey u8 images (Y = texture, U = V = 128). The scene is the reference texture on six planar patches at
+    near-6 m; camera k sees it through a backward warp (two fixed-point steps for the parallax). One layer over all
+    cameras sums their costs (the reference's fusion) with n = max D_k planes (density 1)."""
+    rng = np.random.default_rng(seed)
+    f0 = 0.9 * w
+    cx0, cy0 = (w - 1) / 2.0, (h - 1) / 2.0
+    # the scene on a canvas three times the reference extent (wide cameras see beyond the reference crop)
+    H3, W3 = 3 * h, 3 * w
+    tex = texture(H3, W3, seed * 13 + 1, 255.0)
+    z_inv = 1.0 / np.clip(planar_disparity(H3, W3, 1.0, seed) * (6000.0 - near) + near, near, 6000.0)
+
+    def scene(x, y):  # reference-pixel coordinates -> (texture, 1/Z) by nearest sampling on the canvas
+        xi = np.clip(np.rint(x + w), 0, W3 - 1).astype(np.int64)
+        yi = np.clip(np.rint(y + h), 0, H3 - 1).astype(np.int64)
+        return tex[yi, xi], z_inv[yi, xi]
+
+    R = np.eye(3, dtype=np.float32).reshape(9)
+    K0 = np.array([f0, 0, cx0, 0, f0, cy0, 0, 0, 1], np.float32)
+    imgs, cal, sizes, dk = [], [], [], []
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    t0, _ = scene(xx, yy)
+    imgs.append(gray_rgba(to_u8(np.rint(t0 + rng.standard_normal(t0.shape) * 1.5), 8)))
+    cal.append(CalibData(K0.copy(), np.zeros(3, np.float32), R.copy()))
+    sizes.append((w, h))
+    for k in range(n_others):
+        tele = k >= n_others // 2
+        s = rng.uniform(2.2, 2.7) if tele else rng.uniform(1.0, 1.3)
+        mp = rng.uniform(*crop_mp) * 1e6 * size_scale
+        hk = max(8, int(round(np.sqrt(mp * 3.0 / 4.0))))
+        wk = max(8, int(round(hk * 4.0 / 3.0)))
+        fk = f0 * s
+        d = int(rng.choice(ds))
+        b = d * near / fk
+        ang = rng.uniform(0, 2 * np.pi)
+        t = np.array([b * np.cos(ang), b * np.sin(ang), 0.0], np.float32)
+        cxk, cyk = (wk - 1) / 2.0, (hk - 1) / 2.0
+        v, u = np.mgrid[0:hk, 0:wk].astype(np.float32)
+        # camera k sees the scene point at reference (x, y) at u = cxk + fk·((x - cx0)/f0 + t_x/Z)
+        x = cx0 + f0 * (u - cxk) / fk
+        y = cy0 + f0 * (v - cyk) / fk
+        for _ in range(2):
+            _, zi = scene(x, y)
+            x = cx0 + f0 * ((u - cxk) / fk - t[0] * zi)
+            y = cy0 + f0 * ((v - cyk) / fk - t[1] * zi)
+        tk, _ = scene(x, y)
+        imgs.append(gray_rgba(to_u8(np.rint(tk + rng.standard_normal(tk.shape) * 1.5), 8)))
+        K = np.array([fk, 0, cxk, 0, fk, cyk, 0, 0, 1], np.float32)
+        cal.append(CalibData(K, (-t).astype(np.float32), R.copy()))
+        sizes.append((wk, hk))
+        dk.append(d)
+    params = StereoParams(scale=1, tile=tile, skip_mode=0, plane_density=1.0)
+    return ModuleCapture(imgs, [1] * (n_others + 1), cal, near, far, z_inv[h:2 * h, w:2 * w], sizes, dk, params)

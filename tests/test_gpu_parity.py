@@ -165,6 +165,24 @@ def test_multicamera_layers_bit_exact(ctx, oracle, n_cams, colour, kernel):
 
 
 @pytest.mark.parametrize("kernel", ["fused", "split"])
+def test_module_capture_bit_exact(ctx, oracle, kernel):
+    """A batched capture: 10 module cameras with their own crops, focal scales and disparity ranges, fused at cost level
+    into one layer (the reference's multi-view sum, DenseStereo.cs:242-291)."""
+    from lux_b200 import api, synth
+    mc = synth.module_capture(96, 72, seed=3, size_scale=0.002, tile=8)
+    assert len({s for s in mc.sizes}) > 5
+    filt = _filtered(oracle, mc.images)
+    ol = oracle.layer(filt, mc.gray, mc.calibs, mc.near, mc.far, mc.params, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, mc.gray, mc.calibs, mc.near, mc.far, mc.params, keep_pass1=True, keep_agg=True, sgm=kernel,
+                                ctx=ctx)
+    try:
+        assert gl.sgm_kernel == SGM_FORMS[kernel]
+        _compare_layer(gl, ol, f"module capture {kernel}")
+    finally:
+        gl.close()
+
+
+@pytest.mark.parametrize("kernel", ["fused", "split"])
 def test_pyramid_bit_exact(ctx, oracle, kernel):
     """DenseStereoPyramid.Run: six L16 layers (ragged ranges, skip masks, align choice) against the oracle."""
     from lux_b200 import api, synth
