@@ -216,7 +216,8 @@ __global__ void __launch_bounds__(256) k_cost(const CostArgs a, const LayerGeom 
   }
 }
 
-// Uniform layers (every pixel searches planes [0, n), cap n, n % 8 == 0): lanes over 32 neighbouring pixels of a row,
+// Uniform layers (every pixel searches planes [0, n), cap n, n % 8 == 0; 1 to 15 other cameras): lanes over 32
+// neighbouring pixels of a row,
 // each lane walking its pixel's planes in order like the reference's loop, so the last computed cost of a camera
 // (:273-274) is a register, the plane terms are the same for the whole warp, and the camera constants stay in
 // registers. Eight planes of u8 costs go out per 8-byte store. Skipped pixels get raw 0 (DenseStereoSgm.cs:242).
@@ -229,15 +230,9 @@ __global__ void __launch_bounds__(256) k_cost_rows(const CostArgs a, const Layer
   const int n = g.n_planes;
   const int half = (a.scale + (a.scale >> 31)) >> 1;
   const uint32_t* ref = reinterpret_cast<const uint32_t*>(a.ref);
-  // camera constants
-  float w0[NK], w1[NK], w2[NK], w4[NK], w5[NK], w6[NK];
-  int iwk[NK], ihk[NK];
-#pragma unroll
-  for (int k = 0; k < NK; k++) {
-    w0[k] = a.warp[k][0]; w1[k] = a.warp[k][1]; w2[k] = a.warp[k][2];
-    w4[k] = a.warp[k][4]; w5[k] = a.warp[k][5]; w6[k] = a.warp[k][6];
-    iwk[k] = a.ow[k]; ihk[k] = a.oh[k];
-  }
+  // NK cameras exactly (NK <= 4), or up to NK with a.n_others of them; the camera loops are unrolled, so the camera
+  // constants are kernel-argument operands
+  const int nk = NK <= 4 ? NK : a.n_others;
   for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += (gridDim.x * blockDim.x) >> 5) {
     const int y = t / tiles_x, x = ((t - y * tiles_x) << 5) + lane;
     if (x >= g.W) continue;
@@ -275,13 +270,16 @@ __global__ void __launch_bounds__(256) k_cost_rows(const CostArgs a, const Layer
       uint32_t acc = 0;
 #pragma unroll
       for (int k = 0; k < NK; k++) {
+        if (k >= nk) break;
+        const float* Wm = a.warp[k];
+        const int iwk = a.ow[k], ihk = a.oh[k];
         const float4 zk = __ldg(zt + (size_t)k * n + d);
-        const float px = __fadd_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0[k])), __fmul_rn(yz, w4[k]));
-        const float py = __fadd_rn(__fadd_rn(zk.y, __fmul_rn(xz, w1[k])), __fmul_rn(yz, w5[k]));
-        const float pz = __fadd_rn(__fadd_rn(zk.z, __fmul_rn(xz, w2[k])), __fmul_rn(yz, w6[k]));
+        const float px = __fadd_rn(__fadd_rn(zk.x, __fmul_rn(xz, Wm[0])), __fmul_rn(yz, Wm[4]));
+        const float py = __fadd_rn(__fadd_rn(zk.y, __fmul_rn(xz, Wm[1])), __fmul_rn(yz, Wm[5]));
+        const float pz = __fadd_rn(__fadd_rn(zk.z, __fmul_rn(xz, Wm[2])), __fmul_rn(yz, Wm[6]));
         const float inv = __frcp_rn(pz);
         float fx = __fadd_rn(__fmul_rn(px, inv), 0.25f), fy = __fadd_rn(__fmul_rn(py, inv), 0.25f);
-        const int x1 = iwk[k] - 2, y1 = ihk[k] - 2;
+        const int x1 = iwk - 2, y1 = ihk - 2;
         if (d == 0) {  // the first plane is clamped into the rect (:263-269)
           fx = cs_minf(cs_maxf(fx, 1.0f), (float)(x1 - 1));
           fy = cs_minf(cs_maxf(fy, 1.0f), (float)(y1 - 1));
@@ -290,9 +288,9 @@ __global__ void __launch_bounds__(256) k_cost_rows(const CostArgs a, const Layer
         const int ix = tx >> 1, iy = ty >> 1;
         if (ix >= 1 && ix < x1 && iy >= 1 && iy < y1) {
           const int h = ((ty & 1) << 1) | (tx & 1);
-          const size_t qi = ((size_t)h * ihk[k] + (iy - 1)) * iwk[k] + (ix - 1);
-          last[k] = GREY ? grey_cost(reinterpret_cast<const uint2*>(a.phase[k]) + qi, iwk[k], gr)
-                         : colour_cost(a.phase[k] + qi, iwk[k], re, ro, a.wq[k]);
+          const size_t qi = ((size_t)h * ihk + (iy - 1)) * iwk + (ix - 1);
+          last[k] = GREY ? grey_cost(reinterpret_cast<const uint2*>(a.phase[k]) + qi, iwk, gr)
+                         : colour_cost(a.phase[k] + qi, iwk, re, ro, a.wq[k]);
         } else if (d == 0) {  // the scalar fallback of the reference would read out of the image
           atomicCAS(err, 0, 7);
         }
@@ -450,7 +448,8 @@ static void launch_rows(int nk, int blocks, const CostArgs& a, const LayerGeom& 
     case 1: k_cost_rows<GREY, 1><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
     case 2: k_cost_rows<GREY, 2><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
     case 3: k_cost_rows<GREY, 3><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
-    default: k_cost_rows<GREY, 4><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
+    case 4: k_cost_rows<GREY, 4><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
+    default: k_cost_rows<GREY, kMaxCams - 1><<<blocks, 256, 0, s>>>(a, g, zt, raw, err); break;
   }
 }
 
@@ -458,7 +457,7 @@ int launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t
   const int npx = g.W * g.H;
   const bool grey = cost_all_grey(a);
   int kind = 0;
-  if (g.uniform && g.n_planes % 8 == 0 && a.n_others >= 1 && a.n_others <= 4) {
+  if (g.uniform && g.n_planes % 8 == 0 && a.n_others >= 1 && a.n_others <= kMaxCams - 1) {
     const int tiles = ((g.W + 31) / 32) * g.H;
     int blocks = (tiles + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
