@@ -162,6 +162,39 @@ int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int3
                      const lux_img_rgba8* guide, int32_t set_w, int32_t set_h, float sigma, int32_t scale,
                      const float* prev_conf, float* out_depth, float* out_conf);
 
+/* ---- Request server. No counterpart in the reference: the serving form of the stage. ----
+ * Depth solves of mixed sizes are admitted in arrival order against an HBM budget (a host-side estimate per request;
+ * 0 = no limit; a request runs regardless when nothing else is running) and run on `slots` worker contexts, each with
+ * its own CUDA stream, so requests that arrive while others are on the GPU start as soon as a slot and memory are free
+ * and overlap on the device. A request is one layer, solved exactly as lux_sgm_layer solves it from unfiltered images
+ * (LUX_LAYER_PREFILTER is implied; prev = NULL, align 8), its depth map copied into out_depth (host, the layer's w*h
+ * floats, out_bytes long; NULL: nothing copied). The server copies the request's small arrays at submit; the caller
+ * keeps the image data and out_depth alive until lux_server_wait has returned for the ticket. Every result equals the
+ * same request solved alone. */
+typedef struct lux_server lux_server;
+typedef struct {
+  int32_t n_cams;
+  const lux_img_rgba8* images;
+  const uint8_t* gray;
+  const lux_calib* calibs;
+  float near_, far_;
+  lux_stereo_params params;
+  int32_t flags;
+  float* out_depth;
+  uint64_t out_bytes;
+} lux_request;
+typedef struct {
+  int32_t status;           /* LUX_OK or the status the solve returned */
+  int32_t w, h, n_planes;   /* the layer's size and plane count */
+  double queue_ms, run_ms;  /* submit -> start of the solve, start -> depth in out_depth */
+} lux_result;
+int lux_server_create(int device, uint64_t hbm_budget_bytes, int32_t slots, lux_server** out);
+void lux_server_destroy(lux_server* server);  /* finishes the requests already submitted */
+const char* lux_server_last_error(const lux_server* server);
+int lux_server_submit(lux_server* server, const lux_request* req, uint64_t* ticket);
+/* Waits for a ticket (timeout_ns 0: no limit; LUX_ERR_TIMEOUT when it passes) and releases it. */
+int lux_server_wait(lux_server* server, uint64_t ticket, uint64_t timeout_ns, lux_result* out);
+
 /* No counterpart in the reference. lux_sgm_upsample without any device allocation, for hosts that cannot let this
  * library allocate GPU memory: a process whose HBM is already reserved by another allocator (an inference server or a
  * framework's caching pool holding nearly all of it), where a cudaMalloc here would fail or fragment that pool, and a

@@ -37,6 +37,17 @@ class Params(ctypes.Structure):
                 ("p2scale", ctypes.c_float), ("guidance", ctypes.c_float * 4), ("tile", ctypes.c_int32)]
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("n_cams", ctypes.c_int32), ("images", ctypes.c_void_p), ("gray", ctypes.c_void_p), ("calibs", ctypes.c_void_p),
+                ("near", ctypes.c_float), ("far", ctypes.c_float), ("params", Params), ("flags", ctypes.c_int32),
+                ("out_depth", ctypes.c_void_p), ("out_bytes", ctypes.c_uint64)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("w", ctypes.c_int32), ("h", ctypes.c_int32), ("n_planes", ctypes.c_int32),
+                ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double)]
+
+
 class LayerInfo(ctypes.Structure):
     _fields_ = [("w", ctypes.c_int32), ("h", ctypes.c_int32), ("index", ctypes.c_int32), ("align", ctypes.c_int32),
                 ("n_planes", ctypes.c_int32), ("min_lo", ctypes.c_int32), ("max_hi", ctypes.c_int32), ("tile", ctypes.c_int32),
@@ -72,6 +83,11 @@ SIGNATURES = [
     ("lux_sgm_upsample", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.POINTER(Img), ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_int32,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("lux_server_create", ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    ("lux_server_destroy", None, [ctypes.c_void_p]),
+    ("lux_server_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("lux_server_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]),
+    ("lux_server_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(Result)]),
     ("lux_sgm_upsample_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.POINTER(Img), ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
                                                 ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),

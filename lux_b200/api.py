@@ -358,3 +358,68 @@ class DenseUpsampleLayer:
         ctx.check(rc)
         return UpsampleResult(out.reshape(gi.h, gi.w), gi.w, gi.h,
                               conf_out.reshape(gi.h, gi.w) if conf_out is not None else None)
+
+
+@dataclass
+class ServedResult:
+    """One served request: its depth map (the layer grid) and the times it spent queued and running."""
+    Depth: np.ndarray
+    status: int
+    n_planes: int
+    queue_ms: float
+    run_ms: float
+
+
+class Server:
+    """The request server of the C ABI (lux_server_*; no counterpart in the reference): depth solves of mixed sizes
+    admitted in arrival order against an HBM budget and run on `slots` worker contexts, overlapping on the GPU. A request
+    is one layer solved from unfiltered images exactly as DenseLayer.compute(..., prefilter=True) solves it."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, slots: int = 3):
+        self.lib = L.load()
+        h = ctypes.c_void_p()
+        rc = self.lib.lux_server_create(device, hbm_budget_bytes, slots, ctypes.byref(h))
+        if rc:
+            _raise(rc, "lux_server_create failed")
+        self.handle = h
+        self._pending = {}
+
+    def submit(self, images, gray, calibs, near, far, params: StereoParams, flags: int = 0) -> int:
+        arr = (L.Img * len(images))()
+        keep = []
+        for i, im in enumerate(images):
+            ci, k = _img_c(im)
+            arr[i] = ci
+            keep.append(k)
+        g = np.ascontiguousarray(np.asarray(gray, dtype=np.uint8))
+        cc = _calibs_c(calibs)
+        h0, w0 = np.asarray(images[0]).shape[:2] if not hasattr(images[0], "data_ptr") else images[0].shape[:2]
+        sc = max(1, int(params.scale))
+        out = np.empty(((h0 + sc - 1) // sc, (w0 + sc - 1) // sc), np.float32)
+        req = L.Request(len(images), ctypes.cast(arr, ctypes.c_void_p), g.ctypes.data, ctypes.cast(cc, ctypes.c_void_p), near, far,
+                        params.to_c(), flags, out.ctypes.data, out.nbytes)
+        t = ctypes.c_uint64()
+        rc = self.lib.lux_server_submit(self.handle, ctypes.byref(req), ctypes.byref(t))
+        if rc:
+            _raise(rc, self.lib.lux_server_last_error(self.handle).decode())
+        self._pending[t.value] = (out, keep, arr, g, cc)  # the image data and the output stay alive until wait
+        return t.value
+
+    def wait(self, ticket: int, timeout_ns: int = 0) -> ServedResult:
+        r = L.Result()
+        rc = self.lib.lux_server_wait(self.handle, ticket, timeout_ns, ctypes.byref(r))
+        if rc:
+            _raise(rc, self.lib.lux_server_last_error(self.handle).decode())
+        out = self._pending.pop(ticket)[0]
+        return ServedResult(out, r.status, r.n_planes, r.queue_ms, r.run_ms)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.lux_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
