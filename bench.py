@@ -65,6 +65,8 @@ def args_():
     p.add_argument("--requests", type=int, default=400)
     p.add_argument("--rate", type=float, default=40.0, help="mean arrivals per second of the served stream")
     p.add_argument("--slots", type=int, default=3)
+    p.add_argument("--sweep", action="store_true",
+                   help="throughput with 1, 4, 16 and 64 module captures in flight through the request server")
     p.add_argument("--cpu-rows", type=int, default=130, help="rows of the CPU sample strip")
     p.add_argument("--workload", default="pair13mp", choices=sorted(WORKLOADS),
                    help="pair13mp is the benchmark; the smaller pairs are for profiling captures")
@@ -389,8 +391,46 @@ def run_serve(a):
     print(json.dumps(out))
 
 
+def run_sweep(a):
+    """Saturation: N batched module captures (2080x1560 reference + 10 cameras, two distinct seeded inputs on the device)
+    submitted at once to the request server, for N in 1, 4, 16, 64; MDE/s of the whole batch and its wall time."""
+    import torch
+    from lux_b200 import api, synth
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    caps = []
+    for k in range(2):
+        mc = synth.module_capture(2080, 1560, seed=400 + k, tile=64)
+        n = len(api.DenseStereo.planes(mc.near, mc.far, mc.calibs, mc.params.plane_density, 8))
+        caps.append(([torch.from_numpy(np.ascontiguousarray(im)).cuda() for im in mc.images], mc, 2080 * 1560 * n))
+    torch.cuda.synchronize()
+    srv = api.Server(0, hbm_budget_bytes=120 * 10**9, slots=a.slots)
+    for imgs, mc, _ in caps:  # warm-up
+        srv.wait(srv.submit(imgs, mc.gray, mc.calibs, mc.near, mc.far, mc.params))
+    points = []
+    for n_flight in (1, 4, 16, 64):
+        t0 = time.perf_counter()
+        tickets = [srv.submit(caps[i % 2][0], caps[i % 2][1].gray, caps[i % 2][1].calibs, caps[i % 2][1].near,
+                              caps[i % 2][1].far, caps[i % 2][1].params) for i in range(n_flight)]
+        for t in tickets:
+            assert srv.wait(t).status == 0
+        dt = time.perf_counter() - t0
+        de = sum(caps[i % 2][2] for i in range(n_flight))
+        points.append({"in_flight": n_flight, "mde_per_s": de / dt / 1e6, "wall_s": dt})
+    srv.close()
+    print(json.dumps({"metric": "MDE/s with N module captures in flight (request server)", "value": points[-1]["mde_per_s"],
+                      "unit": "MDE/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "u8 cost / u16 aggregation", "data": "synthetic (two seeded captures on the device)",
+                      "config": {"workload": "batched module capture 2080x1560 + 10 cameras", "slots": a.slots},
+                      "sweep": points}))
+
+
 def main():
     a = args_()
+    if a.sweep:
+        run_sweep(a)
+        return
     if a.serve:
         run_serve(a)
         return
