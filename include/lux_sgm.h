@@ -33,6 +33,8 @@ extern "C" {
 #define LUX_ERR_TIMEOUT 11      /* a bounded device-side wait gave up (the kernel returned without finishing) */
 #define LUX_ERR_UNSUPPORTED 12  /* inputs outside what this implementation supports (message says which) */
 #define LUX_ERR_CANCELED 13     /* OperationCanceledException: the request was canceled before it started */
+#define LUX_ERR_ROI 14          /* InvalidOperationException "invalid ROI requested!" (DepthCache.cs:164) */
+#define LUX_ERR_EMPTY_IMAGE 15  /* InvalidOperationException "empty image!" (DepthCache.cs:67) */
 
 /* Rgba8Image (Lux.Engine/Pipeline/Registration/SparseLnrMatch.cs:8-13): 8-bit RGBA ("YUVA"), stride in pixels.
  * on_device != 0: data is a device pointer of the context's GPU (no copy); else host memory. */
@@ -161,6 +163,17 @@ void lux_layer_destroy(lux_layer* layer);
 int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int32_t ph, int32_t prev_on_device,
                      const lux_img_rgba8* guide, int32_t set_w, int32_t set_h, float sigma, int32_t scale,
                      const float* prev_conf, float* out_depth, float* out_conf);
+
+/* DepthImageCache.Set (Lux.Engine/Pipeline/Export/DepthCache.cs:137-143, fed by FromFullDepth :245-250): the cache image
+ * (cw x ch floats) made from a depth map (w x h): InverseDepth, the nearest 16.16 resample to the cache dims, then
+ * min(rcpps(x), 1e5). depth / cache are device pointers of the context's GPU when *_on_device, else host memory. */
+int lux_depth_cache_set(lux_sgm_ctx* ctx, const float* depth, int32_t w, int32_t h, int32_t depth_on_device, int32_t cw, int32_t ch,
+                        float* cache, int32_t cache_on_device);
+/* DepthImageCache.Fetch (DepthCache.cs:160-183): the ROI [x0, x1) x [y0, y1) of pipeline dims (dims_w, dims_h) read from a
+ * cache image (cw x ch) into out ((x1-x0) x (y1-y0) floats): a plain copy when the scale is 1, else the reciprocal of
+ * the source window, the nearest resample and the division back. LUX_ERR_ROI for an invalid ROI. */
+int lux_depth_cache_fetch(lux_sgm_ctx* ctx, const float* cache, int32_t cw, int32_t ch, int32_t cache_on_device, int32_t x0, int32_t y0,
+                          int32_t x1, int32_t y1, int32_t dims_w, int32_t dims_h, float* out, int32_t out_on_device);
 
 /* ---- Request server. No counterpart in the reference: the serving form of the stage. ----
  * Depth solves of mixed sizes are admitted in arrival order against an HBM budget (a host-side estimate per request;

@@ -37,7 +37,7 @@ class LuxIndexError(LuxError, IndexError):
 
 
 _EXC = {1: InvalidOperationError, 2: InvalidOperationError, 3: InvalidOperationError, 6: InvalidOperationError,
-        4: NotSupportedError, 5: NotSupportedError, 7: LuxIndexError}
+        4: NotSupportedError, 5: NotSupportedError, 7: LuxIndexError, 14: InvalidOperationError, 15: InvalidOperationError}
 
 
 def _raise(code, msg):
@@ -358,6 +358,66 @@ class DenseUpsampleLayer:
         ctx.check(rc)
         return UpsampleResult(out.reshape(gi.h, gi.w), gi.w, gi.h,
                               conf_out.reshape(gi.h, gi.w) if conf_out is not None else None)
+
+
+def _f32_image(a):
+    """(pointer, on_device, keep-alive, (h, w)) of a 2-D float32 image: a numpy array or a contiguous CUDA torch tensor."""
+    if hasattr(a, "data_ptr"):
+        assert a.dim() == 2 and a.is_contiguous() and str(a.dtype) == "torch.float32"
+        return a.data_ptr(), 1 if a.is_cuda else 0, a, tuple(a.shape)
+    d = np.ascontiguousarray(np.asarray(a, np.float32))
+    assert d.ndim == 2
+    return d.ctypes.data, 0, d, d.shape
+
+
+def _f32_like(ref, h, w):
+    if hasattr(ref, "data_ptr"):
+        import torch
+        return torch.empty((h, w), dtype=torch.float32, device=ref.device)
+    return np.empty((h, w), np.float32)
+
+
+class DepthImageCache:
+    """DepthImageCache (DepthCache.cs:87-254) on the GPU: the depth image the renderer and exporter read, made from the
+    upsampled full-resolution depth. Current is a numpy array, or a CUDA torch tensor (device=True) that stays in HBM:
+    Set and Fetch then read and write device memory only."""
+    Clip = 100000.0
+
+    def __init__(self, dims, device: bool = False, ctx: Optional[Context] = None):
+        """The constructor (:96): a zero image at dims = (W, H)."""
+        self.ctx = ctx or default_context()
+        w, h = dims
+        if device:
+            import torch
+            self.Current = torch.zeros((h, w), dtype=torch.float32, device=f"cuda:{self.ctx.device}")
+        else:
+            self.Current = np.zeros((h, w), np.float32)
+
+    def Set(self, depth):
+        """Set (:136-143): inverse depth, nearest resample to the cache dims, min(rcp, 1e5); the result is published."""
+        ptr, on_dev, keep, (h, w) = _f32_image(depth)
+        ch, cw = self.Current.shape
+        out = _f32_like(self.Current, ch, cw)
+        optr, oon, okeep, _ = _f32_image(out)
+        self.ctx.check(self.ctx.lib.lux_depth_cache_set(self.ctx.handle, ptr, w, h, on_dev, cw, ch, optr, oon))
+        self.Current = out
+
+    def Fetch(self, rect, dims):
+        """Fetch (:146) on the published image."""
+        return DepthImageCache.fetch(self.Current, rect, dims, self.ctx)
+
+    @staticmethod
+    def fetch(img, rect, dims, ctx: Optional[Context] = None):
+        """Fetch(img, rect, dims) (:161-181): rect = (x0, y0, x1, y1) in the grid of dims = (W, H); the ROI at that grid
+        as a (y1 - y0, x1 - x0) image of the same kind as img. Raises InvalidOperationError("invalid ROI requested!")."""
+        ctx = ctx or default_context()
+        ptr, on_dev, keep, (ch, cw) = _f32_image(img)
+        x0, y0, x1, y1 = (int(v) for v in rect)
+        out = _f32_like(img, max(y1 - y0, 0), max(x1 - x0, 0))
+        optr, oon, okeep, _ = _f32_image(out)
+        ctx.check(ctx.lib.lux_depth_cache_fetch(ctx.handle, ptr, cw, ch, on_dev, x0, y0, x1, y1, int(dims[0]), int(dims[1]),
+                                                optr, oon))
+        return out
 
 
 @dataclass

@@ -62,6 +62,11 @@ void launch_upsample(const float* prev, int pw, int ph, const uint8_t* guide, in
                      const uint32_t* rcp_table, uint8_t* g2, float* out_depth, const float* prev_conf, float* out_conf,
                      cudaStream_t s);
 
+// depth_cache.cu: DepthImageCache.Set and Fetch (DepthCache.cs)
+void launch_depth_cache_set(const float* src, int w, int h, int cw, int ch, const uint32_t* rcp, float* out, cudaStream_t s);
+void launch_depth_cache_fetch(const float* img, int istride, int vx0, int vy0, int vw, int vh, double offx, double offy, double sx,
+                              double sy, int rw, int rh, const uint32_t* rcp, float* out, cudaStream_t s);
+
 // cost.cu
 // The phase images of every other camera into a.phase (4·ow·oh u32 each); then the cost volume.
 // zt: per other camera and plane, the plane-only projection terms (z·W[8] + W[12], z·W[9] + W[13], z·W[10] + W[14], 0),

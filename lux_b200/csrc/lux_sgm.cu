@@ -80,6 +80,8 @@ const char* default_message(int code) {
     case LUX_ERR_UPSAMPLE_SIZE: return "Incorrect output depth size!";
     case LUX_ERR_INDEX: return "Index was outside the bounds of the array (the reference indexes outside an array for these inputs)";
     case LUX_ERR_TIMEOUT: return "a bounded device-side wait timed out";
+    case LUX_ERR_ROI: return "invalid ROI requested!";
+    case LUX_ERR_EMPTY_IMAGE: return "empty image!";
     default: return "error";
   }
 }
@@ -742,6 +744,91 @@ int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int3
 }
 
 }  // extern "C"
+
+// ---------------- depth image cache (DepthCache.cs) ----------------
+
+namespace {
+
+// A device view of a float image: the caller's device pointer, or a copy of host memory owned by `tmp`.
+int device_floats(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, const float* p, size_t n, int on_device, const float** out) {
+  if (on_device) {
+    *out = p;
+    return LUX_OK;
+  }
+  float* d = nullptr;
+  int rc = alloc_t(ctx, tmp, n, &d);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(d, p, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  *out = d;
+  return LUX_OK;
+}
+
+// Runs `fill` into the caller's output: directly when it is on the device, else through a device buffer copied back.
+template <class F>
+int to_output(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, float* out, size_t n, int on_device, F fill) {
+  float* d = out;
+  int rc = LUX_OK;
+  if (!on_device && (rc = alloc_t(ctx, tmp, n, &d))) return rc;
+  fill(d);
+  CK(cudaGetLastError());
+  if (!on_device) CK(cudaMemcpyAsync(out, d, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return LUX_OK;
+}
+
+}  // namespace
+
+extern "C" int lux_depth_cache_set(lux_sgm_ctx* ctx, const float* depth, int32_t w, int32_t h, int32_t depth_on_device, int32_t cw,
+                                   int32_t ch, float* cache, int32_t cache_on_device) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (cw <= 0 || ch <= 0) return set_err(ctx, LUX_ERR_EMPTY_IMAGE, "%s", default_message(LUX_ERR_EMPTY_IMAGE));  // DepthCache.cs:62
+  if (w <= 0 || h <= 0)  // the reference's resample clamps to index -1 of an empty source
+    return set_err(ctx, LUX_ERR_INDEX, "depth_cache_set: empty depth map");
+  if (!depth || !cache) return set_err(ctx, LUX_ERR_ARG, "depth_cache_set: null pointer");
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  const float* src = nullptr;
+  int rc = device_floats(ctx, tmp, depth, (size_t)w * h, depth_on_device, &src);
+  if (!rc)
+    rc = to_output(ctx, tmp, cache, (size_t)cw * ch, cache_on_device,
+                   [&](float* d) { launch_depth_cache_set(src, w, h, cw, ch, ctx->d_rcp, d, ctx->stream); });
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
+extern "C" int lux_depth_cache_fetch(lux_sgm_ctx* ctx, const float* cache, int32_t cw, int32_t ch, int32_t cache_on_device, int32_t x0,
+                                     int32_t y0, int32_t x1, int32_t y1, int32_t dims_w, int32_t dims_h, float* out, int32_t out_on_device) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  const int rw = x1 - x0, rh = y1 - y0;
+  if (rw == 0 || x1 < x0 || rh == 0 || y1 < y0 || (y0 | x0) < 0 || x1 > dims_w || y1 > dims_h)  // DepthCache.cs:163-164
+    return set_err(ctx, LUX_ERR_ROI, "%s", default_message(LUX_ERR_ROI));
+  if (!cache || !out || cw <= 0 || ch <= 0) return set_err(ctx, LUX_ERR_ARG, "depth_cache_fetch: null pointer or empty cache");
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  const float* img = nullptr;
+  int rc = device_floats(ctx, tmp, cache, (size_t)cw * ch, cache_on_device, &img);
+  const double sx = (double)cw / dims_w, sy = (double)ch / dims_h;
+  if (!rc && sx == 1.0 && sy == 1.0) {  // the plain view of the ROI (:166-172), copied out
+    rc = to_output(ctx, tmp, out, (size_t)rw * rh, out_on_device, [&](float* d) {
+      cudaMemcpy2DAsync(d, (size_t)rw * 4, img + (size_t)y0 * cw + x0, (size_t)cw * 4, (size_t)rw * 4, rh, cudaMemcpyDeviceToDevice,
+                        ctx->stream);
+    });
+  } else if (!rc) {  // the source window and its offsets (:173-181), in double as the reference
+    const int sx0 = std::max((int)std::floor(x0 * sx), 0), sy0 = std::max((int)std::floor(y0 * sy), 0);
+    const int sx1 = std::min((int)std::ceil((rw + (double)x0) * sx), (int)cw), sy1 = std::min((int)std::ceil((rh + (double)y0) * sy), (int)ch);
+    const double offx = (double)((float)x0 + 0.5f) * sx - sx0, offy = (double)((float)y0 + 0.5f) * sy - sy0;
+    const int vw = sx1 <= sx0 || sy1 <= sy0 ? 0 : sx1 - sx0, vh = vw == 0 ? 0 : sy1 - sy0;
+    if (vw == 0) rc = set_err(ctx, LUX_ERR_INDEX, "%s", default_message(LUX_ERR_INDEX));
+    else
+      rc = to_output(ctx, tmp, out, (size_t)rw * rh, out_on_device, [&](float* d) {
+        launch_depth_cache_fetch(img, cw, sx0, sy0, vw, vh, offx, offy, sx, sy, rw, rh, ctx->d_rcp, d, ctx->stream);
+      });
+  }
+  dev_free_all(ctx, tmp);
+  return rc;
+}
 
 // ---------------- allocation-free upsample ----------------
 namespace {

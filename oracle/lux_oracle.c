@@ -1105,3 +1105,74 @@ long lo_traversal_trace(int W, int H, int T, int xsw, int* ev, long max_events) 
   free(last); free(seen);
   return n;
 }
+
+/* ---------------- depth image cache (Lux.Engine/Pipeline/Export/DepthCache.cs) ---------------- */
+
+/* ImageResample0 (DepthCache.cs:38-70): nearest neighbour in 16.16 fixed point, int32 wrap-around, clamped to [0, n-1]. */
+static int lo_nearest(int s16, int o16, int i, int n) {
+  int v = (int32_t)((uint32_t)s16 * (uint32_t)i + (uint32_t)o16) >> 16;
+  return v < 0 ? 0 : v > n - 1 ? n - 1 : v;
+}
+
+/* DepthImageCache.Set (DepthCache.cs:137-143): InverseDepth (rcpps, no Newton step), the nearest resample to the cache
+ * dims (scale = src / dst in double, offset 0), then InverseDepthClip: minps(rcpps(x), 1e5). */
+int lo_depth_cache_set(const float* src, int w, int h, int cw, int ch, float* out) {
+  if (cw <= 0 || ch <= 0) return LO_ERR_EMPTY_IMAGE; /* ImageResample0.Run (DepthCache.cs:62) */
+  if (w <= 0 || h <= 0) return LO_ERR_INDEX;          /* the resample clamps to index -1 of an empty source */
+  if (!src || !out) return LO_ERR_ARG;
+  const int sx16 = (int)((double)w / cw * 65536.0), sy16 = (int)((double)h / ch * 65536.0);
+  const float clip = 100000.0f;
+  for (int y = 0; y < ch; y++) {
+    const int sy = lo_nearest(sy16, 0, y, h);
+    for (int x = 0; x < cw; x++) {
+      const int sx = lo_nearest(sx16, 0, x, w);
+      const float inv = lo_rcp(src[(size_t)sy * w + sx]);
+      const float r = lo_rcp(inv);
+      out[(size_t)y * cw + x] = r < clip ? r : clip; /* minps(a, b): a when a < b, else b */
+    }
+  }
+  return LO_OK;
+}
+
+/* DepthImageCache.Fetch (DepthCache.cs:160-183) on a dense iw x ih image with a full valid rect: the ROI check, the
+ * plain view when the scale is 1, else the source window, its reciprocal (rcpps + one Newton step for the first
+ * (vw/32)·32 columns, division for the rest), the nearest resample with the window offset, and the division back
+ * (FetchFull / FetchSampled, :185-239, which give the same pixels). out holds (x1-x0)·(y1-y0) floats. */
+int lo_depth_cache_fetch(const float* img, int iw, int ih, int x0, int y0, int x1, int y1, int dw, int dh, float* out) {
+  const int rw = x1 - x0, rh = y1 - y0;
+  if (rw == 0 || x1 < x0 || rh == 0 || y1 < y0 || (y0 | x0) < 0 || x1 > dw || y1 > dh) return LO_ERR_ROI;
+  const double sx = (double)iw / dw, sy = (double)ih / dh;
+  if (sx == 1.0 && sy == 1.0) {
+    for (int y = 0; y < rh; y++)
+      for (int x = 0; x < rw; x++) out[(size_t)y * rw + x] = img[(size_t)(y0 + y) * iw + x0 + x];
+    return LO_OK;
+  }
+  int sx0 = (int)floor(x0 * sx), sy0 = (int)floor(y0 * sy);
+  if (sx0 < 0) sx0 = 0;
+  if (sy0 < 0) sy0 = 0;
+  int sx1 = (int)ceil((rw + (double)x0) * sx), sy1 = (int)ceil((rh + (double)y0) * sy);
+  if (sx1 > iw) sx1 = iw;
+  if (sy1 > ih) sy1 = ih;
+  const double offX = (double)((float)x0 + 0.5f) * sx - sx0, offY = (double)((float)y0 + 0.5f) * sy - sy0;
+  const int vx0 = sx0, vy0 = sy0, vx1 = sx1, vy1 = sy1;
+  const int vw = vx1 <= vx0 || vy1 <= vy0 ? 0 : vx1 - vx0, vh = vw == 0 ? 0 : vy1 - vy0;
+  if (vw == 0) return LO_ERR_INDEX; /* an empty source window: the reference's resample would index outside it */
+  const int ox16 = (int)(offX * 65536.0), oy16 = (int)(offY * 65536.0), sx16 = (int)(sx * 65536.0), sy16 = (int)(sy * 65536.0);
+  const int vec = (vw / 32) * 32;
+  for (int y = 0; y < rh; y++) {
+    const int py = lo_nearest(sy16, oy16, y, vh);
+    for (int x = 0; x < rw; x++) {
+      const int px = lo_nearest(sx16, ox16, x, vw);
+      const float v = img[(size_t)(vy0 + py) * iw + vx0 + px];
+      float inv;
+      if (px < vec) {
+        const float r = lo_rcp(v);
+        inv = ((1.0f - v * r) * r + r) * 1.0f;
+      } else {
+        inv = 1.0f / v;
+      }
+      out[(size_t)y * rw + x] = 1.0f / inv;
+    }
+  }
+  return LO_OK;
+}

@@ -32,6 +32,8 @@ enum {
   LO_ERR_INDEX = 7,         /* an access the reference performs out of its arrays (IndexOutOfRangeException) */
   LO_ERR_ALLOC = 8,
   LO_ERR_ARG = 9,
+  LO_ERR_ROI = 14,          /* "invalid ROI requested!"                               DepthCache.cs:164 */
+  LO_ERR_EMPTY_IMAGE = 15,  /* "empty image!"                                         DepthCache.cs:62 */
 };
 
 typedef struct { float K[9], T[3], R[9]; } lo_calib; /* Triangulator.cs:8-19, row-major */
@@ -133,6 +135,10 @@ int lo_upsample(const float* prev_depth, int pw, int ph, const uint8_t* guide, i
  * Event ids count Pixel calls in order over both passes. ev_out receives, per call, {dir, x, y, r, is_revisit, src0..src3}
  * (9 ints). Returns the number of calls, or -1 when max_events is too small. Used to check the GPU schedule. */
 long lo_traversal_trace(int w, int h, int tile, int xsw, int* ev_out, long max_events);
+
+/* Depth image cache (DepthCache.cs): Set into a cw x ch cache, Fetch of a ROI against pipeline dims (dw, dh). */
+int lo_depth_cache_set(const float* src, int w, int h, int cw, int ch, float* out);
+int lo_depth_cache_fetch(const float* img, int iw, int ih, int x0, int y0, int x1, int y1, int dw, int dh, float* out);
 
 #ifdef __cplusplus
 }

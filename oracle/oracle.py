@@ -78,6 +78,9 @@ def lib():
         l.lo_flow_matrix.argtypes = [ctypes.POINTER(LoCalib), ctypes.POINTER(LoCalib), ctypes.POINTER(ctypes.c_float)]
         l.lo_default_params.argtypes = [ctypes.POINTER(LoParams)]
         l.lo_l16_pyramid.argtypes = [ctypes.POINTER(LoParams)]
+        l.lo_depth_cache_set.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        l.lo_depth_cache_fetch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         _lib = l
     return _lib
 
@@ -220,6 +223,29 @@ def upsample(prev_depth, pw, ph, guide, set_w, set_h, sigma=12.0, scale=2, prev_
     if rc:
         raise OracleError(rc, "upsample")
     return out.reshape(gh, gw), (conf.reshape(gh, gw) if conf is not None else None)
+
+
+def depth_cache_set(depth, cw, ch):
+    """DepthImageCache.Set (DepthCache.cs:137-143): the cache image (ch, cw) made from a depth map."""
+    d = np.ascontiguousarray(np.asarray(depth, np.float32))
+    h, w = d.shape
+    out = np.empty((ch, cw), np.float32)
+    rc = lib().lo_depth_cache_set(d.ctypes.data, w, h, cw, ch, out.ctypes.data)
+    if rc:
+        raise OracleError(rc, "depth_cache_set")
+    return out
+
+
+def depth_cache_fetch(cache, rect, dims):
+    """DepthImageCache.Fetch (DepthCache.cs:160-183): rect = (x0, y0, x1, y1) against pipeline dims (w, h)."""
+    c = np.ascontiguousarray(np.asarray(cache, np.float32))
+    ih, iw = c.shape
+    x0, y0, x1, y1 = rect
+    out = np.empty((max(y1 - y0, 0), max(x1 - x0, 0)), np.float32)
+    rc = lib().lo_depth_cache_fetch(c.ctypes.data, iw, ih, x0, y0, x1, y1, dims[0], dims[1], out.ctypes.data)
+    if rc:
+        raise OracleError(rc, "depth_cache_fetch")
+    return out
 
 
 def traversal_trace(w, h, tile, xsw=False):

@@ -87,3 +87,53 @@ def test_skip_mask_one_per_cell(oracle):
     m = oracle.skip_mask(2, 130, 70)
     cells = (m[:70, :130] == 0).reshape(35, 2, 65, 2).sum(axis=(1, 3))
     assert (cells == 1).all()
+
+
+def _nearest16(scale, off, n_out, n_src):
+    """ImageResample0's 16.16 source index (DepthCache.cs:42-51), int32 wrap-around, clamped to the source."""
+    s16, o16 = int(scale * 65536.0), int(off * 65536.0)
+    v = (np.arange(n_out, dtype=np.int64) * s16 + o16) & 0xFFFFFFFF
+    v = np.where(v >= 1 << 31, v - (1 << 32), v) >> 16
+    return np.clip(v, 0, n_src - 1)
+
+
+def test_depth_cache_set_properties(oracle):
+    """Set (DepthCache.cs:136-143): each cache pixel is its nearest source pixel after two rcpps round trips (each within
+    1.5·2^-12 relative, so within 7.5e-4), clipped to 1e5; at equal dims the resample is the identity."""
+    rng = np.random.default_rng(1)
+    d = np.exp(rng.uniform(np.log(300.0), np.log(3e5), (57, 83))).astype(np.float32)
+    same = oracle.depth_cache_set(d, 83, 57)
+    assert np.all(np.abs(same - np.minimum(d, 1e5)) <= 7.5e-4 * np.minimum(d, 1e5))
+    cw, ch = 130, 41
+    got = oracle.depth_cache_set(d, cw, ch)
+    ys, xs = _nearest16(57 / ch, 0.0, ch, 57), _nearest16(83 / cw, 0.0, cw, 83)
+    near = np.minimum(d[np.ix_(ys, xs)], 1e5)
+    assert np.all(np.abs(got - near) <= 7.5e-4 * near)
+    assert got.max() <= 1e5
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.depth_cache_set(d, 0, 5)
+    assert e.value.code == 15
+
+
+def test_depth_cache_fetch_properties(oracle):
+    """Fetch (DepthCache.cs:161-239): the plain window at scale 1; elsewhere the nearest window pixel (offsets from
+    ((float)x0 + 0.5f)·sx − ⌊x0·sx⌋) within 2 ulp after the reciprocal round trip; the reference's ROI checks."""
+    rng = np.random.default_rng(2)
+    img = rng.uniform(500.0, 9e4, (96, 128)).astype(np.float32)
+    assert np.array_equal(oracle.depth_cache_fetch(img, (5, 7, 50, 60), (128, 96)), img[7:60, 5:50])
+    for rect, dims in (((3, 2, 40, 30), (64, 48)), ((10, 11, 200, 150), (256, 192)), ((0, 0, 97, 71), (97, 71))):
+        x0, y0, x1, y1 = rect
+        sx, sy = 128 / dims[0], 96 / dims[1]
+        wx0, wy0 = max(int(np.floor(x0 * sx)), 0), max(int(np.floor(y0 * sy)), 0)
+        wx1, wy1 = min(int(np.ceil(x1 * sx)), 128), min(int(np.ceil(y1 * sy)), 96)
+        offx = float(np.float32(x0) + np.float32(0.5)) * sx - wx0
+        offy = float(np.float32(y0) + np.float32(0.5)) * sy - wy0
+        xs = wx0 + _nearest16(sx, offx, x1 - x0, wx1 - wx0)
+        ys = wy0 + _nearest16(sy, offy, y1 - y0, wy1 - wy0)
+        got = oracle.depth_cache_fetch(img, rect, dims)
+        want = img[np.ix_(ys, xs)]
+        assert np.all(np.abs(got.view(np.int32) - want.view(np.int32)) <= 2), rect
+    for rect in ((4, 4, 4, 8), (-1, 0, 3, 3), (0, 0, 129, 5)):
+        with pytest.raises(oracle.OracleError) as e:
+            oracle.depth_cache_fetch(img, rect, (128, 96))
+        assert e.value.code == 14
