@@ -67,6 +67,8 @@ def args_():
     p.add_argument("--slots", type=int, default=3)
     p.add_argument("--sweep", action="store_true",
                    help="throughput with 1, 4, 16 and 64 module captures in flight through the request server")
+    p.add_argument("--cache", action="store_true",
+                   help="the depth image cache: Set of the 4160x3120 full depth into the 5216x3912 cache, Fetch at the export levels")
     p.add_argument("--cpu-rows", type=int, default=130, help="rows of the CPU sample strip")
     p.add_argument("--workload", default="pair13mp", choices=sorted(WORKLOADS),
                    help="pair13mp is the benchmark; the smaller pairs are for profiling captures")
@@ -426,8 +428,129 @@ def run_sweep(a):
                       "sweep": points}))
 
 
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_depth_cache_set launch, 4160x3120 -> 5216x3912
+SET_TRAFFIC = 52.01e6 + 28.92e6
+
+
+def run_cache(a):
+    """The depth image cache (DepthCache.cs:136-181) on one GPU. Set: the 4160x3120 full depth (the upsample's output)
+    into the 5216x3912 cache of a 10432x7824 canvas (FromFullDepth); Fetch: the whole frame at pipeline levels 0 (the
+    canvas, a 2x upsample of the cache) and 2 (2608x1956). value = cache pixels per second of Set with the depth in HBM,
+    L2 flushed (a 256 MB write) before every timed launch; e2e = the same from a pinned host depth map to a pinned host
+    cache. Roofline: Set reads each source pixel once and writes each cache pixel (4 + 4 bytes per pixel); traffic is
+    ncu's dram__bytes_read.sum + dram__bytes_write.sum of one Set launch of this workload (writes still in L2 when the
+    kernel ends are not counted)."""
+    import torch
+    from lux_b200 import api
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    w, h, cw, ch = 4160, 3120, 5216, 3912
+    rng = np.random.default_rng(7)
+    depth = np.exp(rng.uniform(np.log(400.0), np.log(2.0e5), (h, w))).astype(np.float32)
+    pk = peaks()
+    algo_set = 4 * (w * h + cw * ch)
+    desc = f"depth cache Set {w}x{h} full depth -> {cw}x{ch} cache; Fetch at levels 0 (10432x7824) and 2 (2608x1956)"
+    threads = 1
+    if a.impl == "reference":
+        from oracle import oracle as O
+        for _ in range(a.warmup):
+            O.depth_cache_set(depth, cw, ch)
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            O.depth_cache_set(depth, cw, ch)
+        dt = (time.perf_counter() - t0) / a.steps
+        v = cw * ch / dt / 1e6
+        print(json.dumps({"impl": "reference", "metric": "depth cache Set Mpix/s (cache pixels per second), bit-exact",
+                          "value": v, "unit": "Mpix/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+                          "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f32", "data": "synthetic", "config": {"workload": desc},
+                          "cpu_baseline": {"value": v, "unit": "Mpix/s", "cores": threads, "kind": "port",
+                                           "sample": "the whole Set, oracle port (scalar C)"},
+                          "e2e": {"value": v, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(lib.lux_sgm_stream(ctx.handle), device=torch.device("cuda", 0))
+    d_depth = torch.from_numpy(depth).cuda()
+    d_cache = torch.empty((ch, cw), dtype=torch.float32, device="cuda")
+    h_depth = torch.from_numpy(depth).pin_memory()
+    h_cache = torch.empty((ch, cw), dtype=torch.float32).pin_memory()
+    flush = torch.empty(64 * 2**20, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+
+    def set_dev():
+        ctx.check(lib.lux_depth_cache_set(ctx.handle, d_depth.data_ptr(), w, h, 1, cw, ch, d_cache.data_ptr(), 1))
+
+    def set_host():
+        ctx.check(lib.lux_depth_cache_set(ctx.handle, h_depth.data_ptr(), w, h, 0, cw, ch, h_cache.data_ptr(), 0))
+
+    def timed(fn, k, flush_l2):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        total = 0.0
+        n0 = api.kernel_launches()
+        for _ in range(k):
+            if flush_l2:
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                    torch.cuda._sleep(200000)  # keeps the stream busy while the host reaches the launch: no idle gap timed
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+        return total / k, api.kernel_launches() - n0
+
+    with ClockSampler(0) as clk:
+        ms_set, launches = timed(set_dev, a.steps, True)
+    ms_e2e, _ = timed(set_host, a.steps, False)
+    fetch = {}
+    for lv, dims in ((0, (10432, 7824)), (2, (2608, 1956))):
+        out = torch.empty((dims[1], dims[0]), dtype=torch.float32, device="cuda")
+
+        def fetch_dev():
+            ctx.check(lib.lux_depth_cache_fetch(ctx.handle, d_cache.data_ptr(), cw, ch, 1, 0, 0, dims[0], dims[1], dims[0],
+                                                dims[1], out.data_ptr(), 1))
+        ms, _ = timed(fetch_dev, a.steps, True)
+        # algorithmic bytes: every cache pixel the resample reads, once (all of them for level 0; a quarter for level 2),
+        # plus the output
+        read_px = cw * ch if lv == 0 else dims[0] * dims[1]
+        gbs = 4 * (read_px + dims[0] * dims[1]) / (ms / 1e3) / 1e9
+        fetch[f"level{lv}"] = {"dims": list(dims), "ms": ms, "mpix_per_s": dims[0] * dims[1] / (ms / 1e3) / 1e6, "gbs": gbs,
+                               "frac": gbs / pk.get("hbm_gbs")}
+    achieved = algo_set / (ms_set / 1e3) / 1e9
+    out = {"metric": "depth cache Set Mpix/s (cache pixels per second), bit-exact", "value": cw * ch / (ms_set / 1e3) / 1e6,
+           "unit": "Mpix/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_set,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (log-uniform depth 400 mm .. 200 m)",
+           "config": {"workload": desc, "l2": "flushed (256 MB write) before every timed Set and Fetch"},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
+                        "frac": achieved / pk.get("hbm_gbs"), "traffic": SET_TRAFFIC, "kernel": "k_depth_cache_set",
+                        "bytes_per_pixel": algo_set / (cw * ch),
+                        "peak_source": "fallback" if pk.get("fallback") else "MEASURED_PEAKS.json hbm_gbs (measured)"},
+           "e2e": {"value": cw * ch / (ms_e2e / 1e3) / 1e6, "unit": "Mpix/s", "h2d_bytes_per_step": 4 * w * h,
+                   "d2h_bytes_per_step": 4 * cw * ch},
+           "fetch": fetch, "gpu_launches": int(launches), "clocks": clk.summary()}
+    if not a.no_cpu_baseline:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        for _ in range(3):
+            O.depth_cache_set(depth, cw, ch)
+        dt = (time.perf_counter() - t0) / 3
+        out["cpu_baseline"] = {"value": cw * ch / dt / 1e6, "unit": "Mpix/s", "cores": 1, "kind": "port",
+                               "sample": f"the whole Set ({dt:.2f} s), oracle port (scalar C), 3 runs"}
+    print(json.dumps(out))
+    ctx.close()
+
+
 def main():
     a = args_()
+    if a.cache:
+        run_cache(a)
+        return
     if a.sweep:
         run_sweep(a)
         return

@@ -164,14 +164,18 @@ int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int3
                      const lux_img_rgba8* guide, int32_t set_w, int32_t set_h, float sigma, int32_t scale,
                      const float* prev_conf, float* out_depth, float* out_conf);
 
-/* DepthImageCache.Set (Lux.Engine/Pipeline/Export/DepthCache.cs:137-143, fed by FromFullDepth :245-250): the cache image
+/* DepthImageCache.Set (Lux.Engine/Pipeline/Export/DepthCache.cs:136-143, fed by FromFullDepth :239-244): the cache image
  * (cw x ch floats) made from a depth map (w x h): InverseDepth, the nearest 16.16 resample to the cache dims, then
- * min(rcpps(x), 1e5). depth / cache are device pointers of the context's GPU when *_on_device, else host memory. */
+ * min(rcpps(x), 1e5). depth / cache are device pointers of the context's GPU when *_on_device, else host memory.
+ * LUX_ERR_EMPTY_IMAGE when cw or ch <= 0 ("empty image!", :62). With both on the device the call is asynchronous on the
+ * context's stream (lux_sgm_stream / lux_sgm_sync order later work after it); with either on the host it returns when
+ * the result is there. */
 int lux_depth_cache_set(lux_sgm_ctx* ctx, const float* depth, int32_t w, int32_t h, int32_t depth_on_device, int32_t cw, int32_t ch,
                         float* cache, int32_t cache_on_device);
-/* DepthImageCache.Fetch (DepthCache.cs:160-183): the ROI [x0, x1) x [y0, y1) of pipeline dims (dims_w, dims_h) read from a
+/* DepthImageCache.Fetch (DepthCache.cs:161-239): the ROI [x0, x1) x [y0, y1) of pipeline dims (dims_w, dims_h) read from a
  * cache image (cw x ch) into out ((x1-x0) x (y1-y0) floats): a plain copy when the scale is 1, else the reciprocal of
- * the source window, the nearest resample and the division back. LUX_ERR_ROI for an invalid ROI. */
+ * the source window, the nearest resample and the division back. LUX_ERR_ROI for an invalid ROI ("invalid ROI
+ * requested!", :164). Synchronous or not as lux_depth_cache_set. */
 int lux_depth_cache_fetch(lux_sgm_ctx* ctx, const float* cache, int32_t cw, int32_t ch, int32_t cache_on_device, int32_t x0, int32_t y0,
                           int32_t x1, int32_t y1, int32_t dims_w, int32_t dims_h, float* out, int32_t out_on_device);
 

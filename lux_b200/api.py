@@ -370,6 +370,15 @@ def _f32_image(a):
     return d.ctypes.data, 0, d, d.shape
 
 
+def _torch_ready(*arrays):
+    """Work torch queued on its current stream for these CUDA tensors is done before the library's stream reads them."""
+    for a in arrays:
+        if hasattr(a, "is_cuda") and a.is_cuda:
+            import torch
+            torch.cuda.current_stream(a.device).synchronize()
+            return
+
+
 def _f32_like(ref, h, w):
     if hasattr(ref, "data_ptr"):
         import torch
@@ -399,7 +408,9 @@ class DepthImageCache:
         ch, cw = self.Current.shape
         out = _f32_like(self.Current, ch, cw)
         optr, oon, okeep, _ = _f32_image(out)
+        _torch_ready(depth, out)
         self.ctx.check(self.ctx.lib.lux_depth_cache_set(self.ctx.handle, ptr, w, h, on_dev, cw, ch, optr, oon))
+        self.ctx.check(self.ctx.lib.lux_sgm_sync(self.ctx.handle))  # device in and out: the call is asynchronous
         self.Current = out
 
     def Fetch(self, rect, dims):
@@ -415,8 +426,10 @@ class DepthImageCache:
         x0, y0, x1, y1 = (int(v) for v in rect)
         out = _f32_like(img, max(y1 - y0, 0), max(x1 - x0, 0))
         optr, oon, okeep, _ = _f32_image(out)
+        _torch_ready(img, out)
         ctx.check(ctx.lib.lux_depth_cache_fetch(ctx.handle, ptr, cw, ch, on_dev, x0, y0, x1, y1, int(dims[0]), int(dims[1]),
                                                 optr, oon))
+        ctx.check(ctx.lib.lux_sgm_sync(ctx.handle))
         return out
 
 

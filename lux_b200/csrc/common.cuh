@@ -31,7 +31,16 @@ LUX_DEV float cs_minf(float a, float b) {
   return a < b ? a : b;
 }
 
-// IntelApprox.RcpBits (Lux.Engine/Imaging/IntelApprox.cs:21-29) with the table in global memory.
+// IntelApprox.RcpBits (Lux.Engine/Imaging/IntelApprox.cs:21-29): rcp_entry given the table entry of b,
+// r = table[(b >> 11) & 0xfff], fetched by the caller (from a shared-memory copy); rcp_bits with the table in global memory.
+LUX_DEV uint32_t rcp_entry(uint32_t b, uint32_t r) {
+  uint32_t sign = b & 0x80000000u, e = (b >> 23) & 0xff, m = b & 0x7fffff;
+  if (e == 0xff) return m != 0 ? (b | 0x400000u) : sign;
+  if (e == 0) return sign | 0x7f800000u;
+  int re = (int)((r >> 23) & 0xff) - ((int)e - 127);
+  if (re <= 0) return sign;
+  return sign | ((uint32_t)re << 23) | (r & 0x7fffff);
+}
 LUX_DEV uint32_t rcp_bits(uint32_t b, const uint32_t* __restrict__ table) {
   uint32_t sign = b & 0x80000000u, e = (b >> 23) & 0xff, m = b & 0x7fffff;
   if (e == 0xff) return m != 0 ? (b | 0x400000u) : sign;

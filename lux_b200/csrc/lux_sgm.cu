@@ -764,6 +764,8 @@ int device_floats(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, const float* p, si
 }
 
 // Runs `fill` into the caller's output: directly when it is on the device, else through a device buffer copied back.
+// Device in, device out: nothing to wait for, the work stays queued on the context's stream. Otherwise the call waits
+// for the host copy, or for the work that reads the temporary buffers the caller frees next.
 template <class F>
 int to_output(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, float* out, size_t n, int on_device, F fill) {
   float* d = out;
@@ -772,7 +774,7 @@ int to_output(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, float* out, size_t n, 
   fill(d);
   CK(cudaGetLastError());
   if (!on_device) CK(cudaMemcpyAsync(out, d, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  if (!on_device || !tmp.empty()) CK(cudaStreamSynchronize(ctx->stream));
   return LUX_OK;
 }
 

@@ -61,6 +61,22 @@ def test_set_matches_oracle(api, w, h, cw, ch, device):
     assert np.array_equal(_bits(c.Current), _bits(ref))
 
 
+def test_set_every_exponent(api):
+    """Every sign, exponent and rcpps table index (random low mantissa bits) through Set at equal dims: the one-lookup
+    path for ordinary exponents and the two-step path for the rest give the oracle's bits."""
+    rng = np.random.default_rng(9)
+    e = np.repeat(np.arange(256, dtype=np.uint32), 4096 * 2)
+    i = np.tile(np.arange(4096, dtype=np.uint32), 512)
+    s = np.tile(np.repeat(np.array([0, 1], np.uint32), 4096), 256)
+    b = (s << 31) | (e << 23) | (i << 11) | rng.integers(0, 2048, i.size).astype(np.uint32)
+    d = b.view(np.float32).reshape(1024, 2048)
+    c = api.DepthImageCache((2048, 1024))
+    c.Set(d)
+    assert np.array_equal(_bits(c.Current), _bits(O.depth_cache_set(d, 2048, 1024)))
+    raw = api.DepthImageCache.fetch(d, (0, 0, 1024, 512), (1024, 512))
+    assert np.array_equal(_bits(raw), _bits(O.depth_cache_fetch(d, (0, 0, 1024, 512), (1024, 512))))
+
+
 def test_set_full_resolution(api):
     """FromFullDepth (:239-244): the 4160x3120 full depth into the 5216x3912 level-1 cache, on the device."""
     import torch

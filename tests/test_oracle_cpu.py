@@ -137,3 +137,33 @@ def test_depth_cache_fetch_properties(oracle):
         with pytest.raises(oracle.OracleError) as e:
             oracle.depth_cache_fetch(img, rect, (128, 96))
         assert e.value.code == 14
+
+
+def _rcp_bits_np(b, table):
+    """IntelApprox.RcpBits (IntelApprox.cs:21-29) on uint32 arrays."""
+    b = b.astype(np.uint64)
+    sign, e, m = b & 0x80000000, (b >> 23) & 0xFF, b & 0x7FFFFF
+    r = table[(m >> 11).astype(np.int64)].astype(np.uint64)
+    re = ((r >> 23) & 0xFF).astype(np.int64) - (e.astype(np.int64) - 127)
+    out = sign | (np.clip(re, 0, 255).astype(np.uint64) << 23) | (r & 0x7FFFFF)
+    out = np.where(re <= 0, sign, out)
+    out = np.where(e == 0, sign | 0x7F800000, out)
+    out = np.where(e == 0xFF, np.where(m != 0, b | 0x400000, sign), out)
+    return out.astype(np.uint32)
+
+
+def test_depth_cache_composite_rcp():
+    """The one-lookup rcpps(rcpps(v)) of the depth cache's Set kernel (comp[i] = (E(j) - E(i))·2^23 + M(j), j = M(i) >> 11,
+    added to v's sign and exponent bits) equals the two table steps for every table index, sign and exponent 3..250."""
+    t = np.array(_header_tables()["lux_rcp_table"], np.uint64)
+    ti = t
+    tj = t[((ti & 0x7FFFFF) >> 11).astype(np.int64)]
+    comp = (((tj >> 23) & 0xFF).astype(np.int64) - ((ti >> 23) & 0xFF).astype(np.int64)) * (1 << 23) + (tj & 0x7FFFFF).astype(np.int64)
+    rng = np.random.default_rng(4)
+    i = np.tile(np.arange(4096, dtype=np.uint64), 248 * 2)
+    e = np.repeat(np.arange(3, 251, dtype=np.uint64), 4096 * 2)
+    s = np.tile(np.repeat(np.array([0, 1], np.uint64), 4096), 248)
+    b = ((s << 31) | (e << 23) | (i << 11) | rng.integers(0, 2048, i.size).astype(np.uint64)).astype(np.uint32)
+    two = _rcp_bits_np(_rcp_bits_np(b, t), t)
+    one = ((b.astype(np.int64) & 0xFF800000) + comp[i.astype(np.int64)]) & 0xFFFFFFFF
+    assert np.array_equal(one.astype(np.uint32), two)
