@@ -34,7 +34,9 @@ extern "C" {
 #define LUX_ERR_UNSUPPORTED 12  /* inputs outside what this implementation supports (message says which) */
 #define LUX_ERR_CANCELED 13     /* OperationCanceledException: the request was canceled before it started */
 #define LUX_ERR_ROI 14          /* InvalidOperationException "invalid ROI requested!" (DepthCache.cs:164) */
-#define LUX_ERR_EMPTY_IMAGE 15  /* InvalidOperationException "empty image!" (DepthCache.cs:67) */
+#define LUX_ERR_EMPTY_IMAGE 15  /* InvalidOperationException "empty image!" (DepthCache.cs:62) */
+#define LUX_ERR_IO 16           /* a dump file could not be opened, written or read (IOException) */
+#define LUX_ERR_FORMAT 17       /* InvalidOperationException "expected a 4-byte float dump" (StereoAsyncApi.cs:258) */
 
 /* Rgba8Image (Lux.Engine/Pipeline/Registration/SparseLnrMatch.cs:8-13): 8-bit RGBA ("YUVA"), stride in pixels.
  * on_device != 0: data is a device pointer of the context's GPU (no copy); else host memory. */
@@ -163,6 +165,22 @@ void lux_layer_destroy(lux_layer* layer);
 int lux_sgm_upsample(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int32_t ph, int32_t prev_on_device,
                      const lux_img_rgba8* guide, int32_t set_w, int32_t set_h, float sigma, int32_t scale,
                      const float* prev_conf, float* out_depth, float* out_conf);
+
+/* Dump and golden-file formats of the dense stage (StereoAsyncApi.cs:217-262; host code, no counterpart needed on the
+ * GPU). Every image file starts with int32 {w, h, stride = w, bytes per pixel}.
+ * lux_dump_f32 / lux_load_f32: DumpF32 / LoadF32 (:252-261), the format LUX_DENSE_OVERRIDE reads (ExportBuild.cs:89-96);
+ *   lux_load_f32 with out = NULL only reports w and h; LUX_ERR_FORMAT when bytes per pixel != 4.
+ * lux_dump_rgba8: DumpRgba8 (:217-223), host or device image.
+ * lux_dump_cost_volume: DumpCostVolume (:227-250): <prefix>_offsets.u32, _costvol.bin and (when kept) _costvol_pass1.bin;
+ *   the layer needs its final aggregates (LUX_LAYER_KEEP_AGG on the fast kernels).
+ * lux_dump_dense: the dump of State4And5 (:197-214) for solved layers and their inputs under <prefix>_dense_*; cost
+ *   volumes of layers 0..cv_max (the reference's LUX_DENSE_DUMP_CV, default 2). */
+int lux_dump_f32(const char* path, const float* data, int32_t w, int32_t h);
+int lux_load_f32(const char* path, float* out, uint64_t cap_floats, int32_t* w, int32_t* h);
+int lux_dump_rgba8(const char* path, const lux_img_rgba8* img);
+int lux_dump_cost_volume(const lux_layer* layer, const char* prefix);
+int lux_dump_dense(lux_sgm_ctx* ctx, lux_layer* const* layers, int32_t n_layers, int32_t n_cams, const lux_img_rgba8* images,
+                   const lux_calib* calibs, const char* prefix, int32_t cv_max);
 
 /* DepthImageCache.Set (Lux.Engine/Pipeline/Export/DepthCache.cs:136-143, fed by FromFullDepth :239-244): the cache image
  * (cw x ch floats) made from a depth map (w x h): InverseDepth, the nearest 16.16 resample to the cache dims, then

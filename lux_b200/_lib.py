@@ -13,6 +13,7 @@ ERRORS = {
     1: "LUX_ERR_NEAR_FAR", 2: "LUX_ERR_NONPOSITIVE", 3: "LUX_ERR_BASELINE", 4: "LUX_ERR_SKIPMODE", 5: "LUX_ERR_BUDGET",
     6: "LUX_ERR_UPSAMPLE_SIZE", 7: "LUX_ERR_INDEX", 8: "LUX_ERR_ALLOC", 9: "LUX_ERR_ARG", 10: "LUX_ERR_CUDA",
     11: "LUX_ERR_TIMEOUT", 12: "LUX_ERR_UNSUPPORTED", 13: "LUX_ERR_CANCELED", 14: "LUX_ERR_ROI", 15: "LUX_ERR_EMPTY_IMAGE",
+    16: "LUX_ERR_IO", 17: "LUX_ERR_FORMAT",
 }
 
 FIELD_DEPTH, FIELD_PLANES, FIELD_SKIP, FIELD_START, FIELD_COUNT, FIELD_CAP = 0, 1, 2, 3, 4, 5
@@ -88,6 +89,13 @@ SIGNATURES = [
     ("lux_depth_cache_fetch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]),
+    ("lux_dump_f32", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
+    ("lux_load_f32", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.POINTER(ctypes.c_int32)]),
+    ("lux_dump_rgba8", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(Img)]),
+    ("lux_dump_cost_volume", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    ("lux_dump_dense", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.POINTER(Img), ctypes.POINTER(Calib), ctypes.c_char_p, ctypes.c_int32]),
     ("lux_server_create", ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     ("lux_server_destroy", None, [ctypes.c_void_p]),
     ("lux_server_last_error", ctypes.c_char_p, [ctypes.c_void_p]),

@@ -11,6 +11,7 @@ Errors raise the exception class the reference throws (InvalidOperationError, No
 carrying the C status code.
 """
 import ctypes
+import os
 import struct
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
@@ -37,7 +38,8 @@ class LuxIndexError(LuxError, IndexError):
 
 
 _EXC = {1: InvalidOperationError, 2: InvalidOperationError, 3: InvalidOperationError, 6: InvalidOperationError,
-        4: NotSupportedError, 5: NotSupportedError, 7: LuxIndexError, 14: InvalidOperationError, 15: InvalidOperationError}
+        4: NotSupportedError, 5: NotSupportedError, 7: LuxIndexError, 14: InvalidOperationError, 15: InvalidOperationError,
+        17: InvalidOperationError}
 
 
 def _raise(code, msg):
@@ -291,6 +293,11 @@ class DenseLayer:
     def Guidance(self):
         return self._read(L.FIELD_GUIDANCE, np.uint8, self.W * self.H * 4).reshape(self.H, self.W, 4)
 
+    def dump_cost_volume(self, prefix):
+        """DumpCostVolume (StereoAsyncApi.cs:227-250): <prefix>_offsets.u32, _costvol.bin, _costvol_pass1.bin (when kept).
+        Needs the final aggregates (keep_agg=True on the fast kernels)."""
+        self.ctx.check(self.ctx.lib.lux_dump_cost_volume(self.handle, os.fsencode(prefix)))
+
     def device_ptr(self, field_id):
         return self.ctx.lib.lux_layer_device_ptr(self.handle, field_id)
 
@@ -358,6 +365,52 @@ class DenseUpsampleLayer:
         ctx.check(rc)
         return UpsampleResult(out.reshape(gi.h, gi.w), gi.w, gi.h,
                               conf_out.reshape(gi.h, gi.w) if conf_out is not None else None)
+
+
+def dump_f32(path, data):
+    """DumpF32 (StereoAsyncApi.cs:252-256): int32 {w, h, w, 4} then the rows of a 2-D float32 array."""
+    d = np.ascontiguousarray(np.asarray(data, np.float32))
+    h, w = d.shape
+    rc = L.load().lux_dump_f32(os.fsencode(path), d.ctypes.data, w, h)
+    if rc:
+        _raise(rc, f"lux_dump_f32 {path}")
+
+
+def load_f32(path):
+    """LoadF32 (StereoAsyncApi.cs:257-261), as LUX_DENSE_OVERRIDE reads a layer-5 depth: the (h, w) float32 array."""
+    lib = L.load()
+    w, h = ctypes.c_int32(), ctypes.c_int32()
+    rc = lib.lux_load_f32(os.fsencode(path), None, 0, ctypes.byref(w), ctypes.byref(h))
+    if rc == 0:
+        out = np.empty((h.value, w.value), np.float32)
+        rc = lib.lux_load_f32(os.fsencode(path), out.ctypes.data, out.size, ctypes.byref(w), ctypes.byref(h))
+    if rc:
+        _raise(rc, {17: f"{path}: expected a 4-byte float dump"}.get(rc, f"lux_load_f32 {path}"))
+    return out
+
+
+def dump_rgba8(path, img):
+    """DumpRgba8 (StereoAsyncApi.cs:217-223): int32 {w, h, w, 4} then the rows of an (h, w, 4) uint8 image."""
+    ci, keep = _img_c(img)
+    rc = L.load().lux_dump_rgba8(os.fsencode(path), ctypes.byref(ci))
+    if rc:
+        _raise(rc, f"lux_dump_rgba8 {path}")
+
+
+def dump_dense(prefix, layers, images, calibs, cv_max=2, ctx: Optional[Context] = None):
+    """The dense dump of State4And5 (StereoAsyncApi.cs:197-214) for solved layers and their raw input images:
+    <prefix>_dense_L<i>_{depth.f32, planes.f32, skip.u8}, _dense_L0_guidance.img, _dense_calibs.bin,
+    _dense_img<k>.img, _dense_filt<k>.img and the cost volumes of layers 0..cv_max."""
+    ctx = ctx or default_context()
+    arr = (L.Img * len(images))()
+    keep = []
+    for i, im in enumerate(images):
+        ci, k = _img_c(im)
+        arr[i] = ci
+        keep.append(k)
+    hs = (ctypes.c_void_p * len(layers))(*[l.handle.value if hasattr(l.handle, "value") else l.handle for l in layers])
+    ctx.check(ctx.lib.lux_dump_dense(ctx.handle, hs, len(layers), len(images), arr, _calibs_c(calibs), os.fsencode(prefix),
+                                     cv_max))
 
 
 def _f32_image(a):

@@ -270,3 +270,72 @@ def mt19937_stream(seed, n):
     st = ctypes.create_string_buffer(624 * 4 + 16)
     lib().lo_mt_seed(st, seed)
     return np.array([lib().lo_mt_next(st) for _ in range(n)], np.uint32)
+
+
+# ---------------- dump formats (StereoAsyncApi.cs:197-262), restated for the tests ----------------
+
+def _hdr(w, h, bpp):
+    return np.array([w, h, w, bpp], "<i4").tobytes()
+
+
+def f32_bytes(a):
+    """DumpF32 (StereoAsyncApi.cs:252-256)."""
+    a = np.ascontiguousarray(a, "<f4")
+    return _hdr(a.shape[1], a.shape[0], 4) + a.tobytes()
+
+
+def rgba8_bytes(img):
+    """DumpRgba8 (StereoAsyncApi.cs:217-223)."""
+    a = np.ascontiguousarray(img, np.uint8)
+    return _hdr(a.shape[1], a.shape[0], 4) + a.tobytes()
+
+
+def cost_volume_bytes(L):
+    """DumpCostVolume (StereoAsyncApi.cs:227-250) of an oracle layer dict: {suffix: bytes} for _offsets.u32, _costvol.bin
+    and, when the layer kept them, _costvol_pass1.bin."""
+    w, h = L["W"], L["H"]
+    start, count, cap, skip = (np.asarray(L[k]).reshape(-1) for k in ("Start", "Count", "Cap", "Skip"))
+    off = L["Offsets"]
+    sizes = 8 + cap.astype(np.int64) * np.where(skip == 0, 3, 2)
+    boff = (np.concatenate([[0], np.cumsum(sizes)[:-1]]) & 0xFFFFFFFF).astype("<u4")
+    out = {"_offsets.u32": _hdr(w, h, 4) + boff.tobytes()}
+
+    def body(agg):
+        parts = []
+        for i in range(w * h):
+            o, c = int(off[i]), int(cap[i])
+            parts.append(np.array([start[i], count[i], 1, c], "<u2").tobytes())
+            parts.append(np.ascontiguousarray(agg[o:o + c], "<u2").tobytes())
+            if skip[i] == 0:
+                parts.append(L["Raw"][o:o + c].tobytes())
+        return b"".join(parts)
+
+    out["_costvol.bin"] = body(L["Agg"])
+    if L.get("AggPass1") is not None:
+        out["_costvol_pass1.bin"] = body(L["AggPass1"])
+    return out
+
+
+def dense_dump_bytes(layers, images, filtered, calibs, cv_max=2):
+    """The files of State4And5's dense dump (StereoAsyncApi.cs:197-214), as {name after the prefix: bytes}."""
+    out = {}
+    for i, L in enumerate(layers):
+        p = f"_dense_L{i}"
+        out[p + "_depth.f32"] = f32_bytes(L["Depth"])
+        out[p + "_planes.f32"] = np.ascontiguousarray(L["Planes"], "<f4").tobytes()
+        out[p + "_skip.u8"] = _hdr(L["W"], L["H"], 1) + np.ascontiguousarray(L["Skip"], np.uint8).tobytes()
+        if i == 0:
+            out[p + "_guidance.img"] = rgba8_bytes(L["Guidance"])
+        if i <= cv_max:
+            for k, v in cost_volume_bytes(L).items():
+                out[p + k] = v
+    cb = bytearray(len(calibs) * 0xA8)
+    for c, cal in enumerate(calibs):
+        cb[c * 0xA8:c * 0xA8 + 36] = np.asarray(cal.K, "<f4").reshape(9).tobytes()
+        cb[c * 0xA8 + 0x24:c * 0xA8 + 0x30] = np.asarray(cal.T, "<f4").reshape(3).tobytes()
+        cb[c * 0xA8 + 0x30:c * 0xA8 + 0x54] = np.asarray(cal.R, "<f4").reshape(9).tobytes()
+    out["_dense_calibs.bin"] = bytes(cb)
+    for k, (im, fi) in enumerate(zip(images, filtered)):
+        out[f"_dense_img{k}.img"] = rgba8_bytes(im)
+        out[f"_dense_filt{k}.img"] = rgba8_bytes(fi)
+    return out
