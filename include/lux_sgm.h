@@ -182,6 +182,34 @@ int lux_dump_cost_volume(const lux_layer* layer, const char* prefix);
 int lux_dump_dense(lux_sgm_ctx* ctx, lux_layer* const* layers, int32_t n_layers, int32_t n_cams, const lux_img_rgba8* images,
                    const lux_calib* calibs, const char* prefix, int32_t cv_max);
 
+/* AlignedCalib (Lux.Engine/Pipeline/Geometry/AlignedCalibration.cs:149-178), the geometry of the stereo-image and guide
+ * warps as the host builds it (AlignedCalib.Build): H row-major, the 4096 CRA factors (host memory), centre and scales. */
+typedef struct {
+  float H[9];
+  const float* lut;
+  float cx, cy, sx, sy;
+} lux_aligned_calib;
+
+/* StereoImage.Warp (Lux.Engine/Pipeline/Registration/StereoImage.cs:249-296): dst (dw x dh RGBA floats) from src (sw x sh
+ * RGBA floats, rows of sw pixels) scaled by gain first, 6x6 Lanczos-3 taps, 0 where no tap lands. */
+int lux_warp_f32(lux_sgm_ctx* ctx, const float* src, int32_t sw, int32_t sh, int32_t src_on_device, float gain,
+                 const lux_aligned_calib* ac, int32_t dw, int32_t dh, float* dst, int32_t dst_on_device);
+/* StereoImageBuilder.Create (StereoImageBuilder.cs:61-69, 78), colour sensors after the ISP: the half-resolution ISP
+ * output src scaled by the exposure gain, warped into dw x dh, ConvertToYUV with the sensor's luma basis over the neutral
+ * (StereoImage.cs:140-195), the 8-bit store (:198-209) into out_rgba8 — the dense solve's input image, which can stay on
+ * the device — and, when out_yuv is not NULL, the YUV floats (the reference camera's RefYuv). */
+int lux_stereo_image(lux_sgm_ctx* ctx, const float* src, int32_t sw, int32_t sh, int32_t src_on_device, float gain,
+                     const lux_aligned_calib* ac, int32_t dw, int32_t dh, int32_t sensor_type, const float* neutral,
+                     uint8_t* out_rgba8, int32_t out_on_device, float* out_yuv, int32_t yuv_on_device);
+/* Rgba8Warp.Warp (ReferenceGuide.cs:108-156): the 8-bit warp that makes the upsample's guide from the ISP'd reference
+ * image (every tap clamped to the image). "empty source image!" is LUX_ERR_ARG. */
+int lux_warp_rgba8(lux_sgm_ctx* ctx, const lux_img_rgba8* src, const lux_aligned_calib* ac, int32_t dw, int32_t dh, uint8_t* dst,
+                   int32_t dst_on_device);
+/* StereoImage.LanczosTable (StereoImage.cs:212-237): the 64 x 6 taps the warps use. */
+void lux_lanczos_table(float* out384);
+/* StereoImage.YuvMatrix (StereoImage.cs:140-160): the 3 x 4 rows (v, u', t'). */
+void lux_yuv_matrix(int32_t sensor_type, const float* neutral, float* out12);
+
 /* DepthImageCache.Set (Lux.Engine/Pipeline/Export/DepthCache.cs:136-143, fed by FromFullDepth :239-244): the cache image
  * (cw x ch floats) made from a depth map (w x h): InverseDepth, the nearest 16.16 resample to the cache dims, then
  * min(rcpps(x), 1e5). depth / cache are device pointers of the context's GPU when *_on_device, else host memory.

@@ -49,6 +49,11 @@ class Result(ctypes.Structure):
                 ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double)]
 
 
+class AlignedCalib(ctypes.Structure):
+    _fields_ = [("H", ctypes.c_float * 9), ("lut", ctypes.c_void_p), ("cx", ctypes.c_float), ("cy", ctypes.c_float),
+                ("sx", ctypes.c_float), ("sy", ctypes.c_float)]
+
+
 class LayerInfo(ctypes.Structure):
     _fields_ = [("w", ctypes.c_int32), ("h", ctypes.c_int32), ("index", ctypes.c_int32), ("align", ctypes.c_int32),
                 ("n_planes", ctypes.c_int32), ("min_lo", ctypes.c_int32), ("max_hi", ctypes.c_int32), ("tile", ctypes.c_int32),
@@ -96,6 +101,15 @@ SIGNATURES = [
     ("lux_dump_cost_volume", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("lux_dump_dense", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int32,
                                       ctypes.POINTER(Img), ctypes.POINTER(Calib), ctypes.c_char_p, ctypes.c_int32]),
+    ("lux_warp_f32", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+                                    ctypes.POINTER(AlignedCalib), ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]),
+    ("lux_stereo_image", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_float, ctypes.POINTER(AlignedCalib), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]),
+    ("lux_warp_rgba8", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Img), ctypes.POINTER(AlignedCalib), ctypes.c_int32,
+                                      ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]),
+    ("lux_lanczos_table", None, [ctypes.c_void_p]),
+    ("lux_yuv_matrix", None, [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]),
     ("lux_server_create", ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
     ("lux_server_destroy", None, [ctypes.c_void_p]),
     ("lux_server_last_error", ctypes.c_char_p, [ctypes.c_void_p]),

@@ -487,6 +487,113 @@ class DepthImageCache:
 
 
 @dataclass
+class AlignedCalib:
+    """AlignedCalib (Lux.Engine/Pipeline/Geometry/AlignedCalibration.cs:149-178) as AlignedCalib.Build leaves it: the
+    row-major homography H (view -> module), the 4096 CRA factors lut, the centre (Cx, Cy) and the scales (Sx, Sy)."""
+    H: np.ndarray
+    lut: np.ndarray
+    cx: float
+    cy: float
+    sx: float
+    sy: float
+
+    def to_c(self):
+        c = L.AlignedCalib()
+        for i, v in enumerate(np.asarray(self.H, np.float32).reshape(9)):
+            c.H[i] = float(v)
+        lut = np.ascontiguousarray(np.asarray(self.lut, np.float32))
+        if lut.size != 4096:
+            raise ValueError("the CRA lut has 4096 entries")
+        c.lut = lut.ctypes.data
+        c.cx, c.cy, c.sx, c.sy = float(self.cx), float(self.cy), float(self.sx), float(self.sy)
+        return c, lut
+
+
+def _image_f32(a):
+    """(pointer, on_device, keep-alive, (h, w)) of an (h, w, 4) float32 image: numpy or a contiguous CUDA torch tensor."""
+    if hasattr(a, "data_ptr"):
+        assert a.dim() == 3 and a.shape[2] == 4 and a.is_contiguous() and str(a.dtype) == "torch.float32"
+        return a.data_ptr(), 1 if a.is_cuda else 0, a, tuple(a.shape[:2])
+    d = np.ascontiguousarray(np.asarray(a, np.float32))
+    assert d.ndim == 3 and d.shape[2] == 4
+    return d.ctypes.data, 0, d, d.shape[:2]
+
+
+def _empty_like_kind(ref, shape, dtype):
+    if hasattr(ref, "data_ptr") and ref.is_cuda:
+        import torch
+        return torch.empty(shape, dtype={np.float32: torch.float32, np.uint8: torch.uint8}[dtype], device=ref.device)
+    return np.empty(shape, dtype)
+
+
+def _ptr(a):
+    return (a.data_ptr(), 1 if a.is_cuda else 0) if hasattr(a, "data_ptr") else (a.ctypes.data, 0)
+
+
+class StereoImage:
+    """Stereo-image formation after the ISP (StereoImage.cs, StereoImageBuilder.cs:45-79, colour sensors) on the GPU.
+    Images are numpy arrays or CUDA torch tensors; outputs are of the kind of the source."""
+
+    @staticmethod
+    def lanczos_table() -> np.ndarray:
+        """LanczosTable (StereoImage.cs:212-237): (64, 6) float32."""
+        out = np.empty(384, np.float32)
+        L.load().lux_lanczos_table(out.ctypes.data)
+        return out.reshape(64, 6)
+
+    @staticmethod
+    def yuv_matrix(sensor_type, neutral) -> np.ndarray:
+        """YuvMatrix (StereoImage.cs:140-160): (3, 4) float32 rows (v, u', t')."""
+        n = np.ascontiguousarray(np.asarray(neutral, np.float32).reshape(3))
+        out = np.empty(12, np.float32)
+        L.load().lux_yuv_matrix(int(sensor_type), n.ctypes.data, out.ctypes.data)
+        return out.reshape(3, 4)
+
+    @staticmethod
+    def warp(src, dw, dh, ac: AlignedCalib, gain=1.0, ctx: Optional[Context] = None):
+        """Warp (StereoImage.cs:249-296) of an (sh, sw, 4) float image scaled by gain first: (dh, dw, 4) float32."""
+        ctx = ctx or default_context()
+        ptr, on_dev, keep, (sh, sw) = _image_f32(src)
+        out = _empty_like_kind(src, (dh, dw, 4), np.float32)
+        optr, oon = _ptr(out)
+        c, lut = ac.to_c()
+        _torch_ready(src, out)
+        ctx.check(ctx.lib.lux_warp_f32(ctx.handle, ptr, sw, sh, on_dev, float(gain), ctypes.byref(c), dw, dh, optr, oon))
+        return out
+
+    @staticmethod
+    def create(src, dw, dh, ac: AlignedCalib, sensor_type, neutral, gain=1.0, keep_yuv=False, ctx: Optional[Context] = None):
+        """StereoImageBuilder.Create after RunIspTiled (StereoImageBuilder.cs:61-69, 78): the (dh, dw, 4) uint8 stereo
+        image and, with keep_yuv, its (dh, dw, 4) YUV floats (the reference camera's RefYuv), else None."""
+        ctx = ctx or default_context()
+        ptr, on_dev, keep, (sh, sw) = _image_f32(src)
+        out = _empty_like_kind(src, (dh, dw, 4), np.uint8)
+        yuv = _empty_like_kind(src, (dh, dw, 4), np.float32) if keep_yuv else None
+        optr, oon = _ptr(out)
+        yptr, yon = _ptr(yuv) if yuv is not None else (None, 0)
+        n = np.ascontiguousarray(np.asarray(neutral, np.float32).reshape(3))
+        c, lut = ac.to_c()
+        _torch_ready(src, out, *(() if yuv is None else (yuv,)))
+        ctx.check(ctx.lib.lux_stereo_image(ctx.handle, ptr, sw, sh, on_dev, float(gain), ctypes.byref(c), dw, dh, int(sensor_type),
+                                           n.ctypes.data, optr, oon, yptr, yon))
+        return out, yuv
+
+
+class Rgba8Warp:
+    @staticmethod
+    def warp(src, dw, dh, ac: AlignedCalib, ctx: Optional[Context] = None):
+        """Rgba8Warp.Warp (ReferenceGuide.cs:108-156): the reference guide's 8-bit warp of an (sh, sw, 4) uint8 image."""
+        ctx = ctx or default_context()
+        ci, keep = _img_c(src)
+        out = _empty_like_kind(src, (dh, dw, 4), np.uint8)
+        optr, oon = _ptr(out)
+        c, lut = ac.to_c()
+        _torch_ready(src, out)
+        ctx.check(ctx.lib.lux_warp_rgba8(ctx.handle, ctypes.byref(ci), ctypes.byref(c), dw, dh, optr, oon))
+        return out
+
+
+@dataclass
 class ServedResult:
     """One served request: its depth map (the layer grid) and the times it spent queued and running."""
     Depth: np.ndarray

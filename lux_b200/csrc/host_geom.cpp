@@ -140,6 +140,90 @@ uint32_t host_rsqrt_bits(uint32_t b) {
 
 float host_rcp(float x) { return float_of(host_rcp_bits(bits_of(x))); }
 const uint32_t* host_rcp_table() { return lux_rcp_table; }
+const uint32_t* host_rsqrt_table(bool e128) { return e128 ? lux_rsqrt_table_e128 : lux_rsqrt_table_e127; }
+
+namespace {
+
+// sinf as Wine's ucrtbase evaluates it (Lux.Engine/Pipeline/WineCrt.cs:21-99): quadrant shifts by multiples of pi/2 in
+// double, then the Taylor polynomials of sin and cos to degree 9 and 10 in double, rounded to float once. The Lanczos
+// table only reaches |x| < 3·pi, inside the shifted ranges; the general reduction (n = rint(x·2/pi)) covers the rest.
+float sin_poly(double x) {
+  const double z = x * x;
+  if (x > -0.007817583158612251 && 0.007817583158612251 > x) return (float)((z * -0.16666666666666666 + 1.0) * x);
+  const double s = x * z, w = z * z;
+  const double r = 2.7557319223985893e-06 * z - 0.0001984126984126984, q = z * 0.008333333333333333 - 0.16666666666666666;
+  return (float)((w * s) * r + (q * s + x));
+}
+float cos_poly(double x) {
+  const double z = x * x;
+  if (x > -0.007816314697265625 && 0.007816314697265625 > x) return (float)(z * -0.5 + 1.0);
+  double p = -2.755731922398589e-07 * z + 2.48015873015873e-05;
+  p = p * z - 0.001388888888888889;
+  p = p * z + 0.041666666666666664;
+  p = p * z - 0.5;
+  return (float)(p * z + 1.0);
+}
+float crt_sinf(float x) {
+  const double half_pi = 1.5707963267948966, pi = 3.141592653589793, three_half_pi = 4.71238898038469, two_pi = 6.283185307179586;
+  const uint32_t ax = bits_of(x) & 0x7fffffffu;
+  const bool neg = (bits_of(x) >> 31) != 0;
+  const double d = x;
+  if (ax <= 0x3f490fdau) return ax < 0x39800000u ? x : sin_poly(d);                                      // |x| <= pi/4
+  if (ax <= 0x4016cbe3u) return neg ? -cos_poly(d + half_pi) : cos_poly(d - half_pi);                   // <= 3pi/4
+  if (ax <= 0x407b53d1u) return sin_poly(neg ? -(d + pi) : -(d - pi));                                  // <= 5pi/4
+  if (ax <= 0x40afeddfu) return neg ? cos_poly(d + three_half_pi) : -cos_poly(d - three_half_pi);       // <= 7pi/4
+  if (ax <= 0x40e231d5u) return sin_poly(neg ? d + two_pi : d - two_pi);                                // <= 9pi/4
+  if (ax >= 0x7f800000u) return x - x;
+  const double n = d * 6.36619772367581382433e-01 + 6755399441055744.0 - 6755399441055744.0;
+  const double y = d - n * 1.57079631090164184570e+00 - n * 1.58932547735281966916e-08;
+  switch ((int)n & 3) {
+    case 0: return sin_poly(y);
+    case 1: return cos_poly(y);
+    case 2: return sin_poly(-y);
+    default: return -cos_poly(y);
+  }
+}
+
+}  // namespace
+
+void host_lanczos_table(float out[384]) {
+  const float pi = float_of(0x40490fdbu), pi_3 = float_of(0x3f860a92u), pi_sq = float_of(0x411de9e7u);
+  for (int phase = 0; phase < 64; phase++) {
+    const float p = (float)phase * 0.015625f;
+    float sum = 0.0f;
+    for (int tap = 0; tap < 6; tap++) {
+      const float x = p - (float)(tap - 2);
+      float w = 0.0f;
+      if (x == 0.0f) w = 1.0f;
+      else if (std::fabs(x) < 3.0f) w = (crt_sinf(x * pi_3) * (crt_sinf(x * pi) * 3.0f)) / ((x * x) * pi_sq);
+      out[phase * 6 + tap] = w;
+      sum = sum + w;
+    }
+    const float inv = 1.0f / sum;
+    for (int tap = 0; tap < 6; tap++) out[phase * 6 + tap] *= inv;
+  }
+}
+
+void host_yuv_matrix(int sensor_type, const float neutral[3], float out[12]) {
+  // the luma basis per sensor type: AR1335 (types 2, 3) and the others (StereoImage.cs:135-136)
+  static const uint32_t kAr1335[3] = {0x3e5cb924u, 0x3edd5758u, 0x3eb44c16u}, kOther[3] = {0x3e9e39b4u, 0x3e95ca4bu, 0x3ecbfc22u};
+  const uint32_t* t = (sensor_type == 2 || sensor_type == 3) ? kAr1335 : kOther;
+  const float a = float_of(t[0]), b = float_of(t[1]), c = float_of(t[2]);
+  const float ix = 1.0f / neutral[0], iy = 1.0f / neutral[1], iz = 1.0f / neutral[2];
+  const float s = c + a;
+  const float u0 = (b * (-b) - s * c) * ix, u1 = ((a - c) * b) * iy, u2 = (s * a - b * (-b)) * iz;
+  const float t0 = ix * (-b), t1 = iy * s, t2 = iz * (-b);
+  // 1/|row| by rsqrtss and one Newton step, in the reference's operation order
+  const float v2 = c * c + (b * b + a * a);
+  const float rv = float_of(host_rsqrt_bits(bits_of(v2))), Sv = v2 * rv;
+  const float kv = v2 == 0.0f ? 0.0f : (Sv * rv + (-3.0f)) * (Sv * (-0.5f));
+  const float nu = u2 * u2 + (u1 * u1 + u0 * u0), ru = float_of(host_rsqrt_bits(bits_of(nu)));
+  const float ku = ((ru * (-0.5f)) * kv) * ((nu * ru) * ru + (-3.0f));
+  const float nt = t2 * t2 + (t1 * t1 + t0 * t0), rt = float_of(host_rsqrt_bits(bits_of(nt)));
+  const float kt = ((rt * (-0.5f)) * kv) * ((nt * rt) * rt + (-3.0f));
+  const float m[12] = {a, b, c, 0.0f, u0 * ku, u1 * ku, ku * u2, 0.0f, t0 * kt, t1 * kt, kt * t2, 0.0f};
+  std::memcpy(out, m, sizeof m);
+}
 
 int host_planes(float near_, float far_, const lux_calib* calibs, int ncams, float density, int align, std::vector<float>& planes) {
   if (!(near_ < far_)) return LUX_ERR_NEAR_FAR;

@@ -22,4 +22,11 @@ int host_skip_mask(int mode, int w, int h, std::vector<uint8_t>& m);
 // The plane-index boundaries of RangeFromPrevious (DenseStereoSgm.cs:94-96); returns whether they are non-decreasing.
 bool host_range_bounds(const std::vector<float>& planes, std::vector<float>& b);
 
+// The rsqrtss tables for exponents 127 and 128 (uploaded with the rcp table).
+const uint32_t* host_rsqrt_table(bool e128);
+// StereoImage.LanczosTable (Lux.Engine/Pipeline/Registration/StereoImage.cs:212-237): 64 phases x 6 taps.
+void host_lanczos_table(float out[384]);
+// StereoImage.YuvMatrix (StereoImage.cs:140-160): the rows (v, u', t') of ConvertToYUV for a sensor type and neutral.
+void host_yuv_matrix(int sensor_type, const float neutral[3], float out[12]);
+
 }  // namespace lux

@@ -67,6 +67,23 @@ void launch_depth_cache_set(const float* src, int w, int h, int cw, int ch, cons
 void launch_depth_cache_fetch(const float* img, int istride, int vx0, int vy0, int vw, int vh, double offx, double offy, double sx,
                               double sy, int rw, int rh, const uint32_t* rcp, float* out, cudaStream_t s);
 
+// warp.cu: stereo-image formation after the ISP and the reference guide's 8-bit warp (StereoImage.cs, ReferenceGuide.cs)
+struct WarpGeom {  // AlignedCalib (Lux.Engine/Pipeline/Geometry/AlignedCalibration.cs:149-178) with its lut on the device
+  float h[9];
+  float cx, cy, sx, sy;
+  const float* lut;
+};
+struct YuvRows {  // the rows (v, u', t') of StereoImage.YuvMatrix
+  float m[3][4];
+};
+// taps: the 384-float Lanczos table; rsq: the rsqrt tables for exponents 127 then 128 (4096 entries each).
+// m == nullptr: the warped float image into out_f. Else the stereo image into out_u8 and, when out_f != nullptr, its
+// YUV floats into out_f.
+void launch_warp_f32(const float* src, int sw, int sh, float gain, const WarpGeom& g, const float* taps, const uint32_t* rsq,
+                     int dw, int dh, const YuvRows* m, float* out_f, uint8_t* out_u8, int* err, cudaStream_t s);
+void launch_warp_rgba8(const uint8_t* src, int sw, int sh, int sstride, const WarpGeom& g, const float* taps, const uint32_t* rsq,
+                       int dw, int dh, uint8_t* out, int* err, cudaStream_t s);
+
 // cost.cu
 // The phase images of every other camera into a.phase (4·ow·oh u32 each); then the cost volume.
 // zt: per other camera and plane, the plane-only projection terms (z·W[8] + W[12], z·W[9] + W[13], z·W[10] + W[14], 0),

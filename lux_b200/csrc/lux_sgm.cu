@@ -26,6 +26,7 @@ struct lux_sgm_ctx {
   std::mutex mu;
   std::string last_error;
   uint32_t* d_rcp = nullptr;  // 4096-entry rcp table
+  uint32_t* d_warp = nullptr; // the rsqrt tables (exponents 127, 128; 4096 entries each), then the 384-float Lanczos table
   int* d_err = nullptr;       // device error word of the current call
   cudaEvent_t ev[4] = {};
 };
@@ -426,6 +427,14 @@ int lux_sgm_create(int device, uint64_t hbm_budget_bytes, lux_sgm_ctx** out) {
   if (cudaMalloc(&ctx->d_rcp, 4096 * 4) != cudaSuccess) return fail(LUX_ERR_ALLOC);
   if (cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) return fail(LUX_ERR_ALLOC);
   cudaMemcpy(ctx->d_rcp, host_rcp_table(), 4096 * 4, cudaMemcpyHostToDevice);
+  {
+    std::vector<uint32_t> wt(8192 + 384);
+    std::memcpy(wt.data(), host_rsqrt_table(false), 4096 * 4);
+    std::memcpy(wt.data() + 4096, host_rsqrt_table(true), 4096 * 4);
+    host_lanczos_table(reinterpret_cast<float*>(wt.data() + 8192));
+    if (cudaMalloc(&ctx->d_warp, wt.size() * 4) != cudaSuccess) return fail(LUX_ERR_ALLOC);
+    cudaMemcpy(ctx->d_warp, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice);
+  }
   cudaMemset(ctx->d_err, 0, sizeof(int));
   for (auto& e : ctx->ev) cudaEventCreate(&e);
   *out = ctx;
@@ -438,6 +447,7 @@ void lux_sgm_destroy(lux_sgm_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (auto& e : ctx->ev) cudaEventDestroy(e);
   cudaFree(ctx->d_rcp);
+  cudaFree(ctx->d_warp);
   cudaFree(ctx->d_err);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -766,14 +776,14 @@ int device_floats(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, const float* p, si
 // Runs `fill` into the caller's output: directly when it is on the device, else through a device buffer copied back.
 // Device in, device out: nothing to wait for, the work stays queued on the context's stream. Otherwise the call waits
 // for the host copy, or for the work that reads the temporary buffers the caller frees next.
-template <class F>
-int to_output(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, float* out, size_t n, int on_device, F fill) {
-  float* d = out;
+template <class T, class F>
+int to_output(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, T* out, size_t n, int on_device, F fill) {
+  T* d = out;
   int rc = LUX_OK;
   if (!on_device && (rc = alloc_t(ctx, tmp, n, &d))) return rc;
   fill(d);
   CK(cudaGetLastError());
-  if (!on_device) CK(cudaMemcpyAsync(out, d, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (!on_device) CK(cudaMemcpyAsync(out, d, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
   if (!on_device || !tmp.empty()) CK(cudaStreamSynchronize(ctx->stream));
   return LUX_OK;
 }
@@ -830,6 +840,110 @@ extern "C" int lux_depth_cache_fetch(lux_sgm_ctx* ctx, const float* cache, int32
   }
   dev_free_all(ctx, tmp);
   return rc;
+}
+
+// ---------------- stereo-image formation after the ISP, reference guide warp ----------------
+
+namespace {
+
+// The aligned calibration with its lut copied to the device.
+int warp_geom(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, const lux_aligned_calib* ac, WarpGeom* g) {
+  if (!ac || !ac->lut) return set_err(ctx, LUX_ERR_ARG, "aligned calibration without a lut");
+  std::memcpy(g->h, ac->H, sizeof g->h);
+  g->cx = ac->cx;
+  g->cy = ac->cy;
+  g->sx = ac->sx;
+  g->sy = ac->sy;
+  float* d = nullptr;
+  int rc = alloc_t(ctx, tmp, 4096, &d);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(d, ac->lut, 4096 * 4, cudaMemcpyHostToDevice, ctx->stream));
+  g->lut = d;
+  return LUX_OK;
+}
+
+const float* warp_taps(const lux_sgm_ctx* ctx) { return reinterpret_cast<const float*>(ctx->d_warp + 8192); }
+
+}  // namespace
+
+extern "C" int lux_warp_f32(lux_sgm_ctx* ctx, const float* src, int32_t sw, int32_t sh, int32_t src_on_device, float gain,
+                            const lux_aligned_calib* ac, int32_t dw, int32_t dh, float* dst, int32_t dst_on_device) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!src || !dst || sw < 1 || sh < 1 || dw < 1 || dh < 1) return set_err(ctx, LUX_ERR_ARG, "warp: null pointer or empty image");
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  WarpGeom g;
+  const float* d_src = nullptr;
+  int rc = warp_geom(ctx, tmp, ac, &g);
+  if (!rc) rc = device_floats(ctx, tmp, src, (size_t)sw * sh * 4, src_on_device, &d_src);
+  if (!rc)
+    rc = to_output(ctx, tmp, dst, (size_t)dw * dh * 4, dst_on_device, [&](float* d) {
+      launch_warp_f32(d_src, sw, sh, gain, g, warp_taps(ctx), ctx->d_warp, dw, dh, nullptr, d, nullptr, ctx->d_err, ctx->stream);
+    });
+  if (!rc) rc = take_device_error(ctx);
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
+extern "C" int lux_stereo_image(lux_sgm_ctx* ctx, const float* src, int32_t sw, int32_t sh, int32_t src_on_device, float gain,
+                                const lux_aligned_calib* ac, int32_t dw, int32_t dh, int32_t sensor_type, const float* neutral,
+                                uint8_t* out_rgba8, int32_t out_on_device, float* out_yuv, int32_t yuv_on_device) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!src || !out_rgba8 || !neutral || sw < 1 || sh < 1 || dw < 1 || dh < 1)
+    return set_err(ctx, LUX_ERR_ARG, "stereo image: null pointer or empty image");
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  WarpGeom g;
+  YuvRows m;
+  host_yuv_matrix(sensor_type, neutral, &m.m[0][0]);
+  const float* d_src = nullptr;
+  float* d_yuv = out_yuv && yuv_on_device ? out_yuv : nullptr;
+  const size_t npx = (size_t)dw * dh;
+  int rc = warp_geom(ctx, tmp, ac, &g);
+  if (!rc) rc = device_floats(ctx, tmp, src, (size_t)sw * sh * 4, src_on_device, &d_src);
+  if (!rc && out_yuv && !yuv_on_device) rc = alloc_t(ctx, tmp, npx * 4, &d_yuv);
+  if (!rc)
+    rc = to_output(ctx, tmp, out_rgba8, npx * 4, out_on_device, [&](uint8_t* d) {
+      launch_warp_f32(d_src, sw, sh, gain, g, warp_taps(ctx), ctx->d_warp, dw, dh, &m, d_yuv, d, ctx->d_err, ctx->stream);
+    });
+  if (!rc && out_yuv && !yuv_on_device) {
+    CK(cudaMemcpyAsync(out_yuv, d_yuv, npx * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  if (!rc) rc = take_device_error(ctx);
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
+extern "C" int lux_warp_rgba8(lux_sgm_ctx* ctx, const lux_img_rgba8* src, const lux_aligned_calib* ac, int32_t dw, int32_t dh,
+                              uint8_t* dst, int32_t dst_on_device) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!src || !dst || dw < 1 || dh < 1) return set_err(ctx, LUX_ERR_ARG, "warp: null pointer or empty destination");
+  if (src->w < 1 || src->h < 1) return set_err(ctx, LUX_ERR_ARG, "empty source image!");  // ReferenceGuide.cs:110
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  WarpGeom g;
+  const uint8_t* d_src = nullptr;
+  int rc = warp_geom(ctx, tmp, ac, &g);
+  if (!rc) rc = upload_image(ctx, tmp, *src, &d_src);
+  if (!rc)
+    rc = to_output(ctx, tmp, dst, (size_t)dw * dh * 4, dst_on_device, [&](uint8_t* d) {
+      launch_warp_rgba8(d_src, src->w, src->h, src->w, g, warp_taps(ctx), ctx->d_warp, dw, dh, d, ctx->d_err, ctx->stream);
+    });
+  if (!rc) rc = take_device_error(ctx);
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
+extern "C" void lux_lanczos_table(float* out384) {
+  if (out384) host_lanczos_table(out384);
+}
+
+extern "C" void lux_yuv_matrix(int32_t sensor_type, const float* neutral, float* out12) {
+  if (neutral && out12) host_yuv_matrix(sensor_type, neutral, out12);
 }
 
 // ---------------- allocation-free upsample ----------------

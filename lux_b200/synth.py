@@ -251,3 +251,37 @@ def module_capture(w, h, n_others=10, seed=0, crop_mp=(1.0, 6.0), ds=(64, 96, 12
         dk.append(d)
     params = StereoParams(scale=1, tile=tile, skip_mode=0, plane_density=1.0)
     return ModuleCapture(imgs, [1] * (n_others + 1), cal, near, far, z_inv[h:2 * h, w:2 * w], sizes, dk, params)
+
+
+def isp_image(w, h, seed=0):
+    """A half-resolution ISP output as the stereo images take it: linear RGB in [0, 1] (1/f texture per channel, a
+    colour cast), alpha 1; (h, w, 4) float32."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((h, w, 4), np.float32)
+    for c in range(3):
+        out[..., c] = (texture(h, w, seed * 7 + c, max_value=1.0) * rng.uniform(0.4, 1.0)).astype(np.float32)
+    out[..., 3] = 1.0
+    return out
+
+
+def aligned_calib(sw, sh, dw, dh, seed=0, angle_deg=0.6, focal_ratio=1.02, shift=(3.5, -2.25), lens=4e-9):
+    """An aligned calibration of the stereo-image warp (the fields AlignedCalib.Build leaves): the rotation homography
+    H = K_B·R·K_A^-1 of a dw x dh view onto a sw x sh module (a small rotation about the optical axis and a tilt, focal
+    lengths in the given ratio, a shifted principal point), and a radial CRA lut lut[r] = 1 + lens·r^2 over 4096 radius
+    steps with the scales putting the image corners near r = 3000. Values are float32 as the host computes them."""
+    rng = np.random.default_rng(seed)
+    f_a = 1.1 * dw
+    Ka = np.array([[f_a, 0, dw / 2.0], [0, f_a, dh / 2.0], [0, 0, 1]])
+    Kb = np.array([[f_a * focal_ratio, 0, sw / 2.0 + shift[0]], [0, f_a * focal_ratio, sh / 2.0 + shift[1]], [0, 0, 1]])
+    a = np.deg2rad(angle_deg)
+    t = np.deg2rad(rng.uniform(-0.3, 0.3, 2))
+    Rz = np.array([[np.cos(a), -np.sin(a), 0], [np.sin(a), np.cos(a), 0], [0, 0, 1]])
+    Rx = np.array([[1, 0, 0], [0, np.cos(t[0]), -np.sin(t[0])], [0, np.sin(t[0]), np.cos(t[0])]])
+    Ry = np.array([[np.cos(t[1]), 0, np.sin(t[1])], [0, 1, 0], [-np.sin(t[1]), 0, np.cos(t[1])]])
+    H = (Kb @ Rz @ Rx @ Ry @ np.linalg.inv(Ka)).astype(np.float32)
+    r = np.arange(4096, dtype=np.float64)
+    lut = (1.0 + lens * r * r).astype(np.float32)
+    half_diag = 0.5 * np.hypot(sw, sh)
+    s = np.float32(3000.0 / half_diag)
+    from .api import AlignedCalib
+    return AlignedCalib(H=H, lut=lut, cx=np.float32(sw / 2.0), cy=np.float32(sh / 2.0), sx=s, sy=s)

@@ -1176,3 +1176,245 @@ int lo_depth_cache_fetch(const float* img, int iw, int ih, int x0, int y0, int x
   }
   return LO_OK;
 }
+
+/* ---------------- stereo-image formation after the ISP (StereoImage.cs, ReferenceGuide.cs) ---------------- */
+
+/* WineCrt.Sindf / Cosdf (WineCrt.cs:24-45): Wine's ucrtbase Taylor kernels on a double argument. */
+static float wine_sindf(double x) {
+  double z = x * x;
+  if (x > -0.007817583158612251 && 0.007817583158612251 > x) return (float)((z * -0.16666666666666666 + 1.0) * x);
+  double s = x * z, w = z * z;
+  double r = 2.7557319223985893e-06 * z - 0.0001984126984126984, q = z * 0.008333333333333333 - 0.16666666666666666;
+  return (float)((w * s) * r + (q * s + x));
+}
+static float wine_cosdf(double x) {
+  double z = x * x;
+  if (x > -0.007816314697265625 && 0.007816314697265625 > x) return (float)(z * -0.5 + 1.0);
+  double p = -2.755731922398589e-07 * z + 2.48015873015873e-05;
+  p = p * z - 0.001388888888888889;
+  p = p * z + 0.041666666666666664;
+  p = p * z - 0.5;
+  return (float)(p * z + 1.0);
+}
+
+/* WineCrt.Sinf (WineCrt.cs:77-99) for |x| below 2^28·π/2 (the Lanczos table needs |x| < 3π). */
+float lo_wine_sinf(float x) {
+  const double pio2 = 1.5707963267948966, pi = 3.141592653589793, three_pio2 = 4.71238898038469, two_pi = 6.283185307179586;
+  uint32_t ix = fbits(x);
+  int sign = (int)(ix >> 31);
+  ix &= 0x7fffffffu;
+  if (ix <= 0x3f490fdau) return ix < 0x39800000u ? x : wine_sindf(x);
+  if (ix <= 0x407b53d1u) {
+    double d = x;
+    if (ix <= 0x4016cbe3u) return sign ? -wine_cosdf(d + pio2) : wine_cosdf(d - pio2);
+    return wine_sindf(sign ? -(d + pi) : -(d - pi));
+  }
+  if (ix <= 0x40e231d5u) {
+    double d = x;
+    if (ix <= 0x40afeddfu) return sign ? wine_cosdf(d + three_pio2) : -wine_cosdf(d - three_pio2);
+    return wine_sindf(sign ? d + two_pi : d - two_pi);
+  }
+  if (ix >= 0x7f800000u) return x - x;
+  {
+    /* musl __rem_pio2f, medium path */
+    double fn = (double)x * 6.36619772367581382433e-01 + 6755399441055744.0 - 6755399441055744.0;
+    double y = x - fn * 1.57079631090164184570e+00 - fn * 1.58932547735281966916e-08;
+    int n = (int)fn;
+    switch (n & 3) {
+      case 0: return wine_sindf(y);
+      case 1: return wine_cosdf(y);
+      case 2: return wine_sindf(-y);
+      default: return -wine_cosdf(y);
+    }
+  }
+}
+
+/* StereoImage.LanczosTable (StereoImage.cs:212-237): 64 phases x 6 taps of sinc(x)·sinc(x/3), normalised by the
+ * sequential sum. */
+void lo_lanczos_table(float tbl[384]) {
+  const float step = ffrom(0x3c800000u), pi3 = ffrom(0x3f860a92u), pi = ffrom(0x40490fdbu), pi2 = ffrom(0x411de9e7u), three = 3.0f;
+  for (int k = 0; k < 64; k++) {
+    float p = (float)k * step, sum = 0.0f;
+    for (int j = 0; j < 6; j++) {
+      float x = p - (float)(j - 2), w;
+      if (x == 0.0f) w = 1.0f;
+      else if (fabsf(x) < three) {
+        float s1 = lo_wine_sinf(x * pi), t = s1 * three, s2 = lo_wine_sinf(x * pi3);
+        w = (s2 * t) / ((x * x) * pi2);
+      } else w = 0.0f;
+      tbl[k * 6 + j] = w;
+      sum = sum + w;
+    }
+    float inv = 1.0f / sum;
+    for (int j = 0; j < 6; j++) tbl[k * 6 + j] *= inv;
+  }
+}
+
+/* (int)f as .NET 9+ converts: truncation, saturating, NaN -> 0. */
+static int net_int(float f) {
+  if (f != f) return 0;
+  if (f >= 2147483648.0f) return INT32_MAX;
+  if (f <= -2147483648.0f) return INT32_MIN;
+  return (int)f;
+}
+
+/* The map of one destination pixel through an aligned calibration (StereoImage.cs:260-272): 64ths of a source pixel.
+ * Returns 0, or -1 where the reference would index the lut below 0 (a subnormal r2 makes r = -inf). */
+static int warp_map(const lo_aligned* a, int x, int y, int* px, int* py) {
+  const float* H = a->H;
+  float fx = (float)x, fy = (float)y;
+  float Xn = H[2] + (H[0] * fx + H[1] * fy), Yn = H[5] + (H[3] * fx + H[4] * fy);
+  float den = (H[7] * fy + H[6] * fx) + H[8], w = 1.0f / den;
+  float dx = w * Xn - a->cx, dy = w * Yn - a->cy;
+  float r2 = (a->sy * dy) * (a->sy * dy) + (a->sx * dx) * (a->sx * dx);
+  float r;
+  if (r2 == 0.0f) r = 0.0f;
+  else {
+    float rs = ffrom(lo_rsqrt_bits(fbits(r2)));
+    float S = r2 * rs;
+    r = ((S * rs) + (-3.0f)) * (S * (-0.5f));
+  }
+  int idx = net_int(r);
+  if (idx >= 0x1000) idx = 0xfff;
+  if (idx < 0) return -1;
+  float lu = a->lut[idx];
+  *px = net_int(((a->cx + (-2.0f)) + lu * dx) * 64.0f);
+  *py = net_int(((a->cy + (-2.0f)) + dy * lu) * 64.0f);
+  return 0;
+}
+
+static int clampi(int v, int lo, int hi) { return v < lo ? lo : v > hi ? hi : v; }
+
+int lo_warp_f32(const float* src, int sw, int sh, float gain, int dw, int dh, const lo_aligned* ac, float* dst) {
+  if (sw < 1 || sh < 1 || dw < 0 || dh < 0 || !ac || !ac->lut) return LO_ERR_ARG;
+  float tbl[384];
+  lo_lanczos_table(tbl);
+  memset(dst, 0, (size_t)dw * dh * 16);
+  for (int y = 0; y < dh; y++)
+    for (int x = 0; x < dw; x++) {
+      int px, py;
+      if (warp_map(ac, x, y, &px, &py)) return LO_ERR_INDEX;
+      int i = px >> 6, fx = px & 63, j = py >> 6, fy = py & 63;
+      int interior = i >= 0 && i <= sw - 6 && j >= 0 && j <= sh - 6;
+      if (!interior && !(j < sh && j + 6 > 0 && i < sw && i + 6 > 0)) continue; /* fill 0 */
+      const float *ty = tbl + fy * 6, *tx = tbl + fx * 6;
+      int ro[6], co[6];
+      for (int k = 0; k < 6; k++) {
+        ro[k] = interior ? j + k : clampi(j + k, 0, sh - 1);
+        co[k] = interior ? i + k : clampi(i + k, 0, sw - 1);
+      }
+      for (int c = 0; c < 4; c++) {
+        float C[6];
+        for (int cc = 0; cc < 6; cc++) {
+          float P[6];
+          for (int rr = 0; rr < 6; rr++) {
+            float v = src[((size_t)ro[rr] * sw + co[cc]) * 4 + c];
+            P[rr] = gain != 1.0f ? v * gain : v; /* the source scaled in place before the warp */
+          }
+          C[cc] = (P[5] * ty[5] + P[4] * ty[4]) + ((P[3] * ty[3] + P[2] * ty[2]) + (P[1] * ty[1] + P[0] * ty[0]));
+        }
+        dst[((size_t)y * dw + x) * 4 + c] = (C[5] * tx[5] + C[4] * tx[4]) + ((C[3] * tx[3] + C[2] * tx[2]) + (C[1] * tx[1] + C[0] * tx[0]));
+      }
+    }
+  return LO_OK;
+}
+
+/* StereoImage.GammaEncode (StereoImage.cs:162-178): 255·sign·|m|^(1/2.2) by the log2/exp2 polynomials. */
+float lo_gamma_encode(float m) {
+  int32_t bits = (int32_t)fbits(m);
+  int32_t a = bits & 0x7fffffff;
+  float f = ffrom(((uint32_t)a & 0x007fffffu) | 0x3f800000u);
+  float e = (float)((int32_t)((uint32_t)a + 0xc0800000u) >> 23);
+  float log2 = ((f * ffrom(0x3e511af3u) + ffrom(0xbfa05375u)) * f + ffrom(0x40552f75u)) * f + (e + ffrom(0xc0121769u));
+  float l = log2 * ffrom(0x3ee8ba2eu);
+  l = l < -126.0f ? -126.0f : l; /* MathF.Max(l, -126) then MathF.Min(., 128); l is never NaN here */
+  l = l > 128.0f ? 128.0f : l;
+  int i = (int)l + ((int32_t)fbits(l) >> 31);
+  float fr = l - (float)i;
+  float p2 = ((fr * ffrom(0x3d9fcb52u) + ffrom(0x3e677e26u)) * fr + ffrom(0x3f322226u)) * fr + ffrom(0x3f7ffb19u);
+  float pw = ffrom(((uint32_t)i << 23) + fbits(p2)); /* int32 wrap-around sum */
+  float sgn = a == 0 ? 0.0f : ffrom(((uint32_t)bits & 0x80000000u) | 0x3f800000u);
+  return pw * (sgn * 255.0f);
+}
+
+/* StereoImage.YuvMatrix (StereoImage.cs:140-160): rows (v, u', t') for the sensor type and the AsShot neutral. */
+void lo_yuv_matrix(int sensor_type, const float neutral[3], float M[3][4]) {
+  static const uint32_t ar1335[4] = {0x3e5cb924u, 0x3edd5758u, 0x3eb44c16u, 0x40145fafu};
+  static const uint32_t other[4] = {0x3e9e39b4u, 0x3e95ca4bu, 0x3ecbfc22u, 0x40351eb8u};
+  const uint32_t* t = (sensor_type == 2 || sensor_type == 3) ? ar1335 : other;
+  float a = ffrom(t[0]), b = ffrom(t[1]), c = ffrom(t[2]);
+  float invx = 1.0f / neutral[0], invy = 1.0f / neutral[1], invz = 1.0f / neutral[2];
+  float s = c + a;
+  float u0 = (b * (-b) - s * c) * invx, u1 = ((a - c) * b) * invy, u2 = (s * a - b * (-b)) * invz;
+  float t0 = invx * (-b), t1 = invy * s, t2 = invz * (-b);
+  float v2 = c * c + (b * b + a * a);
+  float rs = ffrom(lo_rsqrt_bits(fbits(v2)));
+  float S = v2 * rs;
+  float kv = ((S * rs + (-3.0f)) * (S * (-0.5f)));
+  if (v2 == 0.0f) kv = 0.0f;
+  float u2n = u2 * u2 + (u1 * u1 + u0 * u0);
+  float rsu = ffrom(lo_rsqrt_bits(fbits(u2n)));
+  float ku = ((rsu * (-0.5f)) * kv) * ((u2n * rsu) * rsu + (-3.0f));
+  float t2n = t2 * t2 + (t1 * t1 + t0 * t0);
+  float rst = ffrom(lo_rsqrt_bits(fbits(t2n)));
+  float kt = ((rst * (-0.5f)) * kv) * ((t2n * rst) * rst + (-3.0f));
+  M[0][0] = a; M[0][1] = b; M[0][2] = c; M[0][3] = 0.0f;
+  M[1][0] = u0 * ku; M[1][1] = u1 * ku; M[1][2] = ku * u2; M[1][3] = 0.0f;
+  M[2][0] = t0 * kt; M[2][1] = t1 * kt; M[2][2] = kt * t2; M[2][3] = 0.0f;
+}
+
+void lo_convert_yuv(float* px, size_t npx, const float M[3][4]) {
+  for (size_t o = 0; o < npx * 4; o += 4) {
+    float x = px[o], y = px[o + 1], z = px[o + 2], ww = px[o + 3];
+    float my = (ww * M[0][3] + z * M[0][2]) + (y * M[0][1] + x * M[0][0]);
+    float mu = (ww * M[1][3] + z * M[1][2]) + (y * M[1][1] + x * M[1][0]);
+    float mv = (ww * M[2][3] + z * M[2][2]) + (y * M[2][1] + x * M[2][0]);
+    px[o] = lo_gamma_encode(my) + 0.0f;
+    px[o + 1] = lo_gamma_encode(mu) + 128.0f;
+    px[o + 2] = lo_gamma_encode(mv) + 128.0f;
+    px[o + 3] = 1.0f;
+  }
+}
+
+/* cvtps2dq (round to nearest even; NaN and out-of-range -> 0x80000000), then packssdw and packuswb. */
+static uint8_t store_u8(float v) {
+  int iv;
+  if (v != v || v >= 2147483648.0f || v < -2147483648.0f) iv = INT32_MIN;
+  else iv = (int)nearbyintf(v);
+  return (uint8_t)clampi(clampi(iv, -32768, 32767), 0, 255);
+}
+
+void lo_to_rgba8(const float* rgba, size_t n, uint8_t* out) {
+  for (size_t i = 0; i < n; i++) out[i] = store_u8(rgba[i]);
+}
+
+int lo_warp_rgba8(const uint8_t* src, int sw, int sh, int dw, int dh, const lo_aligned* ac, uint8_t* dst) {
+  if (sw < 1 || sh < 1) return LO_ERR_ARG; /* "empty source image!" */
+  if (dw < 0 || dh < 0 || !ac || !ac->lut) return LO_ERR_ARG;
+  float tbl[384];
+  lo_lanczos_table(tbl);
+  for (int y = 0; y < dh; y++)
+    for (int x = 0; x < dw; x++) {
+      int px, py;
+      if (warp_map(ac, x, y, &px, &py)) return LO_ERR_INDEX;
+      int i = px >> 6, fx = px & 63, j = py >> 6, fy = py & 63;
+      int interior = i >= 0 && i <= sw - 6 && j >= 0 && j <= sh - 6;
+      int ro[6], co[6];
+      for (int k = 0; k < 6; k++) {
+        ro[k] = interior ? j + k : clampi(j + k, 0, sh - 1);
+        co[k] = interior ? i + k : clampi(i + k, 0, sw - 1);
+      }
+      const float *ty = tbl + fy * 6, *tx = tbl + fx * 6;
+      for (int c = 0; c < 4; c++) {
+        float C[6];
+        for (int cc = 0; cc < 6; cc++) {
+          float acc = (float)src[((size_t)ro[0] * sw + co[cc]) * 4 + c] * ty[0];
+          for (int rr = 1; rr < 6; rr++) acc = acc + (float)src[((size_t)ro[rr] * sw + co[cc]) * 4 + c] * ty[rr];
+          C[cc] = acc;
+        }
+        float v = (C[5] * tx[5] + C[4] * tx[4]) + ((C[3] * tx[3] + C[2] * tx[2]) + (C[1] * tx[1] + C[0] * tx[0]));
+        dst[((size_t)y * dw + x) * 4 + c] = store_u8(v);
+      }
+    }
+  return LO_OK;
+}

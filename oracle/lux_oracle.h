@@ -140,6 +140,25 @@ long lo_traversal_trace(int w, int h, int tile, int xsw, int* ev_out, long max_e
 int lo_depth_cache_set(const float* src, int w, int h, int cw, int ch, float* out);
 int lo_depth_cache_fetch(const float* img, int iw, int ih, int x0, int y0, int x1, int y1, int dw, int dh, float* out);
 
+/* Stereo-image formation after the ISP (StereoImage.cs, ReferenceGuide.cs, WineCrt.cs). An aligned calibration is
+ * the warp's geometry: H row-major, the 4096-entry CRA lut, the centre (cx, cy) and scales (sx, sy). */
+typedef struct {
+  float H[9];
+  const float* lut;
+  float cx, cy, sx, sy;
+} lo_aligned;
+float lo_wine_sinf(float x);                                       /* WineCrt.Sinf, WineCrt.cs:77-99 */
+void lo_lanczos_table(float tbl[384]);                             /* StereoImage.LanczosTable, StereoImage.cs:212-237 */
+float lo_gamma_encode(float m);                                    /* StereoImage.GammaEncode, StereoImage.cs:162-178 */
+void lo_yuv_matrix(int sensor_type, const float neutral[3], float M[3][4]); /* StereoImage.YuvMatrix, StereoImage.cs:140-160 */
+/* StereoImage.Warp (StereoImage.cs:249-296, the vector form's per-lane order): dst (dw x dh x 4 floats, zero-filled
+ * where nothing is sampled) from src (sw x sh x 4 floats), src scaled by gain first (StereoImageBuilder.cs:62). */
+int lo_warp_f32(const float* src, int sw, int sh, float gain, int dw, int dh, const lo_aligned* ac, float* dst);
+void lo_convert_yuv(float* rgba, size_t npx, const float M[3][4]);  /* StereoImage.ConvertToYuv, StereoImage.cs:181-195 */
+void lo_to_rgba8(const float* rgba, size_t n, uint8_t* out);       /* StereoImage.ToRgba8, StereoImage.cs:198-209 */
+/* Rgba8Warp.Warp (ReferenceGuide.cs:108-156): the 8-bit warp of the reference guide. */
+int lo_warp_rgba8(const uint8_t* src, int sw, int sh, int dw, int dh, const lo_aligned* ac, uint8_t* dst);
+
 #ifdef __cplusplus
 }
 #endif

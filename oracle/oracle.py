@@ -81,8 +81,25 @@ def lib():
         l.lo_depth_cache_set.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         l.lo_depth_cache_fetch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        l.lo_wine_sinf.argtypes = [ctypes.c_float]
+        l.lo_wine_sinf.restype = ctypes.c_float
+        l.lo_gamma_encode.argtypes = [ctypes.c_float]
+        l.lo_gamma_encode.restype = ctypes.c_float
+        l.lo_lanczos_table.argtypes = [ctypes.c_void_p]
+        l.lo_yuv_matrix.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        l.lo_warp_f32.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(LoAligned), ctypes.c_void_p]
+        l.lo_convert_yuv.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        l.lo_to_rgba8.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        l.lo_warp_rgba8.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(LoAligned), ctypes.c_void_p]
         _lib = l
     return _lib
+
+
+class LoAligned(ctypes.Structure):
+    _fields_ = [("H", ctypes.c_float * 9), ("lut", ctypes.c_void_p), ("cx", ctypes.c_float), ("cy", ctypes.c_float),
+                ("sx", ctypes.c_float), ("sy", ctypes.c_float)]
 
 
 class OracleError(RuntimeError):
@@ -338,4 +355,87 @@ def dense_dump_bytes(layers, images, filtered, calibs, cv_max=2):
     for k, (im, fi) in enumerate(zip(images, filtered)):
         out[f"_dense_img{k}.img"] = rgba8_bytes(im)
         out[f"_dense_filt{k}.img"] = rgba8_bytes(fi)
+    return out
+
+
+# ---------------- stereo-image formation after the ISP (StereoImage.cs, ReferenceGuide.cs) ----------------
+
+def _aligned(ac):
+    a = LoAligned()
+    for i, v in enumerate(np.asarray(ac.H, np.float32).reshape(9)):
+        a.H[i] = float(v)
+    lut = np.ascontiguousarray(np.asarray(ac.lut, np.float32))
+    assert lut.size == 4096
+    a.lut = lut.ctypes.data
+    a.cx, a.cy, a.sx, a.sy = float(ac.cx), float(ac.cy), float(ac.sx), float(ac.sy)
+    return a, lut
+
+
+def wine_sinf(x):
+    return lib().lo_wine_sinf(float(np.float32(x)))
+
+
+def gamma_encode(m):
+    return np.float32(lib().lo_gamma_encode(float(np.float32(m))))
+
+
+def lanczos_table():
+    """StereoImage.LanczosTable (StereoImage.cs:212-237): (64, 6) float32."""
+    t = np.empty(384, np.float32)
+    lib().lo_lanczos_table(t.ctypes.data)
+    return t.reshape(64, 6)
+
+
+def yuv_matrix(sensor_type, neutral):
+    """StereoImage.YuvMatrix (StereoImage.cs:140-160): (3, 4) float32 rows (v, u', t')."""
+    n = np.ascontiguousarray(np.asarray(neutral, np.float32).reshape(3))
+    M = np.empty((3, 4), np.float32)
+    lib().lo_yuv_matrix(int(sensor_type), n.ctypes.data, M.ctypes.data)
+    return M
+
+
+def warp_f32(src, gain, dw, dh, ac):
+    """StereoImage.Warp (StereoImage.cs:249-296) of an (sh, sw, 4) float32 image scaled by gain first."""
+    s = np.ascontiguousarray(np.asarray(src, np.float32))
+    sh, sw = s.shape[:2]
+    a, keep = _aligned(ac)
+    out = np.empty((dh, dw, 4), np.float32)
+    rc = lib().lo_warp_f32(s.ctypes.data, sw, sh, float(np.float32(gain)), dw, dh, ctypes.byref(a), out.ctypes.data)
+    if rc:
+        raise OracleError(rc, "warp_f32")
+    return out
+
+
+def convert_yuv(rgba, M):
+    """StereoImage.ConvertToYuv (StereoImage.cs:181-195) on a copy."""
+    out = np.array(rgba, np.float32, copy=True, order="C")
+    m = np.ascontiguousarray(M, np.float32)
+    lib().lo_convert_yuv(out.ctypes.data, out.size // 4, m.ctypes.data)
+    return out
+
+
+def to_rgba8(rgba):
+    """StereoImage.ToRgba8 (StereoImage.cs:198-209)."""
+    r = np.ascontiguousarray(rgba, np.float32)
+    out = np.empty(r.shape, np.uint8)
+    lib().lo_to_rgba8(r.ctypes.data, r.size, out.ctypes.data)
+    return out
+
+
+def stereo_image(src, gain, dw, dh, ac, sensor_type, neutral):
+    """StereoImageBuilder.Create, colour path after the ISP (StereoImageBuilder.cs:61-69, 78): gain, warp, YUV, 8 bits.
+    Returns (rgba8, yuv float image)."""
+    yuv = convert_yuv(warp_f32(src, gain, dw, dh, ac), yuv_matrix(sensor_type, neutral))
+    return to_rgba8(yuv), yuv
+
+
+def warp_rgba8(src, dw, dh, ac):
+    """Rgba8Warp.Warp (ReferenceGuide.cs:108-156) of an (sh, sw, 4) uint8 image."""
+    s = np.ascontiguousarray(np.asarray(src, np.uint8))
+    sh, sw = s.shape[:2]
+    a, keep = _aligned(ac)
+    out = np.empty((dh, dw, 4), np.uint8)
+    rc = lib().lo_warp_rgba8(s.ctypes.data, sw, sh, dw, dh, ctypes.byref(a), out.ctypes.data)
+    if rc:
+        raise OracleError(rc, "warp_rgba8")
     return out
