@@ -15,6 +15,7 @@ Multi-GPU (torchrun): independent replicas, one solve per rank per step, no coll
 is the max over ranks.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -69,6 +70,9 @@ def args_():
                    help="throughput with 1, 4, 16 and 64 module captures in flight through the request server")
     p.add_argument("--cache", action="store_true",
                    help="the depth image cache: Set of the 4160x3120 full depth into the 5216x3912 cache, Fetch at the export levels")
+    p.add_argument("--stereo", action="store_true",
+                   help="stereo-image formation after the ISP: ten 2080x1560 module images warped, YUV'd and stored as 8 bits, "
+                        "and the 4160x3120 reference guide's 8-bit warp")
     p.add_argument("--cpu-rows", type=int, default=130, help="rows of the CPU sample strip")
     p.add_argument("--workload", default="pair13mp", choices=sorted(WORKLOADS),
                    help="pair13mp is the benchmark; the smaller pairs are for profiling captures")
@@ -546,8 +550,117 @@ def run_cache(a):
     ctx.close()
 
 
+def run_stereo(a):
+    """Stereo-image formation (StereoImageBuilder.Create after the ISP, StereoImage.cs) for a capture: ten module images,
+    each a 2080x1560 half-resolution ISP output (float RGBA) warped through its own aligned calibration into the
+    2080x1560 view, ConvertToYUV and the 8-bit store (the dense solve's inputs, left in HBM); plus the reference guide's
+    8-bit warp of the 4160x3120 ISP'd reference image (ReferenceGuide.cs). value = stereo-image pixels per second with
+    the ISP outputs in HBM (the 10 sources, 520 MB, exceed L2); e2e = the same from pinned host images to host 8-bit
+    images. Roofline (HBM): per output pixel the 16-byte source pixel read once and the 4-byte result written."""
+    import torch
+    from lux_b200 import api, synth
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    sw, sh, n_img = 2080, 1560, 10
+    srcs = [synth.isp_image(sw, sh, seed=k) for k in range(n_img)]
+    acs = [synth.aligned_calib(sw, sh, sw, sh, seed=k, angle_deg=0.3 * (k - 5)) for k in range(n_img)]
+    neutral = (0.5, 1.0, 0.6)
+    gains = [1.0] + [0.9 + 0.02 * k for k in range(1, n_img)]
+    guide_src = np.random.default_rng(3).integers(0, 256, (3120, 4160, 4), dtype=np.uint8)
+    guide_ac = synth.aligned_calib(4160, 3120, 4160, 3120, seed=99, angle_deg=0.0)
+    desc = (f"{n_img} stereo images {sw}x{sh} (float RGBA ISP output -> Lanczos-3 CRA warp -> YUV -> 8-bit) + the 4160x3120 "
+            "reference guide 8-bit warp")
+    pk = peaks()
+    if a.impl == "reference":
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        O.stereo_image(srcs[0], gains[0], sw, sh, acs[0], 2, neutral)
+        dt = time.perf_counter() - t0
+        v = sw * sh / dt / 1e6
+        print(json.dumps({"impl": "reference", "metric": "stereo images Mpix/s (output pixels per second), bit-exact",
+                          "value": v, "unit": "Mpix/s", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": dt * 1e3 * n_img,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": desc},
+                          "cpu_baseline": {"value": v, "unit": "Mpix/s", "cores": 1, "kind": "port",
+                                           "sample": "one 2080x1560 stereo image, oracle port (scalar C)"},
+                          "e2e": {"value": v, "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(lib.lux_sgm_stream(ctx.handle), device=torch.device("cuda", 0))
+    d_src = [torch.from_numpy(x).cuda() for x in srcs]
+    h_src = [torch.from_numpy(x).pin_memory() for x in srcs]
+    d_out = [torch.empty((sh, sw, 4), dtype=torch.uint8, device="cuda") for _ in range(n_img)]
+    h_out = [torch.empty((sh, sw, 4), dtype=torch.uint8).pin_memory() for _ in range(n_img)]
+    d_yuv = torch.empty((sh, sw, 4), dtype=torch.float32, device="cuda")
+    d_gsrc = torch.from_numpy(guide_src).cuda()
+    d_guide = torch.empty((3120, 4160, 4), dtype=torch.uint8, device="cuda")
+    cac = [ac.to_c() for ac in acs]
+    gac = guide_ac.to_c()
+    nb = np.ascontiguousarray(np.asarray(neutral, np.float32))
+    torch.cuda.synchronize()
+
+    def step(on_dev):
+        for k in range(n_img):
+            src = d_src[k] if on_dev else h_src[k]
+            out = d_out[k] if on_dev else h_out[k]
+            yuv = d_yuv.data_ptr() if k == 0 else None  # the reference camera keeps its YUV floats (RefYuv)
+            ctx.check(lib.lux_stereo_image(ctx.handle, src.data_ptr(), sw, sh, 1 if on_dev else 0, gains[k], ctypes.byref(cac[k][0]),
+                                           sw, sh, 2, nb.ctypes.data, out.data_ptr(), 1 if on_dev else 0, yuv, 1))
+
+    def guide():
+        img = api.L.Img(d_gsrc.data_ptr(), 4160, 3120, 4160, 1)
+        ctx.check(lib.lux_warp_rgba8(ctx.handle, ctypes.byref(img), ctypes.byref(gac[0]), 4160, 3120, d_guide.data_ptr(), 1))
+
+    def timed(fn, k):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        n0 = api.kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k, api.kernel_launches() - n0
+
+    with ClockSampler(0) as clk:
+        ms_v, launches = timed(lambda: step(True), a.steps)
+    ms_e, _ = timed(lambda: step(False), a.steps)
+    ms_g, _ = timed(guide, a.steps)
+    px = n_img * sw * sh
+    algo = px * (16 + 4) + sw * sh * 16  # sources read once, 8-bit results, the reference camera's YUV floats
+    achieved = algo / (ms_v / 1e3) / 1e9
+    out = {"metric": "stereo images Mpix/s (output pixels per second), bit-exact", "value": px / (ms_v / 1e3) / 1e6,
+           "unit": "Mpix/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_v, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (1/f texture ISP images, rotation + CRA calibrations)",
+           "config": {"workload": desc, "l2": f"ten sources of {sw * sh * 16 / 1e6:.0f} MB each, 520 MB per step (larger than L2)"},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
+                        "frac": achieved / pk.get("hbm_gbs"), "traffic": None, "kernel": "k_warp_f32<1> (ten launches)",
+                        "bytes_per_pixel": algo / px,
+                        "peak_source": "fallback" if pk.get("fallback") else "MEASURED_PEAKS.json hbm_gbs (measured)"},
+           "e2e": {"value": px / (ms_e / 1e3) / 1e6, "unit": "Mpix/s", "h2d_bytes_per_step": n_img * sw * sh * 16,
+                   "d2h_bytes_per_step": n_img * sw * sh * 4},
+           "guide": {"ms": ms_g, "mpix_per_s": 4160 * 3120 / (ms_g / 1e3) / 1e6},
+           "gpu_launches": int(launches), "clocks": clk.summary()}
+    if not a.no_cpu_baseline:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        O.stereo_image(srcs[0], gains[0], sw, sh, acs[0], 2, neutral)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": sw * sh / dt / 1e6, "unit": "Mpix/s", "cores": 1, "kind": "port",
+                               "sample": f"one {sw}x{sh} stereo image ({dt:.1f} s), oracle port (scalar C)"}
+    print(json.dumps(out))
+    ctx.close()
+
+
 def main():
     a = args_()
+    if a.stereo:
+        run_stereo(a)
+        return
     if a.cache:
         run_cache(a)
         return

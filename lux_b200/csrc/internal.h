@@ -72,6 +72,7 @@ struct WarpGeom {  // AlignedCalib (Lux.Engine/Pipeline/Geometry/AlignedCalibrat
   float h[9];
   float cx, cy, sx, sy;
   const float* lut;
+  float neg_zero;  // -0.0f, given at run time (the packed products of the warp kernels add it)
 };
 struct YuvRows {  // the rows (v, u', t') of StereoImage.YuvMatrix
   float m[3][4];

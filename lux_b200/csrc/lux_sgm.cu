@@ -854,6 +854,7 @@ int warp_geom(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, const lux_aligned_cali
   g->cy = ac->cy;
   g->sx = ac->sx;
   g->sy = ac->sy;
+  g->neg_zero = -0.0f;
   float* d = nullptr;
   int rc = alloc_t(ctx, tmp, 4096, &d);
   if (rc) return rc;

@@ -6,7 +6,9 @@
 // the correctly rounded reciprocal (__frcp_rn, equal to 1.0f / x); rsqrtss is the reference's table model.
 //
 // One thread per destination pixel, 16x16 blocks so the 6x6 source windows of a block overlap in L1. The tap table sits
-// in shared memory (its rows are indexed by each thread's own phase).
+// in shared memory (its rows are indexed by each thread's own phase). The four channels of a pixel go through the tap
+// sums as two pairs on Blackwell's packed f32x2 instructions: two correctly rounded single-precision operations per
+// instruction, the same bits as the scalar ones, and half the issue slots of the 6x6x4 taps.
 #include "../../include/lux_sgm.h"
 #include "common.cuh"
 #include "internal.h"
@@ -55,14 +57,50 @@ LUX_DEV bool warp_map(const WarpGeom& g, const uint32_t* rsq, int x, int y, int&
   return true;
 }
 
-LUX_DEV float4 f4mul(float4 v, float s) { return make_float4(__fmul_rn(v.x, s), __fmul_rn(v.y, s), __fmul_rn(v.z, s), __fmul_rn(v.w, s)); }
-LUX_DEV float4 f4add(float4 a, float4 b) { return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w)); }
+// Two floats in one 64-bit register pair, and the packed f32x2 product and sum (sm_100a), each element rounded to nearest
+// as __fmul_rn / __fadd_rn. The assembler fuses a packed multiply whose result feeds a packed add into one fused
+// multiply-add (a single rounding) even with the rounding mode spelled out, so the product is made as fma(a, b, z) with
+// z = -0.0 from a kernel argument: a·b + (-0) is a·b for every input, and a value the assembler cannot see is never
+// folded away, so nothing is fused.
+struct F2 {
+  unsigned long long v;
+};
+LUX_DEV F2 f2(float a, float b) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+  return r;
+}
+LUX_DEV float2 unf2(F2 x) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(x.v));
+  return r;
+}
+LUX_DEV F2 mul2(F2 a, F2 b, F2 z) {
+  F2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(z.v));
+  return d;
+}
+LUX_DEV F2 add2(F2 a, F2 b) {
+  F2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+struct Px {  // an RGBA pixel as the pairs (R, G) and (B, A)
+  F2 lo, hi;
+};
+LUX_DEV Px px_mul(Px p, F2 s, F2 z) { return Px{mul2(p.lo, s, z), mul2(p.hi, s, z)}; }
+LUX_DEV Px px_add(Px a, Px b) { return Px{add2(a.lo, b.lo), add2(a.hi, b.hi)}; }
+LUX_DEV Px px_of(float4 v) { return Px{f2(v.x, v.y), f2(v.z, v.w)}; }
+LUX_DEV float4 px_f4(Px p) {
+  const float2 a = unf2(p.lo), b = unf2(p.hi);
+  return make_float4(a.x, a.y, b.x, b.y);
+}
 
 // (c5·t5 + c4·t4) + ((c3·t3 + c2·t2) + (c1·t1 + c0·t0)): the pairing of both tap sums of the float warp and of the row
-// combination of the 8-bit warp.
-LUX_DEV float4 tap6(const float4 (&c)[6], const float* t) {
-  return f4add(f4add(f4mul(c[5], t[5]), f4mul(c[4], t[4])),
-               f4add(f4add(f4mul(c[3], t[3]), f4mul(c[2], t[2])), f4add(f4mul(c[1], t[1]), f4mul(c[0], t[0]))));
+// combination of the 8-bit warp. t holds each tap twice (the pair (t, t)).
+LUX_DEV Px tap6(const Px (&c)[6], const F2* t, F2 z) {
+  return px_add(px_add(px_mul(c[5], t[5], z), px_mul(c[4], t[4], z)),
+                px_add(px_add(px_mul(c[3], t[3], z), px_mul(c[2], t[2], z)), px_add(px_mul(c[1], t[1], z), px_mul(c[0], t[0], z))));
 }
 
 // StereoImage.GammaEncode (StereoImage.cs:162-178): 255·sign·|m|^(1/2.2) by the log2 and exp2 polynomials.
@@ -97,23 +135,28 @@ LUX_DEV uint32_t store_u8(float v) {
 }
 LUX_DEV uint32_t pack_u8(float4 v) { return store_u8(v.x) | store_u8(v.y) << 8 | store_u8(v.z) << 16 | store_u8(v.w) << 24; }
 
-LUX_DEV void load_taps(float* tab, const float* __restrict__ g) {
+// The tap table in shared memory with every tap doubled into a pair.
+LUX_DEV void load_taps(F2* tab, const float* __restrict__ g) {
   const int t = threadIdx.y * blockDim.x + threadIdx.x;
-  for (int i = t; i < 384; i += blockDim.x * blockDim.y) tab[i] = __ldg(g + i);
+  for (int i = t; i < 384; i += blockDim.x * blockDim.y) {
+    const float v = __ldg(g + i);
+    tab[i] = f2(v, v);
+  }
   __syncthreads();
 }
 
 // MODE 0: the warped float image (StereoImage.Warp). MODE 1: the stereo image (StereoImageBuilder.Create after the ISP):
 // ConvertToYUV and the 8-bit store of the warped pixel, and its YUV floats when yuv is not null.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_warp_f32(const float4* __restrict__ src, int sw, int sh, float gain, const WarpGeom g,
+__global__ void __launch_bounds__(256, 4) k_warp_f32(const float4* __restrict__ src, int sw, int sh, float gain, const WarpGeom g,
                                                   const float* __restrict__ taps, const uint32_t* __restrict__ rsq, int dw, int dh,
                                                   YuvRows m, float4* __restrict__ out_f, uint32_t* __restrict__ out_u8, int* err) {
-  __shared__ float tab[384];
+  __shared__ F2 tab[384];
   load_taps(tab, taps);
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= dw || y >= dh) return;
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  const F2 g2 = f2(gain, gain), z = f2(g.neg_zero, g.neg_zero);
   int px, py;
   if (!warp_map(g, rsq, x, y, px, py)) {
     atomicCAS(err, 0, LUX_ERR_INDEX);
@@ -121,23 +164,23 @@ __global__ void __launch_bounds__(256) k_warp_f32(const float4* __restrict__ src
     const int i = px >> 6, j = py >> 6;
     const bool interior = i >= 0 && i <= sw - 6 && j >= 0 && j <= sh - 6;
     if (interior || (j < sh && j + 6 > 0 && i < sw && i + 6 > 0)) {  // else the fill value 0
-      const float *ty = tab + (py & 63) * 6, *tx = tab + (px & 63) * 6;
+      const F2 *ty = tab + (py & 63) * 6, *tx = tab + (px & 63) * 6;
       const float4* row[6];
 #pragma unroll
       for (int k = 0; k < 6; k++) row[k] = src + (size_t)min(max(j + k, 0), sh - 1) * sw;
-      float4 c[6];
+      Px c[6];
 #pragma unroll
       for (int k = 0; k < 6; k++) {
         const int col = min(max(i + k, 0), sw - 1);
-        float4 p[6];
+        Px p[6];
 #pragma unroll
         for (int r = 0; r < 6; r++) {
-          p[r] = __ldg(row[r] + col);
-          if (gain != 1.0f) p[r] = f4mul(p[r], gain);  // the source scaled in place first (StereoImageBuilder.cs:62)
+          p[r] = px_of(__ldg(row[r] + col));
+          if (gain != 1.0f) p[r] = px_mul(p[r], g2, z);  // the source scaled in place first (StereoImageBuilder.cs:62)
         }
-        c[k] = tap6(p, ty);
+        c[k] = tap6(p, ty, z);
       }
-      acc = tap6(c, tx);
+      acc = px_f4(tap6(c, tx, z));
     }
   }
   const size_t o = (size_t)y * dw + x;
@@ -161,7 +204,7 @@ __global__ void __launch_bounds__(256) k_warp_f32(const float4* __restrict__ src
 __global__ void __launch_bounds__(256) k_warp_rgba8(const uchar4* __restrict__ src, int sw, int sh, int sstride, const WarpGeom g,
                                                     const float* __restrict__ taps, const uint32_t* __restrict__ rsq, int dw, int dh,
                                                     uint32_t* __restrict__ out, int* err) {
-  __shared__ float tab[384];
+  __shared__ F2 tab[384];
   load_taps(tab, taps);
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= dw || y >= dh) return;
@@ -171,25 +214,29 @@ __global__ void __launch_bounds__(256) k_warp_rgba8(const uchar4* __restrict__ s
     out[(size_t)y * dw + x] = 0;
     return;
   }
+  // a byte b as a float, exactly: the bits 0x4b0000bb are 2^23 + b, less 2^23 (one byte permute and half a packed add)
+  const F2 bias = f2(-8388608.0f, -8388608.0f), z = f2(g.neg_zero, g.neg_zero);
   const int i = px >> 6, j = py >> 6;
-  const float *ty = tab + (py & 63) * 6, *tx = tab + (px & 63) * 6;
-  const uchar4* row[6];
+  const F2 *ty = tab + (py & 63) * 6, *tx = tab + (px & 63) * 6;
+  const uint32_t* row[6];
 #pragma unroll
-  for (int k = 0; k < 6; k++) row[k] = src + (size_t)min(max(j + k, 0), sh - 1) * sstride;
-  float4 c[6];
+  for (int k = 0; k < 6; k++) row[k] = reinterpret_cast<const uint32_t*>(src) + (size_t)min(max(j + k, 0), sh - 1) * sstride;
+  Px c[6];
 #pragma unroll
   for (int k = 0; k < 6; k++) {
     const int col = min(max(i + k, 0), sw - 1);
-    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    Px s;
 #pragma unroll
     for (int r = 0; r < 6; r++) {
-      const uchar4 b = __ldg(row[r] + col);
-      const float4 p = f4mul(make_float4((float)b.x, (float)b.y, (float)b.z, (float)b.w), ty[r]);
-      s = r == 0 ? p : f4add(s, p);
+      const uint32_t w = __ldg(row[r] + col);
+      const Px v{add2(f2(__uint_as_float(__byte_perm(w, 0x4b000000u, 0x7540)), __uint_as_float(__byte_perm(w, 0x4b000000u, 0x7541))), bias),
+                 add2(f2(__uint_as_float(__byte_perm(w, 0x4b000000u, 0x7542)), __uint_as_float(__byte_perm(w, 0x4b000000u, 0x7543))), bias)};
+      const Px p = px_mul(v, ty[r], z);
+      s = r == 0 ? p : px_add(s, p);
     }
     c[k] = s;
   }
-  out[(size_t)y * dw + x] = pack_u8(tap6(c, tx));
+  out[(size_t)y * dw + x] = pack_u8(px_f4(tap6(c, tx, z)));
 }
 
 }  // namespace
