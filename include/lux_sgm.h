@@ -128,7 +128,8 @@ typedef struct {
   float gpu_ms_sgm;      /* device time of the two aggregation passes */
   float gpu_ms_wta;      /* device time of the winner-take-all */
   int32_t sgm_kernel;    /* 0 = the exact traversal replay, 1 = fast, four paths fused, 2 = fast, path groups as chains */
-  int32_t cost_kernel;   /* 0 = per-pixel warps (any layer), 1 = per-row warps (uniform layer), 2 = per-row warps of an axis-aligned pair */
+  int32_t cost_kernel;   /* 0 = per-pixel warps (any layer), 1 = per-row warps (uniform layer), 2 = per-row warps of an axis-aligned
+                            pair, 3 = the same with block columns shared between neighbouring pixels (grey, scale 1) */
 } lux_layer_info;
 int lux_layer_get_info(const lux_layer* layer, lux_layer_info* info);
 

@@ -57,6 +57,18 @@ __global__ void k_phase_grey(const uint8_t* __restrict__ img, int iw, int ih, ui
     out[((size_t)h * ih + y) * iw + x] = make_uint2(p0 | (p2 << 16), p1);
   }
 }
+// Grey, vertical triples (the shared-column axis kernel): out[h][y][x] = the Y bytes of phase h at rows y, y+1, y+2 of
+// column x as u16 pairs: {y | y+2 << 16, y+1}.
+__global__ void k_phase_grey_v(const uint8_t* __restrict__ img, int iw, int ih, uint2* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= iw) return;
+#pragma unroll
+  for (int h = 0; h < 4; h++) {
+    const uint32_t p0 = phase_byte(img, iw, ih, x, y, h, 0), p1 = phase_byte(img, iw, ih, x, min(y + 1, ih - 1), h, 0),
+                   p2 = phase_byte(img, iw, ih, x, min(y + 2, ih - 1), h, 0);
+    out[((size_t)h * ih + y) * iw + x] = make_uint2(p0 | (p2 << 16), p1);
+  }
+}
 // Colour: out[h][y][x] = the RGBA word of phase h.
 __global__ void k_phase_colour(const uint8_t* __restrict__ img, int iw, int ih, uint32_t* __restrict__ out) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
@@ -424,6 +436,137 @@ __global__ void __launch_bounds__(256) k_cost_axis(const CostArgs a, const Layer
   }
 }
 
+// One block column of the grey cost: the three capped differences of a target column triple t (vertical layout) against
+// a reference column triple, in u16x2 lanes each offset by 256 (as grey_cost); three columns sum to S0 + 12·256.
+struct ColRef {
+  uint32_t ea, eb, oa, ob;
+};
+LUX_DEV ColRef col_ref(uint32_t even, uint32_t odd) { return ColRef{0x01000100u - even, 0x01000100u + even, 0x01000100u - odd, 0x01000100u + odd}; }
+LUX_DEV uint32_t col_cost(uint2 t, const ColRef& c) {
+  return vmin2c(vmax2c(t.x + c.ea, c.eb - t.x), 0x01020102u) + vmin2c(vmax2c(t.y + c.oa, c.ob - t.y), 0x01000102u);
+}
+
+// Uniform layers of one axis-aligned grey pair at scale 1 (the plain stereo pair): the 3x3 blocks of neighbouring
+// pixels overlap, and so do their target blocks wherever the target column advances by one whole pixel with the same
+// half-pixel phase from one pixel to the next. A warp covers 30 pixels of a row (lanes 2..31; lanes 0 and 1 are the two
+// pixels to the left): per plane every lane computes only the right column of its block (reference column x + 1,
+// clamped as the reference clamps its block, against target column ix + 1) and takes the middle and left columns from
+// lanes x - 1 and x - 2 when their target positions are exactly 2 and 4 half-pixels to the left. Where they are not, the
+// lane computes the two columns itself. The terms, and so the sums, are the reference's (:222-246); only who computes a
+// term changes. Normalise (:378-379) of one camera's cost is a function of S0 (0..18), a 19-entry table.
+__global__ void __launch_bounds__(256) k_cost_axis_v(const CostArgs a, const LayerGeom g, const float4* __restrict__ zt,
+                                                     uint8_t* __restrict__ raw, int* err) {
+  __shared__ uint8_t s_norm[32];
+  if (threadIdx.x < 32)
+    s_norm[threadIdx.x] =
+        (uint8_t)(f2i(__fmul_rn((float)(((uint32_t)(min((int)threadIdx.x, 18) * 12240 + 16) >> 5) & 0xffffu), a.norm)) & 0xff);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int tiles_x = (g.W + 29) / 30;
+  const int ntiles = tiles_x * g.H;
+  const int n = g.n_planes;
+  const uint8_t* ref8 = a.ref;
+  const float* Wm = a.warp[0];
+  const float w0 = Wm[0], w1 = Wm[1], w2 = Wm[2], w4 = Wm[4], w5 = Wm[5], w6 = Wm[6];
+  const int iw = a.ow[0], ih = a.oh[0], x1 = iw - 2, y1 = ih - 2;
+  const uint2* q = reinterpret_cast<const uint2*>(a.phase[0]);
+  const int plane_stride = ih * iw;
+  constexpr int kNoRow = INT_MIN;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += (gridDim.x * blockDim.x) >> 5) {
+    const int y = t / tiles_x, x = (t - y * tiles_x) * 30 + lane - 2;
+    const bool in_row = lane >= 2 && x < g.W;
+    const size_t pi = (size_t)y * g.W + min(max(x, 0), g.W - 1);
+    uint8_t* out = raw + pi * n;
+    const bool skipped = in_row && g.skip[pi] != 0;
+    const bool live = in_row && !skipped;
+    if (skipped)
+      for (int d = 0; d < n; d += 8) *reinterpret_cast<uint2*>(out + d) = make_uint2(0u, 0u);
+    if (__ballot_sync(0xffffffffu, live) == 0) continue;
+    // reference column triples (rows y-1, y, y+1 clamped): this lane's right column, and the left and middle ones of
+    // lanes x - 2 and x - 1 (their right columns)
+    const int xImg = min(x, a.rw - 1);  // scale 1: the reference grid is the layer grid
+    ColRef cr;
+    {
+      const int c = min(max(x + 1, 0), a.rw - 1);
+      const int ya = max(y - 1, 0), yb = min(y + 1, a.rh - 1);
+      const uint32_t r0 = ref8[((size_t)ya * a.rw + c) * 4], r1 = ref8[((size_t)y * a.rw + c) * 4], r2 = ref8[((size_t)yb * a.rw + c) * 4];
+      cr = col_ref(r0 | (r2 << 16), r1);
+    }
+    const ColRef cm{__shfl_up_sync(0xffffffffu, cr.ea, 1), __shfl_up_sync(0xffffffffu, cr.eb, 1), __shfl_up_sync(0xffffffffu, cr.oa, 1),
+                    __shfl_up_sync(0xffffffffu, cr.ob, 1)};
+    const ColRef cl{__shfl_up_sync(0xffffffffu, cr.ea, 2), __shfl_up_sync(0xffffffffu, cr.eb, 2), __shfl_up_sync(0xffffffffu, cr.oa, 2),
+                    __shfl_up_sync(0xffffffffu, cr.ob, 2)};
+    const float xf = (float)xImg, yf = (float)y;
+    uint32_t last = 0, pk0 = 0, pk1 = 0;
+    auto put = [&](int d, uint32_t b) {  // eight planes per store
+      const int sh = (d & 3) * 8;
+      if (d & 4) pk1 |= b << sh;
+      else pk0 |= b << sh;
+      if ((d & 7) == 7) {
+        if (live) *reinterpret_cast<uint2*>(out + (d - 7)) = make_uint2(pk0, pk1);
+        pk0 = pk1 = 0;
+      }
+    };
+    auto block = [&](size_t base) {  // the whole block from the target columns base, base + 1, base + 2
+      const uint32_t s = col_cost(__ldg(q + base), cl) + col_cost(__ldg(q + base + 1), cm) + col_cost(__ldg(q + base + 2), cr);
+      return (uint32_t)s_norm[(s & 0xffffu) + (s >> 16) - 12 * 256];
+    };
+    {  // plane 0: the general projection, clamped into the rect (:263-269)
+      const float z = __ldg(g.planes);
+      const float xz = __fmul_rn(xf, z), yz = __fmul_rn(yf, z);
+      const float4 zk = __ldg(zt);
+      const float px = __fadd_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0)), __fmul_rn(yz, w4));
+      const float py = __fadd_rn(__fadd_rn(zk.y, __fmul_rn(xz, w1)), __fmul_rn(yz, w5));
+      const float pz = __fadd_rn(__fadd_rn(zk.z, __fmul_rn(xz, w2)), __fmul_rn(yz, w6));
+      const float inv = __frcp_rn(pz);
+      const float fx = cs_minf(cs_maxf(__fadd_rn(__fmul_rn(px, inv), 0.25f), 1.0f), (float)(x1 - 1));
+      const float fy = cs_minf(cs_maxf(__fadd_rn(__fmul_rn(py, inv), 0.25f), 1.0f), (float)(y1 - 1));
+      const int tx = f2i(__fadd_rn(fx, fx)), ty = f2i(__fadd_rn(fy, fy));
+      const int ix = tx >> 1, iy = ty >> 1;
+      if (ix >= 1 && ix < x1 && iy >= 1 && iy < y1) {
+        if (live) last = block(((size_t)(((ty & 1) << 1) | (tx & 1)) * ih + (iy - 1)) * iw + (ix - 1));
+      } else if (live) {  // the scalar fallback of the reference would read out of the image
+        atomicCAS(err, 0, 7);
+      }
+      put(0, last);
+    }
+    for (int d0 = 0; d0 < n; d0 += 32) {
+      // lane j: the offset of row iy - 1 of phase 2·hy of plane d0 + j (or kNoRow when the row leaves the rect)
+      int rowoff;
+      {
+        const int dj = min(d0 + lane, n - 1);
+        const float4 zj = __ldg(zt + dj);
+        const float yz = __fmul_rn(yf, __ldg(g.planes + dj));
+        const float fy = __fadd_rn(__fmul_rn(__fadd_rn(zj.y, __fmul_rn(yz, w5)), zj.w), 0.25f);
+        const int ty = f2i(__fadd_rn(fy, fy)), iy = ty >> 1;
+        rowoff = (iy >= 1 && iy < y1) ? (((ty & 1) << 1) * ih + iy - 1) * iw : kNoRow;
+      }
+      const int jend = min(32, n - d0);
+      for (int j = (d0 == 0 ? 1 : 0); j < jend; j++) {
+        const int d = d0 + j;
+        const int ro_d = __shfl_sync(0xffffffffu, rowoff, j);
+        if (ro_d != kNoRow) {  // the same for the whole warp
+          const float4 zk = __ldg(zt + d);
+          const float xz = __fmul_rn(xf, __ldg(g.planes + d));
+          const float fx = __fadd_rn(__fmul_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0)), zk.w), 0.25f);
+          const int tx = f2i(__fadd_rn(fx, fx)), ix = tx >> 1;
+          const int base = ro_d + (tx & 1) * plane_stride;
+          const uint32_t c = col_cost(__ldg(q + base + min(max(ix + 1, 0), iw - 1)), cr);
+          const uint32_t c1 = __shfl_up_sync(0xffffffffu, c, 1), c2 = __shfl_up_sync(0xffffffffu, c, 2);
+          const int t1 = __shfl_up_sync(0xffffffffu, tx, 1), t2 = __shfl_up_sync(0xffffffffu, tx, 2);
+          if (live && ix >= 1 && ix < x1) {
+            uint32_t s;
+            if (t1 == tx - 2 && t2 == tx - 4) s = c + c1 + c2;
+            else s = col_cost(__ldg(q + base + ix - 1), cl) + col_cost(__ldg(q + base + ix), cm) + c;
+            last = s_norm[(s & 0xffffu) + (s >> 16) - 12 * 256];
+          }
+        }
+        put(d, last);
+      }
+    }
+  }
+}
+
 bool cost_all_grey(const CostArgs& a) {
   for (int k = 0; k < a.n_others; k++)
     if (!(a.wq[k][0] == 12240 && a.wq[k][1] == 0 && a.wq[k][2] == 0 && a.wq[k][3] == 0)) return false;
@@ -435,7 +578,8 @@ void launch_phases(const CostArgs& a, cudaStream_t s) {
   for (int k = 0; k < a.n_others; k++) {
     dim3 grid((a.ow[k] + 127) / 128, a.oh[k]);
     uint32_t* out = const_cast<uint32_t*>(a.phase[k]);
-    if (grey) k_phase_grey<<<grid, 128, 0, s>>>(a.other[k], a.ow[k], a.oh[k], reinterpret_cast<uint2*>(out));
+    if (a.vcols) k_phase_grey_v<<<grid, 128, 0, s>>>(a.other[k], a.ow[k], a.oh[k], reinterpret_cast<uint2*>(out));
+    else if (grey) k_phase_grey<<<grid, 128, 0, s>>>(a.other[k], a.ow[k], a.oh[k], reinterpret_cast<uint2*>(out));
     else k_phase_colour<<<grid, 128, 0, s>>>(a.other[k], a.ow[k], a.oh[k], out);
     count_launches(1);
   }
@@ -461,7 +605,13 @@ int launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t
     const int tiles = ((g.W + 31) / 32) * g.H;
     int blocks = (tiles + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    if (a.axis) {
+    if (a.vcols) {
+      const int vtiles = ((g.W + 29) / 30) * g.H;
+      int vb = (vtiles + 7) / 8;
+      if (vb > 148 * 16) vb = 148 * 16;
+      k_cost_axis_v<<<vb, 256, 0, s>>>(a, g, zt, raw, err);
+      kind = 3;
+    } else if (a.axis) {
       if (grey) k_cost_axis<true><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);
       else k_cost_axis<false><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);
       kind = 2;

@@ -38,6 +38,7 @@ struct CostArgs {
   float norm;                       // 0x3d17b426 / nOthers
   int scale;
   int axis;                         // one other camera, axis-aligned flow matrix: zt.w holds 1/pz per plane
+  int vcols;                        // axis, grey, scale 1: phase images as vertical triples, blocks from shared columns
 };
 
 // prep.cu

@@ -64,7 +64,7 @@ def test_uniform_layer_bit_exact(ctx, oracle, w, h, d, tile, kernel):
                                 ctx=ctx, **_sgm_args(kernel))
     try:
         assert gl.sgm_kernel == SGM_FORMS[kernel]
-        assert gl.cost_kernel == (2 if d % 8 == 0 else 0)  # a rectified pair: the axis-aligned cost kernel
+        assert gl.cost_kernel == (3 if d % 8 == 0 else 0)  # a rectified grey pair: the shared-column axis cost kernel
         _compare_layer(gl, ol, f"{w}x{h} D{d} T{tile} {kernel}")
     finally:
         gl.close()
@@ -98,6 +98,44 @@ def test_multicamera_colour_layer_bit_exact(ctx, oracle):
     try:
         assert gl.cost_kernel == 1
         _compare_layer(gl, ol, "3cam")
+    finally:
+        gl.close()
+
+
+@pytest.mark.parametrize("focal,skip,w", [(1.0, 0, 157), (1.0, 2, 211), (1.3, 0, 130), (0.77, 2, 97), (1.0, 0, 30)])
+def test_axis_pair_shared_columns(ctx, oracle, focal, skip, w):
+    """The shared-column grey cost kernel: widths that are and are not multiples of its 30-pixel warps, skipped pixels,
+    and a second camera with another focal length, where neighbouring target positions step by more (1.3) or less
+    (0.77) than one pixel so that lanes compute their own block columns."""
+    from lux_b200 import api, synth
+    h, d = 61, 48
+    wl = synth.rectified_pair(w, h, d, seed=w + 3, tile=8)
+    f2 = np.float32(1000.0 * focal)
+    cal = list(wl.calibs)
+    cal[1] = api.CalibData(np.array([f2, 0, w / 2.0 + 1.5, 0, f2, h / 2.0 - 0.5, 0, 0, 1], np.float32),
+                           np.array([-100.0, 0, 0], np.float32), np.eye(3, dtype=np.float32).reshape(9))
+    p = api.StereoParams(scale=1, tile=8, skip_mode=skip, plane_density=1.0)
+    filt = _filtered(oracle, wl.images)
+    ol = oracle.layer(filt, wl.gray, cal, wl.near, wl.far, p, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, wl.gray, cal, wl.near, wl.far, p, keep_pass1=True, keep_agg=True, ctx=ctx)
+    try:
+        assert gl.cost_kernel == (3 if gl.n_planes % 8 == 0 else 0)
+        _compare_layer(gl, ol, f"shared columns f{focal} skip{skip} w{w}")
+    finally:
+        gl.close()
+
+
+def test_axis_pair_scale2_grey(ctx, oracle):
+    """A grey axis-aligned pair at scale 2 (blocks of neighbouring pixels do not overlap): the per-row axis kernel."""
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(180, 120, 64, seed=8, tile=8)
+    p = api.StereoParams(scale=2, tile=8, skip_mode=0, plane_density=1.0)
+    filt = _filtered(oracle, wl.images)
+    ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, p, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, p, keep_pass1=True, keep_agg=True, ctx=ctx)
+    try:
+        assert gl.cost_kernel == (2 if gl.n_planes % 8 == 0 else 0)
+        _compare_layer(gl, ol, "axis grey scale 2")
     finally:
         gl.close()
 
