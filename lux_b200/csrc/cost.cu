@@ -497,16 +497,7 @@ __global__ void __launch_bounds__(256) k_cost_axis_v(const CostArgs a, const Lay
     const ColRef cl{__shfl_up_sync(0xffffffffu, cr.ea, 2), __shfl_up_sync(0xffffffffu, cr.eb, 2), __shfl_up_sync(0xffffffffu, cr.oa, 2),
                     __shfl_up_sync(0xffffffffu, cr.ob, 2)};
     const float xf = (float)xImg, yf = (float)y;
-    uint32_t last = 0, pk0 = 0, pk1 = 0;
-    auto put = [&](int d, uint32_t b) {  // eight planes per store
-      const int sh = (d & 3) * 8;
-      if (d & 4) pk1 |= b << sh;
-      else pk0 |= b << sh;
-      if ((d & 7) == 7) {
-        if (live) *reinterpret_cast<uint2*>(out + (d - 7)) = make_uint2(pk0, pk1);
-        pk0 = pk1 = 0;
-      }
-    };
+    uint32_t last = 0;  // the normalised cost of the last plane computed (:273-274)
     auto block = [&](size_t base) {  // the whole block from the target columns base, base + 1, base + 2
       const uint32_t s = col_cost(__ldg(q + base), cl) + col_cost(__ldg(q + base + 1), cm) + col_cost(__ldg(q + base + 2), cr);
       return (uint32_t)s_norm[(s & 0xffffu) + (s >> 16) - 12 * 256];
@@ -528,24 +519,24 @@ __global__ void __launch_bounds__(256) k_cost_axis_v(const CostArgs a, const Lay
       } else if (live) {  // the scalar fallback of the reference would read out of the image
         atomicCAS(err, 0, 7);
       }
-      put(0, last);
     }
-    for (int d0 = 0; d0 < n; d0 += 32) {
-      // lane j: the offset of row iy - 1 of phase 2·hy of plane d0 + j (or kNoRow when the row leaves the rect)
-      int rowoff;
-      {
-        const int dj = min(d0 + lane, n - 1);
+    // planes in groups of eight (one 8-byte store each); the row offset of plane d comes from lane d % 32
+    int rowoff = 0;
+    for (int d8 = 0; d8 < n; d8 += 8) {
+      if ((d8 & 31) == 0) {  // lane j: the offset of row iy - 1 of phase 2·hy of plane d8 + j (kNoRow: off the rect)
+        const int dj = min(d8 + lane, n - 1);
         const float4 zj = __ldg(zt + dj);
         const float yz = __fmul_rn(yf, __ldg(g.planes + dj));
         const float fy = __fadd_rn(__fmul_rn(__fadd_rn(zj.y, __fmul_rn(yz, w5)), zj.w), 0.25f);
         const int ty = f2i(__fadd_rn(fy, fy)), iy = ty >> 1;
         rowoff = (iy >= 1 && iy < y1) ? (((ty & 1) << 1) * ih + iy - 1) * iw : kNoRow;
       }
-      const int jend = min(32, n - d0);
-      for (int j = (d0 == 0 ? 1 : 0); j < jend; j++) {
-        const int d = d0 + j;
-        const int ro_d = __shfl_sync(0xffffffffu, rowoff, j);
-        if (ro_d != kNoRow) {  // the same for the whole warp
+      uint32_t pk0 = 0, pk1 = 0;
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const int d = d8 + k;
+        const int ro_d = __shfl_sync(0xffffffffu, rowoff, d & 31);
+        if (d != 0 && ro_d != kNoRow) {  // plane 0 was done above; ro_d is the same for the whole warp
           const float4 zk = __ldg(zt + d);
           const float xz = __fmul_rn(xf, __ldg(g.planes + d));
           const float fx = __fadd_rn(__fmul_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0)), zk.w), 0.25f);
@@ -553,16 +544,23 @@ __global__ void __launch_bounds__(256) k_cost_axis_v(const CostArgs a, const Lay
           const int base = ro_d + (tx & 1) * plane_stride;
           const uint32_t c = col_cost(__ldg(q + base + min(max(ix + 1, 0), iw - 1)), cr);
           const uint32_t c1 = __shfl_up_sync(0xffffffffu, c, 1), c2 = __shfl_up_sync(0xffffffffu, c, 2);
-          const int t1 = __shfl_up_sync(0xffffffffu, tx, 1), t2 = __shfl_up_sync(0xffffffffu, tx, 2);
+          // lanes 1..31 whose target is one pixel right of the target of the lane to their left; where all are, the
+          // lane two to the left is two pixels left too
+          const int t1 = __shfl_up_sync(0xffffffffu, tx, 1);
+          const bool all = __all_sync(0xffffffffu, lane == 0 || t1 == tx - 2);
+          int t2 = tx - 4;
+          if (!all) t2 = __shfl_up_sync(0xffffffffu, tx, 2);  // the same branch for the whole warp
           if (live && ix >= 1 && ix < x1) {
-            uint32_t s;
-            if (t1 == tx - 2 && t2 == tx - 4) s = c + c1 + c2;
-            else s = col_cost(__ldg(q + base + ix - 1), cl) + col_cost(__ldg(q + base + ix), cm) + c;
-            last = s_norm[(s & 0xffffu) + (s >> 16) - 12 * 256];
+            uint32_t sum;
+            if (t1 == tx - 2 && t2 == tx - 4) sum = c + c1 + c2;
+            else sum = col_cost(__ldg(q + base + ix - 1), cl) + col_cost(__ldg(q + base + ix), cm) + c;
+            last = s_norm[(sum & 0xffffu) + (sum >> 16) - 12 * 256];
           }
         }
-        put(d, last);
+        if (k < 4) pk0 |= last << (8 * k);
+        else pk1 |= last << (8 * (k - 4));
       }
+      if (live) *reinterpret_cast<uint2*>(out + d8) = make_uint2(pk0, pk1);
     }
   }
 }
