@@ -202,6 +202,16 @@ int lux_warp_f32(lux_sgm_ctx* ctx, const float* src, int32_t sw, int32_t sh, int
 int lux_stereo_image(lux_sgm_ctx* ctx, const float* src, int32_t sw, int32_t sh, int32_t src_on_device, float gain,
                      const lux_aligned_calib* ac, int32_t dw, int32_t dh, int32_t sensor_type, const float* neutral,
                      uint8_t* out_rgba8, int32_t out_on_device, float* out_yuv, int32_t yuv_on_device);
+/* StereoImageBuilder.Create for a non-reference module with the reference crop (StereoImageBuilder.cs:61-65, 71-77): the
+ * stereo image as lux_stereo_image makes it, colour-matched to the crop of the reference camera's YUV image (ref_yuv,
+ * dw x dh RGBA floats: lux_stereo_image's out_yuv of the reference) by StereoColorTransfer.Transfer
+ * (StereoColorTransfer.cs:128-138): the crop rect from ref_view (calib2) and view (calibA), the statistics of both images,
+ * the 4x4 transfer (written to out_F when not NULL, row-major), its application and the 8-bit store. The statistics run on
+ * the host (a serial recurrence over the pixels), the rest on the GPU. "Empty reference yuv." is LUX_ERR_ARG. */
+int lux_stereo_image_transfer(lux_sgm_ctx* ctx, const float* src, int32_t sw, int32_t sh, int32_t src_on_device, float gain,
+                              const lux_aligned_calib* ac, int32_t dw, int32_t dh, int32_t sensor_type, const float* neutral,
+                              const float* ref_yuv, int32_t ref_on_device, const lux_calib* ref_view, const lux_calib* view,
+                              uint8_t* out_rgba8, int32_t out_on_device, float* out_F);
 /* Rgba8Warp.Warp (ReferenceGuide.cs:108-156): the 8-bit warp that makes the upsample's guide from the ISP'd reference
  * image (every tap clamped to the image). "empty source image!" is LUX_ERR_ARG. */
 int lux_warp_rgba8(lux_sgm_ctx* ctx, const lux_img_rgba8* src, const lux_aligned_calib* ac, int32_t dw, int32_t dh, uint8_t* dst,

@@ -106,6 +106,10 @@ SIGNATURES = [
     ("lux_stereo_image", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_float, ctypes.POINTER(AlignedCalib), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]),
+    ("lux_stereo_image_transfer", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                 ctypes.c_float, ctypes.POINTER(AlignedCalib), ctypes.c_int32, ctypes.c_int32,
+                                                 ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Calib),
+                                                 ctypes.POINTER(Calib), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     ("lux_warp_rgba8", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Img), ctypes.POINTER(AlignedCalib), ctypes.c_int32,
                                       ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]),
     ("lux_lanczos_table", None, [ctypes.c_void_p]),

@@ -579,6 +579,28 @@ class StereoImage:
         return out, yuv
 
 
+    @staticmethod
+    def create_transfer(src, dw, dh, ac: AlignedCalib, sensor_type, neutral, ref_yuv, ref_view: CalibData, view: CalibData,
+                        gain=1.0, ctx: Optional[Context] = None):
+        """StereoImageBuilder.Create for a non-reference module with the reference crop (StereoImageBuilder.cs:71-77): the
+        (dh, dw, 4) uint8 stereo image colour-matched to the crop of ref_yuv (the reference's YUV floats, from create(...,
+        keep_yuv=True)), and the (4, 4) float32 transfer. ref_view / view: the reference's and this module's views."""
+        ctx = ctx or default_context()
+        ptr, on_dev, keep, (sh, sw) = _image_f32(src)
+        rptr, ron, rkeep, _ = _image_f32(ref_yuv)
+        out = _empty_like_kind(src, (dh, dw, 4), np.uint8)
+        optr, oon = _ptr(out)
+        n = np.ascontiguousarray(np.asarray(neutral, np.float32).reshape(3))
+        F = np.empty(16, np.float32)
+        c, lut = ac.to_c()
+        rv, vv = ref_view.to_c(), view.to_c()
+        _torch_ready(src, ref_yuv, out)
+        ctx.check(ctx.lib.lux_stereo_image_transfer(ctx.handle, ptr, sw, sh, on_dev, float(gain), ctypes.byref(c), dw, dh,
+                                                    int(sensor_type), n.ctypes.data, rptr, ron, ctypes.byref(rv), ctypes.byref(vv),
+                                                    optr, oon, F.ctypes.data))
+        return out, F.reshape(4, 4)
+
+
 class Rgba8Warp:
     @staticmethod
     def warp(src, dw, dh, ac: AlignedCalib, ctx: Optional[Context] = None):

@@ -141,6 +141,7 @@ uint32_t host_rsqrt_bits(uint32_t b) {
 float host_rcp(float x) { return float_of(host_rcp_bits(bits_of(x))); }
 const uint32_t* host_rcp_table() { return lux_rcp_table; }
 const uint32_t* host_rsqrt_table(bool e128) { return e128 ? lux_rsqrt_table_e128 : lux_rsqrt_table_e127; }
+void host_mat4_mul(const double* a, const double* b, double* o) { mul4(a, b, o); }
 
 namespace {
 

@@ -28,5 +28,18 @@ const uint32_t* host_rsqrt_table(bool e128);
 void host_lanczos_table(float out[384]);
 // StereoImage.YuvMatrix (StereoImage.cs:140-160): the rows (v, u', t') of ConvertToYUV for a sensor type and neutral.
 void host_yuv_matrix(int sensor_type, const float neutral[3], float out[12]);
+// Mat4D.Mul (ViewTransform.cs:88-94): row-major double 4x4 product.
+void host_mat4_mul(const double* a, const double* b, double* o);
+
+// StereoColorTransfer (color_transfer.cpp): the statistics of one YUVA image, the crop rect and the 4x4 transfer.
+struct ColourStats {
+  float mean[4], D[4], O[4], N;
+};
+// CropRect (StereoColorTransfer.cs:32-51) of the rw x rh reference rect, unclamped {x0, y0, x1, y1}.
+void host_crop_rect(const lux_calib& ref_view, const lux_calib& view, int rw, int rh, int out[4]);
+// Accumulate (:56-75) over w x h pixels of rows `stride` pixels apart, starting at pixel `offset`.
+ColourStats host_colour_stats(const float* yuva, int w, int h, int stride, size_t offset);
+// Solve (:94-108): the row-major float transfer (the identity below 100 gated pixels in either image).
+void host_colour_solve(const ColourStats& work, const ColourStats& ref, float F[16]);
 
 }  // namespace lux

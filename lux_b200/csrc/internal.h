@@ -85,6 +85,11 @@ void launch_warp_f32(const float* src, int sw, int sh, float gain, const WarpGeo
                      int dw, int dh, const YuvRows* m, float* out_f, uint8_t* out_u8, int* err, cudaStream_t s);
 void launch_warp_rgba8(const uint8_t* src, int sw, int sh, int sstride, const WarpGeom& g, const float* taps, const uint32_t* rsq,
                        int dw, int dh, uint8_t* out, int* err, cudaStream_t s);
+struct ColourF {  // a row-major 4x4 colour transfer (StereoColorTransfer.Solve)
+  float f[16];
+};
+// StereoColorTransfer.Apply of a YUVA float image and the 8-bit store of the result.
+void launch_colour_apply(const float* yuv, int npx, const ColourF& F, uint8_t* out, cudaStream_t s);
 
 // cost.cu
 // The phase images of every other camera into a.phase (4·ow·oh u32 each); then the cost volume.

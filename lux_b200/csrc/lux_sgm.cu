@@ -920,6 +920,63 @@ extern "C" int lux_stereo_image(lux_sgm_ctx* ctx, const float* src, int32_t sw, 
   return rc;
 }
 
+extern "C" int lux_stereo_image_transfer(lux_sgm_ctx* ctx, const float* src, int32_t sw, int32_t sh, int32_t src_on_device,
+                                         float gain, const lux_aligned_calib* ac, int32_t dw, int32_t dh, int32_t sensor_type,
+                                         const float* neutral, const float* ref_yuv, int32_t ref_on_device, const lux_calib* ref_view,
+                                         const lux_calib* view, uint8_t* out_rgba8, int32_t out_on_device, float* out_F) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ref_yuv || !ref_view) return set_err(ctx, LUX_ERR_ARG, "Empty reference yuv.");  // StereoImageBuilder.cs:73
+  if (!src || !out_rgba8 || !neutral || !view || sw < 1 || sh < 1 || dw < 1 || dh < 1)
+    return set_err(ctx, LUX_ERR_ARG, "stereo image: null pointer or empty image");
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  WarpGeom g;
+  YuvRows m;
+  host_yuv_matrix(sensor_type, neutral, &m.m[0][0]);
+  const size_t npx = (size_t)dw * dh;
+  const float* d_src = nullptr;
+  float* d_yuv = nullptr;
+  uint8_t* d_out = out_on_device ? out_rgba8 : nullptr;
+  int rc = warp_geom(ctx, tmp, ac, &g);
+  if (!rc) rc = device_floats(ctx, tmp, src, (size_t)sw * sh * 4, src_on_device, &d_src);
+  if (!rc) rc = alloc_t(ctx, tmp, npx * 4, &d_yuv);
+  if (!rc && !d_out) rc = alloc_t(ctx, tmp, npx * 4, &d_out);
+  if (rc) {
+    dev_free_all(ctx, tmp);
+    return rc;
+  }
+  // the warped YUV image on the device, then its statistics and the reference crop's on the host (a serial recurrence)
+  launch_warp_f32(d_src, sw, sh, gain, g, warp_taps(ctx), ctx->d_warp, dw, dh, &m, d_yuv, d_out, ctx->d_err, ctx->stream);
+  std::vector<float> work(npx * 4), ref_h;
+  CK(cudaMemcpyAsync(work.data(), d_yuv, npx * 16, cudaMemcpyDeviceToHost, ctx->stream));
+  const float* ref = ref_yuv;
+  if (ref_on_device) {
+    ref_h.resize(npx * 4);
+    CK(cudaMemcpyAsync(ref_h.data(), ref_yuv, npx * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    ref = ref_h.data();
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  rc = take_device_error(ctx);
+  if (!rc) {
+    int rect[4];
+    host_crop_rect(*ref_view, *view, dw, dh, rect);  // StereoColorTransfer.Transfer (StereoColorTransfer.cs:128-138)
+    const int X0 = std::max(0, rect[0]), Y0 = std::max(0, rect[1]), X1 = std::min((int)dw, rect[2]), Y1 = std::min((int)dh, rect[3]);
+    const ColourStats sw_ = host_colour_stats(work.data(), dw, dh, dw, 0);
+    ColourStats sr{};
+    if (X1 - X0 > 0 && Y1 - Y0 > 0) sr = host_colour_stats(ref, X1 - X0, Y1 - Y0, dw, (size_t)Y0 * dw + X0);
+    ColourF F;
+    host_colour_solve(sw_, sr, F.f);
+    if (out_F) std::memcpy(out_F, F.f, sizeof F.f);
+    launch_colour_apply(d_yuv, (int)npx, F, d_out, ctx->stream);
+    CK(cudaGetLastError());
+    if (!out_on_device) CK(cudaMemcpyAsync(out_rgba8, d_out, npx * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
 extern "C" int lux_warp_rgba8(lux_sgm_ctx* ctx, const lux_img_rgba8* src, const lux_aligned_calib* ac, int32_t dw, int32_t dh,
                               uint8_t* dst, int32_t dst_on_device) {
   if (!ctx) return LUX_ERR_ARG;

@@ -239,7 +239,28 @@ __global__ void __launch_bounds__(256) k_warp_rgba8(const uchar4* __restrict__ s
   out[(size_t)y * dw + x] = pack_u8(px_f4(tap6(c, tx, z)));
 }
 
+// StereoColorTransfer.Apply (StereoColorTransfer.cs:112-125) and the 8-bit store: o = a·((1·c3 + z·c2) + (y·c1 + x·c0))
+// per lane with c_j the columns of the row-major F, alpha kept.
+__global__ void __launch_bounds__(256) k_colour_apply(const float4* __restrict__ yuv, int npx, const ColourF F, uint32_t* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npx) return;
+  const float4 p = yuv[i];
+  float o[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const float acc = __fadd_rn(__fadd_rn(__fmul_rn(1.0f, F.f[4 * k + 3]), __fmul_rn(p.z, F.f[4 * k + 2])),
+                                __fadd_rn(__fmul_rn(p.y, F.f[4 * k + 1]), __fmul_rn(p.x, F.f[4 * k])));
+    o[k] = __fmul_rn(p.w, acc);
+  }
+  out[i] = pack_u8(make_float4(o[0], o[1], o[2], p.w));
+}
+
 }  // namespace
+
+void launch_colour_apply(const float* yuv, int npx, const ColourF& F, uint8_t* out, cudaStream_t s) {
+  k_colour_apply<<<(npx + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4*>(yuv), npx, F, reinterpret_cast<uint32_t*>(out));
+  count_launches(1);
+}
 
 void launch_warp_f32(const float* src, int sw, int sh, float gain, const WarpGeom& g, const float* taps, const uint32_t* rsq,
                      int dw, int dh, const YuvRows* m, float* out_f, uint8_t* out_u8, int* err, cudaStream_t s) {

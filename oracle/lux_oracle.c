@@ -1418,3 +1418,165 @@ int lo_warp_rgba8(const uint8_t* src, int sw, int sh, int dw, int dh, const lo_a
     }
   return LO_OK;
 }
+
+/* ---------------- StereoColorTransfer (StereoColorTransfer.cs:15-148) ---------------- */
+
+/* Inv3D (:21-28): the 3x3 double inverse, in its operation order. */
+static void inv3d(const double* m, double* o) {
+  double a = m[0], b = m[1], c = m[2], d = m[3], e = m[4], f = m[5], g = m[6], h = m[7], i = m[8];
+  double c00 = i * e - f * h, c10 = d * i - g * f, c20 = d * h - g * e;
+  double det = ((c20 * c) + (c00 * a)) - (c10 * b);
+  double inv = 1.0 / det;
+  o[0] = c00 * inv; o[1] = (c * h - b * i) * inv; o[2] = (b * f - c * e) * inv;
+  o[3] = -(c10 * inv); o[4] = (i * a - c * g) * inv; o[5] = (c * d - f * a) * inv;
+  o[6] = c20 * inv; o[7] = (g * b - h * a) * inv; o[8] = (e * a - d * b) * inv;
+}
+
+/* CropRect (:32-51) */
+void lo_crop_rect(const lo_calib* calib2, const lo_calib* calibA, int x0, int y0, int x1, int y1, int out[4]) {
+  float xf[16];
+  lo_flow_matrix(calib2, calibA, xf);
+  double D[9], Di[9];
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) D[3 * r + c] = xf[4 * c + r];
+  inv3d(D, Di);
+  const float cx[4] = {(float)x0, (float)x0, (float)x1, (float)x1}, cy[4] = {(float)y0, (float)y1, (float)y0, (float)y1};
+  float minX = 0, minY = 0, maxX = 0, maxY = 0;
+  for (int k = 0; k < 4; k++) {
+    float X = cx[k], Y = cy[k];
+    double w = Di[8] + (Di[7] * Y + Di[6] * X);
+    float wf = (float)w;
+    float r0 = lo_rcp(wf);
+    float r = ((1.0f - wf * r0) * r0 + r0) * 1.0f;
+    float x = (float)(Di[2] + (Di[1] * Y + Di[0] * X)) * r;
+    float y = (float)(Di[5] + (Di[4] * Y + Di[3] * X)) * r;
+    if (k == 0) {
+      minX = maxX = x;
+      minY = maxY = y;
+    } else {
+      if (x <= minX) minX = x;
+      if (maxX <= x) maxX = x;
+      if (y <= minY) minY = y;
+      if (maxY <= y) maxY = y;
+    }
+  }
+  out[0] = net_int(minX); out[1] = net_int(minY); out[2] = net_int(maxX); out[3] = net_int(maxY);
+}
+
+typedef struct {
+  float mean[4], D[4], O[4], N;
+} lo_cstats;
+
+/* Accumulate (:56-75): Welford in float over the pixels with alpha > 0.95, lane by lane as the SSE vectors. */
+static lo_cstats accumulate(const float* yuva, int w, int h, int stride, size_t offset) {
+  static const float c0[4] = {1, 0, 0, 0}, c1[4] = {0, 1, 0, 0}, c2[4] = {0, 0, 1, 0}, e3[4] = {0, 0, 0, 1};
+  lo_cstats s;
+  memset(&s, 0, sizeof s);
+  float n = 0.0f;
+  for (int y = 0; y < h; y++)
+    for (int x = 0; x < w; x++) {
+      const float* p = yuva + (offset + (size_t)y * stride + x) * 4;
+      float px = p[0], py = p[1], pz = p[2], pw = p[3];
+      if (!(pw > 0.95f)) continue;
+      float n1 = n + 1.0f, r = 1.0f / n1;
+      float d[4], t[4];
+      for (int k = 0; k < 4; k++) d[k] = ((pz * c2[k] - s.mean[k]) + pw * e3[k]) + (py * c1[k] + px * c0[k]);
+      for (int k = 0; k < 4; k++) {
+        float rd = r * d[k];
+        t[k] = n * rd;
+        s.mean[k] = rd + s.mean[k];
+        s.D[k] = t[k] * d[k] + s.D[k];
+      }
+      const float ds[4] = {d[1], d[2], d[0], d[3]};
+      for (int k = 0; k < 4; k++) s.O[k] = ds[k] * t[k] + s.O[k];
+      n = n1;
+    }
+  s.N = n;
+  return s;
+}
+
+/* Chol (:77-84) of Cov (:86-91): L = U^T, row-major. */
+static void chol_cov(const lo_cstats* st, double L[9]) {
+  float inv = 1.0f / st->N, Dn[4], On[4];
+  for (int k = 0; k < 4; k++) {
+    Dn[k] = st->D[k] * inv;
+    On[k] = st->O[k] * inv;
+  }
+  const float C[9] = {Dn[0], On[0], On[2], On[0], Dn[1], On[1], On[2], On[1], Dn[2]};
+  const double tol = 0.001;
+  double U00 = C[0] + tol, U01 = C[1], U02 = C[2], U11 = C[4] + tol, U12 = C[5], U22 = C[8] + tol;
+  double d0 = U00;
+  if (d0 > 0) {
+    U00 = sqrt(d0);
+    double q = 1.0 / U00;
+    U01 *= q;
+    U02 *= q;
+    double d1 = U11 - U01 * U01;
+    if (d1 > 0) {
+      U11 = sqrt(d1);
+      U12 = U12 - U02 * U01;
+      q = 1.0 / U11;
+      U12 *= q;
+      double d2 = U22 - (U02 * U02 + U12 * U12);
+      if (d2 > 0) U22 = sqrt(d2);
+    }
+  }
+  L[0] = U00; L[1] = 0; L[2] = 0; L[3] = U01; L[4] = U11; L[5] = 0; L[6] = U02; L[7] = U12; L[8] = U22;
+}
+
+static void ident4(double* m) {
+  memset(m, 0, 16 * sizeof(double));
+  m[0] = m[5] = m[10] = m[15] = 1.0;
+}
+
+/* Solve (:94-108) */
+static void color_solve(const lo_cstats* work, const lo_cstats* ref, float F[16]) {
+  memset(F, 0, 16 * sizeof(float));
+  F[0] = F[5] = F[10] = F[15] = 1.0f;
+  if (net_int(work->N) < 100 || net_int(ref->N) < 100) return;
+  double Lr[9], Lw[9], Li[9], A4[16], Tr[16], Tw[16], M4[16], Minv4[16], t1[16], t2[16], t3[16], X[16];
+  chol_cov(ref, Lr);
+  chol_cov(work, Lw);
+  inv3d(Lw, Li);
+  memset(A4, 0, sizeof A4);
+  A4[15] = 1.0;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) A4[4 * i + j] = (Lr[3 * i] * Li[j] + Lr[3 * i + 1] * Li[3 + j]) + Lr[3 * i + 2] * Li[6 + j];
+  ident4(Tr);
+  ident4(Tw);
+  for (int k = 0; k < 3; k++) {
+    Tr[4 * k + 3] = ref->mean[k];
+    Tw[4 * k + 3] = -(double)work->mean[k];
+  }
+  ident4(M4);
+  ident4(Minv4);
+  Minv4[4] = -0.0;
+  mat4_mul(Tr, A4, t1);
+  mat4_mul(t1, Tw, t2);
+  mat4_mul(Minv4, t2, t3);
+  mat4_mul(t3, M4, X);
+  for (int k = 0; k < 16; k++) F[k] = (float)X[k];
+}
+
+void lo_color_transfer(const float* work, int w, int h, const float* ref, int rw, int rh, const lo_calib* calib2,
+                       const lo_calib* calibA, float* out, float F[16], int crop[4], float* n_work, float* n_ref) {
+  int rect[4];
+  lo_crop_rect(calib2, calibA, 0, 0, rw, rh, rect);
+  int X0 = rect[0] > 0 ? rect[0] : 0, Y0 = rect[1] > 0 ? rect[1] : 0, X1 = rect[2] < rw ? rect[2] : rw, Y1 = rect[3] < rh ? rect[3] : rh;
+  lo_cstats sw = accumulate(work, w, h, w, 0), sr;
+  if (X1 - X0 <= 0 || Y1 - Y0 <= 0) memset(&sr, 0, sizeof sr);
+  else sr = accumulate(ref, X1 - X0, Y1 - Y0, rw, (size_t)Y0 * rw + X0);
+  color_solve(&sw, &sr, F);
+  crop[0] = X0; crop[1] = Y0; crop[2] = X1; crop[3] = Y1;
+  *n_work = sw.N;
+  *n_ref = sr.N;
+  /* Apply (:112-125): o = a·((1·c3 + z·c2) + (y·c1 + x·c0)), o.a = a, with c_j the columns of F */
+  for (size_t p = 0; p < (size_t)w * h; p++) {
+    const float x = work[p * 4], y = work[p * 4 + 1], z = work[p * 4 + 2], a = work[p * 4 + 3];
+    for (int k = 0; k < 3; k++) {
+      float acc = (1.0f * F[4 * k + 3] + z * F[4 * k + 2]) + (y * F[4 * k + 1] + x * F[4 * k]);
+      out[p * 4 + k] = a * acc;
+    }
+    out[p * 4 + 3] = a;
+  }
+}

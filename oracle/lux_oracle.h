@@ -159,6 +159,13 @@ void lo_to_rgba8(const float* rgba, size_t n, uint8_t* out);       /* StereoImag
 /* Rgba8Warp.Warp (ReferenceGuide.cs:108-156): the 8-bit warp of the reference guide. */
 int lo_warp_rgba8(const uint8_t* src, int sw, int sh, int dw, int dh, const lo_aligned* ac, uint8_t* dst);
 
+/* StereoColorTransfer.Transfer (StereoColorTransfer.cs:128-138) of a work YUVA image (w x h x 4 floats) onto the crop of
+ * a reference YUVA image (rw x rh) given by calib2 (the reference view) and calibA (the work view): out (w x h x 4),
+ * F the 4x4 row-major transfer, crop the clamped rect {X0, Y0, X1, Y1}, n_work / n_ref the gated pixel counts. */
+void lo_crop_rect(const lo_calib* calib2, const lo_calib* calibA, int x0, int y0, int x1, int y1, int out[4]);
+void lo_color_transfer(const float* work, int w, int h, const float* ref, int rw, int rh, const lo_calib* calib2,
+                       const lo_calib* calibA, float* out, float F[16], int crop[4], float* n_work, float* n_ref);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,6 +93,11 @@ def lib():
         l.lo_to_rgba8.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
         l.lo_warp_rgba8.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.POINTER(LoAligned), ctypes.c_void_p]
+        l.lo_crop_rect.argtypes = [ctypes.POINTER(LoCalib), ctypes.POINTER(LoCalib), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_void_p]
+        l.lo_color_transfer.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(LoCalib), ctypes.POINTER(LoCalib), ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         _lib = l
     return _lib
 
@@ -439,3 +444,26 @@ def warp_rgba8(src, dw, dh, ac):
     if rc:
         raise OracleError(rc, "warp_rgba8")
     return out
+
+
+def color_transfer(work, ref, calib2, calibA):
+    """StereoColorTransfer.Transfer (StereoColorTransfer.cs:128-138): (out YUVA floats, F 4x4, crop rect, N work, N ref)."""
+    wk = np.ascontiguousarray(np.asarray(work, np.float32))
+    rf = np.ascontiguousarray(np.asarray(ref, np.float32))
+    h, w = wk.shape[:2]
+    rh, rw = rf.shape[:2]
+    out = np.empty_like(wk)
+    F = np.empty(16, np.float32)
+    crop = np.empty(4, np.int32)
+    nw, nr = ctypes.c_float(), ctypes.c_float()
+    lib().lo_color_transfer(wk.ctypes.data, w, h, rf.ctypes.data, rw, rh, _calibs([calib2]), _calibs([calibA]), out.ctypes.data,
+                            F.ctypes.data, crop.ctypes.data, ctypes.byref(nw), ctypes.byref(nr))
+    return out, F.reshape(4, 4), tuple(int(v) for v in crop), nw.value, nr.value
+
+
+def stereo_image_transfer(src, gain, dw, dh, ac, sensor_type, neutral, ref_yuv, ref_view, view):
+    """StereoImageBuilder.Create for a non-reference module with the reference crop (StereoImageBuilder.cs:61-65, 71-77):
+    (rgba8, F)."""
+    yuv = convert_yuv(warp_f32(src, gain, dw, dh, ac), yuv_matrix(sensor_type, neutral))
+    out, F, crop, nw, nr = color_transfer(yuv, ref_yuv, ref_view, view)
+    return to_rgba8(out), F

@@ -129,3 +129,64 @@ def test_warp_errors(api):
     ok = synth.aligned_calib(40, 30, 40, 30, seed=1)
     with pytest.raises(api.LuxError):
         api.Rgba8Warp.warp(np.zeros((0, 4, 4), np.uint8), 8, 8, ok)
+
+
+def _views(dw, dh, angle_deg, shift):
+    """The reference camera's view (calib2) and a module's view (calibA) of the colour transfer: a rotation about the
+    optical axis and a principal-point shift between them."""
+    from lux_b200 import api
+    f = np.float32(1.1 * dw)
+    K2 = np.array([f, 0, dw / 2.0, 0, f, dh / 2.0, 0, 0, 1], np.float32)
+    KA = np.array([f * 1.01, 0, dw / 2.0 + shift[0], 0, f * 1.01, dh / 2.0 + shift[1], 0, 0, 1], np.float32)
+    a = np.deg2rad(angle_deg)
+    R = np.array([[np.cos(a), -np.sin(a), 0], [np.sin(a), np.cos(a), 0], [0, 0, 1]], np.float32).reshape(9)
+    return (api.CalibData(K2, np.zeros(3, np.float32), np.eye(3, dtype=np.float32).reshape(9)),
+            api.CalibData(KA, np.array([-25.0, 3.0, 0.0], np.float32), R))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dw,dh,angle,shift,device", [(180, 140, 2.0, (6.0, -4.0), False), (120, 77, -4.0, (-30.0, 12.0), True),
+                                                      (64, 48, 0.0, (0.0, 0.0), False), (96, 70, 0.5, (400.0, 0.0), False)])
+def test_stereo_image_transfer_matches_oracle(api, dw, dh, angle, shift, device):
+    """The non-reference branch (StereoImageBuilder.cs:71-77): the reference's YUV floats from the reference branch, then
+    the module's image colour-matched to its crop; the 8-bit image and the transfer F bit for bit. The last case's crop
+    lies outside the reference image (an empty crop: the identity transfer)."""
+    import torch
+    from lux_b200 import synth
+    sw, sh = dw + 20, dh + 10
+    neutral = (0.5, 1.0, 0.6)
+    ref_src, mod_src = synth.isp_image(sw, sh, 21), synth.isp_image(sw, sh, 22)
+    ac_ref = synth.aligned_calib(sw, sh, dw, dh, seed=21)
+    ac_mod = synth.aligned_calib(sw, sh, dw, dh, seed=22, angle_deg=angle)
+    ref_view, view = _views(dw, dh, angle, shift)
+    _, ref_yuv = api.StereoImage.create(ref_src, dw, dh, ac_ref, 2, neutral, keep_yuv=True)
+    _, w_ref_yuv = O.stereo_image(ref_src, 1.0, dw, dh, ac_ref, 2, neutral)
+    assert np.array_equal(_bits(ref_yuv), _bits(w_ref_yuv))
+    src = torch.from_numpy(mod_src).cuda() if device else mod_src
+    ry = torch.from_numpy(ref_yuv).cuda() if device else ref_yuv
+    got, F = api.StereoImage.create_transfer(src, dw, dh, ac_mod, 2, neutral, ry, ref_view, view, gain=0.87)
+    want, wF = O.stereo_image_transfer(mod_src, 0.87, dw, dh, ac_mod, 2, neutral, w_ref_yuv, ref_view, view)
+    assert np.array_equal(F.view(np.uint32), wF.view(np.uint32))
+    got = got.cpu().numpy() if hasattr(got, "cpu") else got
+    assert np.array_equal(got, want)
+    if shift[0] > 100:
+        assert np.array_equal(F, np.eye(4, dtype=np.float32))
+    else:
+        assert not np.array_equal(F, np.eye(4, dtype=np.float32))
+
+
+@pytest.mark.gpu
+def test_stereo_image_transfer_needs_reference(api):
+    from lux_b200 import synth
+    src = synth.isp_image(40, 30, 1)
+    ac = synth.aligned_calib(40, 30, 40, 30, seed=1)
+    rv, v = _views(40, 30, 0.0, (0.0, 0.0))
+    with pytest.raises(api.LuxError, match="Empty reference yuv"):
+        api.L.load()  # the library is there; the call refuses the missing reference image
+        ctx = api.default_context()
+        c, lut = ac.to_c()
+        n = np.ascontiguousarray(np.array([0.5, 1.0, 0.6], np.float32))
+        out = np.empty((30, 40, 4), np.uint8)
+        ctx.check(ctx.lib.lux_stereo_image_transfer(ctx.handle, src.ctypes.data, 40, 30, 0, 1.0, api.ctypes.byref(c), 40, 30, 2,
+                                                    n.ctypes.data, None, 0, api.ctypes.byref(rv.to_c()), api.ctypes.byref(v.to_c()),
+                                                    out.ctypes.data, 0, None))
