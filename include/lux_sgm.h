@@ -221,6 +221,26 @@ void lux_lanczos_table(float* out384);
 /* StereoImage.YuvMatrix (StereoImage.cs:140-160): the 3 x 4 rows (v, u', t'). */
 void lux_yuv_matrix(int32_t sensor_type, const float* neutral, float* out12);
 
+/* The opt-in census stereo mode of a rectified pair (no counterpart in the reference, whose dense stage is the plane sweep
+ * above; parity is with this library's own CPU restatement of the method). Census transform over a 9x7 window, Hamming
+ * cost (62 where x - d leaves the image), eight-path semi-global aggregation with constant P1 and P2, the first disparity
+ * of least cost, parabolic subpixel refinement, and a left/right check that marks inconsistent pixels -1. Grey values are
+ * byte 0 of the RGBA8 images (same size). max_disparity 1..256; 8·(62 + p2) must fit 16 bits (p2 <= 8129). */
+typedef struct {
+  int32_t max_disparity;
+  uint32_t p1, p2;
+  int32_t subpixel;     /* nonzero: parabolic refinement */
+  int32_t lr_check;     /* nonzero: left/right consistency */
+  int32_t lr_max_diff;  /* the largest accepted |d_left - d_right| */
+} lux_census_params;
+int lux_census_sgm(lux_sgm_ctx* ctx, const lux_img_rgba8* left, const lux_img_rgba8* right, const lux_census_params* params,
+                   float* out_disp, int32_t out_on_device);
+/* The fusion of a capture's pairs: per pair the depth fb[k] / disparity where the disparity is positive, per pixel the
+ * median of the valid depths (the mean of the two middle ones for an even count), 0 where none is valid. disps: n <= 16
+ * pointers to w x h disparity maps (device pointers when on_device, else host). */
+int lux_fuse_disparities(lux_sgm_ctx* ctx, const float* const* disps, const float* fb, int32_t n, int32_t w, int32_t h,
+                         int32_t on_device, float* out_depth, int32_t out_on_device);
+
 /* DepthImageCache.Set (Lux.Engine/Pipeline/Export/DepthCache.cs:136-143, fed by FromFullDepth :239-244): the cache image
  * (cw x ch floats) made from a depth map (w x h): InverseDepth, the nearest 16.16 resample to the cache dims, then
  * min(rcpps(x), 1e5). depth / cache are device pointers of the context's GPU when *_on_device, else host memory.

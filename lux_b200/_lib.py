@@ -54,6 +54,11 @@ class AlignedCalib(ctypes.Structure):
                 ("sx", ctypes.c_float), ("sy", ctypes.c_float)]
 
 
+class CensusParams(ctypes.Structure):
+    _fields_ = [("max_disparity", ctypes.c_int32), ("p1", ctypes.c_uint32), ("p2", ctypes.c_uint32), ("subpixel", ctypes.c_int32),
+                ("lr_check", ctypes.c_int32), ("lr_max_diff", ctypes.c_int32)]
+
+
 class LayerInfo(ctypes.Structure):
     _fields_ = [("w", ctypes.c_int32), ("h", ctypes.c_int32), ("index", ctypes.c_int32), ("align", ctypes.c_int32),
                 ("n_planes", ctypes.c_int32), ("min_lo", ctypes.c_int32), ("max_hi", ctypes.c_int32), ("tile", ctypes.c_int32),
@@ -110,6 +115,10 @@ SIGNATURES = [
                                                  ctypes.c_float, ctypes.POINTER(AlignedCalib), ctypes.c_int32, ctypes.c_int32,
                                                  ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Calib),
                                                  ctypes.POINTER(Calib), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
+    ("lux_census_sgm", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Img), ctypes.POINTER(Img), ctypes.POINTER(CensusParams),
+                                      ctypes.c_void_p, ctypes.c_int32]),
+    ("lux_fuse_disparities", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_int32,
+                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]),
     ("lux_warp_rgba8", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Img), ctypes.POINTER(AlignedCalib), ctypes.c_int32,
                                       ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]),
     ("lux_lanczos_table", None, [ctypes.c_void_p]),

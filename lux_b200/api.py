@@ -615,6 +615,44 @@ class Rgba8Warp:
         return out
 
 
+class CensusStereo:
+    """The opt-in census stereo mode of a rectified grey pair (no counterpart in the reference): census 9x7, Hamming cost,
+    8-path SGM with constant P1/P2, first-minimum WTA, parabolic subpixel, left/right check (-1 where it fails)."""
+
+    @staticmethod
+    def compute(left, right, max_disparity, p1=10, p2=120, subpixel=True, lr_check=True, lr_max_diff=1,
+                ctx: Optional[Context] = None):
+        """left, right: (h, w, 4) uint8 (grey in channel 0) or (h, w) uint8. Returns (h, w) float32 disparities."""
+        ctx = ctx or default_context()
+        imgs = []
+        for im in (left, right):
+            if not hasattr(im, "data_ptr") and np.asarray(im).ndim == 2:
+                im = np.repeat(np.asarray(im, np.uint8)[..., None], 4, axis=2)
+            imgs.append(_img_c(im))
+        (cl, kl), (cr, kr) = imgs
+        prm = L.CensusParams(int(max_disparity), int(p1), int(p2), 1 if subpixel else 0, 1 if lr_check else 0, int(lr_max_diff))
+        out = _empty_like_kind(left if hasattr(left, "data_ptr") else np.empty(0), (cl.h, cl.w), np.float32)
+        optr, oon = _ptr(out)
+        _torch_ready(left, right, out)
+        ctx.check(ctx.lib.lux_census_sgm(ctx.handle, ctypes.byref(cl), ctypes.byref(cr), ctypes.byref(prm), optr, oon))
+        return out
+
+    @staticmethod
+    def fuse(disps, fbs, ctx: Optional[Context] = None):
+        """The median depth over the pairs' valid disparities (fB / d for d > 0), 0 where none is valid."""
+        ctx = ctx or default_context()
+        keep = [_f32_image(d) for d in disps]
+        h, w = keep[0][3]
+        on_dev = keep[0][1]
+        ptrs = (ctypes.c_void_p * len(keep))(*[k[0] for k in keep])
+        fb = np.ascontiguousarray(np.asarray(fbs, np.float32))
+        out = _f32_like(disps[0], h, w)
+        optr, oon, okeep, _ = _f32_image(out)
+        _torch_ready(*disps, out)
+        ctx.check(ctx.lib.lux_fuse_disparities(ctx.handle, ptrs, fb.ctypes.data, len(keep), w, h, on_dev, optr, oon))
+        return out
+
+
 @dataclass
 class ServedResult:
     """One served request: its depth map (the layer grid) and the times it spent queued and running."""

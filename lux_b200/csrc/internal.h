@@ -88,6 +88,17 @@ void launch_warp_rgba8(const uint8_t* src, int sw, int sh, int sstride, const Wa
 struct ColourF {  // a row-major 4x4 colour transfer (StereoColorTransfer.Solve)
   float f[16];
 };
+// census_sgm.cu: the opt-in census stereo mode (census, Hamming cost, 8-path SGM, WTA, subpixel, left/right, fusion)
+constexpr int kMaxFusePairs = 16;
+int census_lpt(int D);  // disparities per lane: 1, 2, 4 or 8 for D up to 32, 64, 128, 256 (0: too large)
+// left / right: grey pixels at byte 0 of every bpp bytes, rows stride pixels apart; cl, cr: W x H; cost, S: W x H x
+// 32·census_lpt(D); dl, dr: W x H; disp: W x H floats.
+void launch_census_sgm(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int bpp, int D, uint32_t P1, uint32_t P2,
+                       int subpixel, int lr, int max_diff, uint64_t* cl, uint64_t* cr, uint8_t* cost, uint16_t* S, int* dl, int* dr,
+                       float* disp, cudaStream_t s);
+// disps: a device array of n device pointers to W x H disparity maps (n <= kMaxFusePairs); fb: n focal x baseline products.
+void launch_fuse(const float* const* disps, const float* fb, int n, int npx, float* out, cudaStream_t s);
+
 // StereoColorTransfer.Apply of a YUVA float image and the 8-bit store of the result.
 void launch_colour_apply(const float* yuv, int npx, const ColourF& F, uint8_t* out, cudaStream_t s);
 

@@ -977,6 +977,67 @@ extern "C" int lux_stereo_image_transfer(lux_sgm_ctx* ctx, const float* src, int
   return rc;
 }
 
+extern "C" int lux_census_sgm(lux_sgm_ctx* ctx, const lux_img_rgba8* left, const lux_img_rgba8* right, const lux_census_params* p,
+                              float* out_disp, int32_t out_on_device) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!left || !right || !p || !out_disp) return set_err(ctx, LUX_ERR_ARG, "census: null pointer");
+  if (left->w != right->w || left->h != right->h) return set_err(ctx, LUX_ERR_ARG, "census: the two images differ in size");
+  if (p->max_disparity < 1 || p->max_disparity > 256) return set_err(ctx, LUX_ERR_ARG, "census: max_disparity must be 1..256");
+  if (p->p2 > 8129 || p->p1 > 8129) return set_err(ctx, LUX_ERR_ARG, "census: P1/P2 too large, path sums would pass 16 bits");
+  cudaSetDevice(ctx->device);
+  const int w = left->w, h = left->h, D = p->max_disparity, Dp = 32 * census_lpt(D);
+  const size_t npx = (size_t)w * h;
+  std::vector<DevBuf> tmp;
+  const uint8_t *dl_img = nullptr, *dr_img = nullptr;
+  uint64_t *cl = nullptr, *cr = nullptr;
+  uint8_t* cost = nullptr;
+  uint16_t* S = nullptr;
+  int *dl = nullptr, *dr = nullptr;
+  int rc = upload_image(ctx, tmp, *left, &dl_img);
+  if (!rc) rc = upload_image(ctx, tmp, *right, &dr_img);
+  if (!rc) rc = alloc_t(ctx, tmp, npx, &cl);
+  if (!rc) rc = alloc_t(ctx, tmp, npx, &cr);
+  if (!rc) rc = alloc_t(ctx, tmp, npx * Dp, &cost);
+  if (!rc) rc = alloc_t(ctx, tmp, npx * Dp, &S);
+  if (!rc) rc = alloc_t(ctx, tmp, npx, &dl);
+  if (!rc) rc = alloc_t(ctx, tmp, npx, &dr);
+  if (!rc)
+    rc = to_output(ctx, tmp, out_disp, npx, out_on_device, [&](float* d) {
+      launch_census_sgm(dl_img, dr_img, w, h, w, 4, D, p->p1, p->p2, p->subpixel, p->lr_check, p->lr_max_diff, cl, cr, cost, S, dl, dr, d,
+                        ctx->stream);
+    });
+  if (!rc) CK(cudaStreamSynchronize(ctx->stream));
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
+extern "C" int lux_fuse_disparities(lux_sgm_ctx* ctx, const float* const* disps, const float* fb, int32_t n, int32_t w, int32_t h,
+                                    int32_t on_device, float* out_depth, int32_t out_on_device) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!disps || !fb || !out_depth || n < 1 || n > kMaxFusePairs || w < 1 || h < 1)
+    return set_err(ctx, LUX_ERR_ARG, "fuse: null pointer, bad size or more than 16 pairs");
+  cudaSetDevice(ctx->device);
+  const size_t npx = (size_t)w * h;
+  std::vector<DevBuf> tmp;
+  std::vector<const float*> dptr(n);
+  int rc = LUX_OK;
+  for (int k = 0; k < n && !rc; k++) rc = device_floats(ctx, tmp, disps[k], npx, on_device, &dptr[k]);
+  const float** d_list = nullptr;
+  float* d_fb = nullptr;
+  if (!rc) rc = alloc_t(ctx, tmp, (size_t)n, &d_list);
+  if (!rc) rc = alloc_t(ctx, tmp, (size_t)n, &d_fb);
+  if (!rc) {
+    CK(cudaMemcpyAsync(d_list, dptr.data(), n * sizeof(float*), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_fb, fb, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    rc = to_output(ctx, tmp, out_depth, npx, out_on_device, [&](float* d) { launch_fuse(d_list, d_fb, n, (int)npx, d, ctx->stream); });
+  }
+  if (!rc) CK(cudaStreamSynchronize(ctx->stream));
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
 extern "C" int lux_warp_rgba8(lux_sgm_ctx* ctx, const lux_img_rgba8* src, const lux_aligned_calib* ac, int32_t dw, int32_t dh,
                               uint8_t* dst, int32_t dst_on_device) {
   if (!ctx) return LUX_ERR_ARG;
