@@ -73,6 +73,8 @@ def args_():
     p.add_argument("--stereo", action="store_true",
                    help="stereo-image formation after the ISP: ten 2080x1560 module images warped, YUV'd and stored as 8 bits, "
                         "and the 4160x3120 reference guide's 8-bit warp")
+    p.add_argument("--census", action="store_true",
+                   help="the opt-in census mode (census, Hamming, 8-path SGM, WTA + subpixel + left/right) on the workload's pair")
     p.add_argument("--cpu-rows", type=int, default=130, help="rows of the CPU sample strip")
     p.add_argument("--workload", default="pair13mp", choices=sorted(WORKLOADS),
                    help="pair13mp is the benchmark; the smaller pairs are for profiling captures")
@@ -656,8 +658,88 @@ def run_stereo(a):
     ctx.close()
 
 
+def run_census(a):
+    """The opt-in census stereo mode on the workload's pair (default: 4160x3120, D=256): value = W·H·D per second with the
+    images in HBM and the disparities left there; e2e from host images to host disparities. Roofline (HBM), the
+    aggregation's algorithmic bytes: the eight path launches each read the u8 cost volume once and read-modify-write the
+    u16 path sums (the first only writes): 8·1 + 7·4 + 2 = 38 bytes per DE."""
+    import torch
+    from lux_b200 import _lib, api
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    D = D_
+    wl = workload(0)
+    left, right = wl.images[0], wl.images[1]
+    if a.impl == "reference":
+        from oracle import census_oracle as C
+        rows = 48
+        t0 = time.perf_counter()
+        C.census_sgm(left[:rows, :, 0], right[:rows, :, 0], D, 10, 120)
+        dt = time.perf_counter() - t0
+        v = W_ * rows * D / dt / 1e6
+        print(json.dumps({"impl": "reference", "metric": f"census SGM MDE/s, {W_}x{H_} pair D={D}", "value": v, "unit": "MDE/s",
+                          "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "u8 cost / u16 aggregation", "data": "synthetic", "config": {"workload": DESC},
+                          "cpu_baseline": {"value": v, "unit": "MDE/s", "cores": 1, "kind": "port",
+                                           "sample": f"{W_}x{rows} strip, numpy restatement"},
+                          "e2e": {"value": v, "unit": "MDE/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(lib.lux_sgm_stream(ctx.handle), device=torch.device("cuda", 0))
+    d_imgs = [torch.from_numpy(im).cuda() for im in (left, right)]
+    h_imgs = [torch.from_numpy(im).pin_memory() for im in (left, right)]
+    d_out = torch.empty((H_, W_), dtype=torch.float32, device="cuda")
+    h_out = torch.empty((H_, W_), dtype=torch.float32).pin_memory()
+    prm = _lib.CensusParams(D, 10, 120, 1, 1, 1)
+    torch.cuda.synchronize()
+
+    def step(on_dev):
+        src = d_imgs if on_dev else h_imgs
+        il = _lib.Img(src[0].data_ptr(), W_, H_, W_, 1 if on_dev else 0)
+        ir = _lib.Img(src[1].data_ptr(), W_, H_, W_, 1 if on_dev else 0)
+        out = d_out if on_dev else h_out
+        ctx.check(lib.lux_census_sgm(ctx.handle, ctypes.byref(il), ctypes.byref(ir), ctypes.byref(prm), out.data_ptr(),
+                                     1 if on_dev else 0))
+
+    def timed(fn, k):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        n0 = api.kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k, api.kernel_launches() - n0
+
+    with ClockSampler(0) as clk:
+        ms_v, launches = timed(lambda: step(True), a.steps)
+    ms_e, _ = timed(lambda: step(False), a.steps)
+    de = W_ * H_ * D
+    pk = peaks()
+    achieved = 38 * de / (ms_v / 1e3) / 1e9  # the whole step's time: an upper bound on the aggregation's
+    out = {"metric": f"census SGM MDE/s (W·H·D per second), {W_}x{H_} pair D={D}, opt-in mode", "value": de / (ms_v / 1e3) / 1e6,
+           "unit": "MDE/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_v, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "u8 cost / u16 aggregation", "data": "synthetic",
+           "config": {"workload": DESC + " (census mode: 9x7 census, P1 10, P2 120, subpixel, left/right)", "l2": l2_note()},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s", "frac": achieved / pk.get("hbm_gbs"),
+                        "traffic": None, "kernel": "the whole census step (38 B/DE of aggregation over the step's time)",
+                        "peak_source": "fallback" if pk.get("fallback") else "MEASURED_PEAKS.json hbm_gbs (measured)"},
+           "e2e": {"value": de / (ms_e / 1e3) / 1e6, "unit": "MDE/s", "h2d_bytes_per_step": 2 * W_ * H_ * 4, "d2h_bytes_per_step": W_ * H_ * 4},
+           "gpu_launches": int(launches), "clocks": clk.summary()}
+    print(json.dumps(out))
+    ctx.close()
+
+
 def main():
     a = args_()
+    if a.census:
+        run_census(a)
+        return
     if a.stereo:
         run_stereo(a)
         return

@@ -19,6 +19,44 @@ constexpr int kCensusWX = 4, kCensusWY = 3;  // a 9x7 window: 62 bits
 constexpr uint32_t kInvalidCost = 62;        // the cost where x - d leaves the image
 constexpr uint32_t kBig = 1u << 20;          // disparities past D: never a minimum
 
+// value i of a lane's LPT registers (i known only at run time)
+template <int LPT>
+LUX_DEV uint32_t pick(const uint32_t (&v)[LPT], int i) {
+  uint32_t r = v[0];
+#pragma unroll
+  for (int k = 1; k < LPT; k++) r = i == k ? v[k] : r;
+  return r;
+}
+
+// The first disparity with the least path sum S[0..D) of a pixel held by a warp (LPT a lane), with the parabolic subpixel
+// correction (S[d-1] - S[d+1]) / (2 (S[d-1] - 2 S[d] + S[d+1])) where 0 < d < D - 1 and the denominator is positive.
+template <int LPT>
+LUX_DEV void wta_of(const uint32_t (&s)[LPT], int lane, int D, int subpixel, int& d_out, float& disp_out) {
+  uint32_t best = kBig, arg = kBig;
+#pragma unroll
+  for (int i = 0; i < LPT; i++) {
+    const int d = lane * LPT + i;
+    const uint32_t v = d < D ? (s[i] & 0xffffu) : kBig;
+    if (v < best) {
+      best = v;
+      arg = d;
+    }
+  }
+  const uint32_t m = __reduce_min_sync(0xffffffffu, best);
+  const int d = (int)__reduce_min_sync(0xffffffffu, best == m ? arg : kBig);
+  const int dm = max(d - 1, 0), dp = min(d + 1, D - 1);
+  const float a = (float)__shfl_sync(0xffffffffu, pick<LPT>(s, dm % LPT) & 0xffffu, dm / LPT);
+  const float c = (float)__shfl_sync(0xffffffffu, pick<LPT>(s, dp % LPT) & 0xffffu, dp / LPT);
+  float out = (float)d;
+  if (subpixel && d > 0 && d < D - 1) {
+    const float b = (float)m;
+    const float den = __fmul_rn(2.0f, __fadd_rn(__fsub_rn(a, __fmul_rn(2.0f, b)), c));
+    if (den > 0.0f) out = __fadd_rn(out, __fdiv_rn(__fsub_rn(a, c), den));
+  }
+  d_out = d;
+  disp_out = out;
+}
+
 // Bit k (row-major over the window, centre skipped) is set when that neighbour, read at the clamped position, is darker
 // than the centre.
 __global__ void k_census(const uint8_t* __restrict__ img, int w, int h, int stride, int bpp, uint64_t* __restrict__ out) {
@@ -39,34 +77,103 @@ __global__ void k_census(const uint8_t* __restrict__ img, int w, int h, int stri
   out[(size_t)y * w + x] = v;
 }
 
-// C(x, y, d) = popcount(L(x, y) ^ R(x - d, y)), 62 where x - d < 0. A thread makes eight disparities of one pixel (one
-// 8-byte store); threads of a warp take neighbouring pixels, so the right-image reads of a disparity are one coalesced row.
-__global__ void k_hamming(const uint64_t* __restrict__ cl, const uint64_t* __restrict__ cr, int w, int h, int D, int Dp,
-                          uint8_t* __restrict__ cost) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, g = blockIdx.z;
-  if (x >= w) return;
-  const uint64_t a = __ldg(cl + (size_t)y * w + x);
-  uint32_t lo = 0, hi = 0;
+// C(x, y, d) = popcount(L(x, y) ^ R(x - d, y)), 62 where x - d < 0. A warp per pixel, lane j making disparities j, j + 32,
+// ...: each load instruction reads 32 neighbouring right-image words and each store writes 32 consecutive cost bytes.
+template <int LPT>
+__global__ void __launch_bounds__(256) k_hamming(const uint64_t* __restrict__ cl, const uint64_t* __restrict__ cr, int w, int h, int D,
+                                                 uint8_t* __restrict__ cost) {
+  constexpr int Dp = 32 * LPT;
+  const int lane = threadIdx.x & 31;
+  const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (p >= w * h) return;
+  const int y = p / w, x = p - y * w;
+  const uint64_t a = __ldg(cl + p);
+  const uint64_t* row = cr + (size_t)y * w;
+  uint8_t* out = cost + (size_t)p * Dp;
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const int d = g * 8 + k;
-    uint32_t c = kInvalidCost;
-    if (d < D && x - d >= 0) c = (uint32_t)__popcll(a ^ __ldg(cr + (size_t)y * w + x - d));
-    if (k < 4) lo |= c << (8 * k);
-    else hi |= c << (8 * (k - 4));
+  for (int k = 0; k < LPT; k++) {
+    const int d = lane + 32 * k;
+    out[d] = (uint8_t)(d < D && x - d >= 0 ? __popcll(a ^ __ldg(row + x - d)) : kInvalidCost);
   }
-  *reinterpret_cast<uint2*>(cost + ((size_t)y * w + x) * Dp + g * 8) = make_uint2(lo, hi);
 }
+
+// A lane's LPT cost bytes and LPT path sums as one vector access each.
+template <int LPT>
+struct LaneIO;
+template <>
+struct LaneIO<1> {
+  static LUX_DEV void cost(const uint8_t* p, uint32_t (&c)[1]) { c[0] = *p; }
+  static LUX_DEV void load(const uint16_t* p, uint32_t (&v)[1]) { v[0] = *p; }
+  static LUX_DEV void store(uint16_t* p, const uint32_t (&v)[1]) { *p = (uint16_t)v[0]; }
+};
+template <>
+struct LaneIO<2> {
+  static LUX_DEV void cost(const uint8_t* p, uint32_t (&c)[2]) {
+    const uint32_t w = *reinterpret_cast<const uint16_t*>(p);
+    c[0] = w & 0xff;
+    c[1] = w >> 8;
+  }
+  static LUX_DEV void load(const uint16_t* p, uint32_t (&v)[2]) {
+    const uint32_t w = *reinterpret_cast<const uint32_t*>(p);
+    v[0] = w & 0xffff;
+    v[1] = w >> 16;
+  }
+  static LUX_DEV void store(uint16_t* p, const uint32_t (&v)[2]) { *reinterpret_cast<uint32_t*>(p) = v[0] | v[1] << 16; }
+};
+template <>
+struct LaneIO<4> {
+  static LUX_DEV void cost(const uint8_t* p, uint32_t (&c)[4]) {
+    const uint32_t w = *reinterpret_cast<const uint32_t*>(p);
+#pragma unroll
+    for (int i = 0; i < 4; i++) c[i] = (w >> (8 * i)) & 0xff;
+  }
+  static LUX_DEV void load(const uint16_t* p, uint32_t (&v)[4]) {
+    const uint2 w = *reinterpret_cast<const uint2*>(p);
+    v[0] = w.x & 0xffff;
+    v[1] = w.x >> 16;
+    v[2] = w.y & 0xffff;
+    v[3] = w.y >> 16;
+  }
+  static LUX_DEV void store(uint16_t* p, const uint32_t (&v)[4]) {
+    *reinterpret_cast<uint2*>(p) = make_uint2(v[0] | v[1] << 16, v[2] | v[3] << 16);
+  }
+};
+template <>
+struct LaneIO<8> {
+  static LUX_DEV void cost(const uint8_t* p, uint32_t (&c)[8]) {
+    const uint2 w = *reinterpret_cast<const uint2*>(p);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      c[i] = (w.x >> (8 * i)) & 0xff;
+      c[4 + i] = (w.y >> (8 * i)) & 0xff;
+    }
+  }
+  static LUX_DEV void load(const uint16_t* p, uint32_t (&v)[8]) {
+    const uint4 w = *reinterpret_cast<const uint4*>(p);
+    const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      v[2 * i] = ws[i] & 0xffff;
+      v[2 * i + 1] = ws[i] >> 16;
+    }
+  }
+  static LUX_DEV void store(uint16_t* p, const uint32_t (&v)[8]) {
+    *reinterpret_cast<uint4*>(p) = make_uint4(v[0] | v[1] << 16, v[2] | v[3] << 16, v[4] | v[5] << 16, v[6] | v[7] << 16);
+  }
+};
 
 // One warp walks one scanline of direction (dx, dy):
 //   L(p, d) = C(p, d) + min(L(q, d), L(q, d - 1) + P1, L(q, d + 1) + P1, m + P2) - m,  m = min_k L(q, k),
 // with q the previous pixel (L = C at the first pixel), and adds L into the path sums (the first direction stores them).
 // The scanline starts are the pixels whose previous pixel lies outside the image: a whole row for dy != 0, then a whole
-// column (less the corner already counted) for dx != 0.
-template <int LPT>
+// column (less the corner already counted) for dx != 0. The next pixel's cost and sums are loaded while this one is
+// computed, so the HBM latency is off the recurrence.
+template <int LPT, bool LAST>
 __global__ void __launch_bounds__(128) k_census_path(const uint8_t* __restrict__ cost, int w, int h, int D, int dx, int dy, uint32_t P1,
-                                                     uint32_t P2, int first, uint16_t* __restrict__ S) {
+                                                     uint32_t P2, int first, uint16_t* __restrict__ S, int subpixel,
+                                                     int* __restrict__ dl, float* __restrict__ disp) {
   constexpr int Dp = 32 * LPT;
+  using IO = LaneIO<LPT>;
   const int lane = threadIdx.x & 31;
   const int line = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int n_row = dy != 0 ? w : 0, n_col = dx != 0 ? h - (dy != 0 ? 1 : 0) : 0;
@@ -80,16 +187,19 @@ __global__ void __launch_bounds__(128) k_census_path(const uint8_t* __restrict__
     const int k = line - n_row;
     y = dy == 0 ? k : (dy > 0 ? k + 1 : k);  // the corner row was started by the row starts
   }
-  uint32_t L[LPT];
+  auto at = [&](int xx, int yy) { return ((size_t)yy * w + xx) * Dp + lane * LPT; };
+  uint32_t L[LPT], c[LPT], sv[LPT];
   uint32_t m = 0;
+  IO::cost(cost + at(x, y), c);
+  if (!first) IO::load(S + at(x, y), sv);
   bool start = true;
-  for (; x >= 0 && x < w && y >= 0 && y < h; x += dx, y += dy) {
-    const size_t p = (size_t)y * w + x;
-    uint32_t c[LPT];
-    {
-      const uint8_t* cp = cost + p * Dp + lane * LPT;
-#pragma unroll
-      for (int i = 0; i < LPT; i++) c[i] = cp[i];
+  for (;;) {
+    const int xn = x + dx, yn = y + dy;
+    const bool more = xn >= 0 && xn < w && yn >= 0 && yn < h;
+    uint32_t cn[LPT], sn[LPT];
+    if (more) {
+      IO::cost(cost + at(xn, yn), cn);
+      if (!first) IO::load(S + at(xn, yn), sn);
     }
     uint32_t nl[LPT];
     if (start) {
@@ -106,53 +216,32 @@ __global__ void __launch_bounds__(128) k_census_path(const uint8_t* __restrict__
         nl[i] = lane * LPT + i < D ? c[i] + t - m : kBig;
       }
     }
-    uint32_t lmin = kBig;
+    uint32_t lmin = kBig, out[LPT];
 #pragma unroll
     for (int i = 0; i < LPT; i++) {
       L[i] = nl[i];
       lmin = min(lmin, nl[i]);
+      out[i] = first ? nl[i] : sv[i] + nl[i];  // padding lanes store don't-care values (never read)
     }
     m = __reduce_min_sync(0xffffffffu, lmin);
-    uint16_t* sp = S + p * Dp + lane * LPT;
+    IO::store(S + at(x, y), out);
+    if (LAST) {  // the path sums of this pixel are final: the winner-take-all here saves reading them again
+      int d;
+      float v;
+      wta_of<LPT>(out, lane, D, subpixel, d, v);
+      if (lane == 0) {
+        dl[(size_t)y * w + x] = d;
+        disp[(size_t)y * w + x] = v;
+      }
+    }
+    if (!more) break;
+    x = xn;
+    y = yn;
 #pragma unroll
     for (int i = 0; i < LPT; i++) {
-      if (lane * LPT + i >= D) continue;
-      sp[i] = (uint16_t)(first ? L[i] : sp[i] + L[i]);
+      c[i] = cn[i];
+      sv[i] = sn[i];
     }
-  }
-}
-
-// The first disparity with the least path sum of a pixel (a warp per pixel), with the parabolic subpixel correction
-// (S[d-1] - S[d+1]) / (2 (S[d-1] - 2 S[d] + S[d+1])) where 0 < d < D - 1 and the denominator is positive.
-template <int LPT>
-__global__ void __launch_bounds__(256) k_census_wta(const uint16_t* __restrict__ S, int npx, int D, int subpixel, int* __restrict__ dl,
-                                                    float* __restrict__ disp) {
-  constexpr int Dp = 32 * LPT;
-  const int lane = threadIdx.x & 31;
-  const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (p >= npx) return;
-  const uint16_t* sp = S + (size_t)p * Dp;
-  uint32_t best = kBig, arg = kBig;
-#pragma unroll
-  for (int i = 0; i < LPT; i++) {
-    const int d = lane * LPT + i;
-    const uint32_t v = d < D ? sp[d] : kBig;
-    if (v < best) {
-      best = v;
-      arg = d;
-    }
-  }
-  const uint32_t m = __reduce_min_sync(0xffffffffu, best);
-  const uint32_t d = __reduce_min_sync(0xffffffffu, best == m ? arg : kBig);
-  if (lane == 0) {
-    float out = (float)d;
-    if (subpixel && d > 0 && (int)d < D - 1) {
-      const float a = sp[d - 1], b = sp[d], c = sp[d + 1];
-      const float den = __fmul_rn(2.0f, __fadd_rn(__fsub_rn(a, __fmul_rn(2.0f, b)), c));
-      if (den > 0.0f) out = __fadd_rn(out, __fdiv_rn(__fsub_rn(a, c), den));
-    }
-    dl[p] = (int)d;
-    disp[p] = out;
   }
 }
 
@@ -216,11 +305,13 @@ void paths_and_wta(const uint8_t* cost, int w, int h, int D, uint32_t P1, uint32
   for (int k = 0; k < 8; k++) {
     const int dx = dirs[k][0], dy = dirs[k][1];
     const int lines = (dy != 0 ? w : 0) + (dx != 0 ? h - (dy != 0 ? 1 : 0) : 0);
-    k_census_path<LPT><<<(lines + 3) / 4, 128, 0, s>>>(cost, w, h, D, dx, dy, P1, P2, k == 0 ? 1 : 0, S);
+    if (k == 7)
+      k_census_path<LPT, true><<<(lines + 3) / 4, 128, 0, s>>>(cost, w, h, D, dx, dy, P1, P2, 0, S, subpixel, dl, disp);
+    else
+      k_census_path<LPT, false><<<(lines + 3) / 4, 128, 0, s>>>(cost, w, h, D, dx, dy, P1, P2, k == 0 ? 1 : 0, S, subpixel, dl, disp);
   }
   const int npx = w * h;
-  k_census_wta<LPT><<<(npx + 7) / 8, 256, 0, s>>>(S, npx, D, subpixel, dl, disp);
-  count_launches(9);
+  count_launches(8);
   if (lr) {
     k_census_wta_right<LPT><<<(npx + 7) / 8, 256, 0, s>>>(S, w, h, D, dr);
     k_census_lr<<<(npx + 255) / 256, 256, 0, s>>>(dl, dr, w, h, max_diff, disp);
@@ -235,18 +326,30 @@ int census_lpt(int D) { return D <= 32 ? 1 : D <= 64 ? 2 : D <= 128 ? 4 : D <= 2
 void launch_census_sgm(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int bpp, int D, uint32_t P1, uint32_t P2,
                        int subpixel, int lr, int max_diff, uint64_t* cl, uint64_t* cr, uint8_t* cost, uint16_t* S, int* dl, int* dr,
                        float* disp, cudaStream_t s) {
-  const int lpt = census_lpt(D), Dp = 32 * lpt;
+  const int lpt = census_lpt(D);
   const dim3 b2(32, 8), g2((w + 31) / 32, (h + 7) / 8);
   k_census<<<g2, b2, 0, s>>>(left, w, h, stride, bpp, cl);
   k_census<<<g2, b2, 0, s>>>(right, w, h, stride, bpp, cr);
-  k_hamming<<<dim3((w + 127) / 128, h, Dp / 8), 128, 0, s>>>(cl, cr, w, h, D, Dp, cost);
-  count_launches(3);
+  const unsigned hblocks = (unsigned)(((long long)w * h + 7) / 8);
   switch (lpt) {
-    case 1: paths_and_wta<1>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s); break;
-    case 2: paths_and_wta<2>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s); break;
-    case 4: paths_and_wta<4>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s); break;
-    default: paths_and_wta<8>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s); break;
+    case 1:
+      k_hamming<1><<<hblocks, 256, 0, s>>>(cl, cr, w, h, D, cost);
+      paths_and_wta<1>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s);
+      break;
+    case 2:
+      k_hamming<2><<<hblocks, 256, 0, s>>>(cl, cr, w, h, D, cost);
+      paths_and_wta<2>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s);
+      break;
+    case 4:
+      k_hamming<4><<<hblocks, 256, 0, s>>>(cl, cr, w, h, D, cost);
+      paths_and_wta<4>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s);
+      break;
+    default:
+      k_hamming<8><<<hblocks, 256, 0, s>>>(cl, cr, w, h, D, cost);
+      paths_and_wta<8>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s);
+      break;
   }
+  count_launches(3);
 }
 
 void launch_fuse(const float* const* disps, const float* fb, int n, int npx, float* out, cudaStream_t s) {
