@@ -289,6 +289,23 @@ def run_lux(a):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if BITS == 0 and world == 1:
+        # the survey's plain comparator of the batched capture: the reference against each module camera alone, one
+        # two-camera solve (its own planes, D_k) after the other, inputs on the device
+        pairs = []
+        for k in range(1, len(wl.images)):
+            imgs_k = [dev_imgs[0], dev_imgs[k]]
+            pairs.append((imgs_k, [wl.gray[0], wl.gray[k]], [wl.calibs[0], wl.calibs[k]]))
+        n_k = [len(api.DenseStereo.planes(wl.near, wl.far, c, wl.params.plane_density, 8)) for _, _, c in pairs]
+
+        def plain_step():
+            for imgs_k, g_k, c_k in pairs:
+                api.DenseLayer.compute(imgs_k, g_k, c_k, wl.near, wl.far, wl.params, prefilter=True, ctx=ctx).close()
+        ms_p, _, _ = timed(plain_step, a.steps)
+        de_p = sum(W_ * H_ * n for n in n_k)
+        out["config"]["plain_pairs"] = {"solves": len(pairs), "planes": n_k, "ms_per_capture": ms_p / a.steps,
+                                        "mde_per_s": de_p * a.steps / (ms_p / 1e3) / 1e6,
+                                        "note": "ten 2-camera layers one after another (sum of W·H·D_k per second)"}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, dt, de_s = cpu_sample(wl, a.cpu_rows, threads)
