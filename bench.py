@@ -75,6 +75,8 @@ def args_():
                         "and the 4160x3120 reference guide's 8-bit warp")
     p.add_argument("--census", action="store_true",
                    help="the opt-in census mode (census, Hamming, 8-path SGM, WTA + subpixel + left/right) on the workload's pair")
+    p.add_argument("--census-capture", action="store_true",
+                   help="the census mode over a capture of 10 pairs (2080x1560, D in 64..192) batched, against the pairs one by one")
     p.add_argument("--cpu-rows", type=int, default=130, help="rows of the CPU sample strip")
     p.add_argument("--workload", default="pair13mp", choices=sorted(WORKLOADS),
                    help="pair13mp is the benchmark; the smaller pairs are for profiling captures")
@@ -752,8 +754,76 @@ def run_census(a):
     ctx.close()
 
 
+def run_census_capture(a):
+    """The census mode over one capture: 10 pairs on a 2080x1560 reference grid with D cycling 64, 96, 128, 192, images in
+    HBM. Batched: one lux_census_capture (every stage one launch over all pairs, the reference's census once, then the
+    fusion). Plain: ten lux_census_sgm solves one after another, then lux_fuse_disparities. value = Σ W·H·D_k per second
+    of the batched form."""
+    import torch
+    from lux_b200 import _lib, api, synth
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    w, h = 2080, 1560
+    ds = [(64, 96, 128, 192)[k % 4] for k in range(10)]
+    ref, others, fb = synth.census_capture(w, h, ds, seed=11)
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(lib.lux_sgm_stream(ctx.handle), device=torch.device("cuda", 0))
+    rgba = lambda im: torch.from_numpy(np.repeat(im[..., None], 4, axis=2)).cuda()
+    d_ref, d_oth = rgba(ref), [rgba(o) for o in others]
+    img = lambda t: _lib.Img(t.data_ptr(), w, h, w, 1)
+    c_ref = img(d_ref)
+    c_oth = (_lib.Img * len(d_oth))(*[img(t) for t in d_oth])
+    dsa = np.asarray(ds, np.int32)
+    prm = _lib.CensusParams(0, 10, 120, 1, 1, 1)
+    depth = torch.empty((h, w), dtype=torch.float32, device="cuda")
+    disps = [torch.empty((h, w), dtype=torch.float32, device="cuda") for _ in ds]
+    dptrs = (ctypes.c_void_p * len(ds))(*[t.data_ptr() for t in disps])
+    torch.cuda.synchronize()
+
+    def batched():
+        ctx.check(lib.lux_census_capture(ctx.handle, len(ds), ctypes.byref(c_ref), c_oth, dsa.ctypes.data, fb.ctypes.data,
+                                         ctypes.byref(prm), depth.data_ptr(), 1, None))
+
+    def plain():
+        for k, d in enumerate(ds):
+            pk = _lib.CensusParams(d, 10, 120, 1, 1, 1)
+            ctx.check(lib.lux_census_sgm(ctx.handle, ctypes.byref(c_ref), ctypes.byref(c_oth[k]), ctypes.byref(pk), disps[k].data_ptr(), 1))
+        ctx.check(lib.lux_fuse_disparities(ctx.handle, dptrs, fb.ctypes.data, len(ds), w, h, 1, depth.data_ptr(), 1))
+
+    def timed(fn, k):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        n0 = api.kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k, (api.kernel_launches() - n0) // k
+
+    with ClockSampler(0) as clk:
+        ms_b, lb = timed(batched, a.steps)
+    ms_p, lp = timed(plain, a.steps)
+    de = sum(w * h * d for d in ds)
+    print(json.dumps({"metric": "census capture MDE/s (Σ W·H·D_k per second), 10 pairs 2080x1560, batched", "value": de / (ms_b / 1e3) / 1e6,
+                      "unit": "MDE/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_b, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "u8 cost / u16 aggregation", "data": "synthetic",
+                      "config": {"workload": f"census capture: 10 pairs {w}x{h} on the reference grid, D {ds}, fused to one depth map",
+                                 "launches_per_capture": {"batched": int(lb), "plain": int(lp)}},
+                      "plain": {"ms_per_capture": ms_p, "mde_per_s": de / (ms_p / 1e3) / 1e6},
+                      "gpu_launches": int(lb) * a.steps, "clocks": clk.summary()}))
+    ctx.close()
+
+
 def main():
     a = args_()
+    if a.census_capture:
+        run_census_capture(a)
+        return
     if a.census:
         run_census(a)
         return

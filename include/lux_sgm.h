@@ -235,6 +235,13 @@ typedef struct {
 } lux_census_params;
 int lux_census_sgm(lux_sgm_ctx* ctx, const lux_img_rgba8* left, const lux_img_rgba8* right, const lux_census_params* params,
                    float* out_disp, int32_t out_on_device);
+/* The census mode over a capture's pairs in one batch: the reference image against others[0..n) (n <= 16, all the
+ * reference's size, on its grid), pair k with disparity range max_disparity[k] and focal x baseline fb[k]; params gives P1,
+ * P2 and the options (its max_disparity is ignored). Every stage is one launch over all pairs (the reference's census is
+ * made once); the pairs' disparities are fused as lux_fuse_disparities fuses them into out_depth. out_disps, when not
+ * NULL, receives the n disparity maps (host, n x w x h floats). */
+int lux_census_capture(lux_sgm_ctx* ctx, int32_t n, const lux_img_rgba8* ref, const lux_img_rgba8* others, const int32_t* max_disparity,
+                       const float* fb, const lux_census_params* params, float* out_depth, int32_t out_on_device, float* out_disps);
 /* The fusion of a capture's pairs: per pair the depth fb[k] / disparity where the disparity is positive, per pixel the
  * median of the valid depths (the mean of the two middle ones for an even count), 0 where none is valid. disps: n <= 16
  * pointers to w x h disparity maps (device pointers when on_device, else host). */

@@ -117,6 +117,8 @@ SIGNATURES = [
                                                  ctypes.POINTER(Calib), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     ("lux_census_sgm", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Img), ctypes.POINTER(Img), ctypes.POINTER(CensusParams),
                                       ctypes.c_void_p, ctypes.c_int32]),
+    ("lux_census_capture", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Img), ctypes.POINTER(Img), ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.POINTER(CensusParams), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     ("lux_fuse_disparities", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_int32,
                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]),
     ("lux_warp_rgba8", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Img), ctypes.POINTER(AlignedCalib), ctypes.c_int32,

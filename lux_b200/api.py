@@ -638,6 +638,34 @@ class CensusStereo:
         return out
 
     @staticmethod
+    def capture(ref, others, max_disparities, fbs, p1=10, p2=120, subpixel=True, lr_check=True, lr_max_diff=1,
+                ctx: Optional[Context] = None):
+        """A capture's pairs in one batch (the reference image against each other image, all on the reference's grid):
+        (fused (h, w) float32 depth, (n, h, w) float32 disparities)."""
+        ctx = ctx or default_context()
+
+        def rgba(im):
+            if not hasattr(im, "data_ptr") and np.asarray(im).ndim == 2:
+                return np.repeat(np.asarray(im, np.uint8)[..., None], 4, axis=2)
+            return im
+        cr, kr = _img_c(rgba(ref))
+        oth = (L.Img * len(others))()
+        keep = []
+        for i, im in enumerate(others):
+            ci, k = _img_c(rgba(im))
+            oth[i] = ci
+            keep.append(k)
+        ds = np.ascontiguousarray(np.asarray(max_disparities, np.int32))
+        fb = np.ascontiguousarray(np.asarray(fbs, np.float32))
+        prm = L.CensusParams(0, int(p1), int(p2), 1 if subpixel else 0, 1 if lr_check else 0, int(lr_max_diff))
+        depth = np.empty((cr.h, cr.w), np.float32)
+        disps = np.empty((len(others), cr.h, cr.w), np.float32)
+        _torch_ready(ref, *others)
+        ctx.check(ctx.lib.lux_census_capture(ctx.handle, len(others), ctypes.byref(cr), oth, ds.ctypes.data, fb.ctypes.data,
+                                             ctypes.byref(prm), depth.ctypes.data, 0, disps.ctypes.data))
+        return depth, disps
+
+    @staticmethod
     def fuse(disps, fbs, ctx: Optional[Context] = None):
         """The median depth over the pairs' valid disparities (fB / d for d > 0), 0 where none is valid."""
         ctx = ctx or default_context()

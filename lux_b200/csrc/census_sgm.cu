@@ -80,9 +80,12 @@ __global__ void k_census(const uint8_t* __restrict__ img, int w, int h, int stri
 // C(x, y, d) = popcount(L(x, y) ^ R(x - d, y)), 62 where x - d < 0. A warp per pixel, lane j making disparities j, j + 32,
 // ...: each load instruction reads 32 neighbouring right-image words and each store writes 32 consecutive cost bytes.
 template <int LPT>
-__global__ void __launch_bounds__(256) k_hamming(const uint64_t* __restrict__ cl, const uint64_t* __restrict__ cr, int w, int h, int D,
-                                                 uint8_t* __restrict__ cost) {
+__global__ void __launch_bounds__(256) k_hamming(const uint64_t* __restrict__ cl, const CensusPairs ps, int w, int h) {
   constexpr int Dp = 32 * LPT;
+  const CensusPair& pr = ps.p[blockIdx.y];  // one grid row per pair of the batch
+  const uint64_t* __restrict__ cr = pr.cr;
+  uint8_t* __restrict__ cost = pr.cost;
+  const int D = pr.D;
   const int lane = threadIdx.x & 31;
   const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (p >= w * h) return;
@@ -169,10 +172,15 @@ struct LaneIO<8> {
 // column (less the corner already counted) for dx != 0. The next pixel's cost and sums are loaded while this one is
 // computed, so the HBM latency is off the recurrence.
 template <int LPT, bool LAST>
-__global__ void __launch_bounds__(128) k_census_path(const uint8_t* __restrict__ cost, int w, int h, int D, int dx, int dy, uint32_t P1,
-                                                     uint32_t P2, int first, uint16_t* __restrict__ S, int subpixel,
-                                                     int* __restrict__ dl, float* __restrict__ disp) {
+__global__ void __launch_bounds__(128) k_census_path(const CensusPairs ps, int w, int h, int dx, int dy, uint32_t P1, uint32_t P2,
+                                                     int first, int subpixel) {
   constexpr int Dp = 32 * LPT;
+  const CensusPair& pr = ps.p[blockIdx.y];  // one grid row per pair of the batch
+  const uint8_t* __restrict__ cost = pr.cost;
+  uint16_t* __restrict__ S = pr.S;
+  int* __restrict__ dl = pr.dl;
+  float* __restrict__ disp = pr.disp;
+  const int D = pr.D;
   using IO = LaneIO<LPT>;
   const int lane = threadIdx.x & 31;
   const int line = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -247,8 +255,12 @@ __global__ void __launch_bounds__(128) k_census_path(const uint8_t* __restrict__
 
 // The right image's first minimum over d of S(x + d, y, d), x + d < W (a warp per right-image pixel).
 template <int LPT>
-__global__ void __launch_bounds__(256) k_census_wta_right(const uint16_t* __restrict__ S, int w, int h, int D, int* __restrict__ dr) {
+__global__ void __launch_bounds__(256) k_census_wta_right(const CensusPairs ps, int w, int h) {
   constexpr int Dp = 32 * LPT;
+  const CensusPair& pr = ps.p[blockIdx.y];
+  const uint16_t* __restrict__ S = pr.S;
+  int* __restrict__ dr = pr.dr;
+  const int D = pr.D;
   const int lane = threadIdx.x & 31;
   const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (p >= w * h) return;
@@ -269,7 +281,11 @@ __global__ void __launch_bounds__(256) k_census_wta_right(const uint16_t* __rest
 }
 
 // Left/right consistency: a pixel keeps its disparity when |d(x) - d_R(x - d(x))| <= max_diff, else -1.
-__global__ void k_census_lr(const int* __restrict__ dl, const int* __restrict__ dr, int w, int h, int max_diff, float* __restrict__ disp) {
+__global__ void k_census_lr(const CensusPairs ps, int w, int h, int max_diff) {
+  const CensusPair& pr = ps.p[blockIdx.y];
+  const int* __restrict__ dl = pr.dl;
+  const int* __restrict__ dr = pr.dr;
+  float* __restrict__ disp = pr.disp;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= w * h) return;
   const int y = p / w, x = p - y * w, d = dl[p], xr = x - d;
@@ -299,22 +315,22 @@ __global__ void k_fuse(const float* const* __restrict__ disps, const float* __re
 }
 
 template <int LPT>
-void paths_and_wta(const uint8_t* cost, int w, int h, int D, uint32_t P1, uint32_t P2, int subpixel, int lr, int max_diff,
-                   uint16_t* S, int* dl, int* dr, float* disp, cudaStream_t s) {
+void batch_stages(const uint64_t* cl, const CensusPairs& ps, int n, int w, int h, uint32_t P1, uint32_t P2, int subpixel, int lr,
+                  int max_diff, cudaStream_t s) {
+  const int npx = w * h;
+  k_hamming<LPT><<<dim3((unsigned)((npx + 7) / 8), n), 256, 0, s>>>(cl, ps, w, h);
   static const int dirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {1, -1}, {-1, 1}};
   for (int k = 0; k < 8; k++) {
     const int dx = dirs[k][0], dy = dirs[k][1];
     const int lines = (dy != 0 ? w : 0) + (dx != 0 ? h - (dy != 0 ? 1 : 0) : 0);
-    if (k == 7)
-      k_census_path<LPT, true><<<(lines + 3) / 4, 128, 0, s>>>(cost, w, h, D, dx, dy, P1, P2, 0, S, subpixel, dl, disp);
-    else
-      k_census_path<LPT, false><<<(lines + 3) / 4, 128, 0, s>>>(cost, w, h, D, dx, dy, P1, P2, k == 0 ? 1 : 0, S, subpixel, dl, disp);
+    const dim3 grid((lines + 3) / 4, n);
+    if (k == 7) k_census_path<LPT, true><<<grid, 128, 0, s>>>(ps, w, h, dx, dy, P1, P2, 0, subpixel);
+    else k_census_path<LPT, false><<<grid, 128, 0, s>>>(ps, w, h, dx, dy, P1, P2, k == 0 ? 1 : 0, subpixel);
   }
-  const int npx = w * h;
-  count_launches(8);
+  count_launches(9);
   if (lr) {
-    k_census_wta_right<LPT><<<(npx + 7) / 8, 256, 0, s>>>(S, w, h, D, dr);
-    k_census_lr<<<(npx + 255) / 256, 256, 0, s>>>(dl, dr, w, h, max_diff, disp);
+    k_census_wta_right<LPT><<<dim3((npx + 7) / 8, n), 256, 0, s>>>(ps, w, h);
+    k_census_lr<<<dim3((npx + 255) / 256, n), 256, 0, s>>>(ps, w, h, max_diff);
     count_launches(2);
   }
 }
@@ -323,33 +339,26 @@ void paths_and_wta(const uint8_t* cost, int w, int h, int D, uint32_t P1, uint32
 
 int census_lpt(int D) { return D <= 32 ? 1 : D <= 64 ? 2 : D <= 128 ? 4 : D <= 256 ? 8 : 0; }
 
-void launch_census_sgm(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int bpp, int D, uint32_t P1, uint32_t P2,
-                       int subpixel, int lr, int max_diff, uint64_t* cl, uint64_t* cr, uint8_t* cost, uint16_t* S, int* dl, int* dr,
-                       float* disp, cudaStream_t s) {
-  const int lpt = census_lpt(D);
+void launch_census_batch(const uint8_t* ref, const uint8_t* const* others, int n, int w, int h, int stride, int bpp, uint32_t P1,
+                         uint32_t P2, int subpixel, int lr, int max_diff, uint64_t* cl, const CensusPairs& ps, cudaStream_t s) {
   const dim3 b2(32, 8), g2((w + 31) / 32, (h + 7) / 8);
-  k_census<<<g2, b2, 0, s>>>(left, w, h, stride, bpp, cl);
-  k_census<<<g2, b2, 0, s>>>(right, w, h, stride, bpp, cr);
-  const unsigned hblocks = (unsigned)(((long long)w * h + 7) / 8);
-  switch (lpt) {
-    case 1:
-      k_hamming<1><<<hblocks, 256, 0, s>>>(cl, cr, w, h, D, cost);
-      paths_and_wta<1>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s);
-      break;
-    case 2:
-      k_hamming<2><<<hblocks, 256, 0, s>>>(cl, cr, w, h, D, cost);
-      paths_and_wta<2>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s);
-      break;
-    case 4:
-      k_hamming<4><<<hblocks, 256, 0, s>>>(cl, cr, w, h, D, cost);
-      paths_and_wta<4>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s);
-      break;
-    default:
-      k_hamming<8><<<hblocks, 256, 0, s>>>(cl, cr, w, h, D, cost);
-      paths_and_wta<8>(cost, w, h, D, P1, P2, subpixel, lr, max_diff, S, dl, dr, disp, s);
-      break;
+  k_census<<<g2, b2, 0, s>>>(ref, w, h, stride, bpp, cl);  // the reference's census, shared by every pair
+  for (int k = 0; k < n; k++) k_census<<<g2, b2, 0, s>>>(others[k], w, h, stride, bpp, ps.p[k].cr);
+  count_launches(1 + n);
+  // the pairs grouped by lane width (disparities a lane), one launch per stage and group
+  for (const int lpt : {1, 2, 4, 8}) {
+    CensusPairs grp{};
+    int m = 0;
+    for (int k = 0; k < n; k++)
+      if (census_lpt(ps.p[k].D) == lpt) grp.p[m++] = ps.p[k];
+    if (m == 0) continue;
+    switch (lpt) {
+      case 1: batch_stages<1>(cl, grp, m, w, h, P1, P2, subpixel, lr, max_diff, s); break;
+      case 2: batch_stages<2>(cl, grp, m, w, h, P1, P2, subpixel, lr, max_diff, s); break;
+      case 4: batch_stages<4>(cl, grp, m, w, h, P1, P2, subpixel, lr, max_diff, s); break;
+      default: batch_stages<8>(cl, grp, m, w, h, P1, P2, subpixel, lr, max_diff, s); break;
+    }
   }
-  count_launches(3);
 }
 
 void launch_fuse(const float* const* disps, const float* fb, int n, int npx, float* out, cudaStream_t s) {

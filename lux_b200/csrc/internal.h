@@ -91,11 +91,24 @@ struct ColourF {  // a row-major 4x4 colour transfer (StereoColorTransfer.Solve)
 // census_sgm.cu: the opt-in census stereo mode (census, Hamming cost, 8-path SGM, WTA, subpixel, left/right, fusion)
 constexpr int kMaxFusePairs = 16;
 int census_lpt(int D);  // disparities per lane: 1, 2, 4 or 8 for D up to 32, 64, 128, 256 (0: too large)
-// left / right: grey pixels at byte 0 of every bpp bytes, rows stride pixels apart; cl, cr: W x H; cost, S: W x H x
-// 32·census_lpt(D); dl, dr: W x H; disp: W x H floats.
-void launch_census_sgm(const uint8_t* left, const uint8_t* right, int w, int h, int stride, int bpp, int D, uint32_t P1, uint32_t P2,
-                       int subpixel, int lr, int max_diff, uint64_t* cl, uint64_t* cr, uint8_t* cost, uint16_t* S, int* dl, int* dr,
-                       float* disp, cudaStream_t s);
+// One pair of a batch: the other image's census (W x H), its cost and path sums (W x H x 32·census_lpt(D)),
+// its left and right integer disparities and its float disparities (W x H), and its disparity range D.
+struct CensusPair {
+  uint64_t* cr;
+  uint8_t* cost;
+  uint16_t* S;
+  int *dl, *dr;
+  float* disp;
+  int D;
+};
+struct CensusPairs {
+  CensusPair p[kMaxFusePairs];
+};
+// n pairs (<= kMaxFusePairs) of the reference image against others[k] (device pointers), all W x H; grey at byte 0 of
+// every bpp bytes, rows stride pixels apart; pair k's buffers are laid out with 32·census_lpt(D_k) values a pixel; cl:
+// the reference's census (W x H). One launch per stage covers every pair of the same lane width.
+void launch_census_batch(const uint8_t* ref, const uint8_t* const* others, int n, int w, int h, int stride, int bpp, uint32_t P1,
+                         uint32_t P2, int subpixel, int lr, int max_diff, uint64_t* cl, const CensusPairs& ps, cudaStream_t s);
 // disps: a device array of n device pointers to W x H disparity maps (n <= kMaxFusePairs); fb: n focal x baseline products.
 void launch_fuse(const float* const* disps, const float* fb, int n, int npx, float* out, cudaStream_t s);
 

@@ -977,37 +977,90 @@ extern "C" int lux_stereo_image_transfer(lux_sgm_ctx* ctx, const float* src, int
   return rc;
 }
 
+namespace {
+
+// The census mode over n pairs (the reference image against others[0..n)) on the context's stream: per pair device
+// buffers in tmp, disparities in pairs.p[k].disp. Validates the arguments as the public calls document.
+int census_batch(lux_sgm_ctx* ctx, std::vector<DevBuf>& tmp, int n, const lux_img_rgba8& ref, const lux_img_rgba8* others,
+                 const int32_t* Ds, uint32_t p1, uint32_t p2, int subpixel, int lr, int max_diff, CensusPairs& pairs) {
+  if (n < 1 || n > kMaxFusePairs) return set_err(ctx, LUX_ERR_ARG, "census: 1 to 16 pairs");
+  if (p2 > 8129 || p1 > 8129) return set_err(ctx, LUX_ERR_ARG, "census: P1/P2 too large, path sums would pass 16 bits");
+  for (int k = 0; k < n; k++) {
+    if (others[k].w != ref.w || others[k].h != ref.h) return set_err(ctx, LUX_ERR_ARG, "census: the two images differ in size");
+    if (Ds[k] < 1 || Ds[k] > 256) return set_err(ctx, LUX_ERR_ARG, "census: max_disparity must be 1..256");
+  }
+  const int w = ref.w, h = ref.h;
+  const size_t npx = (size_t)w * h;
+  const uint8_t* d_ref = nullptr;
+  std::vector<const uint8_t*> d_oth(n);
+  uint64_t* cl = nullptr;
+  int rc = upload_image(ctx, tmp, ref, &d_ref);
+  if (!rc) rc = alloc_t(ctx, tmp, npx, &cl);
+  for (int k = 0; k < n && !rc; k++) {
+    CensusPair& pr = pairs.p[k];
+    pr.D = Ds[k];
+    const size_t Dp = 32 * (size_t)census_lpt(Ds[k]);
+    if (!rc) rc = upload_image(ctx, tmp, others[k], &d_oth[k]);
+    if (!rc) rc = alloc_t(ctx, tmp, npx, &pr.cr);
+    if (!rc) rc = alloc_t(ctx, tmp, npx * Dp, &pr.cost);
+    if (!rc) rc = alloc_t(ctx, tmp, npx * Dp, &pr.S);
+    if (!rc) rc = alloc_t(ctx, tmp, npx, &pr.dl);
+    if (!rc) rc = alloc_t(ctx, tmp, npx, &pr.dr);
+    if (!rc) rc = alloc_t(ctx, tmp, npx, &pr.disp);
+  }
+  if (rc) return rc;
+  launch_census_batch(d_ref, d_oth.data(), n, w, h, w, 4, p1, p2, subpixel, lr, max_diff, cl, pairs, ctx->stream);
+  CK(cudaGetLastError());
+  return LUX_OK;
+}
+
+}  // namespace
+
 extern "C" int lux_census_sgm(lux_sgm_ctx* ctx, const lux_img_rgba8* left, const lux_img_rgba8* right, const lux_census_params* p,
                               float* out_disp, int32_t out_on_device) {
   if (!ctx) return LUX_ERR_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (!left || !right || !p || !out_disp) return set_err(ctx, LUX_ERR_ARG, "census: null pointer");
-  if (left->w != right->w || left->h != right->h) return set_err(ctx, LUX_ERR_ARG, "census: the two images differ in size");
-  if (p->max_disparity < 1 || p->max_disparity > 256) return set_err(ctx, LUX_ERR_ARG, "census: max_disparity must be 1..256");
-  if (p->p2 > 8129 || p->p1 > 8129) return set_err(ctx, LUX_ERR_ARG, "census: P1/P2 too large, path sums would pass 16 bits");
   cudaSetDevice(ctx->device);
-  const int w = left->w, h = left->h, D = p->max_disparity, Dp = 32 * census_lpt(D);
-  const size_t npx = (size_t)w * h;
   std::vector<DevBuf> tmp;
-  const uint8_t *dl_img = nullptr, *dr_img = nullptr;
-  uint64_t *cl = nullptr, *cr = nullptr;
-  uint8_t* cost = nullptr;
-  uint16_t* S = nullptr;
-  int *dl = nullptr, *dr = nullptr;
-  int rc = upload_image(ctx, tmp, *left, &dl_img);
-  if (!rc) rc = upload_image(ctx, tmp, *right, &dr_img);
-  if (!rc) rc = alloc_t(ctx, tmp, npx, &cl);
-  if (!rc) rc = alloc_t(ctx, tmp, npx, &cr);
-  if (!rc) rc = alloc_t(ctx, tmp, npx * Dp, &cost);
-  if (!rc) rc = alloc_t(ctx, tmp, npx * Dp, &S);
-  if (!rc) rc = alloc_t(ctx, tmp, npx, &dl);
-  if (!rc) rc = alloc_t(ctx, tmp, npx, &dr);
-  if (!rc)
-    rc = to_output(ctx, tmp, out_disp, npx, out_on_device, [&](float* d) {
-      launch_census_sgm(dl_img, dr_img, w, h, w, 4, D, p->p1, p->p2, p->subpixel, p->lr_check, p->lr_max_diff, cl, cr, cost, S, dl, dr, d,
-                        ctx->stream);
-    });
-  if (!rc) CK(cudaStreamSynchronize(ctx->stream));
+  CensusPairs pairs{};
+  const int32_t D = p->max_disparity;
+  int rc = census_batch(ctx, tmp, 1, *left, right, &D, p->p1, p->p2, p->subpixel, p->lr_check, p->lr_max_diff, pairs);
+  const size_t npx = (size_t)left->w * left->h;
+  if (!rc) {
+    CK(cudaMemcpyAsync(out_disp, pairs.p[0].disp, npx * 4, out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
+extern "C" int lux_census_capture(lux_sgm_ctx* ctx, int32_t n, const lux_img_rgba8* ref, const lux_img_rgba8* others,
+                                  const int32_t* max_disparity, const float* fb, const lux_census_params* p, float* out_depth,
+                                  int32_t out_on_device, float* out_disps) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ref || !others || !max_disparity || !fb || !p || !out_depth) return set_err(ctx, LUX_ERR_ARG, "census capture: null pointer");
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  CensusPairs pairs{};
+  int rc = census_batch(ctx, tmp, n, *ref, others, max_disparity, p->p1, p->p2, p->subpixel, p->lr_check, p->lr_max_diff, pairs);
+  const size_t npx = (size_t)ref->w * ref->h;
+  const float** d_list = nullptr;
+  float* d_fb = nullptr;
+  if (!rc) rc = alloc_t(ctx, tmp, (size_t)n, &d_list);
+  if (!rc) rc = alloc_t(ctx, tmp, (size_t)n, &d_fb);
+  if (!rc) {
+    std::vector<const float*> lst(n);
+    for (int k = 0; k < n; k++) lst[k] = pairs.p[k].disp;
+    CK(cudaMemcpyAsync(d_list, lst.data(), n * sizeof(float*), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_fb, fb, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    rc = to_output(ctx, tmp, out_depth, npx, out_on_device, [&](float* d) { launch_fuse(d_list, d_fb, n, (int)npx, d, ctx->stream); });
+    if (!rc && out_disps)
+      for (int k = 0; k < n; k++)
+        CK(cudaMemcpyAsync(out_disps + (size_t)k * npx, pairs.p[k].disp, npx * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
   dev_free_all(ctx, tmp);
   return rc;
 }

@@ -285,3 +285,16 @@ def aligned_calib(sw, sh, dw, dh, seed=0, angle_deg=0.6, focal_ratio=1.02, shift
     s = np.float32(3000.0 / half_diag)
     from .api import AlignedCalib
     return AlignedCalib(H=H, lut=lut, cx=np.float32(sw / 2.0), cy=np.float32(sh / 2.0), sx=s, sy=s)
+
+
+def census_capture(w, h, ds, seed=0, f=1000.0):
+    """A capture for the census mode: one reference image and one other image per pair on the reference's grid, pair k
+    seeing a scene whose disparities span 0..ds[k]-1 (its baseline B_k = ds[k] units, so fb[k] = f·B_k). Returns
+    (reference (h, w) uint8, [others (h, w) uint8], fb float32 array)."""
+    left = np.rint(texture(h, w, seed, 255.0))
+    shape = planar_disparity(h, w, 1.0, seed)  # a common scene depth structure, scaled per pair
+    others = []
+    for k, d in enumerate(ds):
+        others.append(warp_other(left, shape * (d - 1), seed + 31 * (k + 1), 2.0, 255.0).astype(np.uint8))
+    ref = np.clip(left + np.random.default_rng(seed + 7).standard_normal((h, w)) * 2.0, 0, 255).round().astype(np.uint8)
+    return ref, others, np.asarray([f * d for d in ds], np.float32)

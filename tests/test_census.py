@@ -89,3 +89,20 @@ def test_census_errors():
             api.CensusStereo.compute(left, right, d, **kw)
     with pytest.raises(api.LuxError):
         api.CensusStereo.compute(left, right[:, :20].copy(), 16)
+
+
+@pytest.mark.gpu
+def test_census_capture_batch_matches_pairs():
+    """A capture's pairs in one batch (one launch per stage over every pair, the reference's census made once) give each
+    pair's disparities exactly as a solve of that pair alone, and the fused depth of the oracle."""
+    from lux_b200 import api, synth
+    ds = [64, 24, 40, 96]
+    ref, others, fb = synth.census_capture(90, 56, ds, seed=5)
+    depth, disps = api.CensusStereo.capture(ref, others, ds, fb)
+    want = [C.census_sgm(ref, o, d, 10, 120) for o, d in zip(others, ds)]
+    for k in range(len(ds)):
+        assert np.array_equal(disps[k].view(np.uint32), want[k].view(np.uint32)), k
+        alone = api.CensusStereo.compute(ref, others[k], ds[k])
+        assert np.array_equal(alone.view(np.uint32), want[k].view(np.uint32)), k
+    assert np.array_equal(depth.view(np.uint32), C.fuse(want, fb).view(np.uint32))
+    assert (depth > 0).mean() > 0.5
