@@ -77,6 +77,9 @@ def args_():
                    help="the opt-in census mode (census, Hamming, 8-path SGM, WTA + subpixel + left/right) on the workload's pair")
     p.add_argument("--census-capture", action="store_true",
                    help="the census mode over a capture of 10 pairs (2080x1560, D in 64..192) batched, against the pairs one by one")
+    p.add_argument("--pyramid", action="store_true",
+                   help="the reference's whole dense job for a capture: DenseStereoPyramid.Run (six L16 layers) on five "
+                        "2080x1560 colour cameras, then the upsample to 4160x3120")
     p.add_argument("--cpu-rows", type=int, default=130, help="rows of the CPU sample strip")
     p.add_argument("--workload", default="pair13mp", choices=sorted(WORKLOADS),
                    help="pair13mp is the benchmark; the smaller pairs are for profiling captures")
@@ -819,8 +822,70 @@ def run_census_capture(a):
     ctx.close()
 
 
+def run_pyramid(a):
+    """DenseStereoPyramid.Run (DenseStereoSgm.cs:331-353) on a capture's reference group — five 2080x1560 colour cameras
+    (the finest layer is 2080x1560, as in StereoAsyncApi.State4And5) — then DenseUpsampleLayer.Run to 4160x3120 with a
+    guide: the reference's whole dense job for one capture. Images on the device; value = captures per second; the
+    per-layer device times (cost, aggregation, WTA) and kernels are reported."""
+    import torch
+    from lux_b200 import api, synth
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    w, h = 2080, 1560
+    cap = synth.capture(w, h, 5, seed=3)
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(lib.lux_sgm_stream(ctx.handle), device=torch.device("cuda", 0))
+    d_imgs = [torch.from_numpy(im).cuda() for im in cap.images]
+    guide = torch.from_numpy(np.random.default_rng(4).integers(0, 256, (2 * h, 2 * w, 4), dtype=np.uint8)).cuda()
+    torch.cuda.synchronize()
+    info = []
+
+    def step():
+        layers = api.DenseStereoPyramid.run(d_imgs, cap.gray, cap.calibs, cap.near, cap.far, ctx=ctx)
+        top = layers[-1]
+        info[:] = [(L.W, L.H, L.n_planes, L.sgm_kernel, L.cost_kernel, L.gpu_ms_cost, L.gpu_ms_sgm, L.gpu_ms_wta, L.volume / (L.W * L.H))
+                   for L in layers]
+        depth_ptr = top.device_ptr(0)
+        out = torch.empty((2 * h, 2 * w), dtype=torch.float32, device="cuda")
+        gi = api.L.Img(guide.data_ptr(), 2 * w, 2 * h, 2 * w, 1)
+        ctx.check(lib.lux_sgm_upsample(ctx.handle, depth_ptr, top.W, top.H, 1, ctypes.byref(gi), w, h, 12.0, 2, None,
+                                       out.data_ptr(), None))
+        for L in layers:
+            L.close()
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    n0 = api.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        e0.record(stream)
+        for _ in range(a.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    de = sum(W * H * n for (W, H, n, *_) in info)
+    print(json.dumps({"metric": "capture dense jobs/s (DenseStereoPyramid.Run + upsample), 5 cameras 2080x1560", "value": 1e3 / ms,
+                      "unit": "captures/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 cost / u16 aggregation",
+                      "data": "synthetic (colour capture, planar scene 0.4-6 m, 8-40 mm baselines)",
+                      "config": {"workload": "L16 pyramid on 5 colour cameras 2080x1560 + upsample to 4160x3120",
+                                 "layers": [{"w": W, "h": H, "planes": n, "mean_cap": round(mc, 1), "sgm_kernel": sk, "cost_kernel": ck,
+                                             "ms_cost": round(c, 3), "ms_sgm": round(g, 3), "ms_wta": round(t, 3)}
+                                            for (W, H, n, sk, ck, c, g, t, mc) in info],
+                                 "mde_per_s": de / (ms / 1e3) / 1e6},
+                      "gpu_launches": int(api.kernel_launches() - n0), "clocks": clk.summary()}))
+    ctx.close()
+
+
 def main():
     a = args_()
+    if a.pyramid:
+        run_pyramid(a)
+        return
     if a.census_capture:
         run_census_capture(a)
         return

@@ -11,7 +11,8 @@
 //   * inside a tile, pixel (row r, sheared offset u) runs at step u + 2r. Pixels that share or neighbour a slot (at most
 //     two columns and two rows apart) keep the reference's row-major order; pixels of one step are three or more
 //     columns apart. A revisit of the last column runs alone at step 2r.
-// Within a Pixel() call a warp handles the lanes, and the four paths run in order (a path may spill into the next).
+// Within a Pixel() call a warp handles the lanes. The four paths run in order (a path may spill into the next), or at
+// once on four groups of eight lanes where no window of the call leaves its block.
 #include "common.cuh"
 #include "internal.h"
 
@@ -46,7 +47,116 @@ LUX_DEV int rd(const EmuArgs& a, long long i) {  // Rd (DenseStereoSgm.cs:324)
   return i < 0 ? 2000 : i < a.Llen ? (int)__ldcg(a.L + i) : 0;
 }
 
-// Pixel (DenseStereoSgm.cs:234-317), one warp.
+// One path of a Pixel() call (:276-314) over its cap planes, a lane per plane, each index through Rd's bounds and each
+// write checked: the form for windows that reach past the buffer. Returns the lane's running minimum.
+LUX_DEV int emu_path_checked(const EmuArgs& a, long long nb, long long baseCur, long long q, int cap, int count, bool skipped,
+                             const uint8_t* rawp, uint16_t* aggp, int P2p, int minPrev, int lane) {
+  int runMin = 0xffff;
+  for (int k = lane; k < cap; k += 32) {
+    const long long qi = q + k;
+    const int Lm = rd(a, nb + qi - 1), L0 = rd(a, nb + qi), Lp = rd(a, nb + qi + 1);
+    const int m = min(min(min(Lm + a.p1, 65535), L0), min(min(Lp + a.p1, 65535), P2p));
+    const int rv = skipped ? (k < count ? 0 : 255) : rawp[k];
+    int lc = min(rv + m, 65535) - minPrev;
+    if (lc < 0) lc = 0;
+    const long long wi = baseCur + qi;
+    if (wi < 0 || wi >= a.Llen) atomicCAS(a.err, 0, 7);
+    else __stcg(a.L + wi, (uint16_t)lc);
+    runMin = min(runMin, lc);
+    aggp[k] = (uint16_t)min((int)aggp[k] + lc, 65535);
+  }
+  return runMin;
+}
+
+// The same path where the read window Ln[-1 .. cap] and the write window Lw[0 .. cap) lie inside the buffer and do not
+// meet: KB iterations of the lanes have their loads issued before their stores, one L2 round trip per batch. Caps are
+// multiples of 8 here (checked before the launch).
+template <int KB>
+LUX_DEV int emu_path_batched(const uint16_t* Ln, uint16_t* Lw, int p1, int cap, int count, bool skipped, const uint8_t* rawp,
+                             uint16_t* aggp, int P2p, int minPrev, int lane) {
+  int runMin = 0xffff;
+  for (int k0 = lane; k0 < cap; k0 += 32 * KB) {
+    int Lm[KB], L0[KB], Lp[KB], rv[KB], ag[KB];
+#pragma unroll
+    for (int u = 0; u < KB; u++) {
+      const int k = k0 + 32 * u;
+      if (k < cap) {
+        Lm[u] = __ldcg(Ln + k - 1);
+        L0[u] = __ldcg(Ln + k);
+        Lp[u] = __ldcg(Ln + k + 1);
+        rv[u] = skipped ? (k < count ? 0 : 255) : rawp[k];
+        ag[u] = aggp[k];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < KB; u++) {
+      const int k = k0 + 32 * u;
+      if (k >= cap) break;
+      const int m = min(min(min(Lm[u] + p1, 65535), L0[u]), min(min(Lp[u] + p1, 65535), P2p));
+      int lc = min(rv[u] + m, 65535) - minPrev;
+      if (lc < 0) lc = 0;
+      __stcg(Lw + k, (uint16_t)lc);
+      runMin = min(runMin, lc);
+      aggp[k] = (uint16_t)min(ag[u] + lc, 65535);
+    }
+  }
+  return runMin;
+}
+
+// The four paths of a Pixel() call at once, lanes 8p..8p+7 on path p, where every write and cleanup window of the call
+// lies inside its own block (q + cap and q0 + cp at most MaxHi + 1) and every read inside the buffer. Then no path
+// reads what another writes (the reads are neighbour slots or the other half; the writes are this slot's four blocks),
+// so the paths may run together, and the cleanup need only write the part of the old range the new one does not
+// overwrite. The aggregate takes the four paths' sum at once: saturating adds of non-negative terms commute,
+// min(min(a + x, C) + y, C) = min(a + x + y, C). KB chunks of 8 planes have their loads issued before their stores.
+// Caps are multiples of 8 here (checked before the launch), so every lane of a chunk has a plane.
+template <int KB>
+LUX_DEV void emu_pixel_grouped(const EmuArgs& a, long long nb, long long baseCur, long long q, long long q0, int cap, int cp,
+                               int count, bool skipped, const uint8_t* rawp, uint16_t* aggp, int P2p, int minPrev,
+                               uint16_t* minOut, int lane) {
+  const int j = lane & 7, grp = lane >> 3;
+  for (long long k = (q0 < 0 ? -q0 : 0) + j; k < cp; k += 8) {  // stale cleanup (:261-263), outside the new range
+    const long long idx = q0 + k;
+    if (idx < q || idx >= q + cap) __stcg(a.L + baseCur + idx, (uint16_t)2000);
+  }
+  const uint16_t* Ln = a.L + (nb + q);
+  uint16_t* Lw = a.L + (baseCur + q);
+  int runMin = 0xffff;
+  for (int b0 = 0; b0 < cap; b0 += 8 * KB) {  // warp-uniform: the cap is the pixel's
+    int Lm[KB], L0[KB], Lp[KB], rv[KB], ag[KB];
+#pragma unroll
+    for (int u = 0; u < KB; u++) {
+      if (b0 + 8 * u < cap) {
+        const int k = b0 + 8 * u + j;
+        Lm[u] = __ldcg(Ln + k - 1);
+        L0[u] = __ldcg(Ln + k);
+        Lp[u] = __ldcg(Ln + k + 1);
+        rv[u] = skipped ? (k < count ? 0 : 255) : rawp[k];
+        ag[u] = grp == 0 ? (int)aggp[k] : 0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < KB; u++) {
+      if (b0 + 8 * u >= cap) break;
+      const int k = b0 + 8 * u + j;
+      const int m = min(min(min(Lm[u] + a.p1, 65535), L0[u]), min(min(Lp[u] + a.p1, 65535), P2p));
+      int lc = min(rv[u] + m, 65535) - minPrev;
+      if (lc < 0) lc = 0;
+      __stcg(Lw + k, (uint16_t)lc);
+      runMin = min(runMin, lc);
+      int sum = lc + __shfl_xor_sync(0xffffffffu, lc, 8);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+      if (grp == 0) aggp[k] = (uint16_t)min(ag[u] + sum, 65535);
+    }
+  }
+  runMin = min(runMin, __shfl_xor_sync(0xffffffffu, runMin, 1));
+  runMin = min(runMin, __shfl_xor_sync(0xffffffffu, runMin, 2));
+  runMin = min(runMin, __shfl_xor_sync(0xffffffffu, runMin, 4));
+  if (j == 0) __stcg(minOut, (uint16_t)runMin);
+}
+
+// Pixel (DenseStereoSgm.cs:234-317), one warp; KB iterations of a path's plane loop share one L2 round trip.
+template <int KB>
 LUX_DEV void emu_pixel(const EmuArgs& a, int x, int y, int cur, int other, int lane) {
   const int pi = y * a.W + x, slot = x + 1;
   const uchar4 gb = a.guidance[pi];
@@ -57,6 +167,38 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, int y, int cur, int other, int l
   const uint8_t* rawp = a.raw + a.off[pi];
   uint16_t* aggp = a.agg + a.off[pi];
   const int sp = __ldcg(a.RangeS + cur * a.halfR + slot), cp = __ldcg(a.RangeC + cur * a.halfR + slot);
+  // Lanes 8p..8p+7 read path p's neighbour Min and Pix entries and make its P2 up front: this call writes only its own
+  // slot of the current half, and every entry read here is another slot or the other half.
+  const int gp = lane >> 3;
+  const int gns = slot + (gp == 2 ? 0 : gp == 3 ? a.dir : -a.dir);
+  const int ghalf = gp == 0 ? cur : other;
+  const int gMinPrev = __ldcg(a.Min + ghalf * a.halfM + gns * 4 + gp);
+  int gP2;
+  {
+    const float4 pn4 = __ldcg(a.Pix + ghalf * a.halfR + gns);
+    const float pn[4] = {pn4.x, pn4.y, pn4.z, pn4.w};
+    gP2 = sgm_p2(g, pn, a.gw, a.p2base);
+  }
+  {
+    const long long q = start - a.min_lo, q0 = sp - a.min_lo;
+    const long long gnb = (long long)ghalf * a.halfL + (long long)gns * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
+    const long long gbase = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
+    // The grouped form pays where the one-path-at-a-time form would take one batch a path (cap <= 32·KB): it makes
+    // the four round trips one. Larger caps take as many batches either way and stay on the form below.
+    const bool grouped = cap <= 32 * KB && q + cap <= a.max_hi + 1 && (cp == 0 || q0 + cp <= a.max_hi + 1) &&
+                         __all_sync(0xffffffffu, gnb + q + cap + 1 <= a.Llen);
+    if (grouped) {
+      emu_pixel_grouped<KB>(a, gnb, gbase, q, q0, cap, cp, count, skipped, rawp, aggp, min(gP2 + gMinPrev, 65535), gMinPrev,
+                            a.Min + cur * a.halfM + slot * 4 + gp, lane);
+      if (lane == 0) {
+        __stcg(a.RangeS + cur * a.halfR + slot, (uint16_t)start);
+        __stcg(a.RangeC + cur * a.halfR + slot, (uint16_t)cap);
+      }
+      __syncwarp();
+      return;
+    }
+  }
+#pragma unroll 1
   for (int p = 0; p < 4; p++) {
     const long long baseCur = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
     {  // stale cleanup of the previously stored range (:261-263)
@@ -67,10 +209,7 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, int y, int cur, int other, int l
     __syncwarp();
     const int ns = slot + (p == 2 ? 0 : p == 3 ? a.dir : -a.dir);
     const int half = p == 0 ? cur : other;
-    const int minPrev = __ldcg(a.Min + half * a.halfM + ns * 4 + p);
-    const float4 pn4 = __ldcg(a.Pix + half * a.halfR + ns);
-    const float pn[4] = {pn4.x, pn4.y, pn4.z, pn4.w};
-    const int P2 = sgm_p2(g, pn, a.gw, a.p2base);
+    const int minPrev = __shfl_sync(0xffffffffu, gMinPrev, 8 * p), P2 = __shfl_sync(0xffffffffu, gP2, 8 * p);
     const int P2p = min(P2 + minPrev, 65535);
     if (cap == 0) {
       __syncwarp();
@@ -80,24 +219,19 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, int y, int cur, int other, int l
     }
     const long long nb = (long long)half * a.halfL + (long long)ns * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
     const long long q = start - a.min_lo;
-    int runMin = 0xffff;
-    for (int k = lane; k < cap; k += 32) {  // caps are multiples of 8 here (checked before the launch)
-      const long long qi = q + k;
-      const int Lm = rd(a, nb + qi - 1), L0 = rd(a, nb + qi), Lp = rd(a, nb + qi + 1);
-      const int m = min(min(min(Lm + a.p1, 65535), L0), min(min(Lp + a.p1, 65535), P2p));
-      const int rv = skipped ? (k < count ? 0 : 255) : rawp[k];
-      int lc = min(rv + m, 65535) - minPrev;
-      if (lc < 0) lc = 0;
-      const long long wi = baseCur + qi;
-      if (wi < 0 || wi >= a.Llen) atomicCAS(a.err, 0, 7);
-      else __stcg(a.L + wi, (uint16_t)lc);
-      runMin = min(runMin, lc);
-      aggp[k] = (uint16_t)min((int)aggp[k] + lc, 65535);
-    }
+    // A path reads L[nb + q - 1 .. nb + q + cap] and writes L[baseCur + q .. baseCur + q + cap - 1]. The bases lie a
+    // whole half apart (paths 1-3) or one slot stride apart (path 0), so the windows meet only if cap + 2 exceeds the
+    // slot stride (4·MaxHi + 5). Where they stay apart and inside the buffer, the batched form runs; otherwise one plane
+    // per lane step with every index checked, reading and writing in the reference's order.
+    const bool batched = cap + 2 <= a.slot_stride && nb + q - 1 >= 0 && nb + q + cap + 1 <= a.Llen && baseCur + q >= 0 &&
+                         baseCur + q + cap <= a.Llen;
+    int runMin = batched ? emu_path_batched<KB>(a.L + (nb + q), a.L + (baseCur + q), a.p1, cap, count, skipped, rawp, aggp, P2p,
+                                                minPrev, lane)
+                         : emu_path_checked(a, nb, baseCur, q, cap, count, skipped, rawp, aggp, P2p, minPrev, lane);
     runMin = __reduce_min_sync(0xffffffffu, (unsigned)runMin);
-    __syncwarp();
+    __syncwarp();  // this path's stores (a spill reaches the next block) before the next path's cleanup
+    // No lane of this call reads its own Min entry; the next reader runs after the step's __syncthreads.
     if (lane == 0) __stcg(a.Min + cur * a.halfM + slot * 4 + p, (uint16_t)runMin);
-    __syncwarp();
   }
   if (lane == 0) {
     __stcg(a.RangeS + cur * a.halfR + slot, (uint16_t)start);
@@ -106,7 +240,10 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, int y, int cur, int other, int l
   __syncwarp();
 }
 
-__global__ void k_sgm_emulate(const EmuArgs a) {
+// kThreads = 32·T/2 rounded up to the two sizes launched: 512 (T <= 32, four iterations a round trip within the
+// register budget) and 1024 (T = 64, two).
+template <int kThreads, int KB>
+__global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
   __shared__ int s_band, s_stop;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   if (tid == 0) {
@@ -144,7 +281,7 @@ __global__ void k_sgm_emulate(const EmuArgs a) {
         const int x = a.dir > 0 ? xp : a.W - 1 - xp;
         const int y = a.dir > 0 ? yp : a.H - 1 - yp;
         const int cur = (r & 1) == 0 ? 1 : 0;
-        emu_pixel(a, x, y, cur, 1 - cur, lane);
+        emu_pixel<KB>(a, x, y, cur, 1 - cur, lane);
       }
       __syncthreads();
     }
@@ -203,7 +340,8 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   int nw = g.tile / 2;
   if (nw < 1) nw = 1;
   if (nw > 32) nw = 32;
-  k_sgm_emulate<<<a.ghN, nw * 32, 0, s>>>(a);
+  if (nw <= 16) k_sgm_emulate<512, 4><<<a.ghN, nw * 32, 0, s>>>(a);
+  else k_sgm_emulate<1024, 2><<<a.ghN, nw * 32, 0, s>>>(a);
   count_launches(1);
 }
 
