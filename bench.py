@@ -80,6 +80,8 @@ def args_():
     p.add_argument("--pyramid", action="store_true",
                    help="the reference's whole dense job for a capture: DenseStereoPyramid.Run (six L16 layers) on five "
                         "2080x1560 colour cameras, then the upsample to 4160x3120")
+    p.add_argument("--pyramid-size", default="2080x1560",
+                   help="WxH of the --pyramid cameras (the finest layer); a smaller size is for profiling captures")
     p.add_argument("--cpu-rows", type=int, default=130, help="rows of the CPU sample strip")
     p.add_argument("--workload", default="pair13mp", choices=sorted(WORKLOADS),
                    help="pair13mp is the benchmark; the smaller pairs are for profiling captures")
@@ -831,7 +833,7 @@ def run_pyramid(a):
     from lux_b200 import api, synth
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    w, h = 2080, 1560
+    w, h = (int(v) for v in a.pyramid_size.split("x"))
     cap = synth.capture(w, h, 5, seed=3)
     torch.cuda.set_device(0)
     ctx = api.Context(0)
@@ -868,11 +870,11 @@ def run_pyramid(a):
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.steps
     de = sum(W * H * n for (W, H, n, *_) in info)
-    print(json.dumps({"metric": "capture dense jobs/s (DenseStereoPyramid.Run + upsample), 5 cameras 2080x1560", "value": 1e3 / ms,
+    print(json.dumps({"metric": f"capture dense jobs/s (DenseStereoPyramid.Run + upsample), 5 cameras {w}x{h}", "value": 1e3 / ms,
                       "unit": "captures/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 cost / u16 aggregation",
                       "data": "synthetic (colour capture, planar scene 0.4-6 m, 8-40 mm baselines)",
-                      "config": {"workload": "L16 pyramid on 5 colour cameras 2080x1560 + upsample to 4160x3120",
+                      "config": {"workload": f"L16 pyramid on 5 colour cameras {w}x{h} + upsample to {2 * w}x{2 * h}",
                                  "layers": [{"w": W, "h": H, "planes": n, "mean_cap": round(mc, 1), "sgm_kernel": sk, "cost_kernel": ck,
                                              "ms_cost": round(c, 3), "ms_sgm": round(g, 3), "ms_wta": round(t, 3)}
                                             for (W, H, n, sk, ck, c, g, t, mc) in info],
