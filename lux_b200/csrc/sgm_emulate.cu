@@ -6,8 +6,11 @@
 // keeps the flat buffer (2 halves x (W+2) slots x (4·MaxHi+5) u16, plus Min/RangeS/RangeC/Pix) in global memory and runs
 // every Pixel() call of the reference in an order that gives each read the same last writer:
 //   * one CTA per band of T rows (tickets taken in order, so a band only ever waits on a running one);
-//   * tiles of a band in order; band j starts tile i once band j-1 has finished tile i+2: from tile i+3 on, a band
-//     touches no slot that tile i of the band below touches (slots within [iT-T, iT+T+2]);
+//   * tiles of a band in order; band j starts tile i once band j-1 has finished tile i+1. Tile i+2 of band j-1 may then
+//     run beside it: their nearest pixels are band j-1's last row at column iT+T+1 and band j's first row at iT+T-1,
+//     the upper row's pixel two columns right of the lower one, a pair that touches nothing in common (see the row
+//     hand-over below); every other pair is three or more columns apart. Where tile i+2 revisits the last column
+//     ((i+2)·T >= W, a pixel clamped to W-1), band j waits for tile i+2 as well;
 //   * inside a tile, pixel (row r, sheared offset u) runs at step u + 2r. Pixels that share or neighbour a slot (at most
 //     two columns and two rows apart) keep the reference's row-major order; pixels of one step are three or more
 //     columns apart. A revisit of the last column runs alone at step 2r.
@@ -240,11 +243,62 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, int y, int cur, int other, int l
   __syncwarp();
 }
 
+// The tile's pixel (row r, xp offset u) of a band: x, y and whether there is one. The clamped row start revisits the
+// last column at u = 0 only.
+struct EmuTileRow {
+  int yp, xs, xe;
+  bool revisit;
+};
+LUX_DEV EmuTileRow emu_tile_row(const EmuArgs& a, int j, int i, int r) {
+  EmuTileRow t;
+  t.yp = j * a.T + r;
+  t.xs = min(max(i * a.T - r, 0), (a.xsw && a.dir > 0) ? a.W : a.W - 1);
+  t.xe = min(max(i * a.T + a.T - r, -1), a.W);
+  t.revisit = i * a.T - r >= a.W;
+  return t;
+}
+LUX_DEV bool emu_tile_pixel(const EmuArgs& a, const EmuTileRow& t, int i, int r, int u, int& x, int& y) {
+  if (t.yp >= a.H || t.xs == t.xe) return false;  // yEnd (:213); an empty row range
+  int xp;
+  if (t.revisit) {
+    if (u != 0) return false;
+    xp = a.W - 1;
+  } else {
+    xp = i * a.T - r + u;
+    if (xp < t.xs || xp >= t.xe) return false;
+  }
+  x = a.dir > 0 ? xp : a.W - 1 - xp;
+  y = a.dir > 0 ? t.yp : a.H - 1 - t.yp;
+  return true;
+}
+
+constexpr int kFlagRows = 128;  // tiles up to this many rows hand over row to row; taller ones step with a barrier
+
 // kThreads = 32·T/2 rounded up to the two sizes launched: 512 (T <= 32, four iterations a round trip within the
-// register budget) and 1024 (T = 64, two).
-template <int kThreads, int KB>
+// register budget) and 1024 (T >= 64, two). kFlags: the row-to-row hand-over below (T <= kFlagRows), else a barrier per
+// step of the sheared schedule, pixel (r, u) at step u + 2r (pixels of one step are three or more columns apart).
+//
+// Inside a tile, each warp owns whole rows (r = warp, warp + nw, ...) and runs a row's offsets u in order; row r runs
+// offset u once row r-1 has finished offset u (a CTA-scope release/acquire of the row's count in shared memory): the
+// recurrence reads row r-1 at columns x-1, x and x+1, offsets u-2..u. For rows r1 < r2 this orders (r1, u1) before
+// (r2, u2) whenever u1 <= u2. Two pixels touch a common element only when at most two columns apart, x1 - x2 =
+// (r2 - r1) + (u1 - u2) <= 2, so the one pair left unordered is the upper row's pixel two columns right of the lower
+// one (r2 = r1 + 1, u1 = u2 + 1), and it touches nothing in common:
+//   * the lower pixel reads the upper row's half at columns x2-1..x2+1 (each block window +-1 element) and, past its
+//     path-3 window, the pad element of the next slot in memory; the upper pixel writes its own blocks (never its own
+//     pad) and spills at most align - 2 <= 6 elements (q + cap <= MaxHi - MinLo + align - 1) into the pad and first
+//     block-0 elements of its next slot in memory, which is column x2 + 3 (pass +1) or x2 + 1 (pass -1), where the lower
+//     pixel reads only block 3 from index -1 (block 2's last);
+//   * the lower pixel writes the other half, which the upper pixel reads at columns x2+1..x2+3: its spill (pass +1)
+//     reaches slot x2+1's pad and block-0 elements 0..5, and the upper pixel reads that slot's block 1 from index -1,
+//     block 0's last element (index MaxHi >= 8 with align 8; with align 2 nothing spills).
+// Rows then advance at their own pace, one pixel apart, instead of two pixels apart with each step waiting for its
+// slowest pixel.
+template <int kThreads, int KB, bool kFlags>
 __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
-  __shared__ int s_band, s_stop;
+  __shared__ int s_band;
+  __shared__ volatile int s_stop;
+  __shared__ int s_row[kFlagRows];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   if (tid == 0) {
     s_band = atomicAdd(a.ticket, 1);
@@ -255,36 +309,58 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
   const int T = a.T;
   if (j >= a.ghN) return;
   for (int i = 0; i < a.gwN; i++) {
+    for (int r = tid; r < kFlagRows; r += blockDim.x) s_row[r] = 0;
     if (tid == 0) {
-      if (j > 0 && !wait_at_least(a.progress + (j - 1), min(i + 3, a.gwN), a.err, 11 /* LUX_ERR_TIMEOUT */, a.timeout_ns)) s_stop = 1;
+      const int need = min(i + ((i + 2) * T >= a.W ? 3 : 2), a.gwN);  // tiles of band j-1 finished
+      if (j > 0 && !wait_at_least(a.progress + (j - 1), need, a.err, 11 /* LUX_ERR_TIMEOUT */, a.timeout_ns)) s_stop = 1;
       if (*(volatile int*)a.err != 0) s_stop = 1;
     }
     __syncthreads();
     if (s_stop) break;
-    for (int t = 0; t <= 3 * T - 3; t++) {
-      const int rlo = max(0, (t - T + 2) / 2), rhi = min(T - 1, t / 2);
-      for (int r = rlo + warp; r <= rhi; r += nw) {
-        const int u = t - 2 * r;
-        const int yp = j * T + r;
-        if (yp >= a.H) continue;  // yEnd (:213)
-        const int xs = min(max(i * T - r, 0), (a.xsw && a.dir > 0) ? a.W : a.W - 1);
-        const int xe = min(max(i * T + T - r, -1), a.W);
-        if (xs == xe) continue;
-        int xp;
-        if (i * T - r >= a.W) {  // the clamped row start revisits the last column
-          if (u != 0) continue;
-          xp = a.W - 1;
-        } else {
-          xp = i * T - r + u;
-          if (xp < xs || xp >= xe) continue;
+    if (kFlags) {  // T <= kFlagRows (the launcher's choice)
+      for (int r = warp; r < T; r += nw) {
+        const EmuTileRow row = emu_tile_row(a, j, i, r);
+        if (row.yp >= a.H) {  // past the image: this row and every later one have no pixels
+          __syncwarp();
+          if (lane == 0) st_release_cta(&s_row[r], T);
+          continue;
         }
-        const int x = a.dir > 0 ? xp : a.W - 1 - xp;
-        const int y = a.dir > 0 ? yp : a.H - 1 - yp;
-        const int cur = (r & 1) == 0 ? 1 : 0;
-        emu_pixel<KB>(a, x, y, cur, 1 - cur, lane);
+        bool failed = false;
+        for (int u = 0; u < T; u++) {
+          if (r > 0 && __any_sync(0xffffffffu, !wait_shared_at_least(&s_row[r - 1], u + 1, &s_stop, a.timeout_ns))) {
+            if (lane == 0) {
+              atomicCAS(a.err, 0, 11);  // LUX_ERR_TIMEOUT, or another warp's failure
+              s_stop = 1;
+            }
+            failed = true;
+            break;
+          }
+          int x, y;
+          if (emu_tile_pixel(a, row, i, r, u, x, y)) {
+            const int cur = (r & 1) == 0 ? 1 : 0;
+            emu_pixel<KB>(a, x, y, cur, 1 - cur, lane);
+          }
+          __syncwarp();
+          if (lane == 0) st_release_cta(&s_row[r], u + 1);
+        }
+        if (failed) break;
       }
-      __syncthreads();
+    } else {
+      for (int t = 0; t <= 3 * T - 3; t++) {
+        const int rlo = max(0, (t - T + 2) / 2), rhi = min(T - 1, t / 2);
+        for (int r = rlo + warp; r <= rhi; r += nw) {
+          const int u = t - 2 * r;
+          const EmuTileRow row = emu_tile_row(a, j, i, r);
+          int x, y;
+          if (!emu_tile_pixel(a, row, i, r, u, x, y)) continue;
+          const int cur = (r & 1) == 0 ? 1 : 0;
+          emu_pixel<KB>(a, x, y, cur, 1 - cur, lane);
+        }
+        __syncthreads();
+      }
     }
+    __syncthreads();
+    if (s_stop) break;
     if (tid == 0) {
       __threadfence();
       st_release(a.progress + j, i + 1);
@@ -340,8 +416,9 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   int nw = g.tile / 2;
   if (nw < 1) nw = 1;
   if (nw > 32) nw = 32;
-  if (nw <= 16) k_sgm_emulate<512, 4><<<a.ghN, nw * 32, 0, s>>>(a);
-  else k_sgm_emulate<1024, 2><<<a.ghN, nw * 32, 0, s>>>(a);
+  if (g.tile > kFlagRows) k_sgm_emulate<1024, 1, false><<<a.ghN, nw * 32, 0, s>>>(a);
+  else if (nw <= 16) k_sgm_emulate<512, 4, true><<<a.ghN, nw * 32, 0, s>>>(a);
+  else k_sgm_emulate<1024, 2, true><<<a.ghN, nw * 32, 0, s>>>(a);
   count_launches(1);
 }
 
