@@ -94,14 +94,17 @@ LUX_DEV int ld_acquire_cta(const int* p) {
 LUX_DEV void st_release_cta(int* p, int v) {
   asm volatile("st.release.cta.shared.s32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "r"(v) : "memory");
 }
-// Waits (bounded) until the shared counter *p >= target. Returns false on timeout or when *stop is set.
+// Waits (bounded) until the shared counter *p >= target. Returns false on timeout or when *stop is set. The sleep
+// between polls doubles from 32 ns to 256 ns: the waiting warps leave the issue slots to the warps that have work.
 LUX_DEV bool wait_shared_at_least(const int* p, int target, const volatile int* stop, uint64_t timeout_ns) {
   if (ld_acquire_cta(p) >= target) return true;
   const uint64_t t0 = global_ns();
+  unsigned sleep_ns = 32;
   for (unsigned it = 0;; it++) {
-    __nanosleep(16);  // leave the issue slots to the warps that have work
+    __nanosleep(sleep_ns);
+    if (sleep_ns < 256) sleep_ns <<= 1;
     if (ld_acquire_cta(p) >= target) return true;
-    if ((it & 63) == 63) {
+    if ((it & 15) == 15) {
       if (*stop) return false;
       if (global_ns() - t0 > timeout_ns) return false;
     }

@@ -311,8 +311,13 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
   for (int i = 0; i < a.gwN; i++) {
     for (int r = tid; r < kFlagRows; r += blockDim.x) s_row[r] = 0;
     if (tid == 0) {
-      const int need = min(i + ((i + 2) * T >= a.W ? 3 : 2), a.gwN);  // tiles of band j-1 finished
-      if (j > 0 && !wait_at_least(a.progress + (j - 1), need, a.err, 11 /* LUX_ERR_TIMEOUT */, a.timeout_ns)) s_stop = 1;
+      // Whole tiles of band j-1 to wait for (progress counts its last row's offsets, T a tile): the barrier form keeps
+      // a lag of three tiles; the row form waits row by row below, and here only for a tile i+2 that revisits the
+      // last column.
+      int need = 0;
+      if (!kFlags || (i + 2) * T >= a.W) need = min(i + 3, a.gwN) * T;
+      if (j > 0 && need > 0 && !wait_at_least(a.progress + (j - 1), need, a.err, 11 /* LUX_ERR_TIMEOUT */, a.timeout_ns))
+        s_stop = 1;
       if (*(volatile int*)a.err != 0) s_stop = 1;
     }
     __syncthreads();
@@ -326,6 +331,8 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
           continue;
         }
         bool failed = false;
+        int seen = 0;  // row 0: band j-1's last-row offsets seen so far
+        const bool publish = r == T - 1 && j + 1 < a.ghN;
         for (int u = 0; u < T; u++) {
           if (r > 0 && __any_sync(0xffffffffu, !wait_shared_at_least(&s_row[r - 1], u + 1, &s_stop, a.timeout_ns))) {
             if (lane == 0) {
@@ -335,13 +342,30 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
             failed = true;
             break;
           }
+          // Row 0 continues band j-1's last row one row down: offset u of tile i once that row has finished offset u
+          // of tile i+1 (in the sheared frame, the row above at the same offset).
+          const int target = min((i + 1) * T + u + 1, a.gwN * T);
+          if (r == 0 && j > 0 && seen < target) {
+            seen = __reduce_min_sync(0xffffffffu, wait_at_least_value(a.progress + (j - 1), target, a.err, 11, a.timeout_ns));
+            if (seen < 0) {
+              if (lane == 0) s_stop = 1;
+              failed = true;
+              break;
+            }
+          }
           int x, y;
           if (emu_tile_pixel(a, row, i, r, u, x, y)) {
             const int cur = (r & 1) == 0 ? 1 : 0;
             emu_pixel<KB>(a, x, y, cur, 1 - cur, lane);
           }
           __syncwarp();
-          if (lane == 0) st_release_cta(&s_row[r], u + 1);
+          if (lane == 0) {
+            st_release_cta(&s_row[r], u + 1);
+            if (publish) {  // the band below reads this row's progress; all rows above it are through u as well
+              __threadfence();
+              st_release(a.progress + j, i * T + u + 1);
+            }
+          }
         }
         if (failed) break;
       }
@@ -361,9 +385,9 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
     }
     __syncthreads();
     if (s_stop) break;
-    if (tid == 0) {
+    if (!kFlags && tid == 0) {
       __threadfence();
-      st_release(a.progress + j, i + 1);
+      st_release(a.progress + j, (i + 1) * T);
     }
   }
 }
