@@ -380,7 +380,7 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   if ((rc = alloc_t(ctx, tmp, (size_t)2 * (W + 2), &eb.RangeC))) return rc;
   if ((rc = alloc_t(ctx, tmp, (size_t)2 * (W + 2), &eb.Pix))) return rc;
   if ((rc = alloc_t(ctx, tmp, 2, &eb.ticket))) return rc;
-  if ((rc = alloc_t(ctx, tmp, (size_t)2 * bands, &eb.progress))) return rc;
+  if ((rc = alloc_t(ctx, tmp, (size_t)2 * bands * kEmuParts, &eb.progress))) return rc;
   emu_init_buffers(eb, W, L->max_hi, align, bands, s);
   launch_sgm_emulate(g, eb, +1, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, ctx->d_err, s);
   if (L->agg_pass1) CK(cudaMemcpyAsync(L->agg_pass1, L->agg, (L->volume + 8) * 2, cudaMemcpyDeviceToDevice, s));

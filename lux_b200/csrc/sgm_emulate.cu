@@ -23,6 +23,7 @@ namespace lux {
 
 struct EmuArgs {
   int W, H, T, dir, xsw, min_lo, max_hi, slot_stride, halfL, halfM, halfR, gwN, ghN;
+  int parts, part_rows;  // blocks per band and rows per block
   long long Llen;
   uint16_t* L;
   uint16_t* Min;
@@ -106,38 +107,46 @@ LUX_DEV int emu_path_batched(const uint16_t* Ln, uint16_t* Lw, int p1, int cap, 
   return runMin;
 }
 
+// One batch of the grouped form: KB chunks of 8 planes from plane b0, lane j of group grp on plane b0 + 8u + j.
+template <int KB>
+LUX_DEV void emu_group_load(const uint16_t* Ln, int b0, int cap, int count, bool skipped, const uint8_t* rawp,
+                            const uint16_t* aggp, int j, int grp, int (&Lm)[KB], int (&L0)[KB], int (&Lp)[KB], int (&rv)[KB],
+                            int (&ag)[KB]) {
+#pragma unroll
+  for (int u = 0; u < KB; u++) {
+    if (b0 + 8 * u < cap) {
+      const int k = b0 + 8 * u + j;
+      Lm[u] = __ldcg(Ln + k - 1);
+      L0[u] = __ldcg(Ln + k);
+      Lp[u] = __ldcg(Ln + k + 1);
+      rv[u] = skipped ? (k < count ? 0 : 255) : rawp[k];
+      ag[u] = grp == 0 ? (int)aggp[k] : 0;
+    }
+  }
+}
+
 // The four paths of a Pixel() call at once, lanes 8p..8p+7 on path p, where every write and cleanup window of the call
 // lies inside its own block (q + cap and q0 + cp at most MaxHi + 1) and every read inside the buffer. Then no path
 // reads what another writes (the reads are neighbour slots or the other half; the writes are this slot's four blocks),
 // so the paths may run together, and the cleanup need only write the part of the old range the new one does not
 // overwrite. The aggregate takes the four paths' sum at once: saturating adds of non-negative terms commute,
-// min(min(a + x, C) + y, C) = min(a + x + y, C). KB chunks of 8 planes have their loads issued before their stores.
-// Caps are multiples of 8 here (checked before the launch), so every lane of a chunk has a plane.
+// min(min(a + x, C) + y, C) = min(a + x + y, C). KB chunks of 8 planes have their loads issued before their stores;
+// the first batch comes in loaded (its reads are neighbour slots, which no write of this call touches). Caps are
+// multiples of 8 here (checked before the launch), so every lane of a chunk has a plane.
 template <int KB>
-LUX_DEV void emu_pixel_grouped(const EmuArgs& a, long long nb, long long baseCur, long long q, long long q0, int cap, int cp,
-                               int count, bool skipped, const uint8_t* rawp, uint16_t* aggp, int P2p, int minPrev,
-                               uint16_t* minOut, int lane) {
+LUX_DEV void emu_pixel_grouped(const EmuArgs& a, const uint16_t* Ln, long long baseCur, long long q, long long q0, int cap,
+                               int cp, int count, bool skipped, const uint8_t* rawp, uint16_t* aggp, int P2p, int minPrev,
+                               uint16_t* minOut, int lane, int (&Lm)[KB], int (&L0)[KB], int (&Lp)[KB], int (&rv)[KB],
+                               int (&ag)[KB]) {
   const int j = lane & 7, grp = lane >> 3;
   for (long long k = (q0 < 0 ? -q0 : 0) + j; k < cp; k += 8) {  // stale cleanup (:261-263), outside the new range
     const long long idx = q0 + k;
     if (idx < q || idx >= q + cap) __stcg(a.L + baseCur + idx, (uint16_t)2000);
   }
-  const uint16_t* Ln = a.L + (nb + q);
   uint16_t* Lw = a.L + (baseCur + q);
   int runMin = 0xffff;
   for (int b0 = 0; b0 < cap; b0 += 8 * KB) {  // warp-uniform: the cap is the pixel's
-    int Lm[KB], L0[KB], Lp[KB], rv[KB], ag[KB];
-#pragma unroll
-    for (int u = 0; u < KB; u++) {
-      if (b0 + 8 * u < cap) {
-        const int k = b0 + 8 * u + j;
-        Lm[u] = __ldcg(Ln + k - 1);
-        L0[u] = __ldcg(Ln + k);
-        Lp[u] = __ldcg(Ln + k + 1);
-        rv[u] = skipped ? (k < count ? 0 : 255) : rawp[k];
-        ag[u] = grp == 0 ? (int)aggp[k] : 0;
-      }
-    }
+    if (b0 > 0) emu_group_load<KB>(Ln, b0, cap, count, skipped, rawp, aggp, j, grp, Lm, L0, Lp, rv, ag);
 #pragma unroll
     for (int u = 0; u < KB; u++) {
       if (b0 + 8 * u >= cap) break;
@@ -158,17 +167,33 @@ LUX_DEV void emu_pixel_grouped(const EmuArgs& a, long long nb, long long baseCur
   if (j == 0) __stcg(minOut, (uint16_t)runMin);
 }
 
-// Pixel (DenseStereoSgm.cs:234-317), one warp; KB iterations of a path's plane loop share one L2 round trip.
+// A pixel's read-only inputs, loaded before the hand-over that lets it run.
+struct EmuPix {
+  uchar4 gb;
+  int start, count, cap, skip;
+  unsigned long long off;
+};
+LUX_DEV EmuPix emu_load_pix(const EmuArgs& a, int x, int y) {
+  const int pi = y * a.W + x;
+  EmuPix s;
+  s.gb = a.guidance[pi];
+  s.start = a.start[pi];
+  s.count = a.count[pi];
+  s.cap = a.cap[pi];
+  s.skip = a.skip[pi];
+  s.off = a.off[pi];
+  return s;
+}
+
+// Pixel (DenseStereoSgm.cs:234-317), one warp; KB iterations of a path's plane loop share one L2 round trip. The
+// line-state loads (own Range, neighbours' Min and Pix, the grouped form's first batch) go out together.
 template <int KB>
-LUX_DEV void emu_pixel(const EmuArgs& a, int x, int y, int cur, int other, int lane) {
-  const int pi = y * a.W + x, slot = x + 1;
-  const uchar4 gb = a.guidance[pi];
-  const float g[4] = {(float)gb.x, (float)gb.y, (float)gb.z, (float)gb.w};
-  if (lane == 0) __stcg(a.Pix + cur * a.halfR + slot, make_float4(g[0], g[1], g[2], g[3]));
-  const int start = a.start[pi], count = a.count[pi], cap = a.cap[pi];
-  const bool skipped = a.skip[pi] != 0;
-  const uint8_t* rawp = a.raw + a.off[pi];
-  uint16_t* aggp = a.agg + a.off[pi];
+LUX_DEV void emu_pixel(const EmuArgs& a, int x, const EmuPix& px, int cur, int other, int lane) {
+  const int slot = x + 1;
+  const int start = px.start, count = px.count, cap = px.cap;
+  const bool skipped = px.skip != 0;
+  const uint8_t* rawp = a.raw + px.off;
+  uint16_t* aggp = a.agg + px.off;
   const int sp = __ldcg(a.RangeS + cur * a.halfR + slot), cp = __ldcg(a.RangeC + cur * a.halfR + slot);
   // Lanes 8p..8p+7 read path p's neighbour Min and Pix entries and make its P2 up front: this call writes only its own
   // slot of the current half, and every entry read here is another slot or the other half.
@@ -176,23 +201,29 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, int y, int cur, int other, int l
   const int gns = slot + (gp == 2 ? 0 : gp == 3 ? a.dir : -a.dir);
   const int ghalf = gp == 0 ? cur : other;
   const int gMinPrev = __ldcg(a.Min + ghalf * a.halfM + gns * 4 + gp);
+  const float4 pn4 = __ldcg(a.Pix + ghalf * a.halfR + gns);
+  const long long q = start - a.min_lo;
+  const long long gnb = (long long)ghalf * a.halfL + (long long)gns * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
+  // The grouped form pays where the one-path-at-a-time form would take one batch a path (cap <= 32·KB): it makes the
+  // four round trips one. Larger caps take as many batches either way and stay on the form below. Its read and own
+  // write windows are checked here; the cleanup window (from the Range entries) decides below.
+  const bool maybe_grouped = cap <= 32 * KB && q + cap <= a.max_hi + 1 && __all_sync(0xffffffffu, gnb + q + cap + 1 <= a.Llen);
+  int Lm[KB], L0[KB], Lp[KB], rv[KB], ag[KB];
+  const uint16_t* Ln = a.L + (gnb + q);
+  if (maybe_grouped) emu_group_load<KB>(Ln, 0, cap, count, skipped, rawp, aggp, lane & 7, gp, Lm, L0, Lp, rv, ag);
+  const float g[4] = {(float)px.gb.x, (float)px.gb.y, (float)px.gb.z, (float)px.gb.w};
+  if (lane == 0) __stcg(a.Pix + cur * a.halfR + slot, make_float4(g[0], g[1], g[2], g[3]));
   int gP2;
   {
-    const float4 pn4 = __ldcg(a.Pix + ghalf * a.halfR + gns);
     const float pn[4] = {pn4.x, pn4.y, pn4.z, pn4.w};
     gP2 = sgm_p2(g, pn, a.gw, a.p2base);
   }
   {
-    const long long q = start - a.min_lo, q0 = sp - a.min_lo;
-    const long long gnb = (long long)ghalf * a.halfL + (long long)gns * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
+    const long long q0 = sp - a.min_lo;
     const long long gbase = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
-    // The grouped form pays where the one-path-at-a-time form would take one batch a path (cap <= 32·KB): it makes
-    // the four round trips one. Larger caps take as many batches either way and stay on the form below.
-    const bool grouped = cap <= 32 * KB && q + cap <= a.max_hi + 1 && (cp == 0 || q0 + cp <= a.max_hi + 1) &&
-                         __all_sync(0xffffffffu, gnb + q + cap + 1 <= a.Llen);
-    if (grouped) {
-      emu_pixel_grouped<KB>(a, gnb, gbase, q, q0, cap, cp, count, skipped, rawp, aggp, min(gP2 + gMinPrev, 65535), gMinPrev,
-                            a.Min + cur * a.halfM + slot * 4 + gp, lane);
+    if (maybe_grouped && (cp == 0 || q0 + cp <= a.max_hi + 1)) {
+      emu_pixel_grouped<KB>(a, Ln, gbase, q, q0, cap, cp, count, skipped, rawp, aggp, min(gP2 + gMinPrev, 65535), gMinPrev,
+                            a.Min + cur * a.halfM + slot * 4 + gp, lane, Lm, L0, Lp, rv, ag);
       if (lane == 0) {
         __stcg(a.RangeS + cur * a.halfR + slot, (uint16_t)start);
         __stcg(a.RangeC + cur * a.halfR + slot, (uint16_t)cap);
@@ -296,34 +327,45 @@ constexpr int kFlagRows = 128;  // tiles up to this many rows hand over row to r
 // slowest pixel.
 template <int kThreads, int KB, bool kFlags>
 __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
-  __shared__ int s_band;
+  __shared__ int s_part;
   __shared__ volatile int s_stop;
   __shared__ int s_row[kFlagRows];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   if (tid == 0) {
-    s_band = atomicAdd(a.ticket, 1);
+    s_part = atomicAdd(a.ticket, 1);
     s_stop = 0;
   }
   __syncthreads();
-  const int j = s_band;
+  const int k = s_part;  // tickets in order: the part above (k - 1) is running or done
+  const int j = k / a.parts, part = k % a.parts;
   const int T = a.T;
   if (j >= a.ghN) return;
+  const int r0 = part * a.part_rows, r1 = min(r0 + a.part_rows, T);  // this part's rows of the tile frame
+  // A part below the image has no pixels, and neither has any part after it: nothing waits on its progress. (It must
+  // not wait either: the last row of the part above, below the image too, publishes none.)
+  if (j * T + r0 >= a.H) return;
+  int* const above = a.progress + (k - 1);  // the part above: its last row's offsets
   for (int i = 0; i < a.gwN; i++) {
     for (int r = tid; r < kFlagRows; r += blockDim.x) s_row[r] = 0;
     if (tid == 0) {
-      // Whole tiles of band j-1 to wait for (progress counts its last row's offsets, T a tile): the barrier form keeps
-      // a lag of three tiles; the row form waits row by row below, and here only for a tile i+2 that revisits the
-      // last column.
+      // Whole tiles to wait for (progress counts a part's last row's offsets, T a tile). The barrier form keeps a
+      // lag of three tiles on the band above. The row form waits row by row below, and here only around revisits of
+      // the last column, which do not follow the sheared columns: for the first part, tile i+2 of the band above when
+      // it revisits (the band above comes first in the reference); for a part whose rows revisit in tile i, tile i-1
+      // of the part below in this band (a band's tiles come in order, so the rows below finish tile i-1 first).
       int need = 0;
-      if (!kFlags || (i + 2) * T >= a.W) need = min(i + 3, a.gwN) * T;
-      if (j > 0 && need > 0 && !wait_at_least(a.progress + (j - 1), need, a.err, 11 /* LUX_ERR_TIMEOUT */, a.timeout_ns))
+      if (!kFlags) need = min(i + 3, a.gwN) * T;
+      else if (part == 0 && (i + 2) * T >= a.W) need = min(i + 3, a.gwN) * T;
+      if (k > 0 && need > 0 && !wait_at_least(above, need, a.err, 11 /* LUX_ERR_TIMEOUT */, a.timeout_ns)) s_stop = 1;
+      if (kFlags && part + 1 < a.parts && i > 0 && i * T - r0 >= a.W && j * T + r1 < a.H &&
+          !wait_at_least(a.progress + (k + 1), i * T, a.err, 11, a.timeout_ns))
         s_stop = 1;
       if (*(volatile int*)a.err != 0) s_stop = 1;
     }
     __syncthreads();
     if (s_stop) break;
     if (kFlags) {  // T <= kFlagRows (the launcher's choice)
-      for (int r = warp; r < T; r += nw) {
+      for (int r = r0 + warp; r < r1; r += nw) {
         const EmuTileRow row = emu_tile_row(a, j, i, r);
         if (row.yp >= a.H) {  // past the image: this row and every later one have no pixels
           __syncwarp();
@@ -331,10 +373,29 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
           continue;
         }
         bool failed = false;
-        int seen = 0;  // row 0: band j-1's last-row offsets seen so far
-        const bool publish = r == T - 1 && j + 1 < a.ghN;
+        int seen = 0;  // first row: the part above's last-row offsets seen so far
+        // The publisher is the part's last row inside the image; the part below (or the band below) waits on it, and
+        // the part above on its last offset of a tile where the part above revisits next.
+        const int r_pub = min(r1, a.H - j * T) - 1;
+        const bool publish = r == r_pub;
+        // Another block reads what this part's last two rows write (the row above it in the other half, the row two
+        // above in its own half: the Range entries of its stale cleanup, the line state it overwrites), and, on a tile
+        // before the part above revisits, what any row writes near the last column. Those rows' lanes make their
+        // writes visible to the GPU before the row's count moves on; the CTA-scope hand-over alone only orders them
+        // for this block.
+        const bool fence = r >= r_pub - 1 || (part > 0 && (i + 1) * T - (r0 - a.part_rows) >= a.W);
+        int nx, ny;
+        bool has_next = emu_tile_pixel(a, row, i, r, 0, nx, ny);
+        EmuPix next;
+        if (has_next) next = emu_load_pix(a, nx, ny);
         for (int u = 0; u < T; u++) {
-          if (r > 0 && __any_sync(0xffffffffu, !wait_shared_at_least(&s_row[r - 1], u + 1, &s_stop, a.timeout_ns))) {
+          const bool has = has_next;
+          const int x = nx;
+          const EmuPix px = next;
+          // The next offset's read-only inputs, loaded while this offset waits and runs.
+          has_next = u + 1 < T && emu_tile_pixel(a, row, i, r, u + 1, nx, ny);
+          if (has_next) next = emu_load_pix(a, nx, ny);
+          if (r > r0 && __any_sync(0xffffffffu, !wait_shared_at_least(&s_row[r - 1], u + 1, &s_stop, a.timeout_ns))) {
             if (lane == 0) {
               atomicCAS(a.err, 0, 11);  // LUX_ERR_TIMEOUT, or another warp's failure
               s_stop = 1;
@@ -342,29 +403,28 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
             failed = true;
             break;
           }
-          // Row 0 continues band j-1's last row one row down: offset u of tile i once that row has finished offset u
-          // of tile i+1 (in the sheared frame, the row above at the same offset).
-          const int target = min((i + 1) * T + u + 1, a.gwN * T);
-          if (r == 0 && j > 0 && seen < target) {
-            seen = __reduce_min_sync(0xffffffffu, wait_at_least_value(a.progress + (j - 1), target, a.err, 11, a.timeout_ns));
-            if (seen < 0) {
-              if (lane == 0) s_stop = 1;
-              failed = true;
-              break;
+          // The first row continues the part above's last row one row down: within the band, that row at the same
+          // tile and offset; across bands, the band above's last row at offset u of tile i+1 (the same sheared frame).
+          if (r == r0 && k > 0) {
+            const int target = part > 0 ? i * T + u + 1 : min((i + 1) * T + u + 1, a.gwN * T);
+            if (seen < target) {
+              seen = __reduce_min_sync(0xffffffffu, wait_at_least_value(above, target, a.err, 11, a.timeout_ns));
+              if (seen < 0) {
+                if (lane == 0) s_stop = 1;
+                failed = true;
+                break;
+              }
             }
           }
-          int x, y;
-          if (emu_tile_pixel(a, row, i, r, u, x, y)) {
+          if (has) {
             const int cur = (r & 1) == 0 ? 1 : 0;
-            emu_pixel<KB>(a, x, y, cur, 1 - cur, lane);
+            emu_pixel<KB>(a, x, px, cur, 1 - cur, lane);
           }
+          if (fence) __threadfence();
           __syncwarp();
           if (lane == 0) {
             st_release_cta(&s_row[r], u + 1);
-            if (publish) {  // the band below reads this row's progress; all rows above it are through u as well
-              __threadfence();
-              st_release(a.progress + j, i * T + u + 1);
-            }
+            if (publish) st_release(a.progress + k, i * T + u + 1);  // all rows above it are through u as well
           }
         }
         if (failed) break;
@@ -378,7 +438,7 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
           int x, y;
           if (!emu_tile_pixel(a, row, i, r, u, x, y)) continue;
           const int cur = (r & 1) == 0 ? 1 : 0;
-          emu_pixel<KB>(a, x, y, cur, 1 - cur, lane);
+          emu_pixel<KB>(a, x, emu_load_pix(a, x, y), cur, 1 - cur, lane);
         }
         __syncthreads();
       }
@@ -387,7 +447,7 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
     if (s_stop) break;
     if (!kFlags && tid == 0) {
       __threadfence();
-      st_release(a.progress + j, (i + 1) * T);
+      st_release(a.progress + k, (i + 1) * T);
     }
   }
 }
@@ -410,7 +470,7 @@ void emu_init_buffers(const EmuBuffers& b, int W, int max_hi, int align, int ban
   k_emu_init<<<(2 * slots * 4 + 255) / 256, 256, 0, s>>>(b.Min, b.RangeS, b.RangeC, b.Pix, slots, align);
   count_launches(1);
   cudaMemsetAsync(b.ticket, 0, 2 * sizeof(int), s);
-  cudaMemsetAsync(b.progress, 0, (size_t)2 * bands * sizeof(int), s);
+  cudaMemsetAsync(b.progress, 0, (size_t)2 * bands * kEmuParts * sizeof(int), s);
 }
 
 void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xsw, uint16_t p1, float p2scale, const float gw[4],
@@ -433,16 +493,21 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   a.p2base = p1f * p2scale;  // (float)P1 * P2Scale (:256)
   for (int i = 0; i < 4; i++) a.gw[i] = gw[i];
   int pass = dir > 0 ? 0 : 1;
+  // The row form splits a band of T >= 4 rows between two blocks (parts) of T/2 rows, a warp a row up to 32 rows.
+  const bool flags = g.tile <= kFlagRows;
+  a.parts = flags && g.tile >= 4 ? kEmuParts : 1;
+  a.part_rows = (g.tile + a.parts - 1) / a.parts;
   a.ticket = b.ticket + pass;
-  a.progress = b.progress + (size_t)pass * a.ghN;
+  a.progress = b.progress + (size_t)pass * a.ghN * kEmuParts;
   a.err = err;
   a.timeout_ns = kTimeoutNs;
-  int nw = g.tile / 2;
+  int nw = flags ? a.part_rows : g.tile / 2;
   if (nw < 1) nw = 1;
   if (nw > 32) nw = 32;
-  if (g.tile > kFlagRows) k_sgm_emulate<1024, 1, false><<<a.ghN, nw * 32, 0, s>>>(a);
-  else if (nw <= 16) k_sgm_emulate<512, 4, true><<<a.ghN, nw * 32, 0, s>>>(a);
-  else k_sgm_emulate<1024, 2, true><<<a.ghN, nw * 32, 0, s>>>(a);
+  const int blocks = a.ghN * a.parts;
+  if (!flags) k_sgm_emulate<1024, 1, false><<<blocks, nw * 32, 0, s>>>(a);
+  else if (nw <= 16) k_sgm_emulate<512, 4, true><<<blocks, nw * 32, 0, s>>>(a);
+  else k_sgm_emulate<1024, 2, true><<<blocks, nw * 32, 0, s>>>(a);
   count_launches(1);
 }
 

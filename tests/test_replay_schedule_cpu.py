@@ -1,0 +1,157 @@
+"""The exact replay's schedule (lux_b200/csrc/sgm_emulate.cu), checked on the CPU as a model of its waits.
+
+The reference runs DenseLayer.Pixel() (DenseStereoSgm.cs:234-317) band by band, tile by tile, row by row, column by
+column (DenseStereoSgm.cs:206-224), and its result depends on that order through the flat line buffer. The GPU replay
+runs pixels concurrently: a band of T rows is split into parts (blocks) of T/2 rows, a warp per row; inside a part row
+r runs offset u once row r-1 has finished offset u; a part's first row follows the last row of the part above (same
+tile and offset within a band, offset u of tile i+1 across bands); whole-tile waits cover the revisits of the last
+column. This test builds the happens-before graph of those waits and checks that every two Pixel() calls that touch a
+common line-buffer region, one of them writing, are ordered as the reference orders them, and that the graph has no
+cycle (no wait can deadlock).
+
+A call's footprint, in the sheared column xp of its pass (memory order runs with xp in pass +1, against it in pass -1):
+it writes its own slot (blocks and Min/Pix/Range entries) and spills past block 3 into the pad and first block-0
+elements of the next slot in memory; it reads the other half's slots xp-1..xp+1 (each block window +-1 element, which
+stays inside the blocks), the pad after its path-3 window, its own half's slot xp-1 (path 0, from that slot's pad) and
+the Min/Pix/Range entries of those slots and its own.
+"""
+from collections import deque
+
+import pytest
+
+
+def _footprint(h, xp, dirn):
+    hb = 1 - h
+    nxt = (lambda c: c + 1) if dirn > 0 else (lambda c: c - 1)
+    writes = {(h, "body", xp), (h, "meta", xp), (h, "pad", nxt(xp)), (h, "b0", nxt(xp))}
+    reads = {(hb, "body", xp - 1), (hb, "body", xp), (hb, "body", xp + 1), (hb, "pad", nxt(xp + 1)),
+             (h, "body", xp - 1), (h, "pad", xp - 1),
+             (hb, "meta", xp - 1), (hb, "meta", xp), (hb, "meta", xp + 1), (h, "meta", xp - 1), (h, "meta", xp)}
+    return writes, reads
+
+
+def _pixel_xp(W, T, i, r, u):
+    """The column of tile i's row r at offset u, or None (the kernel's emu_tile_pixel for rows inside the image)."""
+    xs = min(max(i * T - r, 0), W - 1)
+    xe = min(max(i * T + T - r, -1), W)
+    if xs == xe:
+        return None
+    if i * T - r >= W:  # the clamped row start revisits the last column
+        return W - 1 if u == 0 else None
+    xp = i * T - r + u
+    return xp if xs <= xp < xe else None
+
+
+def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False):
+    """Conflicting pairs the waits leave unordered (or -1 for a cycle). lower_part_rule plants the wrong rule: a lower
+    part waiting for the part above to finish its revisiting tile i+1, instead of the part above waiting for it."""
+    ghN, gwN = (H + T - 1) // T, (W + 2 * T - 1) // T
+    R = (T + parts - 1) // parts
+    ids, preds, pixels = {}, {}, []
+
+    def node(key):
+        if key not in ids:
+            ids[key] = len(ids)
+        return ids[key]
+
+    def edge(a, b):
+        preds.setdefault(b, set()).add(a)
+
+    def pub_row(j, part):
+        return min(part * R + R, T, H - j * T) - 1
+
+    for j in range(ghN):
+        for part in range(parts):
+            r0, r1 = part * R, min(part * R + R, T)
+            if j * T + r0 >= H:
+                continue  # a part below the image returns at once
+            rows = [r for r in range(r0, r1) if j * T + r < H]
+            for i in range(gwN):
+                for r in rows:
+                    for u in range(T):
+                        n = node((j, part, r, i, u))
+                        if u > 0:
+                            edge(node((j, part, r, i, u - 1)), n)
+                        if r > r0:  # the row above in this part through offset u
+                            edge(node((j, part, r - 1, i, u)), n)
+                        if u == 0 and i > 0:  # the block's barrier between tiles
+                            for r2 in rows:
+                                edge(node((j, part, r2, i - 1, T - 1)), n)
+                        if r == r0 and (j, part) != (0, 0):  # the part above's last row
+                            if part > 0:
+                                key = (j, part - 1, pub_row(j, part - 1), i, u)
+                            else:
+                                tgt = min((i + 1) * T + u + 1, gwN * T)
+                                key = (j - 1, parts - 1, pub_row(j - 1, parts - 1), (tgt - 1) // T, (tgt - 1) % T)
+                            edge(node(key), n)
+                        xp = _pixel_xp(W, T, i, r, u)
+                        if xp is not None:
+                            ref = (j, i, r, u if i * T - r < W else 0)
+                            pixels.append((ref, n, _footprint(1 if r % 2 == 0 else 0, xp, dirn)))
+                tile_waits = []
+                if part == 0 and j > 0 and (i + 2) * T >= W:
+                    tile_waits.append((j - 1, parts - 1, min(i + 3, gwN) - 1))
+                if lower_part_rule:
+                    if part > 0 and (i + 1) * T - (r0 - R) >= W:
+                        tile_waits.append((j, part - 1, min(i + 2, gwN) - 1))
+                elif part + 1 < parts and i > 0 and i * T - r0 >= W and j * T + r1 < H:
+                    tile_waits.append((j, part + 1, i - 1))
+                for (pj, pp, ti) in tile_waits:
+                    for r in rows:
+                        edge(node((pj, pp, pub_row(pj, pp), ti, T - 1)), node((j, part, r, i, 0)))
+    n_nodes = len(ids)
+    succ = [[] for _ in range(n_nodes)]
+    indeg = [0] * n_nodes
+    for b, ps in preds.items():
+        for a in ps:
+            succ[a].append(b)
+            indeg[b] += 1
+    queue, topo = deque(k for k in range(n_nodes) if indeg[k] == 0), []
+    while queue:
+        a = queue.popleft()
+        topo.append(a)
+        for b in succ[a]:
+            indeg[b] -= 1
+            if indeg[b] == 0:
+                queue.append(b)
+    if len(topo) != n_nodes:
+        return -1
+    before = [0] * n_nodes  # bitset of the nodes that happen before each node
+    for b in topo:
+        m = 0
+        for a in preds.get(b, ()):
+            m |= before[a] | (1 << a)
+        before[b] = m
+    pixels.sort(key=lambda p: p[0])
+    touches = {}
+    for idx, (_, _, (w, rd)) in enumerate(pixels):
+        for g in w:
+            touches.setdefault(g, []).append((idx, True))
+        for g in rd:
+            touches.setdefault(g, []).append((idx, False))
+    bad = set()
+    for lst in touches.values():
+        for x in range(len(lst)):
+            for y in range(x + 1, len(lst)):
+                (ia, wa), (ib, wb) = lst[x], lst[y]
+                if ia == ib or not (wa or wb):
+                    continue
+                a, b = min(ia, ib), max(ia, ib)
+                if not (before[pixels[b][1]] >> pixels[a][1]) & 1:
+                    bad.add((a, b))
+    return len(bad)
+
+
+@pytest.mark.parametrize("W,H,T", [(65, 49, 4), (48, 40, 8), (97, 61, 16), (70, 45, 32), (66, 65, 64), (33, 17, 2),
+                                   (40, 10, 4)])
+@pytest.mark.parametrize("dirn", [1, -1])
+def test_replay_waits_keep_the_reference_order(W, H, T, dirn):
+    parts = 2 if T >= 4 else 1  # as the launcher splits a band
+    assert unordered_pairs(W, H, T, parts, dirn) == 0
+    assert unordered_pairs(W, H, T, 1, dirn) == 0  # one block per band (tiles taller than the flag rows aside)
+
+
+def test_order_check_catches_a_wrong_revisit_rule():
+    """A lower part that waits for the upper part's revisiting tile i+1 runs the reference's order backwards there."""
+    assert unordered_pairs(65, 49, 4, 2, 1, lower_part_rule=True) > 0
+    assert unordered_pairs(30, 20, 4, 2, -1, lower_part_rule=True) > 0
