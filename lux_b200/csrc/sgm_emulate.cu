@@ -5,15 +5,19 @@
 // past a block see whatever the flat buffer holds there, and pass -1 starts from the state pass +1 left. This kernel
 // keeps the flat buffer (2 halves x (W+2) slots x (4·MaxHi+5) u16, plus Min/RangeS/RangeC/Pix) in global memory and runs
 // every Pixel() call of the reference in an order that gives each read the same last writer:
-//   * one CTA per band of T rows (tickets taken in order, so a band only ever waits on a running one);
-//   * tiles of a band in order; band j starts tile i once band j-1 has finished tile i+1. Tile i+2 of band j-1 may then
-//     run beside it: their nearest pixels are band j-1's last row at column iT+T+1 and band j's first row at iT+T-1,
-//     the upper row's pixel two columns right of the lower one, a pair that touches nothing in common (see the row
-//     hand-over below); every other pair is three or more columns apart. Where tile i+2 revisits the last column
-//     ((i+2)·T >= W, a pixel clamped to W-1), band j waits for tile i+2 as well;
-//   * inside a tile, pixel (row r, sheared offset u) runs at step u + 2r. Pixels that share or neighbour a slot (at most
-//     two columns and two rows apart) keep the reference's row-major order; pixels of one step are three or more
-//     columns apart. A revisit of the last column runs alone at step 2r.
+//   * a band of T >= 4 rows runs on two blocks (parts) of T/2 rows, a warp per row (one block below); blocks take tickets
+//     in order, so a part only ever waits on a running one;
+//   * a part runs its tiles in order (a block barrier between tiles); inside a tile, row r runs its offset u (pixel
+//     column iT - r + u) once row r-1 has finished offset u, and a part's first row follows the part above's last row:
+//     at the same tile and offset within a band, at offset u of tile i+1 across bands (the same sheared frame);
+//   * two calls touch a common element only when at most two columns apart, and the one pair this leaves unordered,
+//     the upper row's pixel two columns right of the lower one, touches nothing in common (see the row hand-over);
+//   * the revisits of the last column do not follow the sheared columns: a band's first part waits for tile i+2 of
+//     the band above when that tile revisits, and a part whose rows revisit in tile i first waits for the part below
+//     to finish tile i-1 (a band's tiles come in order in the reference);
+//   * tiles taller than the flag rows step with a block barrier instead, pixel (r, u) at step u + 2r (pixels of one step
+//     are three or more columns apart), one block per band, three tiles behind the band above.
+// tests/test_replay_schedule_cpu.py checks these waits against the reference's order as a happens-before model.
 // Within a Pixel() call a warp handles the lanes. The four paths run in order (a path may spill into the next), or at
 // once on four groups of eight lanes where no window of the call leaves its block.
 #include "common.cuh"
