@@ -307,7 +307,7 @@ LUX_DEV bool emu_tile_pixel(const EmuArgs& a, const EmuTileRow& t, int i, int r,
   return true;
 }
 
-constexpr int kFlagRows = 128;  // tiles up to this many rows hand over row to row; taller ones step with a barrier
+constexpr int kFlagRows = 64;  // tiles up to this many rows hand over row to row (a warp a row); taller ones step with a barrier
 
 // kThreads = 32·T/2 rounded up to the two sizes launched: 512 (T <= 32, four iterations a round trip within the
 // register budget) and 1024 (T >= 64, two). kFlags: the row-to-row hand-over below (T <= kFlagRows), else a barrier per
@@ -349,110 +349,125 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
   // not wait either: the last row of the part above, below the image too, publishes none.)
   if (j * T + r0 >= a.H) return;
   int* const above = a.progress + (k - 1);  // the part above: its last row's offsets
-  for (int i = 0; i < a.gwN; i++) {
+  if constexpr (kFlags) {
+    // One row per warp; s_row[r] counts row r's offsets done across tiles (i·T + u + 1). A row goes on into the next
+    // tile by itself: the only pixels of a later tile that lower rows' earlier tiles can touch are revisits of the
+    // last column, and a row waits for its part's last row to finish tile i-1 before revisiting in tile i.
     for (int r = tid; r < kFlagRows; r += blockDim.x) s_row[r] = 0;
+    __syncthreads();
+    const int r = r0 + warp;
+    if (r >= r1) return;
+    const int r_pub = min(r1, a.H - j * T) - 1;  // the part's last row inside the image, which publishes
+    if (j * T + r >= a.H) {                       // past the image: no pixels, and only rows past it wait on it
+      if (lane == 0) st_release_cta(&s_row[r], 0x7fffffff);
+      return;
+    }
+    const bool publish = r == r_pub;
+    int seen = 0;  // first row: the part above's last-row offsets seen so far
+    for (int i = 0; i < a.gwN; i++) {
+      const EmuTileRow row = emu_tile_row(a, j, i, r);
+      // Another block reads what this part's last two rows write (the row above it in the other half, the row two
+      // above in its own half: the Range entries of its stale cleanup, the line state it overwrites), and, on a tile
+      // before the part above revisits, what any row writes near the last column. Those rows' lanes make their
+      // writes visible to the GPU before the row's count moves on; the CTA-scope hand-over alone only orders them
+      // for this block.
+      const bool fence = r >= r_pub - 1 || (part > 0 && (i + 1) * T - (r0 - a.part_rows) >= a.W);
+      // Waits at the tile's start, around revisits of the last column (which do not follow the sheared columns):
+      // the first part's first row waits for tile i+2 of the band above when that tile revisits (the band above comes
+      // first in the reference); a first row whose part revisits in tile i waits for the part below to finish tile
+      // i-1, and any revisiting row for its own part's last row (a band's tiles come in order in the reference).
+      int gneed = 0;
+      int* gflag = above;
+      if (r == r0 && part == 0 && k > 0 && (i + 2) * T >= a.W) gneed = min(i + 3, a.gwN) * T;
+      if (r == r0 && part + 1 < a.parts && i > 0 && i * T - r0 >= a.W && j * T + r1 < a.H) {
+        gneed = i * T;  // (a first part's row r0 revisiting at tile i has no tile i+2 wait: i * T >= W)
+        gflag = a.progress + (k + 1);
+      }
+      bool failed = false;
+      if (gneed > 0 && __reduce_min_sync(0xffffffffu, wait_at_least_value(gflag, gneed, a.err, 11, a.timeout_ns)) < 0) {
+        failed = true;
+      } else if (i > 0 && i * T - r >= a.W && r != r_pub &&
+                 __any_sync(0xffffffffu, !wait_shared_at_least(&s_row[r_pub], i * T, &s_stop, a.timeout_ns))) {
+        failed = true;
+      }
+      if (failed) {
+        if (lane == 0) {
+          atomicCAS(a.err, 0, 11);  // LUX_ERR_TIMEOUT, or another warp's failure
+          s_stop = 1;
+        }
+        return;
+      }
+      int nx, ny;
+      bool has_next = emu_tile_pixel(a, row, i, r, 0, nx, ny);
+      EmuPix next;
+      if (has_next) next = emu_load_pix(a, nx, ny);
+      for (int u = 0; u < T; u++) {
+        const bool has = has_next;
+        const int x = nx;
+        const EmuPix px = next;
+        // The next offset's read-only inputs, loaded while this offset waits and runs.
+        has_next = u + 1 < T && emu_tile_pixel(a, row, i, r, u + 1, nx, ny);
+        if (has_next) next = emu_load_pix(a, nx, ny);
+        if (r > r0 && __any_sync(0xffffffffu, !wait_shared_at_least(&s_row[r - 1], i * T + u + 1, &s_stop, a.timeout_ns))) {
+          if (lane == 0) {
+            atomicCAS(a.err, 0, 11);
+            s_stop = 1;
+          }
+          return;
+        }
+        // The first row continues the part above's last row one row down: within the band, that row at the same
+        // tile and offset; across bands, the band above's last row at offset u of tile i+1 (the same sheared frame).
+        if (r == r0 && k > 0) {
+          const int target = part > 0 ? i * T + u + 1 : min((i + 1) * T + u + 1, a.gwN * T);
+          if (seen < target) {
+            seen = __reduce_min_sync(0xffffffffu, wait_at_least_value(above, target, a.err, 11, a.timeout_ns));
+            if (seen < 0) {
+              if (lane == 0) s_stop = 1;
+              return;
+            }
+          }
+        }
+        if (has) {
+          const int cur = (r & 1) == 0 ? 1 : 0;
+          emu_pixel<KB>(a, x, px, cur, 1 - cur, lane);
+        }
+        if (fence) __threadfence();
+        __syncwarp();
+        if (lane == 0) {
+          st_release_cta(&s_row[r], i * T + u + 1);
+          if (publish) st_release(a.progress + k, i * T + u + 1);  // all rows above it are through u as well
+        }
+      }
+    }
+  } else {
+  // Tiles taller than the flag rows: a block barrier per step of the sheared schedule, three tiles behind the band
+  // above (progress counts tiles times T).
+  for (int i = 0; i < a.gwN; i++) {
     if (tid == 0) {
-      // Whole tiles to wait for (progress counts a part's last row's offsets, T a tile). The barrier form keeps a
-      // lag of three tiles on the band above. The row form waits row by row below, and here only around revisits of
-      // the last column, which do not follow the sheared columns: for the first part, tile i+2 of the band above when
-      // it revisits (the band above comes first in the reference); for a part whose rows revisit in tile i, tile i-1
-      // of the part below in this band (a band's tiles come in order, so the rows below finish tile i-1 first).
-      int need = 0;
-      if (!kFlags) need = min(i + 3, a.gwN) * T;
-      else if (part == 0 && (i + 2) * T >= a.W) need = min(i + 3, a.gwN) * T;
-      if (k > 0 && need > 0 && !wait_at_least(above, need, a.err, 11 /* LUX_ERR_TIMEOUT */, a.timeout_ns)) s_stop = 1;
-      if (kFlags && part + 1 < a.parts && i > 0 && i * T - r0 >= a.W && j * T + r1 < a.H &&
-          !wait_at_least(a.progress + (k + 1), i * T, a.err, 11, a.timeout_ns))
-        s_stop = 1;
+      if (k > 0 && !wait_at_least(above, min(i + 3, a.gwN) * T, a.err, 11 /* LUX_ERR_TIMEOUT */, a.timeout_ns)) s_stop = 1;
       if (*(volatile int*)a.err != 0) s_stop = 1;
     }
     __syncthreads();
     if (s_stop) break;
-    if (kFlags) {  // T <= kFlagRows (the launcher's choice)
-      for (int r = r0 + warp; r < r1; r += nw) {
+    for (int t = 0; t <= 3 * T - 3; t++) {
+      const int rlo = max(0, (t - T + 2) / 2), rhi = min(T - 1, t / 2);
+      for (int r = rlo + warp; r <= rhi; r += nw) {
+        const int u = t - 2 * r;
         const EmuTileRow row = emu_tile_row(a, j, i, r);
-        if (row.yp >= a.H) {  // past the image: this row and every later one have no pixels
-          __syncwarp();
-          if (lane == 0) st_release_cta(&s_row[r], T);
-          continue;
-        }
-        bool failed = false;
-        int seen = 0;  // first row: the part above's last-row offsets seen so far
-        // The publisher is the part's last row inside the image; the part below (or the band below) waits on it, and
-        // the part above on its last offset of a tile where the part above revisits next.
-        const int r_pub = min(r1, a.H - j * T) - 1;
-        const bool publish = r == r_pub;
-        // Another block reads what this part's last two rows write (the row above it in the other half, the row two
-        // above in its own half: the Range entries of its stale cleanup, the line state it overwrites), and, on a tile
-        // before the part above revisits, what any row writes near the last column. Those rows' lanes make their
-        // writes visible to the GPU before the row's count moves on; the CTA-scope hand-over alone only orders them
-        // for this block.
-        const bool fence = r >= r_pub - 1 || (part > 0 && (i + 1) * T - (r0 - a.part_rows) >= a.W);
-        int nx, ny;
-        bool has_next = emu_tile_pixel(a, row, i, r, 0, nx, ny);
-        EmuPix next;
-        if (has_next) next = emu_load_pix(a, nx, ny);
-        for (int u = 0; u < T; u++) {
-          const bool has = has_next;
-          const int x = nx;
-          const EmuPix px = next;
-          // The next offset's read-only inputs, loaded while this offset waits and runs.
-          has_next = u + 1 < T && emu_tile_pixel(a, row, i, r, u + 1, nx, ny);
-          if (has_next) next = emu_load_pix(a, nx, ny);
-          if (r > r0 && __any_sync(0xffffffffu, !wait_shared_at_least(&s_row[r - 1], u + 1, &s_stop, a.timeout_ns))) {
-            if (lane == 0) {
-              atomicCAS(a.err, 0, 11);  // LUX_ERR_TIMEOUT, or another warp's failure
-              s_stop = 1;
-            }
-            failed = true;
-            break;
-          }
-          // The first row continues the part above's last row one row down: within the band, that row at the same
-          // tile and offset; across bands, the band above's last row at offset u of tile i+1 (the same sheared frame).
-          if (r == r0 && k > 0) {
-            const int target = part > 0 ? i * T + u + 1 : min((i + 1) * T + u + 1, a.gwN * T);
-            if (seen < target) {
-              seen = __reduce_min_sync(0xffffffffu, wait_at_least_value(above, target, a.err, 11, a.timeout_ns));
-              if (seen < 0) {
-                if (lane == 0) s_stop = 1;
-                failed = true;
-                break;
-              }
-            }
-          }
-          if (has) {
-            const int cur = (r & 1) == 0 ? 1 : 0;
-            emu_pixel<KB>(a, x, px, cur, 1 - cur, lane);
-          }
-          if (fence) __threadfence();
-          __syncwarp();
-          if (lane == 0) {
-            st_release_cta(&s_row[r], u + 1);
-            if (publish) st_release(a.progress + k, i * T + u + 1);  // all rows above it are through u as well
-          }
-        }
-        if (failed) break;
+        int x, y;
+        if (!emu_tile_pixel(a, row, i, r, u, x, y)) continue;
+        const int cur = (r & 1) == 0 ? 1 : 0;
+        emu_pixel<KB>(a, x, emu_load_pix(a, x, y), cur, 1 - cur, lane);
       }
-    } else {
-      for (int t = 0; t <= 3 * T - 3; t++) {
-        const int rlo = max(0, (t - T + 2) / 2), rhi = min(T - 1, t / 2);
-        for (int r = rlo + warp; r <= rhi; r += nw) {
-          const int u = t - 2 * r;
-          const EmuTileRow row = emu_tile_row(a, j, i, r);
-          int x, y;
-          if (!emu_tile_pixel(a, row, i, r, u, x, y)) continue;
-          const int cur = (r & 1) == 0 ? 1 : 0;
-          emu_pixel<KB>(a, x, emu_load_pix(a, x, y), cur, 1 - cur, lane);
-        }
-        __syncthreads();
-      }
+      __syncthreads();
     }
     __syncthreads();
     if (s_stop) break;
-    if (!kFlags && tid == 0) {
+    if (tid == 0) {
       __threadfence();
       st_release(a.progress + k, (i + 1) * T);
     }
+  }
   }
 }
 
@@ -497,8 +512,11 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   a.p2base = p1f * p2scale;  // (float)P1 * P2Scale (:256)
   for (int i = 0; i < 4; i++) a.gw[i] = gw[i];
   int pass = dir > 0 ? 0 : 1;
-  // The row form splits a band of T >= 4 rows between two blocks (parts) of T/2 rows, a warp a row up to 32 rows.
-  const bool flags = g.tile <= kFlagRows;
+  // The row form splits a band of T >= 4 rows between two blocks (parts) of T/2 rows, a warp a row up to 32 rows. It
+  // needs an even T: the line-buffer half of a row follows its row in the tile (as in the reference), so with an odd T
+  // a band's last row and the next band's first row share a half, and the pair two columns apart that the row form
+  // leaves unordered would then meet (the upper pixel's path-0 read of the slot the lower one spills into).
+  const bool flags = g.tile <= kFlagRows && g.tile % 2 == 0;
   a.parts = flags && g.tile >= 4 ? kEmuParts : 1;
   a.part_rows = (g.tile + a.parts - 1) / a.parts;
   a.ticket = b.ticket + pass;

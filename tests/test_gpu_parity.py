@@ -70,6 +70,23 @@ def test_uniform_layer_bit_exact(ctx, oracle, w, h, d, tile, kernel):
         gl.close()
 
 
+@pytest.mark.parametrize("w,h,d,tile", [(50, 23, 24, 3), (41, 30, 16, 5), (150, 140, 16, 96)])
+def test_replay_barrier_form_bit_exact(ctx, oracle, w, h, d, tile):
+    """Tiles the row hand-over does not take (odd tiles, whose bands' boundary rows share a line-buffer half, and tiles
+    past 64 rows) step with a block barrier: the exact replay, bit for bit."""
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(w, h, d, seed=w * h, tile=tile)
+    filt = _filtered(oracle, wl.images)
+    ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, keep_agg=True,
+                                ctx=ctx, force_replay=True)
+    try:
+        assert gl.sgm_kernel == SGM_FORMS["replay"]
+        _compare_layer(gl, ol, f"{w}x{h} D{d} T{tile} replay")
+    finally:
+        gl.close()
+
+
 @pytest.mark.parametrize("kernel", ["fused", "split"])
 def test_uniform_fast_depth_without_kept_aggregates(ctx, oracle, kernel):
     """The production form (no Agg kept, WTA fused into the last kernel of pass -1) gives the same depth."""

@@ -2,12 +2,12 @@
 
 The reference runs DenseLayer.Pixel() (DenseStereoSgm.cs:234-317) band by band, tile by tile, row by row, column by
 column (DenseStereoSgm.cs:206-224), and its result depends on that order through the flat line buffer. The GPU replay
-runs pixels concurrently: a band of T rows is split into parts (blocks) of T/2 rows, a warp per row; inside a part row
-r runs offset u once row r-1 has finished offset u; a part's first row follows the last row of the part above (same
-tile and offset within a band, offset u of tile i+1 across bands); whole-tile waits cover the revisits of the last
-column. This test builds the happens-before graph of those waits and checks that every two Pixel() calls that touch a
-common line-buffer region, one of them writing, are ordered as the reference orders them, and that the graph has no
-cycle (no wait can deadlock).
+runs pixels concurrently: a band of T rows is split into parts (blocks) of T/2 rows, a warp per row, and each row goes
+through its tiles on its own; row r runs offset u of tile i once row r-1 has finished it; a part's first row follows
+the last row of the part above (same tile and offset within a band, offset u of tile i+1 across bands); waits at a
+tile's start cover the revisits of the last column. This test builds the happens-before graph of those waits and
+checks that every two Pixel() calls that touch a common line-buffer region, one of them writing, are ordered as the
+reference orders them, and that the graph has no cycle (no wait can deadlock).
 
 A call's footprint, in the sheared column xp of its pass (memory order runs with xp in pass +1, against it in pass -1):
 it writes its own slot (blocks and Min/Pix/Range entries) and spills past block 3 into the pad and first block-0
@@ -42,9 +42,10 @@ def _pixel_xp(W, T, i, r, u):
     return xp if xs <= xp < xe else None
 
 
-def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False):
-    """Conflicting pairs the waits leave unordered (or -1 for a cycle). lower_part_rule plants the wrong rule: a lower
-    part waiting for the part above to finish its revisiting tile i+1, instead of the part above waiting for it."""
+def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False, own_part_rule=True):
+    """Conflicting pairs the waits leave unordered (or -1 for a cycle). Planted mistakes: lower_part_rule makes a lower
+    part wait for the part above to finish its revisiting tile i+1 (instead of the part above waiting for it);
+    own_part_rule=False drops the wait of a revisiting row for its own part's last row."""
     ghN, gwN = (H + T - 1) // T, (W + 2 * T - 1) // T
     R = (T + parts - 1) // parts
     ids, preds, pixels = {}, {}, []
@@ -66,17 +67,17 @@ def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False):
             if j * T + r0 >= H:
                 continue  # a part below the image returns at once
             rows = [r for r in range(r0, r1) if j * T + r < H]
-            for i in range(gwN):
-                for r in rows:
+            rp = pub_row(j, part)
+            for r in rows:
+                for i in range(gwN):
                     for u in range(T):
                         n = node((j, part, r, i, u))
                         if u > 0:
                             edge(node((j, part, r, i, u - 1)), n)
+                        elif i > 0:  # the row's own previous tile
+                            edge(node((j, part, r, i - 1, T - 1)), n)
                         if r > r0:  # the row above in this part through offset u
                             edge(node((j, part, r - 1, i, u)), n)
-                        if u == 0 and i > 0:  # the block's barrier between tiles
-                            for r2 in rows:
-                                edge(node((j, part, r2, i - 1, T - 1)), n)
                         if r == r0 and (j, part) != (0, 0):  # the part above's last row
                             if part > 0:
                                 key = (j, part - 1, pub_row(j, part - 1), i, u)
@@ -84,21 +85,23 @@ def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False):
                                 tgt = min((i + 1) * T + u + 1, gwN * T)
                                 key = (j - 1, parts - 1, pub_row(j - 1, parts - 1), (tgt - 1) // T, (tgt - 1) % T)
                             edge(node(key), n)
+                        if u == 0:  # waits at the tile's start
+                            waits = []
+                            if r == r0 and part == 0 and j > 0 and (i + 2) * T >= W:
+                                waits.append((j - 1, parts - 1, min(i + 3, gwN) - 1))
+                            if lower_part_rule:
+                                if r == r0 and part > 0 and (i + 1) * T - (r0 - R) >= W:
+                                    waits.append((j, part - 1, min(i + 2, gwN) - 1))
+                            elif r == r0 and part + 1 < parts and i > 0 and i * T - r0 >= W and j * T + r1 < H:
+                                waits.append((j, part + 1, i - 1))
+                            if own_part_rule and i > 0 and i * T - r >= W and r != rp:
+                                waits.append((j, part, i - 1))
+                            for (pj, pp, ti) in waits:
+                                edge(node((pj, pp, pub_row(pj, pp), ti, T - 1)), n)
                         xp = _pixel_xp(W, T, i, r, u)
                         if xp is not None:
                             ref = (j, i, r, u if i * T - r < W else 0)
                             pixels.append((ref, n, _footprint(1 if r % 2 == 0 else 0, xp, dirn)))
-                tile_waits = []
-                if part == 0 and j > 0 and (i + 2) * T >= W:
-                    tile_waits.append((j - 1, parts - 1, min(i + 3, gwN) - 1))
-                if lower_part_rule:
-                    if part > 0 and (i + 1) * T - (r0 - R) >= W:
-                        tile_waits.append((j, part - 1, min(i + 2, gwN) - 1))
-                elif part + 1 < parts and i > 0 and i * T - r0 >= W and j * T + r1 < H:
-                    tile_waits.append((j, part + 1, i - 1))
-                for (pj, pp, ti) in tile_waits:
-                    for r in rows:
-                        edge(node((pj, pp, pub_row(pj, pp), ti, T - 1)), node((j, part, r, i, 0)))
     n_nodes = len(ids)
     succ = [[] for _ in range(n_nodes)]
     indeg = [0] * n_nodes
@@ -143,15 +146,23 @@ def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False):
 
 
 @pytest.mark.parametrize("W,H,T", [(65, 49, 4), (48, 40, 8), (97, 61, 16), (70, 45, 32), (66, 65, 64), (33, 17, 2),
-                                   (40, 10, 4)])
+                                   (40, 10, 4), (20, 11, 6)])
 @pytest.mark.parametrize("dirn", [1, -1])
 def test_replay_waits_keep_the_reference_order(W, H, T, dirn):
     parts = 2 if T >= 4 else 1  # as the launcher splits a band
     assert unordered_pairs(W, H, T, parts, dirn) == 0
-    assert unordered_pairs(W, H, T, 1, dirn) == 0  # one block per band (tiles taller than the flag rows aside)
 
 
 def test_order_check_catches_a_wrong_revisit_rule():
-    """A lower part that waits for the upper part's revisiting tile i+1 runs the reference's order backwards there."""
+    """A lower part that waits for the upper part's revisiting tile i+1 runs the reference's order backwards there, and
+    a revisiting row that does not wait for the rows below it in its part overtakes their previous tile."""
     assert unordered_pairs(65, 49, 4, 2, 1, lower_part_rule=True) > 0
     assert unordered_pairs(30, 20, 4, 2, -1, lower_part_rule=True) > 0
+    assert unordered_pairs(70, 45, 32, 2, 1, own_part_rule=False) > 0
+    assert unordered_pairs(40, 10, 4, 2, -1, own_part_rule=False) > 0
+
+
+def test_odd_tiles_need_the_barrier_form():
+    """With an odd T a band's last row and the next band's first row share a line-buffer half, and the row form's
+    hand-over leaves a conflicting pair unordered there: the launcher gives odd tiles the barrier form."""
+    assert unordered_pairs(20, 11, 3, 1, 1) > 0
