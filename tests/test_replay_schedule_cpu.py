@@ -42,6 +42,52 @@ def _pixel_xp(W, T, i, r, u):
     return xp if xs <= xp < xe else None
 
 
+def _count_unordered(ids, preds, pixels):
+    """Conflicting pairs of calls the happens-before graph leaves unordered against the reference's order, or -1 when
+    the graph has a cycle."""
+    n_nodes = len(ids)
+    succ = [[] for _ in range(n_nodes)]
+    indeg = [0] * n_nodes
+    for b, ps in preds.items():
+        for a in ps:
+            succ[a].append(b)
+            indeg[b] += 1
+    queue, topo = deque(k for k in range(n_nodes) if indeg[k] == 0), []
+    while queue:
+        a = queue.popleft()
+        topo.append(a)
+        for b in succ[a]:
+            indeg[b] -= 1
+            if indeg[b] == 0:
+                queue.append(b)
+    if len(topo) != n_nodes:
+        return -1
+    before = [0] * n_nodes  # bitset of the nodes that happen before each node
+    for b in topo:
+        m = 0
+        for a in preds.get(b, ()):
+            m |= before[a] | (1 << a)
+        before[b] = m
+    pixels.sort(key=lambda p: p[0])
+    touches = {}
+    for idx, (_, _, (w, rd)) in enumerate(pixels):
+        for g in w:
+            touches.setdefault(g, []).append((idx, True))
+        for g in rd:
+            touches.setdefault(g, []).append((idx, False))
+    bad = set()
+    for lst in touches.values():
+        for x in range(len(lst)):
+            for y in range(x + 1, len(lst)):
+                (ia, wa), (ib, wb) = lst[x], lst[y]
+                if ia == ib or not (wa or wb):
+                    continue
+                a, b = min(ia, ib), max(ia, ib)
+                if not (before[pixels[b][1]] >> pixels[a][1]) & 1:
+                    bad.add((a, b))
+    return len(bad)
+
+
 def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False, own_part_rule=True):
     """Conflicting pairs the waits leave unordered (or -1 for a cycle). Planted mistakes: lower_part_rule makes a lower
     part wait for the part above to finish its revisiting tile i+1 (instead of the part above waiting for it);
@@ -102,47 +148,49 @@ def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False, own_part_rule=T
                         if xp is not None:
                             ref = (j, i, r, u if i * T - r < W else 0)
                             pixels.append((ref, n, _footprint(1 if r % 2 == 0 else 0, xp, dirn)))
-    n_nodes = len(ids)
-    succ = [[] for _ in range(n_nodes)]
-    indeg = [0] * n_nodes
-    for b, ps in preds.items():
-        for a in ps:
-            succ[a].append(b)
-            indeg[b] += 1
-    queue, topo = deque(k for k in range(n_nodes) if indeg[k] == 0), []
-    while queue:
-        a = queue.popleft()
-        topo.append(a)
-        for b in succ[a]:
-            indeg[b] -= 1
-            if indeg[b] == 0:
-                queue.append(b)
-    if len(topo) != n_nodes:
-        return -1
-    before = [0] * n_nodes  # bitset of the nodes that happen before each node
-    for b in topo:
-        m = 0
-        for a in preds.get(b, ()):
-            m |= before[a] | (1 << a)
-        before[b] = m
-    pixels.sort(key=lambda p: p[0])
-    touches = {}
-    for idx, (_, _, (w, rd)) in enumerate(pixels):
-        for g in w:
-            touches.setdefault(g, []).append((idx, True))
-        for g in rd:
-            touches.setdefault(g, []).append((idx, False))
-    bad = set()
-    for lst in touches.values():
-        for x in range(len(lst)):
-            for y in range(x + 1, len(lst)):
-                (ia, wa), (ib, wb) = lst[x], lst[y]
-                if ia == ib or not (wa or wb):
-                    continue
-                a, b = min(ia, ib), max(ia, ib)
-                if not (before[pixels[b][1]] >> pixels[a][1]) & 1:
-                    bad.add((a, b))
-    return len(bad)
+    return _count_unordered(ids, preds, pixels)
+
+
+def unordered_pairs_barrier_form(W, H, T, dirn, lag=3):
+    """The same check for the barrier form (odd tiles, tiles past 64 rows): one block per band, pixel (r, u) of a tile at
+    step u + 2r with a block barrier after every step and tile, a band starting tile i once the band above finished tile
+    i + lag - 1 (lag 3 in the kernel)."""
+    ghN, gwN = (H + T - 1) // T, (W + 2 * T - 1) // T
+    ids, preds, pixels = {}, {}, []
+
+    def node(key):
+        if key not in ids:
+            ids[key] = len(ids)
+        return ids[key]
+
+    def edge(a, b):
+        preds.setdefault(b, set()).add(a)
+
+    steps = 3 * T - 2
+    for j in range(ghN):
+        for i in range(gwN):
+            start = node((j, i, "start"))
+            if i > 0:
+                edge(node((j, i - 1, "step", steps - 1)), start)
+            if j > 0:
+                edge(node((j - 1, min(i + lag - 1, gwN - 1), "step", steps - 1)), start)
+            prev = start
+            for t in range(steps):
+                done = node((j, i, "step", t))
+                for r in range(max(0, (t - T + 2) // 2), min(T - 1, t // 2) + 1):
+                    u = t - 2 * r
+                    if j * T + r >= H:
+                        continue
+                    xp = _pixel_xp(W, T, i, r, u)
+                    if xp is None:
+                        continue
+                    n = node((j, i, r, u))
+                    edge(prev, n)
+                    edge(n, done)
+                    pixels.append(((j, i, r, u if i * T - r < W else 0), n, _footprint(1 if r % 2 == 0 else 0, xp, dirn)))
+                edge(prev, done)
+                prev = done
+    return _count_unordered(ids, preds, pixels)
 
 
 @pytest.mark.parametrize("W,H,T", [(65, 49, 4), (48, 40, 8), (97, 61, 16), (70, 45, 32), (66, 65, 64), (33, 17, 2),
@@ -166,3 +214,14 @@ def test_odd_tiles_need_the_barrier_form():
     """With an odd T a band's last row and the next band's first row share a line-buffer half, and the row form's
     hand-over leaves a conflicting pair unordered there: the launcher gives odd tiles the barrier form."""
     assert unordered_pairs(20, 11, 3, 1, 1) > 0
+
+
+@pytest.mark.parametrize("W,H,T", [(20, 11, 3), (41, 30, 5), (23, 16, 3)])
+@pytest.mark.parametrize("dirn", [1, -1])
+def test_barrier_form_keeps_the_reference_order(W, H, T, dirn):
+    assert unordered_pairs_barrier_form(W, H, T, dirn) == 0
+
+
+def test_barrier_form_needs_its_band_lag():
+    """A one-tile band lag lets a band run beside the band above's next tile, which an odd tile's shared half forbids."""
+    assert unordered_pairs_barrier_form(20, 11, 3, 1, lag=1) > 0
