@@ -134,7 +134,7 @@ struct EmuBuffers {
   int* ticket;    // [2]
   int* progress;  // [2 * bands * kEmuParts]
 };
-constexpr int kEmuParts = 2;  // blocks per band of the exact replay (row halves)
+constexpr int kEmuParts = 4;  // at most, blocks per band of the exact replay (parts of min(16, T/2) rows)
 size_t emu_line_buffer_elems(int W, int max_hi);
 void emu_init_buffers(const EmuBuffers& b, int W, int max_hi, int align, int bands, cudaStream_t s);
 void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xsw, uint16_t p1, float p2scale, const float gw[4],

@@ -5,16 +5,16 @@
 // past a block see whatever the flat buffer holds there, and pass -1 starts from the state pass +1 left. This kernel
 // keeps the flat buffer (2 halves x (W+2) slots x (4·MaxHi+5) u16, plus Min/RangeS/RangeC/Pix) in global memory and runs
 // every Pixel() call of the reference in an order that gives each read the same last writer:
-//   * a band of T >= 4 rows runs on two blocks (parts) of T/2 rows, a warp per row (one block below); blocks take tickets
-//     in order, so a part only ever waits on a running one;
+//   * a band of T >= 4 rows runs on blocks (parts) of min(16, T/2) rows, a warp per row (one block below); blocks take
+//     tickets in order, so a part only ever waits on a running one;
 //   * a part runs its tiles in order (a block barrier between tiles); inside a tile, row r runs its offset u (pixel
 //     column iT - r + u) once row r-1 has finished offset u, and a part's first row follows the part above's last row:
 //     at the same tile and offset within a band, at offset u of tile i+1 across bands (the same sheared frame);
 //   * two calls touch a common element only when at most two columns apart, and the one pair this leaves unordered,
 //     the upper row's pixel two columns right of the lower one, touches nothing in common (see the row hand-over);
 //   * the revisits of the last column do not follow the sheared columns: a band's first part waits for tile i+2 of
-//     the band above when that tile revisits, and a part whose rows revisit in tile i first waits for the part below
-//     to finish tile i-1 (a band's tiles come in order in the reference);
+//     the band above when that tile revisits, and a part whose rows revisit in tile i first waits for the band's last
+//     part to finish tile i-1 (a band's tiles come in order in the reference);
 //   * tiles taller than the flag rows step with a block barrier instead, pixel (r, u) at step u + 2r (pixels of one step
 //     are three or more columns apart), one block per band, three tiles behind the band above.
 // tests/test_replay_schedule_cpu.py checks these waits against the reference's order as a happens-before model.
@@ -309,12 +309,13 @@ LUX_DEV bool emu_tile_pixel(const EmuArgs& a, const EmuTileRow& t, int i, int r,
 
 constexpr int kFlagRows = 64;  // tiles up to this many rows hand over row to row (a warp a row); taller ones step with a barrier
 
-// kThreads = 32·T/2 rounded up to the two sizes launched: 512 (T <= 32, four iterations a round trip within the
-// register budget) and 1024 (T >= 64, two). kFlags: the row-to-row hand-over below (T <= kFlagRows), else a barrier per
+// kThreads bounds the block: 512 for the row form (parts of at most 16 rows; four iterations a round trip within the
+// register budget), 1024 for the barrier form (T/2 warps, one iteration). kFlags: the row hand-over below (even
+// T <= kFlagRows), else a barrier per
 // step of the sheared schedule, pixel (r, u) at step u + 2r (pixels of one step are three or more columns apart).
 //
-// Inside a tile, each warp owns whole rows (r = warp, warp + nw, ...) and runs a row's offsets u in order; row r runs
-// offset u once row r-1 has finished offset u (a CTA-scope release/acquire of the row's count in shared memory): the
+// Each warp owns one row of its part and runs the row's offsets u in order through all tiles; row r runs offset u of a
+// tile once row r-1 has finished offset u (a CTA-scope release/acquire of the row's count in shared memory): the
 // recurrence reads row r-1 at columns x-1, x and x+1, offsets u-2..u. For rows r1 < r2 this orders (r1, u1) before
 // (r2, u2) whenever u1 <= u2. Two pixels touch a common element only when at most two columns apart, x1 - x2 =
 // (r2 - r1) + (u1 - u2) <= 2, so the one pair left unordered is the upper row's pixel two columns right of the lower
@@ -371,17 +372,19 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
       // before the part above revisits, what any row writes near the last column. Those rows' lanes make their
       // writes visible to the GPU before the row's count moves on; the CTA-scope hand-over alone only orders them
       // for this block.
-      const bool fence = r >= r_pub - 1 || (part > 0 && (i + 1) * T - (r0 - a.part_rows) >= a.W);
+      const bool fence = r >= r_pub - 1 || (part > 0 && (i + 1) * T >= a.W);
       // Waits at the tile's start, around revisits of the last column (which do not follow the sheared columns):
       // the first part's first row waits for tile i+2 of the band above when that tile revisits (the band above comes
-      // first in the reference); a first row whose part revisits in tile i waits for the part below to finish tile
-      // i-1, and any revisiting row for its own part's last row (a band's tiles come in order in the reference).
+      // first in the reference); a first row whose part revisits in tile i waits for the band's last part (and so
+      // every part below it) to finish tile i-1, and any revisiting row for its own part's last row (a band's tiles
+      // come in order in the reference).
       int gneed = 0;
       int* gflag = above;
       if (r == r0 && part == 0 && k > 0 && (i + 2) * T >= a.W) gneed = min(i + 3, a.gwN) * T;
-      if (r == r0 && part + 1 < a.parts && i > 0 && i * T - r0 >= a.W && j * T + r1 < a.H) {
+      const int last = min(a.parts - 1, (a.H - j * T - 1) / a.part_rows);  // the band's last part inside the image
+      if (r == r0 && part < last && i > 0 && i * T - r0 >= a.W) {
         gneed = i * T;  // (a first part's row r0 revisiting at tile i has no tile i+2 wait: i * T >= W)
-        gflag = a.progress + (k + 1);
+        gflag = a.progress + ((size_t)j * a.parts + last);
       }
       bool failed = false;
       if (gneed > 0 && __reduce_min_sync(0xffffffffu, wait_at_least_value(gflag, gneed, a.err, 11, a.timeout_ns)) < 0) {
@@ -512,13 +515,13 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   a.p2base = p1f * p2scale;  // (float)P1 * P2Scale (:256)
   for (int i = 0; i < 4; i++) a.gw[i] = gw[i];
   int pass = dir > 0 ? 0 : 1;
-  // The row form splits a band of T >= 4 rows between two blocks (parts) of T/2 rows, a warp a row up to 32 rows. It
-  // needs an even T: the line-buffer half of a row follows its row in the tile (as in the reference), so with an odd T
+  // The row form splits a band of T >= 4 rows between blocks (parts) of min(16, T/2) rows, a warp a row (up to 16
+  // warps a block: 128 registers a thread, four iterations a round trip). It needs an even T: the line-buffer half of a row follows its row in the tile (as in the reference), so with an odd T
   // a band's last row and the next band's first row share a half, and the pair two columns apart that the row form
   // leaves unordered would then meet (the upper pixel's path-0 read of the slot the lower one spills into).
   const bool flags = g.tile <= kFlagRows && g.tile % 2 == 0;
-  a.parts = flags && g.tile >= 4 ? kEmuParts : 1;
-  a.part_rows = (g.tile + a.parts - 1) / a.parts;
+  a.part_rows = flags && g.tile >= 4 ? min(16, g.tile / 2) : g.tile;
+  a.parts = (g.tile + a.part_rows - 1) / a.part_rows;  // at most kEmuParts (T <= kFlagRows = 64)
   a.ticket = b.ticket + pass;
   a.progress = b.progress + (size_t)pass * a.ghN * kEmuParts;
   a.err = err;
@@ -528,8 +531,7 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   if (nw > 32) nw = 32;
   const int blocks = a.ghN * a.parts;
   if (!flags) k_sgm_emulate<1024, 1, false><<<blocks, nw * 32, 0, s>>>(a);
-  else if (nw <= 16) k_sgm_emulate<512, 4, true><<<blocks, nw * 32, 0, s>>>(a);
-  else k_sgm_emulate<1024, 2, true><<<blocks, nw * 32, 0, s>>>(a);
+  else k_sgm_emulate<512, 4, true><<<blocks, nw * 32, 0, s>>>(a);  // nw = part_rows <= 16
   count_launches(1);
 }
 

@@ -2,7 +2,7 @@
 
 The reference runs DenseLayer.Pixel() (DenseStereoSgm.cs:234-317) band by band, tile by tile, row by row, column by
 column (DenseStereoSgm.cs:206-224), and its result depends on that order through the flat line buffer. The GPU replay
-runs pixels concurrently: a band of T rows is split into parts (blocks) of T/2 rows, a warp per row, and each row goes
+runs pixels concurrently: a band of T rows is split into parts (blocks) of min(16, T/2) rows, a warp per row, and each row goes
 through its tiles on its own; row r runs offset u of tile i once row r-1 has finished it; a part's first row follows
 the last row of the part above (same tile and offset within a band, offset u of tile i+1 across bands); waits at a
 tile's start cover the revisits of the last column. This test builds the happens-before graph of those waits and
@@ -139,7 +139,8 @@ def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False, own_part_rule=T
                                 if r == r0 and part > 0 and (i + 1) * T - (r0 - R) >= W:
                                     waits.append((j, part - 1, min(i + 2, gwN) - 1))
                             elif r == r0 and part + 1 < parts and i > 0 and i * T - r0 >= W and j * T + r1 < H:
-                                waits.append((j, part + 1, i - 1))
+                                last = min(parts - 1, (H - j * T - 1) // R)  # the band's last part with rows in the image
+                                waits.append((j, last, i - 1))
                             if own_part_rule and i > 0 and i * T - r >= W and r != rp:
                                 waits.append((j, part, i - 1))
                             for (pj, pp, ti) in waits:
@@ -197,7 +198,7 @@ def unordered_pairs_barrier_form(W, H, T, dirn, lag=3):
                                    (40, 10, 4), (20, 11, 6)])
 @pytest.mark.parametrize("dirn", [1, -1])
 def test_replay_waits_keep_the_reference_order(W, H, T, dirn):
-    parts = 2 if T >= 4 else 1  # as the launcher splits a band
+    parts = T // min(16, T // 2) if T >= 4 else 1  # as the launcher splits a band: parts of min(16, T/2) rows
     assert unordered_pairs(W, H, T, parts, dirn) == 0
 
 
@@ -208,6 +209,12 @@ def test_order_check_catches_a_wrong_revisit_rule():
     assert unordered_pairs(30, 20, 4, 2, -1, lower_part_rule=True) > 0
     assert unordered_pairs(70, 45, 32, 2, 1, own_part_rule=False) > 0
     assert unordered_pairs(40, 10, 4, 2, -1, own_part_rule=False) > 0
+
+
+def test_four_parts_wait_for_the_last_part():
+    """With more than two parts, a revisiting part must wait for the band's last part, not only the next one down."""
+    assert unordered_pairs(66, 65, 64, 4, 1) == 0
+    assert unordered_pairs(66, 100, 64, 4, -1) == 0
 
 
 def test_odd_tiles_need_the_barrier_form():
