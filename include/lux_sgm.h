@@ -78,6 +78,17 @@ uint64_t lux_sgm_kernel_launches(void);
 /* The context's CUDA stream (a cudaStream_t), for callers that record events or order work against it. */
 void* lux_sgm_stream(lux_sgm_ctx* ctx);
 
+/* Failure detection (no counterpart in the reference, whose CPU loops cannot stall on another thread's progress). Every
+ * device-side wait of the aggregation kernels (a block waiting for the block above it, a warp for its neighbour) is
+ * bounded by this limit in ns of the GPU's global timer; when it passes, the kernel stops, the solve returns
+ * LUX_ERR_TIMEOUT and the context stays usable. 0 restores the default (20 s). */
+int lux_sgm_set_wait_limit(lux_sgm_ctx* ctx, uint64_t limit_ns);
+uint64_t lux_sgm_get_wait_limit(const lux_sgm_ctx* ctx);
+/* For tests of the failure path only: the aggregation block with ticket `block` (>= 1; -1 turns it off) waits for the
+ * block before it on a counter that nothing publishes, so the wait runs out after the wait limit and the solve returns
+ * LUX_ERR_TIMEOUT. Nothing faults; the other blocks see the error word and return. */
+int lux_sgm_debug_stall(lux_sgm_ctx* ctx, int32_t block);
+
 /* StereoParams defaults / L16Pyramid() (DenseStereo.cs:15-30). */
 void lux_sgm_default_params(lux_stereo_params* p);
 void lux_sgm_l16_pyramid(lux_stereo_params out[6]);
@@ -159,6 +170,11 @@ enum {
 int lux_layer_read(const lux_layer* layer, int32_t field, void* dst, uint64_t bytes);
 /* The device pointer of a field (valid until lux_layer_destroy), or NULL. */
 const void* lux_layer_device_ptr(const lux_layer* layer, int32_t field);
+/* A previous layer made from a stored depth map (host w×h floats) and skip mask (host w×h bytes, 0 = computed; NULL: all
+ * computed): the two DenseLayer fields the next layer's RangeFromPrevious reads (DenseStereoSgm.cs:91-142). It resumes a
+ * pyramid from a dumped layer (lux_load_f32 of the reference's `_dense_L<i>_depth` dump, StereoAsyncApi.cs:197-214), so one
+ * layer can be solved against the C# build's own previous layer. Only LUX_FIELD_DEPTH and LUX_FIELD_SKIP are readable. */
+int lux_layer_from_depth(lux_sgm_ctx* ctx, int32_t w, int32_t h, const float* depth, const uint8_t* skip, lux_layer** out);
 void lux_layer_destroy(lux_layer* layer);
 
 /* DenseUpsampleLayer.Run (DenseUpsampleLayer.cs:35-48): prev depth pw×ph (host, or device when prev_on_device), guide RGBA8,
@@ -307,7 +323,10 @@ int lux_server_wait(lux_server* server, uint64_t ticket, uint64_t timeout_ns, lu
  * writes every byte of it that it reads, so nothing has to start at zero. The first call on a device looks the array up
  * (cudaGetSymbolAddress, with the context's device current): make that first call before any stream capture. All calls
  * share the array and it keeps the last call's contents, so calls that overlap in time on one device (through different
- * contexts) race: serialise them. Returns after the context's stream has finished the work. */
+ * contexts) race: serialise them. The work runs on the context's stream (lux_sgm_stream), a non-blocking stream that
+ * nothing orders after the caller's own streams: prev_depth, prev_conf and the guide must be complete before the call
+ * (synchronise the stream that wrote them, or make lux_sgm_stream wait on an event recorded after the writes).
+ * Returns after the context's stream has finished the work. */
 #define LUX_UPSAMPLE_NOALLOC_MAX_PIXELS (4u << 20)
 int lux_sgm_upsample_noalloc(lux_sgm_ctx* ctx, const float* prev_depth, int32_t pw, int32_t ph, const lux_img_rgba8* guide,
                              int32_t set_w, int32_t set_h, float sigma, int32_t scale, const float* prev_conf,

@@ -75,6 +75,9 @@ SIGNATURES = [
     ("lux_sgm_sync", ctypes.c_int, [ctypes.c_void_p]),
     ("lux_sgm_kernel_launches", ctypes.c_uint64, []),
     ("lux_sgm_stream", ctypes.c_void_p, [ctypes.c_void_p]),
+    ("lux_sgm_set_wait_limit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("lux_sgm_get_wait_limit", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("lux_sgm_debug_stall", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ("lux_sgm_revisit_schedule", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     ("lux_sgm_default_params", None, [ctypes.POINTER(Params)]),
@@ -91,6 +94,8 @@ SIGNATURES = [
     ("lux_layer_read", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint64]),
     ("lux_layer_device_ptr", ctypes.c_void_p, [ctypes.c_void_p, ctypes.c_int32]),
     ("lux_layer_destroy", None, [ctypes.c_void_p]),
+    ("lux_layer_from_depth", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
     ("lux_sgm_upsample", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.POINTER(Img), ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_int32,
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),

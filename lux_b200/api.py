@@ -132,6 +132,19 @@ class Context:
         if rc:
             _raise(rc, self.lib.lux_sgm_last_error(self.handle).decode())
 
+    @property
+    def wait_limit_ns(self) -> int:
+        """The bound of every device-side wait of the aggregation kernels (ns; default 20 s)."""
+        return int(self.lib.lux_sgm_get_wait_limit(self.handle))
+
+    @wait_limit_ns.setter
+    def wait_limit_ns(self, ns: int):
+        self.check(self.lib.lux_sgm_set_wait_limit(self.handle, int(ns)))
+
+    def debug_stall(self, block: int):
+        """Failure-path tests only: aggregation block `block` (>= 1) waits on a counter nothing publishes (-1: off)."""
+        self.check(self.lib.lux_sgm_debug_stall(self.handle, int(block)))
+
     def close(self):
         if self.handle:
             self.lib.lux_sgm_destroy(self.handle)
@@ -241,6 +254,19 @@ class DenseLayer:
                                    prev.handle if prev is not None else None,
                                    _flags(keep_pass1, keep_agg, prefilter, force_replay, sgm), ctypes.byref(out))
         ctx.check(rc)
+        return DenseLayer(ctx, out)
+
+    @staticmethod
+    def from_depth(depth, skip=None, ctx: Optional[Context] = None) -> "DenseLayer":
+        """A previous layer made from a stored depth map (h, w) float32 and skip mask (0 = computed; None: all computed),
+        for resuming a pyramid from a dumped layer: the next layer's RangeFromPrevious reads only these two fields."""
+        ctx = ctx or default_context()
+        d = np.ascontiguousarray(np.asarray(depth, np.float32))
+        h, w = d.shape
+        sk = None if skip is None else np.ascontiguousarray(np.asarray(skip, np.uint8).reshape(h, w))
+        out = ctypes.c_void_p()
+        ctx.check(ctx.lib.lux_layer_from_depth(ctx.handle, w, h, d.ctypes.data, None if sk is None else sk.ctypes.data,
+                                               ctypes.byref(out)))
         return DenseLayer(ctx, out)
 
     def _read(self, field_id, dtype, count):

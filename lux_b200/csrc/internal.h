@@ -11,7 +11,7 @@ constexpr int kMaxCams = 16;        // reference + up to 15 other cameras per la
 void count_launches(int n);
 uint64_t kernel_launches();
 
-constexpr uint64_t kTimeoutNs = 20ull * 1000 * 1000 * 1000;  // bounded device waits: 20 s of %globaltimer
+constexpr uint64_t kTimeoutNs = 20ull * 1000 * 1000 * 1000;  // bounded device waits: 20 s of %globaltimer (default)
 
 // Layer geometry and per-pixel ranges, all device pointers.
 struct LayerGeom {
@@ -25,6 +25,12 @@ struct LayerGeom {
   const uint64_t* off;
   uint64_t volume;
   bool uniform;  // every pixel searches [0, n) with cap n (first layer)
+  // Bounded device waits: every cross-block or cross-warp wait of the aggregation kernels gives up after timeout_ns of
+  // %globaltimer (error 11). stall_block >= 0 (failure-path tests only): the block with that ticket waits for the block
+  // before it on `never`, a zero counter that nothing publishes, so its wait runs out and the launch ends with error 11.
+  uint64_t timeout_ns;
+  int stall_block;
+  const int* never;
 };
 
 struct CostArgs {

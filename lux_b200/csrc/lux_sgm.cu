@@ -29,6 +29,9 @@ struct lux_sgm_ctx {
   uint32_t* d_warp = nullptr; // the rsqrt tables (exponents 127, 128; 4096 entries each), then the 384-float Lanczos table
   int* d_err = nullptr;       // device error word of the current call
   cudaEvent_t ev[4] = {};
+  uint64_t wait_limit_ns = kTimeoutNs;  // bound of every device-side wait of the aggregation kernels
+  int stall_block = -1;                 // failure-path tests: the block whose cross-block wait can never be satisfied
+  int* d_never = nullptr;               // the zero counter that block waits on (nothing writes it)
 };
 
 struct DevBuf {
@@ -278,6 +281,9 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   g.W = W; g.H = H; g.n_planes = L->n; g.align = align; g.min_lo = L->min_lo; g.max_hi = L->max_hi; g.tile = p.tile;
   g.planes = L->planes; g.guidance = L->guidance; g.skip = L->skip; g.start = L->start; g.count = L->count; g.cap = L->cap;
   g.off = L->off; g.volume = L->volume; g.uniform = uniform;
+  g.timeout_ns = ctx->wait_limit_ns;
+  g.stall_block = ctx->stall_block;
+  g.never = ctx->d_never;
   // matching cost (DenseStereo.BuildContext + MatchingCost + Normalise)
   CostArgs ca;
   std::memset(&ca, 0, sizeof ca);
@@ -427,7 +433,8 @@ int lux_sgm_create(int device, uint64_t hbm_budget_bytes, lux_sgm_ctx** out) {
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
   if (cudaMalloc(&ctx->d_rcp, 4096 * 4) != cudaSuccess) return fail(LUX_ERR_ALLOC);
-  if (cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) return fail(LUX_ERR_ALLOC);
+  if (cudaMalloc(&ctx->d_err, 2 * sizeof(int)) != cudaSuccess) return fail(LUX_ERR_ALLOC);
+  ctx->d_never = ctx->d_err + 1;
   cudaMemcpy(ctx->d_rcp, host_rcp_table(), 4096 * 4, cudaMemcpyHostToDevice);
   {
     std::vector<uint32_t> wt(8192 + 384);
@@ -437,7 +444,7 @@ int lux_sgm_create(int device, uint64_t hbm_budget_bytes, lux_sgm_ctx** out) {
     if (cudaMalloc(&ctx->d_warp, wt.size() * 4) != cudaSuccess) return fail(LUX_ERR_ALLOC);
     cudaMemcpy(ctx->d_warp, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice);
   }
-  cudaMemset(ctx->d_err, 0, sizeof(int));
+  cudaMemset(ctx->d_err, 0, 2 * sizeof(int));
   for (auto& e : ctx->ev) cudaEventCreate(&e);
   *out = ctx;
   return LUX_OK;
@@ -460,6 +467,22 @@ const char* lux_sgm_last_error(const lux_sgm_ctx* ctx) { return ctx ? ctx->last_
 uint64_t lux_sgm_kernel_launches(void) { return lux::kernel_launches(); }
 
 void* lux_sgm_stream(lux_sgm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int lux_sgm_set_wait_limit(lux_sgm_ctx* ctx, uint64_t limit_ns) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->wait_limit_ns = limit_ns ? limit_ns : kTimeoutNs;
+  return LUX_OK;
+}
+
+uint64_t lux_sgm_get_wait_limit(const lux_sgm_ctx* ctx) { return ctx ? ctx->wait_limit_ns : 0; }
+
+int lux_sgm_debug_stall(lux_sgm_ctx* ctx, int32_t block) {
+  if (!ctx || block < -1 || block == 0) return set_err(ctx, LUX_ERR_ARG, "debug_stall: block must be -1 (off) or >= 1");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->stall_block = block;
+  return LUX_OK;
+}
 
 int lux_sgm_revisit_schedule(int32_t w, int32_t h, int32_t tile, int32_t second_pass, int32_t* out, int32_t* y_b) {
   if (w <= 0 || h <= 0 || tile <= 0 || !out) return LUX_ERR_ARG;
@@ -692,6 +715,34 @@ int lux_layer_read(const lux_layer* L, int32_t field, void* dst, uint64_t bytes)
                                     (unsigned long long)bytes);
   CK(cudaMemcpyAsync(dst, p, need, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  return LUX_OK;
+}
+
+int lux_layer_from_depth(lux_sgm_ctx* ctx, int32_t w, int32_t h, const float* depth, const uint8_t* skip, lux_layer** out) {
+  if (!ctx || !depth || !out || w <= 0 || h <= 0) return set_err(ctx, LUX_ERR_ARG, "layer_from_depth: null pointer or empty size");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  lux_layer* L = new lux_layer();
+  L->ctx = ctx;
+  L->w = w;
+  L->h = h;
+  L->index = -1;
+  const size_t npx = (size_t)w * h;
+  int rc;
+  if ((rc = alloc_t(ctx, L->bufs, npx, &L->depth)) || (rc = alloc_t(ctx, L->bufs, npx, &L->skip))) {
+    destroy_layer(L);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(L->depth, depth, npx * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = skip ? cudaMemcpyAsync(L->skip, skip, npx, cudaMemcpyHostToDevice, ctx->stream) : cudaMemsetAsync(L->skip, 0, npx, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    destroy_layer(L);
+    return set_err(ctx, LUX_ERR_CUDA, "layer_from_depth: %s", cudaGetErrorString(e));
+  }
+  *out = L;
   return LUX_OK;
 }
 

@@ -1,5 +1,6 @@
 // Box filter, guidance, plane ranges from the previous layer, CSR offsets, WTA and the upsample chain.
 // Each kernel restates one reference function with its exact operation order (file:line in each comment).
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 
@@ -145,7 +146,7 @@ void launch_range_from_previous(const float* prev_depth, const uint8_t* prev_ski
   int npx = pw * ph;
   k_plane_index<<<(npx + 255) / 256, 256, 0, s>>>(prev_depth, npx, b, n, monotone, rcp_table, idx);
   count_launches(1);
-  dim3 g1((pw + 127) / 128, ph);
+  dim3 g1((pw + 127) / 128, std::min(ph, 65535));
   k_hminmax<<<g1, 128, 0, s>>>(idx, prev_skip, pw, ph, hmin, hmax);
   count_launches(1);
   float fy = (float)(ph - 1) / (float)(H - 1), fx = (float)(pw - 1) / (float)(W - 1);
@@ -277,8 +278,9 @@ struct ShiftTaps {
 // only ever read at these positions, so only they are computed.
 __global__ void k_shift_resize(const uint8_t* __restrict__ guide, int gw, int gh, int gstride, int pw, int ph, ShiftTaps t,
                                uint8_t* __restrict__ g2) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= pw) return;
+  for (int y = blockIdx.y; y < ph; y += gridDim.y) {  // gridDim.y is capped at 65535 rows; taller images loop
   int sy = (int)((unsigned)y * (unsigned)t.stepY) >> 16;  // the accumulated yAcc (int, wraps like the reference's sum)
   int sx = (int)((unsigned)x * (unsigned)t.stepX) >> 16;
   int rows[4];
@@ -299,6 +301,7 @@ __global__ void k_shift_resize(const uint8_t* __restrict__ guide, int gw, int gh
     outv[ch] = (uint8_t)(q < 0 ? 0 : q > 255 ? 255 : q);
   }
   *reinterpret_cast<uchar4*>(g2 + ((size_t)y * pw + x) * 4) = make_uchar4(outv[0], outv[1], outv[2], outv[3]);
+  }
 }
 
 LUX_DEV float up_exp2(float t) {  // Exp2Fast (:151-159)
@@ -321,8 +324,9 @@ LUX_DEV float spatial_w(float f, int i) {  // SpatialW (:212-217)
 __global__ void k_bilateral(const float* __restrict__ prev, int lw, int lh, const uint8_t* __restrict__ guide, int W, int H, int gstride,
                             const uint8_t* __restrict__ g2, float k, int inverse, const uint32_t* __restrict__ rcp_table,
                             float* __restrict__ out) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= W) return;
+  for (int y = blockIdx.y; y < H; y += gridDim.y) {  // gridDim.y is capped at 65535 rows; taller images loop
   const float eps = __uint_as_float(0x322bcc77u);
   int wm1 = lw - 1, hm1 = lh - 1;
   int iy0 = (y - 1) / 2;
@@ -363,6 +367,7 @@ __global__ void k_bilateral(const float* __restrict__ prev, int lw, int lh, cons
   }
   float r = __fdiv_rn(accV, accS);
   out[(size_t)y * W + x] = inverse ? rcp_approx(r, rcp_table) : r;
+  }
 }
 
 static float cubic_tap_host(float x) {  // CubicTap (:56-62)
@@ -388,12 +393,12 @@ void launch_upsample(const float* prev, int pw, int ph, const uint8_t* guide, in
   double sy = (double)gh * 65536.0 / (double)ph, sx = (double)gw * 65536.0 / (double)pw;
   t.stepY = sy >= 2147483648.0 ? 0x7fffffff : (int)sy;
   t.stepX = sx >= 2147483648.0 ? 0x7fffffff : (int)sx;
-  dim3 g1((pw + 127) / 128, ph);
+  dim3 g1((pw + 127) / 128, std::min(ph, 65535));
   k_shift_resize<<<g1, 128, 0, s>>>(guide, gw, gh, gstride, pw, ph, t, g2);
   count_launches(1);
   volatile float ss = sigma * sigma;
   float k = 0.5f / ss;
-  dim3 g3((gw + 127) / 128, gh);
+  dim3 g3((gw + 127) / 128, std::min(gh, 65535));
   k_bilateral<<<g3, 128, 0, s>>>(prev, pw, ph, guide, gw, gh, gstride, g2, k, 1, rcp_table, out_depth);
   count_launches(1);
   if (prev_conf && out_conf) {

@@ -49,6 +49,8 @@ struct EmuArgs {
   int* progress;
   int* err;
   unsigned long long timeout_ns;
+  int stall_block;  // failure-path tests: this part's waits on the part above read `never` (-1: none)
+  const int* never;
 };
 
 LUX_DEV int rd(const EmuArgs& a, long long i) {  // Rd (DenseStereoSgm.cs:324)
@@ -349,7 +351,7 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
   // A part below the image has no pixels, and neither has any part after it: nothing waits on its progress. (It must
   // not wait either: the last row of the part above, below the image too, publishes none.)
   if (j * T + r0 >= a.H) return;
-  int* const above = a.progress + (k - 1);  // the part above: its last row's offsets
+  int* const above = k == a.stall_block ? const_cast<int*>(a.never) : a.progress + (k - 1);  // the part above: its last row's offsets
   if constexpr (kFlags) {
     // One row per warp; s_row[r] counts row r's offsets done across tiles (i·T + u + 1). A row goes on into the next
     // tile by itself: the only pixels of a later tile that lower rows' earlier tiles can touch are revisits of the
@@ -525,7 +527,9 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   a.ticket = b.ticket + pass;
   a.progress = b.progress + (size_t)pass * a.ghN * kEmuParts;
   a.err = err;
-  a.timeout_ns = kTimeoutNs;
+  a.timeout_ns = g.timeout_ns;
+  a.stall_block = g.stall_block;
+  a.never = g.never;
   int nw = flags ? a.part_rows : g.tile / 2;
   if (nw < 1) nw = 1;
   if (nw > 32) nw = 32;

@@ -51,6 +51,8 @@ struct UniArgs {
   int keep_agg, wta;
   int* err;
   unsigned long long timeout_ns;
+  int stall_block;    // failure-path tests: this block's cross-block wait reads `never` (-1: none)
+  const int* never;
 };
 
 template <int LPT>

@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
         if (!ok) break;
         if (avail < se) {
           int v = 0;
-          if (lane == 0) v = wait_at_least_value(u.progress + (cb - 1), se, u.err, 11, u.timeout_ns);
+          if (lane == 0) v = wait_at_least_value(cb == u.stall_block ? u.never : u.progress + (cb - 1), se, u.err, 11, u.timeout_ns);
           v = __shfl_sync(0xffffffffu, v, 0);
           __syncwarp();
           if (v < 0) {
@@ -648,7 +648,9 @@ int run_sgm_split(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const
   u.cs_min = reinterpret_cast<uint16_t*>(base + L.cs_min);
   u.y_b = sch[0].y_b;
   u.err = err;
-  u.timeout_ns = kTimeoutNs;
+  u.timeout_ns = g.timeout_ns;
+  u.stall_block = g.stall_block;
+  u.never = g.never;
   u.keep_agg = keep_agg;
   u.p2t = reinterpret_cast<const uint2*>(base + L.p2t);
   const int lpt = lpt_of(n);

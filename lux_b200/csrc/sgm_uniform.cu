@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
         if (!ok) break;
         if (avail < xe) {
           int v = 0;
-          if (lane == 0) v = wait_at_least_value(a.progress + (cb - 1), xe, a.err, 11, a.timeout_ns);
+          if (lane == 0) v = wait_at_least_value(cb == a.stall_block ? a.never : a.progress + (cb - 1), xe, a.err, 11, a.timeout_ns);
           v = __shfl_sync(0xffffffffu, v, 0);
           __syncwarp();  // lane 0's acquire orders the band-buffer reads of every lane
           if (v < 0) {
@@ -539,7 +539,9 @@ int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, con
   a.cs_min = reinterpret_cast<uint16_t*>(base + L.cs_min);
   a.y_b = sch[0].y_b;
   a.err = err;
-  a.timeout_ns = kTimeoutNs;
+  a.timeout_ns = g.timeout_ns;
+  a.stall_block = g.stall_block;
+  a.never = g.never;
   a.keep_agg = keep_agg;
   const int lpt = lpt_for(n);
   for (int pass = 0; pass < 2; pass++) {

@@ -671,11 +671,23 @@ typedef struct {
   int slotStride, halfL, halfM, halfR;
   uint8_t* rawTmp;             /* the shared scratch `raw` of Compute (n + 8 bytes) */
   int err;
+  const lo_costctx* cctx;      /* inline_cost: the cost context and the `costTmp` scratch of Compute */
+  uint16_t* costTmp;
 } sgm_state;
 
 static inline int lidx(const sgm_state* s, int half, int slot, int path) {
   return half * s->halfL + slot * s->slotStride + 1 + path * (s->L->max_hi + 1);
 }
+/* The reference runs Pixel's 8-lane vector form (DenseStereoSgm.cs:280-299) where its guard holds and the scalar form
+   (:300-313) elsewhere; both give the same values there, since the guard keeps the block loads clear of the stores.
+   The oracle takes the scalar form unless lo_set_vector_form(1), which restates the vector form too, so a test can
+   check the two against each other; lo_vector_calls() counts the path blocks that took it. */
+static int g_vector_form = 0;
+static long g_vector_calls = 0;
+void lo_set_vector_form(int on) { g_vector_form = on; g_vector_calls = 0; }
+long lo_vector_calls(void) { return g_vector_calls; }
+static inline int sat16(int v) { return v > 65535 ? 65535 : v; }
+
 /* Rd (DenseStereoSgm.cs:324): before the buffer 2000, past its end 0 */
 static inline int rd(const sgm_state* s, long i) { return i < 0 ? 2000 : (size_t)i < s->Llen ? s->Lb[i] : 0; }
 
@@ -691,6 +703,13 @@ static void pixel(sgm_state* s, int x, int y, int dir, int cur, int other) {
   if (L->skip[pi] != 0) {
     memset(raw, 0, (size_t)cap);
     for (int k = count; k < cap; k++) raw[k] = 255;
+  } else if (dir > 0 && s->cctx) { /* Threads == 1: pass +1 computes the costs at every visit and stores them (:243-249) */
+    int W0 = L->iw[0], H0 = L->ih[0], sc = L->p.scale, hf = (sc + (sc >> 31)) >> 1;
+    int xImg = imin(sc * x + hf, W0 - 1), yImg = imin(sc * y + hf, H0 - 1);
+    int rc = lo_matching_cost(s->cctx, xImg, yImg, start, count, s->costTmp);
+    if (rc) { s->err = rc; return; }
+    lo_normalise(s->costTmp, count, cap, s->cctx->n_others, raw);
+    memcpy(L->raw + L->off[pi], raw, (size_t)cap);
   } else {
     memcpy(raw, L->raw + L->off[pi], (size_t)cap); /* the stored costs (prepass == pass-1 costs, :176-180) */
   }
@@ -724,8 +743,36 @@ static void pixel(sgm_state* s, int x, int y, int dir, int cur, int other) {
     int nb = lidx(s, half, ns, p);
     int runMin = 0xffff;
     int q = start - L->min_lo;
-    /* the scalar form: every read through Rd, lanes in order (DenseStereoSgm.cs:300-313); it equals the 8-lane form
-       whenever that one applies (:280-299) */
+    /* the 8-lane form (DenseStereoSgm.cs:280-299): whole blocks, every neighbour read and every write inside the buffer,
+       the written range clear of the range read, a P2 term that fits 16 bits */
+    if (g_vector_form && (cap & 7) == 0 && P2p >= 0 && (long)nb + q - 1 >= 0 && (size_t)((long)nb + q + cap + 1) <= s->Llen &&
+        (long)baseCur + q >= 0 && (size_t)((long)baseCur + q + cap) <= s->Llen && labs((long)baseCur - nb) >= cap + 16) {
+      const uint16_t* pn = s->Lb + nb + q;
+      uint16_t* pw = s->Lb + baseCur + q;
+      uint16_t vrun[8];
+      for (int l = 0; l < 8; l++) vrun[l] = 0xffff;
+      for (int b = 0; b < cap; b += 8) {
+        uint16_t lm[8], l0[8], lp[8], lc[8];
+        memcpy(lm, pn + b - 1, sizeof lm); /* Vector128.Load of the three neighbour blocks, before the block's store */
+        memcpy(l0, pn + b, sizeof l0);
+        memcpy(lp, pn + b + 1, sizeof lp);
+        for (int l = 0; l < 8; l++) {
+          int m = imin(imin(sat16(lm[l] + P1), l0[l]), imin(sat16(lp[l] + P1), P2p)); /* Min(Min(AddSat(Lm,P1),L0), Min(AddSat(Lp,P1),P2)) */
+          int v = sat16(raw[b + l] + m) - minPrev;                                        /* SubtractSaturate(AddSaturate(r16, m), minPrev) */
+          lc[l] = (uint16_t)(v < 0 ? 0 : v);
+        }
+        memcpy(pw + b, lc, sizeof lc);
+        for (int l = 0; l < 8; l++) {
+          if (lc[l] < vrun[l]) vrun[l] = lc[l];
+          agg[b + l] = (uint16_t)sat16(agg[b + l] + lc[l]);
+        }
+      }
+      for (int l = 0; l < 8; l++) runMin = imin(runMin, vrun[l]);
+      g_vector_calls++;
+      s->Min[cur * s->halfM + slot * 4 + p] = (uint16_t)runMin;
+      continue;
+    }
+    /* the scalar form: every read through Rd, lanes in order (DenseStereoSgm.cs:300-313) */
     for (int b = 0; b < cap; b += 8)
       for (int l = 0; l < 8; l++) {
         long qi = (long)q + b + l;
@@ -813,11 +860,25 @@ static void compute_raw(lo_layer* L, int* err) {
 
 int lo_layer_compute(lo_layer* L) {
   int err = 0;
-  compute_raw(L, &err);
-  if (err) return err;
+  lo_costctx cctx;
+  memset(&cctx, 0, sizeof(cctx));
+  if (!L->inline_cost) {
+    compute_raw(L, &err);
+    if (err) return err;
+  } else {
+    cctx.ref = L->images[0]; cctx.w = L->iw[0]; cctx.h = L->ih[0];
+    cctx.n_others = L->n_cams - 1;
+    cctx.others = L->images + 1; cctx.ow = L->iw + 1; cctx.oh = L->ih + 1;
+    cctx.warps = (const float (*)[16])L->warps; cctx.wq = (const uint16_t (*)[4])L->wq;
+    cctx.planes = L->planes; cctx.n_planes = L->n_planes;
+  }
   sgm_state s;
   memset(&s, 0, sizeof(s));
   s.L = L;
+  if (L->inline_cost) {
+    s.cctx = &cctx;
+    s.costTmp = (uint16_t*)malloc(sizeof(uint16_t) * ((size_t)L->n_planes + 8));
+  }
   int W = L->w, H = L->h, T = L->p.tile;
   int maxCnt = L->max_hi;
   s.slotStride = 4 * maxCnt + 5;
@@ -857,7 +918,7 @@ int lo_layer_compute(lo_layer* L) {
       memcpy(L->agg_pass1, L->agg, sizeof(uint16_t) * L->off[(size_t)W * H]);
     }
   }
-  free(s.Lb); free(s.Min); free(s.RangeS); free(s.RangeC); free(s.Pix); free(s.rawTmp);
+  free(s.Lb); free(s.Min); free(s.RangeS); free(s.RangeC); free(s.Pix); free(s.rawTmp); free(s.costTmp);
   if (s.err) return s.err;
   /* WTA (DenseStereoSgm.cs:225-231) */
   L->depth = (float*)malloc(sizeof(float) * (size_t)W * H);

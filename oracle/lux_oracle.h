@@ -105,7 +105,16 @@ typedef struct {
   int n_cams; const uint8_t* const* images; const int* iw; const int* ih;
   float (*warps)[16]; uint16_t (*wq)[4];
   int threads; int keep_pass1; int xsw;  /* xsw = LUX_SGM_XSW=1 behaviour (DenseStereoSgm.cs:31) */
+  /* inline_cost = 1: the reference's Threads == 1 form (DenseStereoSgm.cs:243-249): no prepass; every visit of pass +1
+     computes its pixel's costs and stores them, and pass -1 reads the stored ones. 0: the Threads > 1 form, a row-parallel
+     prepass on `threads` workers (:186-205), which the reference states gives the same values (:176-180). */
+  int inline_cost;
 } lo_layer;
+
+/* Pixel's 8-lane vector form (DenseStereoSgm.cs:280-299) where its guard holds (on = 1), else the scalar form only (0,
+   the default); lo_vector_calls: path blocks that took the vector form since the last lo_set_vector_form. */
+void lo_set_vector_form(int on);
+long lo_vector_calls(void);
 
 /* DenseLayer.Init (DenseStereoSgm.cs:34-62). images are the box-filtered camera images (camera 0 = reference). */
 int lo_layer_init(lo_layer* L, const lo_params* p, int index, int n_cams, const uint8_t* const* images, const int* iw, const int* ih,

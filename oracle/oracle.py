@@ -38,7 +38,7 @@ class LoLayer(ctypes.Structure):
                 ("depth", ctypes.POINTER(ctypes.c_float)),
                 ("n_cams", ctypes.c_int), ("images", ctypes.c_void_p), ("iw", ctypes.c_void_p), ("ih", ctypes.c_void_p),
                 ("warps", ctypes.c_void_p), ("wq", ctypes.c_void_p),
-                ("threads", ctypes.c_int), ("keep_pass1", ctypes.c_int), ("xsw", ctypes.c_int)]
+                ("threads", ctypes.c_int), ("keep_pass1", ctypes.c_int), ("xsw", ctypes.c_int), ("inline_cost", ctypes.c_int)]
 
 
 _lib = None
@@ -67,6 +67,8 @@ def lib():
                                   ctypes.c_void_p, ctypes.c_void_p]
         l.lo_traversal_trace.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_long]
         l.lo_traversal_trace.restype = ctypes.c_long
+        l.lo_set_vector_form.argtypes = [ctypes.c_int]
+        l.lo_vector_calls.restype = ctypes.c_long
         l.lo_rcp_bits.argtypes = [ctypes.c_uint32]
         l.lo_rcp_bits.restype = ctypes.c_uint32
         l.lo_rsqrt_bits.argtypes = [ctypes.c_uint32]
@@ -185,8 +187,11 @@ def _images(images):
     return imgs, ptrs, iw, ih
 
 
-def layer(filtered, gray, calibs, near, far, params, index=0, align=8, prev=None, keep_pass1=False, threads=1, xsw=False):
-    """DenseLayer.Init + Compute on box-filtered images. prev: a dict from a previous call (needs its Depth and Skip)."""
+def layer(filtered, gray, calibs, near, far, params, index=0, align=8, prev=None, keep_pass1=False, threads=1, xsw=False,
+          inline_cost=False):
+    """DenseLayer.Init + Compute on box-filtered images. prev: a dict from a previous call (needs its Depth and Skip).
+    inline_cost: the reference's Threads == 1 form (costs computed at every pass +1 visit) instead of the row-parallel
+    prepass on `threads` workers (its Threads > 1 form)."""
     imgs, ptrs, iw, ih = _images(filtered)
     g = np.ascontiguousarray(np.asarray(gray, np.uint8))
     cc = _calibs(calibs)
@@ -206,12 +211,23 @@ def layer(filtered, gray, calibs, near, far, params, index=0, align=8, prev=None
         if rc:
             raise OracleError(rc, "layer_init")
         L.threads, L.keep_pass1, L.xsw = threads, 1 if keep_pass1 else 0, 1 if xsw else 0
+        L.inline_cost = 1 if inline_cost else 0
         rc = lib().lo_layer_compute(ctypes.byref(L))
         if rc:
             raise OracleError(rc, "layer_compute")
         return _extract(L)
     finally:
         lib().lo_layer_free(ctypes.byref(L))
+
+
+def set_vector_form(on):
+    """Pixel's 8-lane vector form where the reference takes it (True), or the scalar form only (False, the default)."""
+    lib().lo_set_vector_form(1 if on else 0)
+
+
+def vector_calls():
+    """Path blocks that took the vector form since the last set_vector_form."""
+    return int(lib().lo_vector_calls())
 
 
 def pyramid(images, gray, calibs, near, far, threads=1, keep_pass1=False):

@@ -1,7 +1,11 @@
 """Writes the committed golden fixtures of the dense-stereo tests.
 
 intel_tables.json: SHA-256 digests of the three approximation tables of Lux.Engine/Imaging/IntelApprox.Tables.cs, read as
-text from a checkout of the reference (default /root/reference, or argv[1]). The product's tables
+text from a checkout of the reference whose root is the required first argument:
+
+    python tests/golden/make_golden.py <path of the mprovenz/lux checkout>
+
+The product's tables
 (lux_b200/csrc/intel_approx_tables.h) are regenerated from the rcpss/rsqrtss instructions of an Intel host, not copied;
 the test compares their digests with these.
 
@@ -30,7 +34,9 @@ def reference_table_digests(ref_root):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: python tests/golden/make_golden.py <path of the mprovenz/lux checkout>")
+    ref_root = sys.argv[1]
     d = reference_table_digests(ref_root)
     with open(os.path.join(HERE, "intel_tables.json"), "w") as f:
         json.dump({"source": "Lux.Engine/Imaging/IntelApprox.Tables.cs", "tables": d}, f, indent=1)

@@ -167,3 +167,59 @@ def test_depth_cache_composite_rcp():
     two = _rcp_bits_np(_rcp_bits_np(b, t), t)
     one = ((b.astype(np.int64) & 0xFF800000) + comp[i.astype(np.int64)]) & 0xFFFFFFFF
     assert np.array_equal(one.astype(np.uint32), two)
+
+
+def _layer_cases():
+    """Uniform grey pairs (T 4-64, D 16-64), a colour multi-camera layer and ragged layers after a previous layer."""
+    from lux_b200 import api, synth
+    cases = []
+    for (w, h, d, t) in [(48, 40, 16, 8), (65, 33, 32, 4), (70, 40, 64, 64)]:
+        wl = synth.rectified_pair(w, h, d, seed=w + d, tile=t)
+        cases.append((wl.images, wl.gray, wl.calibs, wl.near, wl.far, [wl.params]))
+    cap = synth.capture(160, 120, 3, seed=4, f=130.0)
+    cases.append((cap.images, cap.gray, cap.calibs, cap.near, cap.far, api.StereoParams.l16_pyramid()[:4]))
+    return cases
+
+
+def _run_chain(oracle, imgs, gray, calibs, near, far, plist, **kw):
+    filt = [oracle.box_filter3(im) for im in imgs]
+    out, prev = [], None
+    for i, p in enumerate(plist):
+        L = oracle.layer(filt, gray, calibs, near, far, p, index=i, prev=prev, keep_pass1=True, **kw)
+        out.append(L)
+        prev = L
+    return out
+
+
+def _same(a, b):
+    for k in ("Raw", "AggPass1", "Agg", "Start", "Count", "Cap"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(a["Depth"].view(np.uint32), b["Depth"].view(np.uint32))
+
+
+def test_vector_pixel_form_equals_scalar_form(oracle):
+    """Pixel's 8-lane vector form (DenseStereoSgm.cs:280-299), where its guard lets the reference take it, gives the
+    values of the scalar form (:300-313) that the oracle otherwise runs: both restated, compared on every layer output."""
+    try:
+        for case in _layer_cases():
+            oracle.set_vector_form(False)
+            scalar = _run_chain(oracle, *case)
+            oracle.set_vector_form(True)
+            vector = _run_chain(oracle, *case)
+            assert oracle.vector_calls() > 0  # the guard held for some path blocks
+            for a, b in zip(scalar, vector):
+                _same(a, b)
+    finally:
+        oracle.set_vector_form(False)
+
+
+def test_single_thread_form_equals_parallel_prepass(oracle):
+    """The reference's guarantee that the thread count does not change the result (StereoAsyncApi.cs:44-47,
+    DenseStereoSgm.cs:176-180): Threads == 1 (costs computed at each pass +1 visit) equals the row-parallel prepass on
+    1 and on 4 workers."""
+    for case in _layer_cases():
+        one = _run_chain(oracle, *case, inline_cost=True)
+        for threads in (1, 4):
+            par = _run_chain(oracle, *case, threads=threads)
+            for a, b in zip(one, par):
+                _same(a, b)

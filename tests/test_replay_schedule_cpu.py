@@ -88,12 +88,19 @@ def _count_unordered(ids, preds, pixels):
     return len(bad)
 
 
-def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False, own_part_rule=True):
-    """Conflicting pairs the waits leave unordered (or -1 for a cycle). Planted mistakes: lower_part_rule makes a lower
-    part wait for the part above to finish its revisiting tile i+1 (instead of the part above waiting for it);
-    own_part_rule=False drops the wait of a revisiting row for its own part's last row."""
+def launcher_part_rows(T):
+    """Rows per part (block) of a band, as the launcher splits it: min(16, T/2) rows for T >= 4, the whole band below."""
+    return min(16, T // 2) if T >= 4 else T
+
+
+def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False, own_part_rule=True, part_rows=None):
+    """Conflicting pairs the waits leave unordered (or -1 for a cycle). The band is split into parts of part_rows rows
+    (the last part holds the rest: 16 + 16 + 8 at T = 40), or into `parts` equal parts when part_rows is None. Planted
+    mistakes: lower_part_rule makes a lower part wait for the part above to finish its revisiting tile i+1 (instead of
+    the part above waiting for it); own_part_rule=False drops the wait of a revisiting row for its own part's last row."""
     ghN, gwN = (H + T - 1) // T, (W + 2 * T - 1) // T
-    R = (T + parts - 1) // parts
+    R = part_rows if part_rows is not None else (T + parts - 1) // parts
+    parts = (T + R - 1) // R
     ids, preds, pixels = {}, {}, []
 
     def node(key):
@@ -195,11 +202,12 @@ def unordered_pairs_barrier_form(W, H, T, dirn, lag=3):
 
 
 @pytest.mark.parametrize("W,H,T", [(65, 49, 4), (48, 40, 8), (97, 61, 16), (70, 45, 32), (66, 65, 64), (33, 17, 2),
-                                   (40, 10, 4), (20, 11, 6)])
+                                   (40, 10, 4), (20, 11, 6), (75, 70, 34), (83, 90, 40), (61, 55, 50), (90, 130, 62)])
 @pytest.mark.parametrize("dirn", [1, -1])
 def test_replay_waits_keep_the_reference_order(W, H, T, dirn):
-    parts = T // min(16, T // 2) if T >= 4 else 1  # as the launcher splits a band: parts of min(16, T/2) rows
-    assert unordered_pairs(W, H, T, parts, dirn) == 0
+    """Even tiles whose band the launcher splits into parts of min(16, T/2) rows, including the tiles between 32 and 64
+    rows that are not multiples of 16, where the last part is shorter (T = 34: 16 + 16 + 2; T = 40: 16 + 16 + 8)."""
+    assert unordered_pairs(W, H, T, 0, dirn, part_rows=launcher_part_rows(T)) == 0
 
 
 def test_order_check_catches_a_wrong_revisit_rule():

@@ -85,3 +85,35 @@ def test_noalloc_limits(ctx):
                                           d_out.data_ptr(), None)
     with pytest.raises(api.InvalidOperationError):
         ctx.check(rc)
+
+
+def test_noalloc_inputs_ordered_by_an_event(ctx):
+    """Inputs written on another stream reach the call through an event that the context's stream waits on, with no
+    device-wide synchronisation: the result equals lux_sgm_upsample's."""
+    import torch
+    from lux_b200 import _lib, api
+    pw, ph = 96, 64
+    depth, guide, conf = _inputs(pw, ph, 7)
+    ref = api.DenseUpsampleLayer.run(depth, pw, ph, guide, pw, ph, prev_confidence=conf, ctx=ctx)
+    dev = torch.device("cuda", 0)
+    h_prev = torch.from_numpy(depth).pin_memory()
+    h_conf = torch.from_numpy(conf).pin_memory()
+    h_guide = torch.from_numpy(guide).pin_memory()
+    side = torch.cuda.Stream(dev)
+    with torch.cuda.stream(side):
+        d_prev = h_prev.to(dev, non_blocking=True)
+        d_conf = h_conf.to(dev, non_blocking=True)
+        d_guide = h_guide.to(dev, non_blocking=True)
+        d_out = torch.empty((2 * ph, 2 * pw), dtype=torch.float32, device=dev)
+        d_oc = torch.empty((2 * ph, 2 * pw), dtype=torch.float32, device=dev)
+        written = torch.cuda.Event()
+        written.record(side)
+    lux_stream = torch.cuda.ExternalStream(ctx.lib.lux_sgm_stream(ctx.handle), device=dev)
+    lux_stream.wait_event(written)
+    img = _lib.Img(d_guide.data_ptr(), 2 * pw, 2 * ph, 2 * pw, 1)
+    rc = ctx.lib.lux_sgm_upsample_noalloc(ctx.handle, d_prev.data_ptr(), pw, ph, ctypes.byref(img), pw, ph, 12.0, 2,
+                                          d_conf.data_ptr(), d_out.data_ptr(), d_oc.data_ptr())
+    ctx.check(rc)
+    side.synchronize()
+    assert np.array_equal(d_out.cpu().numpy().view(np.uint32), ref.Depth.view(np.uint32))
+    assert np.array_equal(d_oc.cpu().numpy().view(np.uint32), ref.Confidence.view(np.uint32))
