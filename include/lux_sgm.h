@@ -110,6 +110,7 @@ int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst
  * library picks by size; these flags force one form (tuning and tests). */
 #define LUX_LAYER_SGM_FUSED 16
 #define LUX_LAYER_SGM_SPLIT 32
+#define LUX_LAYER_SGM_WAVE 64    /* the fused wavefront in its lean form (progress counters, packed minima) */
 
 /* DenseLayer.Init + DenseLayer.Compute (DenseStereoSgm.cs:34-62, 181-232): one pyramid layer on the GPU.
  * images: n_cams camera images (camera 0 = reference), box-FILTERED already unless LUX_LAYER_PREFILTER (as
@@ -138,7 +139,8 @@ typedef struct {
   float gpu_ms_cost;     /* device time of the matching-cost kernel (CUDA events on the context's stream) */
   float gpu_ms_sgm;      /* device time of the two aggregation passes */
   float gpu_ms_wta;      /* device time of the winner-take-all */
-  int32_t sgm_kernel;    /* 0 = the exact traversal replay, 1 = fast, four paths fused, 2 = fast, path groups as chains */
+  int32_t sgm_kernel;    /* 0 = the exact traversal replay, 1 = fast, four paths fused, 2 = fast, path groups as chains,
+                            3 = fast, four paths fused, lean wavefront */
   int32_t cost_kernel;   /* 0 = per-pixel warps (any layer), 1 = per-row warps (uniform layer), 2 = per-row warps of an axis-aligned
                             pair, 3 = the same with block columns shared between neighbouring pixels (grey, scale 1) */
 } lux_layer_info;
@@ -279,15 +281,18 @@ int lux_depth_cache_set(lux_sgm_ctx* ctx, const float* depth, int32_t w, int32_t
 int lux_depth_cache_fetch(lux_sgm_ctx* ctx, const float* cache, int32_t cw, int32_t ch, int32_t cache_on_device, int32_t x0, int32_t y0,
                           int32_t x1, int32_t y1, int32_t dims_w, int32_t dims_h, float* out, int32_t out_on_device);
 
-/* ---- Request server. No counterpart in the reference: the serving form of the stage. ----
- * Depth solves of mixed sizes are admitted in arrival order against an HBM budget (a host-side estimate per request;
- * 0 = no limit; a request runs regardless when nothing else is running) and run on `slots` worker contexts, each with
- * its own CUDA stream, so requests that arrive while others are on the GPU start as soon as a slot and memory are free
- * and overlap on the device. A request is one layer, solved exactly as lux_sgm_layer solves it from unfiltered images
- * (LUX_LAYER_PREFILTER is implied; prev = NULL, align 8), its depth map copied into out_depth (host, the layer's w*h
- * floats, out_bytes long; NULL: nothing copied). The server copies the request's small arrays at submit; the caller
- * keeps the image data and out_depth alive until lux_server_wait has returned for the ticket. Every result equals the
- * same request solved alone. */
+/* ---- Request server: the serving form of the stage, admitted like Lux.Library's job queue
+ * (Lux.Library/Core/JobQueue.cs:23-28, Dispatch :474-531). ----
+ * Depth solves of mixed sizes wait in (priority, arrival) order, lower priority values first. Whenever one of the
+ * `slots` worker contexts is free, the first waiting request whose host-side estimate of device memory fits what the
+ * running requests leave of the HBM budget starts (0 = no limit; when nothing runs, the first request starts
+ * regardless). A heavy request (estimate above 1.5 GiB, the queue's LightBytes) that does not fit holds back every heavy
+ * request behind it (no overtaking), while light ones may pass it. Each worker has its own CUDA stream, so requests
+ * that arrive while others are on the GPU start as soon as a slot and memory are free and overlap on the device. A
+ * request is one layer, solved exactly as lux_sgm_layer solves it from unfiltered images (LUX_LAYER_PREFILTER is
+ * implied; prev = NULL, align 8), its depth map copied into out_depth (host, the layer's w*h floats, out_bytes long;
+ * NULL: nothing copied). The server copies the request's small arrays at submit; the caller keeps the image data and
+ * out_depth alive until lux_server_wait has returned for the ticket. Every result equals the same request solved alone. */
 typedef struct lux_server lux_server;
 typedef struct {
   int32_t n_cams;
@@ -299,6 +304,7 @@ typedef struct {
   int32_t flags;
   float* out_depth;
   uint64_t out_bytes;
+  int32_t priority;  /* JobInfo.Priority: lower values start first; equal values in arrival order */
 } lux_request;
 typedef struct {
   int32_t status;           /* LUX_OK or the status the solve returned */
@@ -311,6 +317,13 @@ const char* lux_server_last_error(const lux_server* server);
 int lux_server_submit(lux_server* server, const lux_request* req, uint64_t* ticket);
 /* Waits for a ticket (timeout_ns 0: no limit; LUX_ERR_TIMEOUT when it passes) and releases it. */
 int lux_server_wait(lux_server* server, uint64_t ticket, uint64_t timeout_ns, lux_result* out);
+/* The device bytes the server reserves for a request against its budget (JobInfo.EstimatedMemoryBytes). */
+int lux_server_estimate(const lux_request* req, uint64_t* bytes);
+/* How many requests started ahead of an earlier-queued one that had to wait (light requests passing a heavy one). */
+uint64_t lux_server_passed(const lux_server* server);
+/* The high-water mark of the device memory this library's allocations hold in the device's memory pool (the stream-
+ * ordered pool every context allocates from), in bytes; reset != 0 resets it to the current use afterwards. */
+int lux_sgm_pool_high_water(int device, int32_t reset, uint64_t* bytes);
 
 /* No counterpart in the reference. lux_sgm_upsample without any device allocation, for hosts that cannot let this
  * library allocate GPU memory: a process whose HBM is already reserved by another allocator (an inference server or a

@@ -20,7 +20,7 @@ FIELD_DEPTH, FIELD_PLANES, FIELD_SKIP, FIELD_START, FIELD_COUNT, FIELD_CAP = 0, 
 FIELD_OFFSETS, FIELD_AGG, FIELD_AGG_PASS1, FIELD_RAW, FIELD_GUIDANCE = 6, 7, 8, 9, 10
 
 LAYER_KEEP_PASS1, LAYER_KEEP_AGG, LAYER_PREFILTER, LAYER_FORCE_REPLAY = 1, 2, 4, 8
-LAYER_SGM_FUSED, LAYER_SGM_SPLIT = 16, 32
+LAYER_SGM_FUSED, LAYER_SGM_SPLIT, LAYER_SGM_WAVE = 16, 32, 64
 
 
 class Img(ctypes.Structure):
@@ -41,7 +41,7 @@ class Params(ctypes.Structure):
 class Request(ctypes.Structure):
     _fields_ = [("n_cams", ctypes.c_int32), ("images", ctypes.c_void_p), ("gray", ctypes.c_void_p), ("calibs", ctypes.c_void_p),
                 ("near", ctypes.c_float), ("far", ctypes.c_float), ("params", Params), ("flags", ctypes.c_int32),
-                ("out_depth", ctypes.c_void_p), ("out_bytes", ctypes.c_uint64)]
+                ("out_depth", ctypes.c_void_p), ("out_bytes", ctypes.c_uint64), ("priority", ctypes.c_int32)]
 
 
 class Result(ctypes.Structure):
@@ -135,6 +135,9 @@ SIGNATURES = [
     ("lux_server_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("lux_server_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]),
     ("lux_server_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(Result)]),
+    ("lux_server_estimate", ctypes.c_int, [ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]),
+    ("lux_server_passed", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("lux_sgm_pool_high_water", ctypes.c_int, [ctypes.c_int, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
     ("lux_sgm_upsample_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.POINTER(Img), ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
                                                 ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),

@@ -161,11 +161,12 @@ _default_ctx = None
 
 
 def _flags(keep_pass1, keep_agg, prefilter, force_replay, sgm="auto"):
-    if sgm not in ("auto", "fused", "split"):
-        raise ValueError(f"sgm must be 'auto', 'fused' or 'split', not {sgm!r}")
+    if sgm not in ("auto", "fused", "split", "wave"):
+        raise ValueError(f"sgm must be 'auto', 'fused', 'split' or 'wave', not {sgm!r}")
     return ((L.LAYER_KEEP_PASS1 if keep_pass1 else 0) | (L.LAYER_KEEP_AGG if keep_agg else 0) |
             (L.LAYER_PREFILTER if prefilter else 0) | (L.LAYER_FORCE_REPLAY if force_replay else 0) |
-            (L.LAYER_SGM_FUSED if sgm == "fused" else 0) | (L.LAYER_SGM_SPLIT if sgm == "split" else 0))
+            (L.LAYER_SGM_FUSED if sgm == "fused" else 0) | (L.LAYER_SGM_SPLIT if sgm == "split" else 0) |
+            (L.LAYER_SGM_WAVE if sgm == "wave" else 0))
 
 
 def revisit_schedule(w, h, tile, second_pass):
@@ -717,6 +718,15 @@ class ServedResult:
     run_ms: float
 
 
+def pool_high_water(device: int = 0, reset: bool = False) -> int:
+    """High-water mark (bytes) of the device memory pool this library allocates from; reset restarts it."""
+    b = ctypes.c_uint64()
+    rc = L.load().lux_sgm_pool_high_water(device, 1 if reset else 0, ctypes.byref(b))
+    if rc:
+        _raise(rc, "lux_sgm_pool_high_water failed")
+    return int(b.value)
+
+
 class Server:
     """The request server of the C ABI (lux_server_*; no counterpart in the reference): depth solves of mixed sizes
     admitted in arrival order against an HBM budget and run on `slots` worker contexts, overlapping on the GPU. A request
@@ -731,7 +741,38 @@ class Server:
         self.handle = h
         self._pending = {}
 
-    def submit(self, images, gray, calibs, near, far, params: StereoParams, flags: int = 0) -> int:
+    @staticmethod
+    def _request(images, gray, calibs, near, far, params, flags, priority, out):
+        arr = (L.Img * len(images))()
+        keep = []
+        for i, im in enumerate(images):
+            ci, k = _img_c(im)
+            arr[i] = ci
+            keep.append(k)
+        g = np.ascontiguousarray(np.asarray(gray, dtype=np.uint8))
+        cc = _calibs_c(calibs)
+        req = L.Request(len(images), ctypes.cast(arr, ctypes.c_void_p), g.ctypes.data, ctypes.cast(cc, ctypes.c_void_p), near, far,
+                        params.to_c(), flags, out.ctypes.data if out is not None else None, out.nbytes if out is not None else 0,
+                        int(priority))
+        return req, (keep, arr, g, cc)
+
+    @staticmethod
+    def estimate(images, gray, calibs, near, far, params: StereoParams, flags: int = 0) -> int:
+        """The device bytes the server reserves for this request against its budget."""
+        req, _keep = Server._request(images, gray, calibs, near, far, params, flags, 0, None)
+        b = ctypes.c_uint64()
+        rc = L.load().lux_server_estimate(ctypes.byref(req), ctypes.byref(b))
+        if rc:
+            _raise(rc, "lux_server_estimate failed")
+        return int(b.value)
+
+    @property
+    def passed(self) -> int:
+        """Requests that started ahead of an earlier-queued one that had to wait for memory."""
+        return int(self.lib.lux_server_passed(self.handle))
+
+    def submit(self, images, gray, calibs, near, far, params: StereoParams, flags: int = 0, priority: int = 0) -> int:
+        """Queues a request (lower priority values start first; equal ones in arrival order) and returns its ticket."""
         arr = (L.Img * len(images))()
         keep = []
         for i, im in enumerate(images):
@@ -744,7 +785,7 @@ class Server:
         sc = max(1, int(params.scale))
         out = np.empty(((h0 + sc - 1) // sc, (w0 + sc - 1) // sc), np.float32)
         req = L.Request(len(images), ctypes.cast(arr, ctypes.c_void_p), g.ctypes.data, ctypes.cast(cc, ctypes.c_void_p), near, far,
-                        params.to_c(), flags, out.ctypes.data, out.nbytes)
+                        params.to_c(), flags, out.ctypes.data, out.nbytes, int(priority))
         t = ctypes.c_uint64()
         rc = self.lib.lux_server_submit(self.handle, ctypes.byref(req), ctypes.byref(t))
         if rc:

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "liblux_sgm.so")
 
-SOURCES = ["prep.cu", "cost.cu", "sgm_emulate.cu", "sgm_uniform.cu", "sgm_split.cu", "depth_cache.cu", "warp.cu", "census_sgm.cu", "lux_sgm.cu", "host_geom.cpp", "server.cpp", "dump.cpp", "color_transfer.cpp"]
+SOURCES = ["prep.cu", "cost.cu", "sgm_emulate.cu", "sgm_uniform.cu", "sgm_split.cu", "sgm_wave.cu", "depth_cache.cu", "warp.cu", "census_sgm.cu", "lux_sgm.cu", "host_geom.cpp", "server.cpp", "dump.cpp", "color_transfer.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

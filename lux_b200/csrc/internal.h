@@ -163,6 +163,10 @@ size_t uniform_scratch_bytes(int W, int H, int n_planes, int tile);
 size_t split_scratch_bytes(int W, int H, int n);
 int run_sgm_split(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
                   uint16_t* agg_pass1, float* depth, int keep_agg, void* scratch, size_t scratch_bytes, int* err, cudaStream_t s);
+// sgm_wave.cu: the fused four-path wavefront in its lean form (progress counters, packed minima, 16 rows a block)
+size_t wave_scratch_bytes(int W, int H, int n);
+int run_sgm_wave(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
+                 uint16_t* agg_pass1, float* depth, int keep_agg, void* scratch, size_t scratch_bytes, int* err, cudaStream_t s);
 int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, const float gw[4], const uint8_t* raw, uint16_t* agg,
                     uint16_t* agg_pass1, float* depth, int keep_agg, void* scratch, size_t scratch_bytes, int* err,
                     cudaStream_t s);

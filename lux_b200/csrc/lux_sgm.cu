@@ -355,19 +355,22 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   if (fast) {
     void* scr = nullptr;
     // the path-group chains win from about 2 MP (their critical path is W or H steps instead of 2H + W)
-    const bool split = (flags & LUX_LAYER_SGM_SPLIT) ? true : (flags & LUX_LAYER_SGM_FUSED) ? false : (size_t)W * H >= 2000000;
-    const size_t sb = split ? split_scratch_bytes(W, H, L->n) : uniform_scratch_bytes(W, H, L->n, p.tile);
+    const int form = (flags & LUX_LAYER_SGM_WAVE) ? 3 : (flags & LUX_LAYER_SGM_SPLIT) ? 2 : (flags & LUX_LAYER_SGM_FUSED) ? 1
+                     : (size_t)W * H >= 2000000 ? 2 : 1;
+    const size_t sb = form == 2 ? split_scratch_bytes(W, H, L->n) : form == 3 ? wave_scratch_bytes(W, H, L->n)
+                                : uniform_scratch_bytes(W, H, L->n, p.tile);
     if ((rc = dev_alloc(ctx, tmp, sb, &scr))) return rc;
-    if (split)
-      rc = run_sgm_split(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth,
-                         (flags & LUX_LAYER_KEEP_AGG) ? 1 : 0, scr, sb, ctx->d_err, s);
+    const int keep = (flags & LUX_LAYER_KEEP_AGG) ? 1 : 0;
+    if (form == 2)
+      rc = run_sgm_split(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
+    else if (form == 3)
+      rc = run_sgm_wave(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
     else
-      rc = run_sgm_uniform(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth,
-                           (flags & LUX_LAYER_KEEP_AGG) ? 1 : 0, scr, sb, ctx->d_err, s);
+      rc = run_sgm_uniform(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
     if (rc) return set_err(ctx, LUX_ERR_CUDA, "uniform aggregation launch failed (%d)", rc);
     CK(cudaEventRecord(ctx->ev[2], s));
     CK(cudaEventRecord(ctx->ev[3], s));
-    L->sgm_kernel = split ? 2 : 1;
+    L->sgm_kernel = form;
     L->agg_final = (flags & LUX_LAYER_KEEP_AGG) != 0;
     CK(cudaGetLastError());
     if ((rc = take_device_error(ctx))) return rc;
@@ -467,6 +470,20 @@ const char* lux_sgm_last_error(const lux_sgm_ctx* ctx) { return ctx ? ctx->last_
 uint64_t lux_sgm_kernel_launches(void) { return lux::kernel_launches(); }
 
 void* lux_sgm_stream(lux_sgm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int lux_sgm_pool_high_water(int device, int32_t reset, uint64_t* bytes) {
+  if (!bytes) return LUX_ERR_ARG;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return LUX_ERR_CUDA;
+  uint64_t v = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &v) != cudaSuccess) return LUX_ERR_CUDA;
+  *bytes = v;
+  if (reset) {
+    uint64_t zero = 0;
+    if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero) != cudaSuccess) return LUX_ERR_CUDA;
+  }
+  return LUX_OK;
+}
 
 int lux_sgm_set_wait_limit(lux_sgm_ctx* ctx, uint64_t limit_ns) {
   if (!ctx) return LUX_ERR_ARG;

@@ -1,11 +1,16 @@
-// Request server for depth solves of mixed sizes (no counterpart in the reference; the serving form of the stage).
+// Request server for depth solves of mixed sizes (the serving form of the stage; its admission rule is the one of
+// Lux.Library's job queue, Lux.Library/Core/JobQueue.cs:23-28 and Dispatch :474-531).
 //
-// Requests are admitted in arrival order against an HBM budget, each with a host-side estimate of its device memory,
-// and run on `slots` worker contexts (each its own CUDA stream, error word and events, all drawing on the device's
-// memory pool), so requests that arrive while others are on the GPU start as soon as a slot and memory are free and
-// their work overlaps on the device with the host-side work (copies, planes, schedules) of the others. A request is
-// one layer solved exactly as lux_sgm_layer solves it (prefilter included), its depth map read back into the caller's
-// host buffer; the server adds no arithmetic of its own, so every result equals the same request run alone.
+// Requests wait in a queue ordered by priority (lower first), then by arrival. Whenever a worker is free the dispatcher
+// walks that order and starts the first request that may start: one whose estimated device memory fits what the running
+// requests leave of the HBM budget (or any request when nothing runs). A heavy request (estimate above 1.5 GiB, the
+// queue's LightBytes) that does not fit holds back every heavy request behind it, so heavy requests never overtake each
+// other, while light ones (previews) may pass it. Requests run on `slots` worker contexts (each its own CUDA stream,
+// error word and events, all drawing on the device's memory pool), so requests that arrive while others are on the GPU
+// start as soon as a slot and memory are free and their work overlaps on the device with the host-side work (copies,
+// planes, schedules) of the others. A request is one layer solved exactly as lux_sgm_layer solves it (prefilter
+// included), its depth map read back into the caller's host buffer; the server adds no arithmetic of its own, so every
+// result equals the same request run alone.
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -33,8 +38,11 @@ struct Pending {
   float* out_depth = nullptr;
   uint64_t out_bytes = 0;
   uint64_t estimate = 0;
+  int32_t priority = 0;
   Clock::time_point submitted, started;
 };
+
+constexpr uint64_t kLightBytes = 3ull << 29;  // 1.5 GiB: JobQueue.LightBytes (JobQueue.cs:47)
 
 struct Done {
   lux_result result{};
@@ -57,6 +65,7 @@ struct lux_server {
   int running = 0;
   bool stop = false;
   std::string last_error;
+  uint64_t passed = 0;  // requests started ahead of an earlier-queued request that had to wait
 };
 
 namespace {
@@ -79,18 +88,37 @@ uint64_t estimate_bytes(const Pending& p) {
   return b;
 }
 
+// The request a free worker starts (JobQueue.Dispatch, JobQueue.cs:496-521): the queue is kept in (priority, arrival)
+// order; the first request whose memory fits starts, a heavy one that does not fit blocks the heavy ones behind it.
+// Returns the index in the queue, or -1 when nothing may start now.
+long pick(const lux_server* s) {
+  const bool anything = s->in_use > 0 || s->running > 0;
+  bool heavy_blocked = false;
+  for (size_t i = 0; i < s->queue.size(); i++) {
+    const Pending& p = s->queue[i];
+    const bool heavy = p.estimate > kLightBytes;
+    if (heavy && heavy_blocked) continue;
+    const bool fits = s->budget == 0 || s->in_use + p.estimate <= s->budget;
+    if (anything && !fits) {
+      if (heavy) heavy_blocked = true;
+      continue;
+    }
+    return (long)i;
+  }
+  return -1;
+}
+
 void worker(lux_server* s, lux_sgm_ctx* ctx) {
   for (;;) {
     Pending p;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      // arrival order: the head request runs once its memory fits the budget (or nothing else is running)
-      s->cv_work.wait(lk, [&] {
-        return s->stop || (!s->queue.empty() && (s->running == 0 || s->budget == 0 || s->in_use + s->queue.front().estimate <= s->budget));
-      });
-      if (s->queue.empty()) return;  // stop with nothing left
-      p = std::move(s->queue.front());
-      s->queue.pop_front();
+      long i = -1;
+      s->cv_work.wait(lk, [&] { return (s->stop && s->queue.empty()) || (i = pick(s)) >= 0; });
+      if (i < 0) return;  // stop with nothing left
+      if (i > 0) s->passed++;
+      p = std::move(s->queue[(size_t)i]);
+      s->queue.erase(s->queue.begin() + i);
       s->in_use += p.estimate;
       s->running++;
     }
@@ -177,6 +205,7 @@ int lux_server_submit(lux_server* s, const lux_request* req, uint64_t* ticket) {
   p.out_depth = req->out_depth;
   p.out_bytes = req->out_bytes;
   p.estimate = estimate_bytes(p);
+  p.priority = req->priority;
   p.submitted = Clock::now();
   {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -184,10 +213,32 @@ int lux_server_submit(lux_server* s, const lux_request* req, uint64_t* ticket) {
     p.ticket = s->next_ticket++;
     *ticket = p.ticket;
     s->results[p.ticket] = Done{};
-    s->queue.push_back(std::move(p));
+    // insert after every waiting request of the same or a lower priority value (priority, then arrival)
+    auto at = s->queue.end();
+    while (at != s->queue.begin() && (at - 1)->priority > p.priority) --at;
+    s->queue.insert(at, std::move(p));
   }
   s->cv_work.notify_all();
   return LUX_OK;
+}
+
+int lux_server_estimate(const lux_request* req, uint64_t* bytes) {
+  if (!req || !bytes || req->n_cams < 2 || req->n_cams > 16 || !req->images || !req->calibs) return LUX_ERR_ARG;
+  Pending p;
+  p.images.assign(req->images, req->images + req->n_cams);
+  p.calibs.assign(req->calibs, req->calibs + req->n_cams);
+  p.near_ = req->near_;
+  p.far_ = req->far_;
+  p.params = req->params;
+  p.flags = req->flags;
+  *bytes = estimate_bytes(p);
+  return LUX_OK;
+}
+
+uint64_t lux_server_passed(const lux_server* s) {
+  if (!s) return 0;
+  std::lock_guard<std::mutex> lk(const_cast<lux_server*>(s)->mu);
+  return s->passed;
 }
 
 int lux_server_wait(lux_server* s, uint64_t ticket, uint64_t timeout_ns, lux_result* out) {

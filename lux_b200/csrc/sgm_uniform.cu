@@ -34,58 +34,6 @@ constexpr int kBandBufs = 4;   // band buffers in rotation
 constexpr int kRing = 8;       // slots of the hand-over ring between neighbouring rows of a block
 constexpr int kPublish = 8;    // the publisher releases the global band progress every kPublish pixels
 
-// A revisit R(c, y) (DenseStereoSgm.cs:234-317 replayed at the last column), run by one warp.
-template <int LPT>
-LUX_DEV void run_revisit(const UniArgs& a, int y, int lane, bool active) {
-  const int c = a.W - 1;
-  Src<LPT> s[4];
-  const int e[3] = {a.src0[y], a.src1[y], a.src2[y]};
-  const int xsrc[3] = {c - 1, c - 1, c};
-#pragma unroll
-  for (int p = 0; p < 3; p++) {
-    const int kind = src_kind(e[p]), row = src_row(e[p]);
-    if (kind == kSrcInit) src_init(s[p]);
-    else if (kind == kSrcEdge) src_edge<LPT>(a, s[p], a.dir > 0 ? xsrc[p] : a.W - 1 - xsrc[p], p, lane);
-    else src_cs<LPT>(a, s[p], row, kind - kSrcCs, xsrc[p], lane);
-  }
-  src_init(s[3]);
-  const float4 g = pix_of(a, c, y);
-  int p2 = 0;
-  if (lane < 4) p2 = p2_of(a, g, pick_pix<LPT>(s, lane));
-  V<LPT> raw2, acc, out[4];
-  load_raw<LPT>(a, c, y, raw2, active, lane);
-#pragma unroll
-  for (int i = 0; i < LPT / 2; i++) acc.r[i] = 0;
-  const uint32_t p1x2 = dup16((uint32_t)a.p1);
-  uint32_t mins[4];
-#pragma unroll
-  for (int p = 0; p < 4; p++) {
-    const int P2 = __shfl_sync(0xffffffffu, p2, p);
-    const uint32_t p2p = (uint32_t)min(P2 + (int)s[p].mn, 65535);
-    uint32_t rmin = 0xffffffffu;
-    path_step<LPT>(s[p].L, s[p].mn, p2p, p1x2, raw2, active, lane, out[p], acc, rmin);
-    mins[p] = warp_min<LPT>(rmin);
-  }
-  uint16_t* ap = agg_ptr<LPT>(a, c, y, lane);  // the revisit adds its four paths once more (:311)
-  V<LPT> old;
-  agg_load<LPT>(ap, old, active);
-#pragma unroll
-  for (int i = 0; i < LPT / 2; i++) old.r[i] += acc.r[i];
-  agg_store<LPT>(ap, old, active);
-  cs_put<LPT>(a, out[1], mins[1], y, 3, lane);
-  cs_put<LPT>(a, out[2], mins[2], y, 4, lane);
-  if (a.edge_write && (a.extra[y] & 1)) {  // R(y_b) is what pass -1 will read at the last column
-    constexpr int Dp = Dp_of(LPT);
-    vstore<LPT>(out[1], a.edge + ((size_t)c * 3 + 0) * Dp, lane);
-    vstore<LPT>(out[2], a.edge + ((size_t)c * 3 + 1) * Dp, lane);
-    if (lane == 0) {
-      __stcg(a.edge_min + (size_t)c * 3 + 0, (uint16_t)mins[1]);
-      __stcg(a.edge_min + (size_t)c * 3 + 1, (uint16_t)mins[2]);
-    }
-  }
-  __syncwarp();
-}
-
 // Shared memory of a block: kRows + 1 hand-over rings (ring kRows is the row above the block, filled by the loader warp),
 // their minima, and a full and an empty mbarrier per ring slot.
 template <int LPT>

@@ -18,7 +18,7 @@ def _compute(api, ctx, wl, filt, kernel):
                                   ctx=ctx, **args)
 
 
-@pytest.mark.parametrize("kernel", ["fused", "split", "replay"])
+@pytest.mark.parametrize("kernel", ["fused", "split", "wave", "replay"])
 def test_stalled_block_times_out_and_context_recovers(oracle, kernel):
     from lux_b200 import api, synth
     ctx = api.Context(0)

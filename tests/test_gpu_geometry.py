@@ -53,13 +53,13 @@ def _solve_both_forms(ctx, oracle, wl, forms, tag, cost_kernel):
 def test_pair_1040x780_d64_full_frame(ctx, oracle):
     from lux_b200 import synth
     wl = synth.rectified_pair(1040, 780, 64, seed=0, tile=64)
-    _solve_both_forms(ctx, oracle, wl, ["fused", "split"], "1040x780 D64", cost_kernel=3)
+    _solve_both_forms(ctx, oracle, wl, ["fused", "split", "wave"], "1040x780 D64", cost_kernel=3)
 
 
 def test_pair_13mp_geometry_strip(ctx, oracle):
     from lux_b200 import synth
     wl = synth.rectified_pair(4160, 600, 256, seed=1, bits=12, tile=64)
-    _solve_both_forms(ctx, oracle, wl, ["split", "fused"], "4160x600 D256", cost_kernel=3)
+    _solve_both_forms(ctx, oracle, wl, ["split", "fused", "wave"], "4160x600 D256", cost_kernel=3)
 
 
 def test_align2_ragged_layer_index_error(ctx, oracle):

@@ -46,14 +46,14 @@ UNIFORM_CASES = [(48, 40, 16, 8), (65, 49, 16, 4), (160, 120, 32, 16), (257, 93,
                  (200, 35, 136, 8), (71, 66, 256, 64), (33, 17, 40, 2), (64, 9, 192, 32)]
 
 
-SGM_FORMS = {"fused": 1, "split": 2, "replay": 0}  # kernel -> lux_layer_info.sgm_kernel
+SGM_FORMS = {"fused": 1, "split": 2, "replay": 0, "wave": 3}  # kernel -> lux_layer_info.sgm_kernel
 
 
 def _sgm_args(kernel):
     return dict(force_replay=True) if kernel == "replay" else dict(sgm=kernel)
 
 
-@pytest.mark.parametrize("kernel", ["fused", "split", "replay"])
+@pytest.mark.parametrize("kernel", ["fused", "split", "wave", "replay"])
 @pytest.mark.parametrize("w,h,d,tile", UNIFORM_CASES)
 def test_uniform_layer_bit_exact(ctx, oracle, w, h, d, tile, kernel):
     from lux_b200 import api, synth
@@ -87,7 +87,7 @@ def test_replay_barrier_form_bit_exact(ctx, oracle, w, h, d, tile):
         gl.close()
 
 
-@pytest.mark.parametrize("kernel", ["fused", "split"])
+@pytest.mark.parametrize("kernel", ["fused", "split", "wave"])
 def test_uniform_fast_depth_without_kept_aggregates(ctx, oracle, kernel):
     """The production form (no Agg kept, WTA fused into the last kernel of pass -1) gives the same depth."""
     from lux_b200 import api, synth
@@ -157,7 +157,7 @@ def test_axis_pair_scale2_grey(ctx, oracle):
         gl.close()
 
 
-@pytest.mark.parametrize("kernel", ["fused", "split"])
+@pytest.mark.parametrize("kernel", ["fused", "split", "wave"])
 def test_axis_pair_colour_bit_exact(ctx, oracle, kernel):
     """A rectified colour pair: the axis-aligned cost kernel with the colour block (the tests above are grey)."""
     from lux_b200 import api, synth
@@ -182,7 +182,7 @@ def test_axis_pair_colour_bit_exact(ctx, oracle, kernel):
         gl.close()
 
 
-@pytest.mark.parametrize("kernel", ["fused", "split", "replay"])
+@pytest.mark.parametrize("kernel", ["fused", "split", "wave", "replay"])
 def test_uniform_layer_with_skip_mask(ctx, oracle, kernel):
     """A first layer with SkipMode 2: skipped pixels aggregate raw 0 (DenseStereoSgm.cs:242)."""
     from lux_b200 import api, synth
@@ -200,7 +200,7 @@ def test_uniform_layer_with_skip_mask(ctx, oracle, kernel):
         gl.close()
 
 
-@pytest.mark.parametrize("kernel", ["fused", "split"])
+@pytest.mark.parametrize("kernel", ["fused", "split", "wave"])
 @pytest.mark.parametrize("n_cams,colour", [(4, False), (6, True), (6, False)])
 def test_multicamera_layers_bit_exact(ctx, oracle, n_cams, colour, kernel):
     """Grey and colour layers with 3 and 5 other cameras (the per-camera cost loop with its camera count at run time)."""
@@ -219,7 +219,7 @@ def test_multicamera_layers_bit_exact(ctx, oracle, n_cams, colour, kernel):
         gl.close()
 
 
-@pytest.mark.parametrize("kernel", ["fused", "split"])
+@pytest.mark.parametrize("kernel", ["fused", "split", "wave"])
 def test_module_capture_bit_exact(ctx, oracle, kernel):
     """A batched capture: 10 module cameras with their own crops, focal scales and disparity ranges, fused at cost level
     into one layer (the reference's multi-view sum, DenseStereo.cs:242-291)."""
@@ -237,7 +237,7 @@ def test_module_capture_bit_exact(ctx, oracle, kernel):
         gl.close()
 
 
-@pytest.mark.parametrize("kernel", ["fused", "split"])
+@pytest.mark.parametrize("kernel", ["fused", "split", "wave"])
 def test_pyramid_bit_exact(ctx, oracle, kernel):
     """DenseStereoPyramid.Run: six L16 layers (ragged ranges, skip masks, align choice) against the oracle."""
     from lux_b200 import api, synth
