@@ -97,6 +97,15 @@ void lux_sgm_l16_pyramid(lux_stereo_params out[6]);
 int lux_sgm_planes(float near_, float far_, const lux_calib* calibs, int32_t n_cams, float density, int32_t align, float* out,
                    int32_t* n_out);
 
+/* A grey camera image of `bits` (9..16) bits per sample stored as uint16 (src: host, or device when src_on_device; stride
+ * in samples) made into the reference's grey image domain on the GPU: Rgba8Image bytes (Y, 128, 128, 255) with
+ * Y = (v + 2^(bits-9)) >> (bits - 8) saturated (12-bit: (v + 8) >> 4), the mapping every 12-bit input of this library
+ * follows (the reference's only image type is Rgba8Image, SparseLnrMatch.cs:8-13). dst: a device buffer of w*h*4 bytes,
+ * then usable as an on_device lux_img_rgba8 (stride w). From host memory the samples cross as 2 bytes a pixel; the call
+ * returns once the host buffer has been read, and the result is ordered on the context's stream. */
+int lux_image_from_grey16(lux_sgm_ctx* ctx, const uint16_t* src, int32_t w, int32_t h, int32_t stride, int32_t src_on_device,
+                          int32_t bits, uint8_t* dst);
+
 /* DenseStereo.BoxFilter3 (DenseStereo.cs:93-123) of one image; dst is host memory of w*h*4 bytes (dense). */
 int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst);
 

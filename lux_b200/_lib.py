@@ -85,6 +85,8 @@ SIGNATURES = [
     ("lux_sgm_planes", ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.POINTER(Calib), ctypes.c_int32, ctypes.c_float,
                                       ctypes.c_int32, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int32)]),
     ("lux_sgm_box_filter3", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Img), ctypes.c_void_p]),
+    ("lux_image_from_grey16", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]),
     ("lux_sgm_layer", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(Img), ctypes.c_void_p, ctypes.POINTER(Calib),
                                      ctypes.c_float, ctypes.c_float, ctypes.POINTER(Params), ctypes.c_int32, ctypes.c_int32,
                                      ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),

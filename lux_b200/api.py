@@ -216,6 +216,27 @@ class DenseStereo:
         return out
 
 
+def image_from_grey16(samples, bits: int = 12, ctx: Optional[Context] = None, out=None):
+    """A grey camera image of `bits` bits per sample (uint16; a numpy array or a torch tensor, host or CUDA) made into the
+    reference's grey Rgba8Image bytes (Y, 128, 128, 255), Y = (v + 2^(bits-9)) >> (bits - 8) saturated, on the GPU: a CUDA
+    uint8 tensor (h, w, 4) usable as an on-device image of DenseLayer.compute. Host samples cross as 2 bytes a pixel."""
+    import torch
+    ctx = ctx or default_context()
+    if hasattr(samples, "data_ptr"):
+        h, w = samples.shape
+        assert samples.element_size() == 2
+        on_dev, ptr, stride = (1 if samples.is_cuda else 0), samples.data_ptr(), samples.stride(0)
+        _torch_ready(samples)
+    else:
+        a = np.ascontiguousarray(samples, np.uint16)
+        h, w = a.shape
+        on_dev, ptr, stride = 0, a.ctypes.data, w
+    if out is None:
+        out = torch.empty((h, w, 4), dtype=torch.uint8, device=torch.device("cuda", ctx.device))
+    ctx.check(ctx.lib.lux_image_from_grey16(ctx.handle, ptr, w, h, stride, on_dev, int(bits), out.data_ptr()))
+    return out
+
+
 class DenseLayer:
     """A computed DenseLayer (DenseStereoSgm.cs:13-232) whose state lives on the GPU until close()."""
 

@@ -63,6 +63,8 @@ void launch_estimate_terms(const uint16_t* count, const uint8_t* skip, int npx, 
 void launch_check_caps(const uint16_t* cap, int npx, int* err, cudaStream_t s);
 void launch_wta(const LayerGeom& g, const uint16_t* agg, float* depth, int* err, cudaStream_t s);
 void launch_fill_u16(uint16_t* p, size_t n, uint16_t v, cudaStream_t s);
+// grey u16 samples of `bits` (9..16) bits -> the reference's grey YUVA bytes, dense w x h RGBA8 (h <= 65535)
+void launch_grey16_to_rgba8(const uint16_t* src, int w, int h, int stride, int bits, uint8_t* dst, cudaStream_t s);
 void launch_uniform_ranges(uint16_t* start, uint16_t* count, uint16_t* cap, uint64_t* off, int npx, int n, cudaStream_t s);
 // upsample chain (DenseUpsampleLayer.cs): g2 = NearestResize(ImageShift(guide)), then the bilateral upsample of 1/depth
 void launch_upsample(const float* prev, int pw, int ph, const uint8_t* guide, int gw, int gh, int gstride, float sigma,

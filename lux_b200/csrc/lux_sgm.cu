@@ -566,6 +566,28 @@ int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst
   return rc;
 }
 
+int lux_image_from_grey16(lux_sgm_ctx* ctx, const uint16_t* src, int32_t w, int32_t h, int32_t stride, int32_t src_on_device,
+                          int32_t bits, uint8_t* dst) {
+  if (!ctx || !src || !dst || w <= 0 || h <= 0 || stride < w || h > 65535 || bits < 9 || bits > 16)
+    return set_err(ctx, LUX_ERR_ARG, "image_from_grey16: null pointer, empty size, stride < w, h > 65535 or bits outside 9..16");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  std::vector<DevBuf> tmp;
+  const uint16_t* d_src = src;
+  int rc = LUX_OK;
+  if (!src_on_device) {  // the samples cross as 2 bytes a pixel; the expansion to 4 bytes happens on the GPU
+    uint16_t* d = nullptr;
+    if ((rc = alloc_t(ctx, tmp, (size_t)w * h, &d))) return rc;
+    CK(cudaMemcpy2DAsync(d, (size_t)w * 2, src, (size_t)stride * 2, (size_t)w * 2, h, cudaMemcpyHostToDevice, ctx->stream));
+    d_src = d;
+  }
+  launch_grey16_to_rgba8(d_src, w, h, src_on_device ? stride : w, bits, dst, ctx->stream);
+  CK(cudaGetLastError());
+  if (!src_on_device) CK(cudaStreamSynchronize(ctx->stream));  // the host buffer may be reused once this returns
+  dev_free_all(ctx, tmp);
+  return rc;
+}
+
 int lux_sgm_layer(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
                   float near_, float far_, const lux_stereo_params* params, int32_t index, int32_t align, const lux_layer* prev,
                   int32_t flags, lux_layer** out) {

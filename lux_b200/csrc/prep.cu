@@ -209,6 +209,25 @@ void launch_check_caps(const uint16_t* cap, int npx, int* err, cudaStream_t s) {
   count_launches(1);
 }
 
+// A grey image of `bits` per sample (9..16, u16) as the reference's grey YUVA bytes (Y, 128, 128, 255): Y = (v + half) >>
+// (bits - 8) saturated at 255, half = 1 << (bits - 9) (12-bit: (v + 8) >> 4). Four pixels a thread.
+__global__ void k_grey16_to_rgba8(const uint16_t* __restrict__ src, int w, int h, int stride, int bits, uchar4* __restrict__ dst) {
+  const int shift = bits - 8, half = 1 << (shift - 1);
+  const int x4 = (blockIdx.x * blockDim.x + threadIdx.x) * 4, y = blockIdx.y;
+  if (x4 >= w || y >= h) return;
+  const uint16_t* row = src + (size_t)y * stride;
+  uchar4* out = dst + (size_t)y * w;
+  for (int k = 0; k < 4 && x4 + k < w; k++) {
+    const int v = min(255, ((int)row[x4 + k] + half) >> shift);
+    out[x4 + k] = make_uchar4((unsigned char)v, 128, 128, 255);
+  }
+}
+void launch_grey16_to_rgba8(const uint16_t* src, int w, int h, int stride, int bits, uint8_t* dst, cudaStream_t s) {
+  dim3 grid((w + 4 * 128 - 1) / (4 * 128), h);
+  k_grey16_to_rgba8<<<grid, 128, 0, s>>>(src, w, h, stride, bits, reinterpret_cast<uchar4*>(dst));
+  count_launches(1);
+}
+
 __global__ void k_fill_u16(uint16_t* p, size_t n, uint16_t v) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t stride = (size_t)gridDim.x * blockDim.x;

@@ -115,6 +115,7 @@ class PairWorkload:
     params: StereoParams
     disparity: np.ndarray         # ground truth (reference grid)
     d: int
+    samples: List[np.ndarray] = None  # the cameras' grey samples as uint16 (pairs of more than 8 bits), before the byte mapping
 
     @property
     def de(self):
@@ -130,9 +131,11 @@ def rectified_pair(w, h, d, seed=0, bits=8, noise_sigma=2.0, tile=64, f=1000.0, 
     right = warp_other(left, disp, seed, noise_sigma, maxv)
     left = np.clip(left + np.random.default_rng(seed + 15485863).standard_normal((h, w)) * noise_sigma, 0, maxv)
     imgs = [gray_rgba(to_u8(np.rint(left), bits)), gray_rgba(to_u8(right, bits))]
+    samples = [np.rint(left).astype(np.uint16), right.astype(np.uint16)] if bits > 8 else None
     near = np.float32(f * baseline / (d - 1))
     params = StereoParams(scale=1, tile=tile, skip_mode=0, plane_density=1.0)
-    return PairWorkload(imgs, [1, 1], rectified_calibs(f, w / 2.0, h / 2.0, baseline), float(near), 1e30, params, disp, d)
+    return PairWorkload(imgs, [1, 1], rectified_calibs(f, w / 2.0, h / 2.0, baseline), float(near), 1e30, params, disp, d,
+                        samples)
 
 
 @dataclass

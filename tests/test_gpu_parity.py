@@ -285,3 +285,26 @@ def test_layer_errors(ctx):
     bad = api.StereoParams(scale=1, tile=8, skip_mode=3, plane_density=1.0)
     with pytest.raises(api.NotSupportedError):
         api.DenseLayer.compute(wl.images, wl.gray, wl.calibs, wl.near, wl.far, bad, ctx=ctx)
+
+
+@pytest.mark.parametrize("bits,w,h,stride", [(12, 333, 47, 333), (12, 4160, 20, 4200), (10, 65, 9, 70), (16, 31, 5, 31)])
+def test_image_from_grey16(ctx, bits, w, h, stride):
+    """u16 grey samples made into the reference's byte domain on the GPU, host and device sources, equal to the mapping
+    the 12-bit workloads apply on the host ((v + 8) >> 4 saturated for 12 bits)."""
+    import torch
+    from lux_b200 import api, synth
+    rng = np.random.default_rng(bits * w)
+    full = rng.integers(0, 1 << bits, (h, stride), dtype=np.uint16)
+    full[0, : min(w, 8)] = [(1 << bits) - 1, 0, 7, 8, 4087, 4088, 4095, 1][: min(w, 8)]  # rounding and saturation edges
+    sh = bits - 8
+    want = synth.gray_rgba(np.clip((full[:, :w].astype(np.int64) + (1 << (sh - 1))) >> sh, 0, 255).astype(np.uint8))
+    if bits == 12:
+        assert np.array_equal(want, synth.gray_rgba(synth.to_u8(full[:, :w], 12)))
+    host = api.image_from_grey16(np.ascontiguousarray(full[:, :w]), bits, ctx=ctx)
+    ctx.check(ctx.lib.lux_sgm_sync(ctx.handle))
+    assert np.array_equal(host.cpu().numpy(), want)
+    dev = torch.from_numpy(full.view(np.int16)).cuda()[:, :w]  # a strided device view
+    assert dev.stride(0) == stride
+    out = api.image_from_grey16(dev, bits, ctx=ctx)
+    ctx.check(ctx.lib.lux_sgm_sync(ctx.handle))
+    assert np.array_equal(out.cpu().numpy(), want)
