@@ -120,6 +120,15 @@ int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst
 #define LUX_LAYER_SGM_FUSED 16
 #define LUX_LAYER_SGM_SPLIT 32
 #define LUX_LAYER_SGM_WAVE 64    /* the fused wavefront in its lean form (progress counters, packed minima) */
+/* Autotuning of the fast form (no counterpart in the reference, which has one CPU loop): with none of the three flags
+ * above, a uniform layer of a shape (w, h, planes, tile) not seen before is aggregated once with every fast form on its
+ * own cost volume, timed with CUDA events; the fastest is kept for later solves of that shape by every context of the
+ * process (all forms give the same bits, so the result does not depend on the choice). Without autotuning, or for a
+ * shape not yet tuned, the choice is by size. lux_sgm_set_tuned_form sets or (form 0) clears a choice, e.g. to restore
+ * choices saved from an earlier process. */
+int lux_sgm_set_autotune(lux_sgm_ctx* ctx, int32_t on);
+int32_t lux_sgm_tuned_form(int32_t w, int32_t h, int32_t n_planes, int32_t tile);
+int lux_sgm_set_tuned_form(int32_t w, int32_t h, int32_t n_planes, int32_t tile, int32_t form);
 
 /* DenseLayer.Init + DenseLayer.Compute (DenseStereoSgm.cs:34-62, 181-232): one pyramid layer on the GPU.
  * images: n_cams camera images (camera 0 = reference), box-FILTERED already unless LUX_LAYER_PREFILTER (as
@@ -152,6 +161,7 @@ typedef struct {
                             3 = fast, four paths fused, lean wavefront */
   int32_t cost_kernel;   /* 0 = per-pixel warps (any layer), 1 = per-row warps (uniform layer), 2 = per-row warps of an axis-aligned
                             pair, 3 = the same with block columns shared between neighbouring pixels (grey, scale 1) */
+  int32_t tuned;         /* the fast form the autotuner chose on this solve (it timed every form), 0 when it did not run */
 } lux_layer_info;
 int lux_layer_get_info(const lux_layer* layer, lux_layer_info* info);
 

@@ -64,7 +64,7 @@ class LayerInfo(ctypes.Structure):
                 ("n_planes", ctypes.c_int32), ("min_lo", ctypes.c_int32), ("max_hi", ctypes.c_int32), ("tile", ctypes.c_int32),
                 ("volume", ctypes.c_uint64), ("gpu_ms_cost", ctypes.c_float), ("gpu_ms_sgm", ctypes.c_float),
                 ("gpu_ms_wta", ctypes.c_float), ("sgm_kernel", ctypes.c_int32),
-                ("cost_kernel", ctypes.c_int32)]
+                ("cost_kernel", ctypes.c_int32), ("tuned", ctypes.c_int32)]
 
 
 # every exported symbol with its signature: (name, restype, argtypes)
@@ -76,6 +76,9 @@ SIGNATURES = [
     ("lux_sgm_kernel_launches", ctypes.c_uint64, []),
     ("lux_sgm_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("lux_sgm_set_wait_limit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("lux_sgm_set_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
+    ("lux_sgm_tuned_form", ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    ("lux_sgm_set_tuned_form", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     ("lux_sgm_get_wait_limit", ctypes.c_uint64, [ctypes.c_void_p]),
     ("lux_sgm_debug_stall", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     ("lux_sgm_revisit_schedule", ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

@@ -141,6 +141,10 @@ class Context:
     def wait_limit_ns(self, ns: int):
         self.check(self.lib.lux_sgm_set_wait_limit(self.handle, int(ns)))
 
+    def set_autotune(self, on: bool):
+        """Untuned uniform layer shapes time every fast aggregation form on their first solve (the default) or not."""
+        self.check(self.lib.lux_sgm_set_autotune(self.handle, 1 if on else 0))
+
     def debug_stall(self, block: int):
         """Failure-path tests only: aggregation block `block` (>= 1) waits on a counter nothing publishes (-1: off)."""
         self.check(self.lib.lux_sgm_debug_stall(self.handle, int(block)))
@@ -251,6 +255,7 @@ class DenseLayer:
         self.gpu_ms_cost, self.gpu_ms_sgm, self.gpu_ms_wta = info.gpu_ms_cost, info.gpu_ms_sgm, info.gpu_ms_wta
         self.sgm_kernel = info.sgm_kernel
         self.cost_kernel = info.cost_kernel
+        self.tuned = info.tuned
 
     @staticmethod
     def compute(images, gray, calibs, near, far, params: StereoParams, index=0, align=8, prev: Optional["DenseLayer"] = None,
@@ -737,6 +742,21 @@ class ServedResult:
     n_planes: int
     queue_ms: float
     run_ms: float
+
+
+SGM_FORM_NAMES = {1: "fused", 2: "split", 3: "wave"}
+
+
+def tuned_form(w, h, n_planes, tile) -> int:
+    """The fast aggregation form the autotuner chose for a layer shape (1 fused, 2 split, 3 wave), 0 if none yet."""
+    return int(L.load().lux_sgm_tuned_form(w, h, n_planes, tile))
+
+
+def set_tuned_form(w, h, n_planes, tile, form: int):
+    """Sets (1-3) or clears (0) the autotuner's choice for a layer shape."""
+    rc = L.load().lux_sgm_set_tuned_form(w, h, n_planes, tile, int(form))
+    if rc:
+        _raise(rc, "lux_sgm_set_tuned_form failed")
 
 
 def pool_high_water(device: int = 0, reset: bool = False) -> int:

@@ -7,7 +7,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -32,12 +34,31 @@ struct lux_sgm_ctx {
   uint64_t wait_limit_ns = kTimeoutNs;  // bound of every device-side wait of the aggregation kernels
   int stall_block = -1;                 // failure-path tests: the block whose cross-block wait can never be satisfied
   int* d_never = nullptr;               // the zero counter that block waits on (nothing writes it)
+  bool autotune = true;                 // untuned layer shapes time every fast form on their first solve
 };
 
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
 };
+
+// The autotuner's choices, per layer shape (W, H, planes, tile), shared by every context of the process: the fast
+// aggregation form (1 fused wavefront, 2 path-group chains, 3 lean wavefront) measured fastest on the first solve of
+// that shape.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tuned;
+int tuned_form(int W, int H, int n, int T) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tuned.find(std::make_tuple(W, H, n, T));
+  return it == g_tuned.end() ? 0 : it->second;
+}
+void set_tuned_form(int W, int H, int n, int T, int form) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (form) g_tuned[std::make_tuple(W, H, n, T)] = form;
+  else g_tuned.erase(std::make_tuple(W, H, n, T));
+}
+}  // namespace
 
 struct lux_layer {
   lux_sgm_ctx* ctx = nullptr;
@@ -46,6 +67,7 @@ struct lux_layer {
   float ms_cost = 0.f, ms_sgm = 0.f, ms_wta = 0.f;
   int sgm_kernel = 0;
   int cost_kernel = 0;
+  int tuned = 0;  // the form the autotuner chose on this solve (0: no tuning ran)
   bool agg_final = false;  // agg holds the final aggregates (always for the replay kernel, on request for the fast one)
   std::vector<float> planes_h;
   float* planes = nullptr;
@@ -353,21 +375,61 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   CK(cudaEventRecord(ctx->ev[1], s));
   const int xsw = 0;  // LUX_SGM_XSW unset: the reference default (DenseStereoSgm.cs:31)
   if (fast) {
-    void* scr = nullptr;
-    // the path-group chains win from about 2 MP (their critical path is W or H steps instead of 2H + W)
-    const int form = (flags & LUX_LAYER_SGM_WAVE) ? 3 : (flags & LUX_LAYER_SGM_SPLIT) ? 2 : (flags & LUX_LAYER_SGM_FUSED) ? 1
-                     : (size_t)W * H >= 2000000 ? 2 : 1;
-    const size_t sb = form == 2 ? split_scratch_bytes(W, H, L->n) : form == 3 ? wave_scratch_bytes(W, H, L->n)
-                                : uniform_scratch_bytes(W, H, L->n, p.tile);
-    if ((rc = dev_alloc(ctx, tmp, sb, &scr))) return rc;
+    const int forced = (flags & LUX_LAYER_SGM_WAVE) ? 3 : (flags & LUX_LAYER_SGM_SPLIT) ? 2 : (flags & LUX_LAYER_SGM_FUSED) ? 1 : 0;
+    int form = forced;
+    bool tune = false;
+    if (!forced) {
+      form = tuned_form(W, H, L->n, p.tile);
+      tune = form == 0 && ctx->autotune;
+      if (form == 0) form = (size_t)W * H >= 2000000 ? 2 : 1;  // untuned: the path-group chains from about 2 MP
+    }
     const int keep = (flags & LUX_LAYER_KEEP_AGG) ? 1 : 0;
-    if (form == 2)
-      rc = run_sgm_split(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
-    else if (form == 3)
-      rc = run_sgm_wave(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
-    else
-      rc = run_sgm_uniform(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
-    if (rc) return set_err(ctx, LUX_ERR_CUDA, "uniform aggregation launch failed (%d)", rc);
+    auto scratch_of = [&](int f) {
+      return f == 2 ? split_scratch_bytes(W, H, L->n) : f == 3 ? wave_scratch_bytes(W, H, L->n) : uniform_scratch_bytes(W, H, L->n, p.tile);
+    };
+    auto run_form = [&](int f, void* scr, size_t sb) {
+      if (f == 2) return run_sgm_split(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
+      if (f == 3) return run_sgm_wave(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
+      return run_sgm_uniform(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
+    };
+    if (tune) {
+      // The first solve of this shape times every form on the layer's own volume and keeps the fastest for later solves.
+      // Each form writes every aggregate and depth it produces and all forms give the same bits, so the layer keeps the
+      // last run's results. The reported aggregation time is the chosen form's.
+      static const int kForms[3] = {3, 2, 1};
+      size_t sb = 0;
+      for (int f : kForms) sb = std::max(sb, scratch_of(f));
+      void* scr = nullptr;
+      if ((rc = dev_alloc(ctx, tmp, sb, &scr))) return rc;
+      CK(cudaEventSynchronize(ctx->ev[1]));
+      CK(cudaEventElapsedTime(&L->ms_cost, ctx->ev[0], ctx->ev[1]));  // before the timing runs reuse the events
+      float best_ms = 0.f;
+      int best = 0;
+      for (int f : kForms) {
+        CK(cudaEventRecord(ctx->ev[1], s));
+        if ((rc = run_form(f, scr, sb))) return set_err(ctx, LUX_ERR_CUDA, "uniform aggregation launch failed (%d)", rc);
+        CK(cudaEventRecord(ctx->ev[2], s));
+        CK(cudaGetLastError());
+        if ((rc = take_device_error(ctx))) return rc;
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]));
+        if (best == 0 || ms < best_ms) {
+          best = f;
+          best_ms = ms;
+        }
+      }
+      set_tuned_form(W, H, L->n, p.tile, best);
+      L->sgm_kernel = kForms[2];  // the last run's results are in place
+      L->agg_final = keep != 0;
+      L->ms_sgm = best_ms;
+      L->ms_wta = 0.f;
+      L->tuned = best;
+      return LUX_OK;
+    }
+    void* scr = nullptr;
+    const size_t sb = scratch_of(form);
+    if ((rc = dev_alloc(ctx, tmp, sb, &scr))) return rc;
+    if ((rc = run_form(form, scr, sb))) return set_err(ctx, LUX_ERR_CUDA, "uniform aggregation launch failed (%d)", rc);
     CK(cudaEventRecord(ctx->ev[2], s));
     CK(cudaEventRecord(ctx->ev[3], s));
     L->sgm_kernel = form;
@@ -482,6 +544,21 @@ int lux_sgm_pool_high_water(int device, int32_t reset, uint64_t* bytes) {
     uint64_t zero = 0;
     if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero) != cudaSuccess) return LUX_ERR_CUDA;
   }
+  return LUX_OK;
+}
+
+int lux_sgm_set_autotune(lux_sgm_ctx* ctx, int32_t on) {
+  if (!ctx) return LUX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->autotune = on != 0;
+  return LUX_OK;
+}
+
+int32_t lux_sgm_tuned_form(int32_t w, int32_t h, int32_t n_planes, int32_t tile) { return tuned_form(w, h, n_planes, tile); }
+
+int lux_sgm_set_tuned_form(int32_t w, int32_t h, int32_t n_planes, int32_t tile, int32_t form) {
+  if (w <= 0 || h <= 0 || n_planes <= 0 || tile <= 0 || form < 0 || form > 3) return LUX_ERR_ARG;
+  set_tuned_form(w, h, n_planes, tile, form);
   return LUX_OK;
 }
 
@@ -721,6 +798,7 @@ int lux_layer_get_info(const lux_layer* L, lux_layer_info* info) {
   info->gpu_ms_cost = L->ms_cost; info->gpu_ms_sgm = L->ms_sgm; info->gpu_ms_wta = L->ms_wta;
   info->sgm_kernel = L->sgm_kernel;
   info->cost_kernel = L->cost_kernel;
+  info->tuned = L->tuned;
   return LUX_OK;
 }
 
