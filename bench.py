@@ -335,6 +335,8 @@ def run_lux(a):
         # ten-pair comparator (inputs on the device; wall clock for the stream, CUDA events for the capture)
         out["served"] = serve_stream(a)
         out["capture"] = capture_batched_vs_plain(a)
+        # the reference's whole dense job of a capture (six-layer pyramid + upsample) beside its CPU port
+        out["pyramid"] = pyramid_job(a, 2080, 1560, steps=5, warmup=3, cpu=not a.no_cpu_baseline)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, dt, de_s = cpu_sample(wl, a.cpu_rows, threads)
@@ -897,16 +899,14 @@ def run_census_capture(a):
     ctx.close()
 
 
-def run_pyramid(a):
-    """DenseStereoPyramid.Run (DenseStereoSgm.cs:331-353) on a capture's reference group — five 2080x1560 colour cameras
-    (the finest layer is 2080x1560, as in StereoAsyncApi.State4And5) — then DenseUpsampleLayer.Run to 4160x3120 with a
-    guide: the reference's whole dense job for one capture. Images on the device; value = captures per second; the
-    per-layer device times (cost, aggregation, WTA) and kernels are reported."""
+def pyramid_job(a, w, h, steps, warmup, cpu=True):
+    """DenseStereoPyramid.Run (DenseStereoSgm.cs:331-353) on a capture's reference group — five colour cameras of w x h
+    (2080x1560: the finest layer is 2080x1560, as in StereoAsyncApi.State4And5) — then DenseUpsampleLayer.Run to 2w x 2h
+    with a guide: the reference's whole dense job for one capture. Images on the device; ms per capture on the library's
+    stream, per-layer device times and kernels; cpu: the oracle's pyramid on the host cores (cost prepass on every core,
+    serial aggregation as the reference) on the same capture, as the job's CPU baseline."""
     import torch
     from lux_b200 import api, synth
-    if int(os.environ.get("RANK", "0")) != 0:
-        return
-    w, h = (int(v) for v in a.pyramid_size.split("x"))
     cap = synth.capture(w, h, 5, seed=3)
     torch.cuda.set_device(0)
     ctx = api.Context(0)
@@ -914,6 +914,7 @@ def run_pyramid(a):
     stream = torch.cuda.ExternalStream(lib.lux_sgm_stream(ctx.handle), device=torch.device("cuda", 0))
     d_imgs = [torch.from_numpy(im).cuda() for im in cap.images]
     guide = torch.from_numpy(np.random.default_rng(4).integers(0, 256, (2 * h, 2 * w, 4), dtype=np.uint8)).cuda()
+    out = torch.empty((2 * h, 2 * w), dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
     info = []
 
@@ -922,38 +923,59 @@ def run_pyramid(a):
         top = layers[-1]
         info[:] = [(L.W, L.H, L.n_planes, L.sgm_kernel, L.cost_kernel, L.gpu_ms_cost, L.gpu_ms_sgm, L.gpu_ms_wta, L.volume / (L.W * L.H))
                    for L in layers]
-        depth_ptr = top.device_ptr(0)
-        out = torch.empty((2 * h, 2 * w), dtype=torch.float32, device="cuda")
         gi = api.L.Img(guide.data_ptr(), 2 * w, 2 * h, 2 * w, 1)
-        ctx.check(lib.lux_sgm_upsample(ctx.handle, depth_ptr, top.W, top.H, 1, ctypes.byref(gi), w, h, 12.0, 2, None,
+        ctx.check(lib.lux_sgm_upsample(ctx.handle, top.device_ptr(0), top.W, top.H, 1, ctypes.byref(gi), w, h, 12.0, 2, None,
                                        out.data_ptr(), None))
         for L in layers:
             L.close()
 
-    for _ in range(a.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     n0 = api.kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(0) as clk:
         e0.record(stream)
-        for _ in range(a.steps):
+        for _ in range(steps):
             step()
         e1.record(stream)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / a.steps
-    de = sum(W * H * n for (W, H, n, *_) in info)
-    print(json.dumps({"metric": f"capture dense jobs/s (DenseStereoPyramid.Run + upsample), 5 cameras {w}x{h}", "value": 1e3 / ms,
-                      "unit": "captures/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
-                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 cost / u16 aggregation",
-                      "data": "synthetic (colour capture, planar scene 0.4-6 m, 8-40 mm baselines)",
-                      "config": {"workload": f"L16 pyramid on 5 colour cameras {w}x{h} + upsample to {2 * w}x{2 * h}",
-                                 "layers": [{"w": W, "h": H, "planes": n, "mean_cap": round(mc, 1), "sgm_kernel": sk, "cost_kernel": ck,
-                                             "ms_cost": round(c, 3), "ms_sgm": round(g, 3), "ms_wta": round(t, 3)}
-                                            for (W, H, n, sk, ck, c, g, t, mc) in info],
-                                 "mde_per_s": de / (ms / 1e3) / 1e6},
-                      "gpu_launches": int(api.kernel_launches() - n0), "clocks": clk.summary()}))
+    ms = e0.elapsed_time(e1) / steps
+    launches = api.kernel_launches() - n0
     ctx.close()
+    de = sum(W * H * n for (W, H, n, *_) in info)
+    res = {"workload": f"L16 pyramid on 5 colour cameras {w}x{h} + upsample to {2 * w}x{2 * h}", "ms_per_capture": ms,
+           "captures_per_s": 1e3 / ms, "mde_per_s": de / (ms / 1e3) / 1e6, "gpu_launches": int(launches),
+           "clocks": clk.summary(),
+           "layers": [{"w": W, "h": H, "planes": n, "mean_cap": round(mc, 1), "sgm_kernel": sk, "cost_kernel": ck,
+                       "ms_cost": round(c, 3), "ms_sgm": round(g, 3), "ms_wta": round(t, 3)}
+                      for (W, H, n, sk, ck, c, g, t, mc) in info]}
+    if cpu:
+        from oracle import oracle as O
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        O.pyramid(cap.images, cap.gray, cap.calibs, cap.near, cap.far, threads=threads)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": 1.0 / dt, "unit": "captures/s", "cores": threads, "kind": "port",
+                               "sample": f"the same capture's DenseStereoPyramid.Run ({dt:.1f} s): oracle port, cost prepass on "
+                                         f"{threads} threads, serial aggregation as the reference (the upsample not included)"}
+    return res
+
+
+def run_pyramid(a):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    w, h = (int(v) for v in a.pyramid_size.split("x"))
+    r = pyramid_job(a, w, h, a.steps, a.warmup, cpu=not a.no_cpu_baseline)
+    line = {"metric": f"capture dense jobs/s (DenseStereoPyramid.Run + upsample), 5 cameras {w}x{h}", "value": r["captures_per_s"],
+            "unit": "captures/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": r["ms_per_capture"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 cost / u16 aggregation",
+            "data": "synthetic (colour capture, planar scene 0.4-6 m, 8-40 mm baselines)",
+            "config": {"workload": r["workload"], "layers": r["layers"], "mde_per_s": r["mde_per_s"]},
+            "gpu_launches": r["gpu_launches"], "clocks": r["clocks"]}
+    if "cpu_baseline" in r:
+        line["cpu_baseline"] = r["cpu_baseline"]
+    print(json.dumps(line))
 
 
 def main():

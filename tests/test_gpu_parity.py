@@ -308,3 +308,17 @@ def test_image_from_grey16(ctx, bits, w, h, stride):
     out = api.image_from_grey16(dev, bits, ctx=ctx)
     ctx.check(ctx.lib.lux_sgm_sync(ctx.handle))
     assert np.array_equal(out.cpu().numpy(), want)
+
+
+def test_pyramid_index_error_parity(ctx, oracle):
+    """A capture whose finest layer makes the reference write past the end of its line buffer (a last-column pixel of
+    the second half whose range spills beyond the buffer, DenseStereoSgm.cs:300-313, an IndexOutOfRangeException in the
+    C#): the oracle and the GPU pyramid both report LUX_ERR_INDEX."""
+    from lux_b200 import api, synth
+    cap = synth.capture(520, 390, 5, seed=3)
+    with pytest.raises(oracle.OracleError) as eo:
+        oracle.pyramid(cap.images, cap.gray, cap.calibs, cap.near, cap.far, threads=4)
+    assert eo.value.code == 7
+    with pytest.raises(api.LuxIndexError):
+        for g in api.DenseStereoPyramid.run(cap.images, cap.gray, cap.calibs, cap.near, cap.far, ctx=ctx):
+            g.close()
