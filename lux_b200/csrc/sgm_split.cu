@@ -33,8 +33,7 @@ namespace {
 constexpr int kMaxChainWarps = 15;     // chain warps per block at most (two chains each), sized to the register file
 constexpr int kMaxWarpsS = kMaxChainWarps + 2;  // plus the loader and the publisher
 constexpr int kRingS = 8;              // slots of a chain's hand-over ring
-constexpr int kPublishS = 8;           // global progress released every kPublishS steps
-constexpr int kStage = 4;              // steps of HBM input staged ahead per chain
+constexpr int kStageS = 6;             // steps of raw costs and aggregates staged ahead per chain warp (cp.async)
 
 struct SplitArgs {
   UniArgs u;              // layer, pass and revisit-schedule fields shared with the fused kernel
@@ -133,6 +132,107 @@ LUX_DEV void chain_above(const SplitArgs& a, const uint16_t* bnd_up, const uint1
   }
 }
 
+// Vector loads and stores of a lane's planes in shared memory (16, 8 or 4 bytes).
+template <int LPT>
+LUX_DEV void sload(V<LPT>& v, const uint16_t* base, int lane) {
+  if constexpr (LPT == 8) {
+    const uint4 t = reinterpret_cast<const uint4*>(base)[lane];
+    v.r[0] = t.x; v.r[1] = t.y; v.r[2] = t.z; v.r[3] = t.w;
+  } else if constexpr (LPT == 4) {
+    const uint2 t = reinterpret_cast<const uint2*>(base)[lane];
+    v.r[0] = t.x; v.r[1] = t.y;
+  } else {
+    v.r[0] = reinterpret_cast<const uint32_t*>(base)[lane];
+  }
+}
+template <int LPT>
+LUX_DEV void sstore(const V<LPT>& v, uint16_t* base, int lane) {
+  if constexpr (LPT == 8) reinterpret_cast<uint4*>(base)[lane] = make_uint4(v.r[0], v.r[1], v.r[2], v.r[3]);
+  else if constexpr (LPT == 4) reinterpret_cast<uint2*>(base)[lane] = make_uint2(v.r[0], v.r[1]);
+  else reinterpret_cast<uint32_t*>(base)[lane] = v.r[0];
+}
+
+// The hand-over between blocks: the block's last chain writes each step's L vector and minimum into its band buffer with
+// bit 15 of every u16 set (L and its minimum stay below 2001, so the bit is free), and the next block's loader polls the
+// entries themselves until every u16 of the step carries the bit. The buffer is cleared before each launch and each entry
+// is written once per launch, so a set bit can only mean this launch's value; no fence or progress counter sits between
+// the two blocks. Relaxed GPU-scope accesses of a lane's planes (16, 8 or 4 bytes) and of one u16.
+constexpr uint32_t kMark2 = 0x80008000u;
+template <int LPT>
+LUX_DEV void st_marked(uint16_t* p, const V<LPT>& v, int lane) {
+  uint32_t* q = reinterpret_cast<uint32_t*>(p + lane * LPT);
+  if constexpr (LPT == 8)
+    asm volatile("st.relaxed.gpu.global.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(q), "r"(v.r[0] | kMark2), "r"(v.r[1] | kMark2),
+                 "r"(v.r[2] | kMark2), "r"(v.r[3] | kMark2) : "memory");
+  else if constexpr (LPT == 4)
+    asm volatile("st.relaxed.gpu.global.v2.u32 [%0], {%1, %2};" ::"l"(q), "r"(v.r[0] | kMark2), "r"(v.r[1] | kMark2) : "memory");
+  else
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(q), "r"(v.r[0] | kMark2) : "memory");
+}
+// Loads a marked entry; returns whether every u16 of it carries the mark, and the values without it.
+template <int LPT>
+LUX_DEV bool ld_marked(const uint16_t* p, V<LPT>& v, int lane) {
+  const uint32_t* q = reinterpret_cast<const uint32_t*>(p + lane * LPT);
+  if constexpr (LPT == 8)
+    asm volatile("ld.relaxed.gpu.global.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.r[0]), "=r"(v.r[1]), "=r"(v.r[2]), "=r"(v.r[3]) : "l"(q) : "memory");
+  else if constexpr (LPT == 4)
+    asm volatile("ld.relaxed.gpu.global.v2.u32 {%0, %1}, [%2];" : "=r"(v.r[0]), "=r"(v.r[1]) : "l"(q) : "memory");
+  else
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v.r[0]) : "l"(q) : "memory");
+  uint32_t all = kMark2;
+#pragma unroll
+  for (int i = 0; i < LPT / 2; i++) {
+    all &= v.r[i];
+    v.r[i] &= ~kMark2;
+  }
+  return all == kMark2;
+}
+LUX_DEV void st_marked16(uint16_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u16 [%0], %1;" ::"l"(p), "h"((unsigned short)(v | 0x8000u)) : "memory");
+}
+LUX_DEV bool ld_marked16(const uint16_t* p, uint32_t& v) {
+  unsigned short t;
+  asm volatile("ld.relaxed.gpu.global.u16 %0, [%1];" : "=h"(t) : "l"(p) : "memory");
+  v = t & 0x7fffu;
+  return (t & 0x8000u) != 0;
+}
+
+// One path step of a lane's planes (DenseStereoSgm.cs:276-313) with the neighbour's minimum carried in both u16 halves:
+// the d-1 / d+1 words come from one byte permute per pair (the pair of planes 2i+1, 2i+2 is the d+1 word of pair i and
+// the d-1 word of pair i+1). p2d: this path's P2 in both halves. Returns the new L and its warp minimum (both halves).
+template <int LPT, bool FULL>
+LUX_DEV void lean_path(const V<LPT>& nb, uint32_t md, uint32_t p2d, uint32_t p1x2, const V<LPT>& raw2, bool active, int lane,
+                       V<LPT>& out, uint32_t& mdo) {
+  constexpr int NR = LPT / 2;
+  uint32_t prev = __shfl_up_sync(0xffffffffu, nb.r[NR - 1], 1);
+  uint32_t next = __shfl_down_sync(0xffffffffu, nb.r[0], 1);
+  if (lane == 0) prev = kInit2;   // plane -1: 2000
+  if (lane == 31) next = kInit2;  // plane n (or a padding lane): 2000
+  const uint32_t p2x = p2d + md;  // P2 + minPrev <= 3744 in each half: no carry between the halves
+  uint32_t u[NR + 1];
+  u[0] = pair_of(prev, nb.r[0]);
+#pragma unroll
+  for (int i = 0; i + 1 < NR; i++) u[i + 1] = pair_of(nb.r[i], nb.r[i + 1]);
+  u[NR] = pair_of(nb.r[NR - 1], next);
+  uint32_t m = 0xffffffffu;
+#pragma unroll
+  for (int i = 0; i < NR; i++) {
+    uint32_t t = vmin2(u[i], u[i + 1]) + p1x2;  // min(L[d-1], L[d+1]) + P1
+    t = vmin2(vmin2(t, nb.r[i]), p2x);          // with L[d] and P2 + minPrev
+    uint32_t lc = t + raw2.r[i] - md;            // raw + m - minPrev, each half in [0, 2000)
+    if (!FULL) lc = active ? lc : kInit2;        // padding lanes keep 2000
+    out.r[i] = lc;
+    m = vmin2(m, lc);
+  }
+  m = vmin2(m, __byte_perm(m, 0, 0x1032));
+  mdo = __reduce_min_sync(0xffffffffu, m);
+}
+
+// The path groups of one pass. Chains of the block: two per chain warp (A from the warp above through the ring, B from
+// A's previous step in registers); warp nw is the loader (chain j0-1 from the block above's band buffer into ring nw),
+// warp nw+1 the publisher (the block's last chain out to its band buffer). A step's raw costs, aggregates and P2 are read
+// straight from HBM two steps ahead into registers; the ring hands over one L vector and its minimum (both halves) per
+// step through shared memory, ordered by full / empty mbarriers.
 template <int LPT, bool FULL, bool PASS2, int GROUP>
 __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a) {
   constexpr int NR = LPT / 2, Dp = Dp_of(LPT), kBatch = 4;
@@ -140,12 +240,13 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
   const int nw = (int)(blockDim.x >> 5) - 2;  // chain warps of this launch (two chains each)
   extern __shared__ __align__(16) uint16_t smem_chain[];
   auto ring = [&](int set, int slot) { return smem_chain + ((size_t)set * kRingS + slot) * Dp; };
-  uint16_t* ring_min = smem_chain + (size_t)(kMaxChainWarps + 1) * kRingS * Dp;
-  auto rmin_at = [&](int set, int slot) -> uint16_t& { return ring_min[set * kRingS + slot]; };
-  uint64_t* bars = reinterpret_cast<uint64_t*>(ring_min + (size_t)(kMaxChainWarps + 1) * kRingS + 8);
+  uint32_t* ring_md = reinterpret_cast<uint32_t*>(smem_chain + (size_t)(kMaxChainWarps + 1) * kRingS * Dp);
+  auto rmd = [&](int set, int slot) -> uint32_t& { return ring_md[set * kRingS + slot]; };
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring_md + (kMaxChainWarps + 1) * kRingS);
   auto full = [&](int set, int slot) { return bars + set * kRingS + slot; };
   auto empty = [&](int set, int slot) { return bars + (kMaxChainWarps + 1) * kRingS + set * kRingS + slot; };
-  uint8_t* stage_base = reinterpret_cast<uint8_t*>(bars + 2 * (kMaxChainWarps + 1) * kRingS);  // 16-B aligned
+  // staging: per chain warp kStageS slots of [chain][agg 2n B (when read), raw n B]
+  uint8_t* stage_base = reinterpret_cast<uint8_t*>(bars + 2 * (kMaxChainWarps + 1) * kRingS);
   __shared__ int s_cb;
   __shared__ volatile int s_stop;
   __shared__ float s_planes[256];  // the WTA's plane depths (group B of pass -1)
@@ -178,33 +279,50 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
     // ---------------- loader: chain j0-1 into ring nw ----------------
     // (group B's first block has none: its chain 0 is column c, whose path-3 neighbour is the margin)
     if (j0 < a.nchains && !(GROUP == 1 && cb == 0)) {
-      int avail = cb > 0 ? 0 : a.nsteps;
+      const bool stalled = cb == u.stall_block;  // failure-path tests: this block's upstream entries never count as written
+      const uint64_t t0 = global_ns();
       for (int sb = 0; sb < a.nsteps && !s_stop; sb += kBatch) {
         const int se = min(a.nsteps, sb + kBatch);
         bool ok = true;
         for (int s = sb; s < se && ok; s++) ok = wait_free(nw, s);
         if (!ok) break;
-        if (avail < se) {
-          int v = 0;
-          if (lane == 0) v = wait_at_least_value(cb == u.stall_block ? u.never : u.progress + (cb - 1), se, u.err, 11, u.timeout_ns);
-          v = __shfl_sync(0xffffffffu, v, 0);
-          __syncwarp();
-          if (v < 0) {
-            s_stop = 1;
-            break;
-          }
-          avail = v;
-        }
         Src<LPT> st[kBatch];
+        if (cb > 0) {
+          // poll the band buffer entries of steps sb..se-1 of the block above until all of them are written
+          for (unsigned it = 0;; it++) {
+            bool ready = !stalled;
 #pragma unroll
-        for (int k = 0; k < kBatch; k++)
-          if (sb + k < se) chain_above<LPT, PASS2>(a, bnd_up, bnd_up_min, cb, sb + k, st[k], lane);
+            for (int k = 0; k < kBatch; k++) {
+              if (sb + k >= se) break;
+              ready &= ld_marked<LPT>(bnd_up + (size_t)(sb + k) * Dp, st[k].L, lane);
+              uint32_t mn = 0;
+              const bool mk = ld_marked16(bnd_up_min + sb + k, mn);
+              st[k].mn = mn;
+              ready &= mk;
+            }
+            if (__all_sync(0xffffffffu, ready)) break;
+            __nanosleep(64);
+            if ((it & 15) == 15 && (s_stop || *(volatile int*)u.err != 0 || global_ns() - t0 > u.timeout_ns)) {
+              if (lane == 0) {
+                atomicCAS(u.err, 0, 11);
+                s_stop = 1;
+              }
+              ok = false;
+              break;
+            }
+          }
+          if (!ok) break;
+        } else {
+#pragma unroll
+          for (int k = 0; k < kBatch; k++)
+            if (sb + k < se) chain_above<LPT, PASS2>(a, bnd_up, bnd_up_min, cb, sb + k, st[k], lane);
+        }
 #pragma unroll
         for (int k = 0; k < kBatch; k++) {
           if (sb + k >= se) break;
           const int sl = (sb + k) & (kRingS - 1);
-          vstore_s<LPT>(st[k].L, ring(nw, sl), lane);
-          if (lane == 0) rmin_at(nw, sl) = (uint16_t)st[k].mn;
+          sstore<LPT>(st[k].L, ring(nw, sl), lane);
+          if (lane == 0) rmd(nw, sl) = dup16(st[k].mn);
         }
         __syncwarp();
         if (lane == 0)
@@ -220,16 +338,13 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
         if (!wait_filled(nw - 1, s)) break;
         const int sl = s & (kRingS - 1);
         V<LPT> v;
-        vload_s<LPT>(v, ring(nw - 1, sl), lane);
-        vstore<LPT>(v, bnd_me + (size_t)s * Dp, lane);
-        if (lane == 0) __stcg(bnd_me_min + s, rmin_at(nw - 1, sl));
+        sload<LPT>(v, ring(nw - 1, sl), lane);
+        st_marked<LPT>(bnd_me + (size_t)s * Dp, v, lane);
+        if (lane == 0) st_marked16(bnd_me_min + s, rmd(nw - 1, sl) & 0xffffu);
         __syncwarp();
         if (lane == 0) mbar_arrive(empty(nw - 1, sl));
-        if ((s + 1) % kPublishS == 0) st_release(u.progress + cb, s + 1);
       }
     }
-    __syncwarp();
-    if (lane == 0) st_release(u.progress + cb, a.nsteps);
     return;
   }
 
@@ -243,84 +358,79 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
   const int c = u.W - 1;
   const bool colc = GROUP == 1 && jA == 0;  // the last column: revisits, the special path-2 read
   const uint32_t p1x2 = dup16((uint32_t)u.p1);
-  // memory step between consecutive steps of a chain (pixels), and the P2 table step
-  const long long dpix = GROUP == 0 ? (PASS2 ? -1 : 1) : (PASS2 ? -(long long)u.W : (long long)u.W);
-  const long long dp2 = GROUP == 0 ? 1 : u.W;
-  struct Chain {
-    long long pix0;     // memory index of the chain's first pixel
-    const uint2* p2p0;  // its P2 table entry
-    Src<LPT> own;       // the chain's own-path state (path 0 / 2) after the previous step
-  };
-  Chain ch[2];
+  const int n = u.n;
+  // consecutive steps of a chain are dpix pixels apart in memory, its P2 table entries dp2 apart
+  const int dpix = GROUP == 0 ? (PASS2 ? -1 : 1) : (PASS2 ? -u.W : u.W);
+  const int dp2 = GROUP == 0 ? 1 : u.W;
+  constexpr bool kReadAgg = PASS2 || GROUP == 1;  // A of pass +1 is the first writer
+  // per chain: memory pixel index and P2 index of the current step, own-path state (path 0 / 2) and its minimum
+  int pix[2], p2i[2];
+  V<LPT> oL[2];
+  uint32_t om[2];
   const int jj[2] = {jA, jB};
 #pragma unroll
   for (int k = 0; k < 2; k++) {
     const int xm0 = GROUP == 0 ? 0 : u.W - 1 - jj[k], ym0 = GROUP == 0 ? jj[k] : 0;
-    ch[k].pix0 = (long long)pixel_index(u, xm0, ym0, PASS2);
-    ch[k].p2p0 = u.p2t + (size_t)ym0 * u.W + xm0;
-    if (GROUP == 1 && PASS2) src_edge<LPT>(u, ch[k].own, u.W - 1 - xm0, 2, lane);  // row -1 of pass -1: path 2 of row y_b
-    else src_init(ch[k].own);
+    pix[k] = (int)pixel_index(u, xm0, ym0, PASS2);
+    p2i[k] = ym0 * u.W + xm0;
+    Src<LPT> s0;
+    if (GROUP == 1 && PASS2) src_edge<LPT>(u, s0, u.W - 1 - xm0, 2, lane);  // row -1 of pass -1: path 2 of row y_b
+    else src_init(s0);
+    oL[k] = s0.L;
+    om[k] = dup16(s0.mn);
   }
-  // HBM inputs of a step, staged kStage steps ahead by cp.async: per chain and slot [agg 2n B][raw n B][P2 8 B] (agg only
-  // where it is read). The first n/8 lanes copy 16 B of aggregates and 8 B of raw costs each, lane 0 the P2 word.
-  constexpr bool kReadAgg = PASS2 || GROUP == 1;  // A of pass +1 is the first writer
-  const int n = u.n, gran = n >> 3;
-  const int raw_off = kReadAgg ? 2 * n : 0, p2_off = raw_off + n;
-  const int sbytes = (p2_off + 8 + 15) & ~15;
-  uint8_t* stage = stage_base + (size_t)(2 * w) * kStage * sbytes;
-  auto stage_at = [&](int k, int s) { return stage + ((size_t)k * kStage + (s % kStage)) * sbytes; };
-  auto issue = [&](int s) {
-    if (s < a.nsteps) {
-#pragma unroll
-      for (int k = 0; k < 2; k++) {
-        uint8_t* d = stage_at(k, s);
-        const long long pix = ch[k].pix0 + dpix * s;
-        if (lane < gran) {
-          if constexpr (kReadAgg) cp_async16(d + lane * 16, reinterpret_cast<const uint8_t*>(u.agg + pix * n) + lane * 16);
-          cp_async8(d + raw_off + lane * 8, u.raw + pix * n + lane * 8);
-        }
-        if (lane == 0) cp_async8(d + p2_off, ch[k].p2p0 + dp2 * s);
-      }
-    }
-    cp_async_commit();  // one group per step, empty past the end
-  };
-  struct Queued {
+  const uint32_t* p2w = reinterpret_cast<const uint32_t*>(u.p2t) + (GROUP == 0 ? 0 : 1);  // the P2 word of this group's paths
+  struct In {
     RawB<LPT> raw;
     V<LPT> agg;
     uint32_t p2;
   };
-  auto staged = [&](int k, int s, Queued& q) {  // after the step's group completed and a __syncwarp
-    const uint8_t* d = stage_at(k, s);
+  // Raw costs and aggregates are staged kStageS steps ahead by cp.async into this warp's slots: per step and chain
+  // [agg 2n B (when read)][raw n B]; lane j < n/8 copies planes 8j..8j+7 (16 B of aggregates, 8 B of raw costs), and
+  // each lane then reads its own LPT planes. One commit group per step (empty past the chain's end).
+  const int cbytes = ((kReadAgg ? 2 * n : 0) + n + 15) & ~15;  // one chain's bytes of a step, in 16-byte units
+  const int gran = n >> 3;
+  uint8_t* stage = stage_base + (size_t)w * kStageS * 2 * cbytes;
+  auto stage_at = [&](int slot, int k) { return stage + ((size_t)slot * 2 + k) * cbytes; };
+  auto issue = [&](int s) {
+    if (s < a.nsteps && lane < gran) {
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        if (k == 1 && !hasB) break;
+        const long long pi = (long long)pix[k] + (long long)dpix * s;
+        uint8_t* d = stage_at(s % kStageS, k);
+        if constexpr (kReadAgg) cp_async16(d + lane * 16, reinterpret_cast<const uint8_t*>(u.agg + pi * n) + lane * 16);
+        cp_async8(d + (kReadAgg ? 2 * n : 0) + lane * 8, u.raw + pi * n + lane * 8);
+      }
+    }
+    cp_async_commit();
+  };
+  auto staged = [&](int k, int s, In& q) {  // chain k's inputs of step s from its slot (after the step's group completed)
+    const uint8_t* d = stage_at(s % kStageS, hasB ? k : 0);
     if (!active) {
       q.raw.r[0] = 0;
       if constexpr (LPT >= 8) q.raw.r[1] = 0;
 #pragma unroll
       for (int i = 0; i < NR; i++) q.agg.r[i] = 0;
-    } else {
-      if constexpr (LPT == 8) {
-        const uint2 t = *reinterpret_cast<const uint2*>(d + raw_off + lane * 8);
-        q.raw.r[0] = t.x;
-        q.raw.r[1] = t.y;
-      } else if constexpr (LPT == 4) {
-        q.raw.r[0] = *reinterpret_cast<const uint32_t*>(d + raw_off + lane * 4);
-      } else {
-        q.raw.r[0] = *reinterpret_cast<const uint16_t*>(d + raw_off + lane * 2);
-      }
-      if constexpr (kReadAgg) {
-        if constexpr (LPT == 8) {
-          const uint4 t = *reinterpret_cast<const uint4*>(d + lane * 16);
-          q.agg.r[0] = t.x; q.agg.r[1] = t.y; q.agg.r[2] = t.z; q.agg.r[3] = t.w;
-        } else if constexpr (LPT == 4) {
-          const uint2 t = *reinterpret_cast<const uint2*>(d + lane * 8);
-          q.agg.r[0] = t.x; q.agg.r[1] = t.y;
-        } else {
-          q.agg.r[0] = *reinterpret_cast<const uint32_t*>(d + lane * 4);
-        }
-      }
+      return;
     }
-    const uint2 pp = *reinterpret_cast<const uint2*>(d + p2_off);
-    q.p2 = GROUP == 0 ? pp.x : pp.y;
+    const uint8_t* r = d + (kReadAgg ? 2 * n : 0) + lane * LPT;
+    if constexpr (LPT == 8) {
+      const uint2 t = *reinterpret_cast<const uint2*>(r);
+      q.raw.r[0] = t.x;
+      q.raw.r[1] = t.y;
+    } else if constexpr (LPT == 4) {
+      q.raw.r[0] = *reinterpret_cast<const uint32_t*>(r);
+    } else {
+      q.raw.r[0] = *reinterpret_cast<const uint16_t*>(r);
+    }
+    if constexpr (kReadAgg) {
+      V<LPT> v;
+      sload<LPT>(v, reinterpret_cast<const uint16_t*>(d), lane);
+      q.agg = v;
+    }
   };
+  auto fetch = [&](int k, int s, In& q) { q.p2 = __ldg(p2w + 2 * (long long)(p2i[k] + dp2 * s)); };  // step s's P2 word
   // revisit R(c, y) of paths 2 and 3 (column c only): adds them to agg(c, y), keeps R.p2 for later revisits
   auto revisit23 = [&](int y) {
     Src<LPT> s2[1], s3[1];
@@ -348,8 +458,10 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
     }
     __syncwarp();
   };
-  Src<LPT> prevAb;  // chain A's neighbour-path output of the previous step: chain B's neighbour
-  auto step = [&](int s) -> bool {
+  V<LPT> pbL;  // chain A's neighbour-path output of the previous step: chain B's neighbour
+  uint32_t pbm = kInit2;
+  vinit(pbL);
+  auto step = [&](int s, In (&q)[2]) -> bool {
     // ---- hand-over in: the warp above finished step s-1; the warp below is done with the slot this step reuses ----
     const bool nb_ring = s > 0 && !colc;
     if (nb_ring && !wait_filled(up_set, s - 1)) return false;
@@ -360,42 +472,62 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
     if (colc) {  // revisits that the reference runs before N(c, y), and the special path-2 read
       const int cnt = u.batch_count[ym[0]], fr = u.batch_first[ym[0]];
       for (int k = 0; k < cnt; k++) revisit23(fr + k);
-      if (u.flags[ym[0]] & 1) src_cs<LPT>(u, ch[0].own, ym[0] - 1, 4, c, lane);
+      if (u.flags[ym[0]] & 1) {
+        Src<LPT> r;
+        src_cs<LPT>(u, r, ym[0] - 1, 4, c, lane);
+        oL[0] = r.L;
+        om[0] = dup16(r.mn);
+      }
     }
-    Src<LPT> own[2] = {ch[0].own, ch[1].own}, nb[2];
+    V<LPT> nbL[2];
+    uint32_t nbm[2];
     if (nb_ring) {
       const int sl = (s - 1) & (kRingS - 1);
-      vload_s<LPT>(nb[0].L, ring(up_set, sl), lane);
-      nb[0].mn = rmin_at(up_set, sl);
+      sload<LPT>(nbL[0], ring(up_set, sl), lane);
+      nbm[0] = rmd(up_set, sl);
     } else if (GROUP == 1 && PASS2 && !colc) {  // row -1 of pass -1: path 3 of pass +1's row y_b at x+1
-      src_edge<LPT>(u, nb[0], u.W - 1 - (xm[0] + 1), 3, lane);
+      Src<LPT> e;
+      src_edge<LPT>(u, e, u.W - 1 - (xm[0] + 1), 3, lane);
+      nbL[0] = e.L;
+      nbm[0] = dup16(e.mn);
     } else {
-      src_init(nb[0]);
+      vinit(nbL[0]);
+      nbm[0] = kInit2;
     }
-    if (s > 0) nb[1] = prevAb;
-    else if (GROUP == 1 && PASS2) src_edge<LPT>(u, nb[1], u.W - 1 - (xm[1] + 1), 3, lane);
-    else src_init(nb[1]);
-    Queued qa, qb;
-    staged(0, s, qa);
-    staged(1, s, qb);
-    const uint32_t p2o[2] = {qa.p2 & 0xffffu, qb.p2 & 0xffffu}, p2b[2] = {qa.p2 >> 16, qb.p2 >> 16};
-    V<LPT> raw2[2], acc[2], oo[2], ob[2];
-    raw_unpack<LPT>(qa.raw, raw2[0]);
-    raw_unpack<LPT>(qb.raw, raw2[1]);
-    if constexpr (kReadAgg) {
-      acc[0] = qa.agg;
-      acc[1] = qb.agg;
+    if (s > 0) {
+      nbL[1] = pbL;
+      nbm[1] = pbm;
+    } else if (GROUP == 1 && PASS2) {
+      Src<LPT> e;
+      src_edge<LPT>(u, e, u.W - 1 - (xm[1] + 1), 3, lane);
+      nbL[1] = e.L;
+      nbm[1] = dup16(e.mn);
     } else {
-#pragma unroll
-      for (int i = 0; i < NR; i++) acc[0].r[i] = acc[1].r[i] = 0;
+      vinit(nbL[1]);
+      nbm[1] = kInit2;
     }
+    cp_async_wait<kStageS - 1>();  // this lane's copies of step s have landed
+    __syncwarp();                  // and every lane's
+    staged(0, s, q[0]);
+    staged(1, s, q[1]);
+    __syncwarp();  // every lane has read the slot before it is refilled
+    issue(s + kStageS);
+    V<LPT> oo[2], ob[2], acc[2];
     uint32_t mo[2], mb[2];
-    chain_paths<LPT, FULL, 2>(own, p2o, nb, p2b, p1x2, raw2, active, lane, oo, ob, acc, mo, mb);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      V<LPT> raw2;
+      raw_unpack<LPT>(q[k].raw, raw2);
+      lean_path<LPT, FULL>(oL[k], om[k], dup16(q[k].p2 & 0xffffu), p1x2, raw2, active, lane, oo[k], mo[k]);
+      lean_path<LPT, FULL>(nbL[k], nbm[k], __byte_perm(q[k].p2, 0, 0x3232), p1x2, raw2, active, lane, ob[k], mb[k]);
+#pragma unroll
+      for (int i = 0; i < NR; i++) acc[k].r[i] = (kReadAgg ? q[k].agg.r[i] : 0u) + oo[k].r[i] + ob[k].r[i];
+    }
     // ---- hand-over out: chain B's neighbour-path state for the warp below ----
     const int sl = s & (kRingS - 1);
     if (has_consumer) {
-      vstore_s<LPT>(ob[1], ring(w, sl), lane);
-      if (lane == 0) rmin_at(w, sl) = (uint16_t)mb[1];
+      sstore<LPT>(ob[1], ring(w, sl), lane);
+      if (lane == 0) rmd(w, sl) = mb[1];
     }
     __syncwarp();
     if (lane == 0) {
@@ -406,8 +538,8 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
 #pragma unroll
     for (int k = 0; k < 2; k++) {
       if (k == 1 && !hasB) break;
-      const size_t pi = pixel_index(u, xm[k], ym[k], PASS2);
-      uint16_t* ap = u.agg + pi * u.n + lane * LPT;
+      const size_t pi = (size_t)(pix[k] + dpix * s);
+      uint16_t* ap = u.agg + pi * n + lane * LPT;
       if (GROUP == 1 && PASS2 && !(k == 0 && colc)) {
         if (u.keep_agg) agg_store<LPT>(ap, acc[k], active);
         const int arg = wta_arg<LPT>(acc[k], active, lane);
@@ -416,45 +548,62 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
         agg_store<LPT>(ap, acc[k], active);
       }
       if (GROUP == 0 && xm[k] == c - 1) {  // N(c-1): paths 0 and 1 are revisit sources
-        cs_put<LPT>(u, oo[k], mo[k], ym[k], 0, lane);
-        cs_put<LPT>(u, ob[k], mb[k], ym[k], 1, lane);
+        cs_put<LPT>(u, oo[k], mo[k] & 0xffffu, ym[k], 0, lane);
+        cs_put<LPT>(u, ob[k], mb[k] & 0xffffu, ym[k], 1, lane);
       }
-      if (k == 0 && colc) cs_put<LPT>(u, oo[0], mo[0], ym[0], 2, lane);  // N(c).p2
+      if (k == 0 && colc) cs_put<LPT>(u, oo[0], mo[0] & 0xffffu, ym[0], 2, lane);  // N(c).p2
       if (!PASS2 && ym[k] == u.y_b) {  // pass +1's row y_b: what pass -1 reads above its first row
         if (GROUP == 0) {
           vstore<LPT>(ob[k], u.edge + ((size_t)xm[k] * 3 + 0) * Dp, lane);
-          if (lane == 0) __stcg(u.edge_min + (size_t)xm[k] * 3 + 0, (uint16_t)mb[k]);
+          if (lane == 0) __stcg(u.edge_min + (size_t)xm[k] * 3 + 0, (uint16_t)(mb[k] & 0xffffu));
         } else {
           vstore<LPT>(oo[k], u.edge + ((size_t)xm[k] * 3 + 1) * Dp, lane);
           vstore<LPT>(ob[k], u.edge + ((size_t)xm[k] * 3 + 2) * Dp, lane);
           if (lane == 0) {
-            __stcg(u.edge_min + (size_t)xm[k] * 3 + 1, (uint16_t)mo[k]);
-            __stcg(u.edge_min + (size_t)xm[k] * 3 + 2, (uint16_t)mb[k]);
+            __stcg(u.edge_min + (size_t)xm[k] * 3 + 1, (uint16_t)(mo[k] & 0xffffu));
+            __stcg(u.edge_min + (size_t)xm[k] * 3 + 2, (uint16_t)(mb[k] & 0xffffu));
           }
         }
       }
     }
-    ch[0].own.L = oo[0];
-    ch[0].own.mn = mo[0];
-    ch[1].own.L = oo[1];
-    ch[1].own.mn = mo[1];
-    prevAb.L = ob[0];
-    prevAb.mn = mb[0];
+    oL[0] = oo[0];
+    om[0] = mo[0];
+    oL[1] = oo[1];
+    om[1] = mo[1];
+    pbL = ob[0];
+    pbm = mb[0];
     return true;
   };
-  for (int s = 0; s < kStage; s++) issue(s);
+  // Step s reads queue entry s & 1: the inputs of step s + 2 are fetched once step s has consumed its entry.
+  for (int s = 0; s < kStageS; s++) issue(s);
+  In q0[2], q1[2];
+  fetch(0, 0, q0[0]);
+  fetch(1, 0, q0[1]);
+  if (a.nsteps > 1) {
+    fetch(0, 1, q1[0]);
+    fetch(1, 1, q1[1]);
+  }
   bool ok = true;
-  for (int s = 0; s < a.nsteps; s++) {
-    cp_async_wait<kStage - 1>();  // step s's group is complete
-    __syncwarp();
-    if (!step(s)) {
+  for (int s = 0; s < a.nsteps; s += 2) {
+    if (!step(s, q0)) {
       ok = false;
       break;
     }
-    __syncwarp();  // every lane has read the slot before it is refilled
-    issue(s + kStage);
+    if (s + 2 < a.nsteps) {
+      fetch(0, s + 2, q0[0]);
+      fetch(1, s + 2, q0[1]);
+    }
+    if (s + 1 >= a.nsteps) break;
+    if (!step(s + 1, q1)) {
+      ok = false;
+      break;
+    }
+    if (s + 3 < a.nsteps) {
+      fetch(0, s + 3, q1[0]);
+      fetch(1, s + 3, q1[1]);
+    }
   }
-  cp_async_wait<0>();
+  cp_async_wait<0>();  // no copy is in flight when the warp leaves
   if (ok && colc)  // the last band's revisits when no later visit of the column follows them
     for (int k = 0; k < u.end_count; k++) revisit23(u.end_first + k);
 }
@@ -513,18 +662,22 @@ int chain_blocks(int nchains) {
   return (nchains + per - 1) / per;
 }
 
-// Dynamic shared memory of a launch: the rings, their minima and mbarriers, then the staging slots of its chains.
+// Dynamic shared memory of a launch: the rings, their minima (u32 each) and their full / empty mbarriers.
 template <int LPT>
 size_t chain_smem_bytes(int nw, int n, bool read_agg) {
-  const size_t rings = (size_t)(kMaxChainWarps + 1) * kRingS * Dp_of(LPT) * 2 + (size_t)(kMaxChainWarps + 1) * kRingS * 2 + 16 +
+  const size_t rings = (size_t)(kMaxChainWarps + 1) * kRingS * Dp_of(LPT) * 2 + (size_t)(kMaxChainWarps + 1) * kRingS * 4 +
                        (size_t)2 * (kMaxChainWarps + 1) * kRingS * 8;
-  const size_t slot = ((size_t)n * (read_agg ? 3 : 1) + 8 + 15) & ~(size_t)15;
-  return rings + (size_t)2 * nw * kStage * slot;
+  const size_t staging = (size_t)nw * kStageS * 2 * (size_t)(((read_agg ? 2 * n : 0) + n + 15) & ~15);
+  return rings + staging;
 }
 
 template <int LPT, bool FULL, bool PASS2, int GROUP>
 void launch_chains_t(const SplitArgs& a, cudaStream_t s) {
   const int nw = chain_warps(a.nchains);
+  // every band-buffer entry this launch reads starts unwritten (bit 15 clear)
+  const size_t entries = (size_t)chain_blocks(a.nchains) * a.nsteps;
+  cudaMemsetAsync(a.bnd, 0, entries * Dp_of(LPT) * 2, s);
+  cudaMemsetAsync(a.bnd_min, 0, entries * 2, s);
   const size_t smem = chain_smem_bytes<LPT>(nw, a.u.n, PASS2 || GROUP == 1);
   static size_t configured = 0;
   if (smem > configured) {

@@ -20,6 +20,7 @@
 //     three-input adds per word.
 // Exactness without saturation is as in k_sgm_uniform: with P2 <= 1744 every stored L is below 2000 (a never-written
 // word), every candidate of the minimum is at least the previous minimum, and 16 contributions never exceed 65535.
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -143,7 +144,7 @@ constexpr size_t wave_smem_bytes() {
   return (size_t)(kWRows + 1) * kWRing * 3 * Dp_of(LPT) * 2 + (size_t)(kWRows + 1) * kWRing * 16;
 }
 
-template <int LPT, bool FULL, bool PASS2>
+template <int LPT, bool FULL, bool PASS2, bool MB>
 __global__ void __launch_bounds__(kWWarps * 32, 1) k_wave(const WaveArgs wa) {
   constexpr int NR = LPT / 2, Dp = Dp_of(LPT);
   const UniArgs& a = wa.u;
@@ -153,6 +154,9 @@ __global__ void __launch_bounds__(kWWarps * 32, 1) k_wave(const WaveArgs wa) {
   auto mrec = [&](int set, int slot) -> uint4& { return mins[set * kWRing + slot]; };
   // prog[r]: pixels finished by row r (r < kWRows), loaded by the loader (kWRows), copied out by the publisher (kWRows+1)
   __shared__ int prog[kWRows + 2];
+  // MB: the hand-over in is a full mbarrier per ring slot (the waiting warp is suspended by the hardware instead of
+  // polling the counter); the counters then serve only the check that a slot is free again
+  __shared__ uint64_t full_bar[MB ? (kWRows + 1) * kWRing : 1];
   __shared__ int s_cb;
   __shared__ volatile int s_stop;
   __shared__ float s_planes[256];  // the WTA's plane depths (pass -1)
@@ -160,6 +164,7 @@ __global__ void __launch_bounds__(kWWarps * 32, 1) k_wave(const WaveArgs wa) {
   if (PASS2)
     for (int i = tid; i < a.n; i += blockDim.x) s_planes[i] = a.planes[i];
   if (tid < kWRows + 2) prog[tid] = 0;
+  if (MB && tid < (kWRows + 1) * kWRing) mbar_init(&full_bar[tid], 1);
   if (tid == 0) {
     s_cb = atomicAdd(a.ticket, 1);
     s_stop = 0;
@@ -176,6 +181,10 @@ __global__ void __launch_bounds__(kWWarps * 32, 1) k_wave(const WaveArgs wa) {
   uint16_t* bnd_me = wa.bnd + (size_t)(cb % kWBandBufs) * W * 3 * Dp;
   uint4* bnd_me_md = wa.bnd_md + (size_t)(cb % kWBandBufs) * W;
   auto wait = [&](int idx, int target, int& seen) { return wait_prog(&prog[idx], target, seen, &s_stop, a.err, a.timeout_ns); };
+  // MB: pixel p of set `set` is in its ring slot (phase p / kWRing of the slot's full barrier)
+  auto wait_full = [&](int set, int p) {
+    return mbar_wait(&full_bar[set * kWRing + (p & (kWRing - 1))], (uint32_t)(p / kWRing) & 1u, &s_stop, a.err, a.timeout_ns);
+  };
 
   if (w == kWRows) {
     // ---------------- loader: the row above the block into set kWRows ----------------
@@ -230,7 +239,12 @@ __global__ void __launch_bounds__(kWWarps * 32, 1) k_wave(const WaveArgs wa) {
         if (lane == 0) mrec(kWRows, sl) = md[k];
       }
       __syncwarp();
-      if (lane == 0) st_release_cta(&prog[kWRows], xe);
+      if (lane == 0) {
+        if constexpr (MB)
+          for (int x = xb; x < xe; x++) mbar_arrive(&full_bar[kWRows * kWRing + (x & (kWRing - 1))]);
+        else
+          st_release_cta(&prog[kWRows], xe);
+      }
     }
     return;
   }
@@ -239,7 +253,7 @@ __global__ void __launch_bounds__(kWWarps * 32, 1) k_wave(const WaveArgs wa) {
     if (below_exists) {
       int seen = 0;
       for (int x = 0; x < W; x++) {
-        if (!wait(kWRows - 1, x + 1, seen)) break;
+        if (MB ? !wait_full(kWRows - 1, x) : !wait(kWRows - 1, x + 1, seen)) break;
         const int sl = x & (kWRing - 1);
 #pragma unroll
         for (int p = 0; p < 3; p++) {
@@ -274,7 +288,7 @@ __global__ void __launch_bounds__(kWWarps * 32, 1) k_wave(const WaveArgs wa) {
   float* depth_row = a.depth + (size_t)yu * W;
   const int flags = a.flags[y];
   const bool edge_row = !PASS2 && y == a.y_b;  // pass +1's row y_b is what pass -1 reads above its first row
-  int seen_up = 0, seen_cons = 0;
+  int seen_up = MB ? -1 : 0, seen_cons = 0;
   V<LPT> leftL;   // path 0: the pixel to the left
   uint32_t leftm = kInit2;
   vinit(leftL);
@@ -307,7 +321,15 @@ __global__ void __launch_bounds__(kWWarps * 32, 1) k_wave(const WaveArgs wa) {
   auto pixel = [&](int x, Queued& q, auto kind) -> bool {
     constexpr int KIND = decltype(kind)::value;
     // ---- hand-over in: the row above finished x+1 (x for the last column); the next row is done with this slot ----
-    if (!wait(up, min(x + 2, W), seen_up)) return false;
+    if constexpr (MB) {
+      const int tp = min(x + 1, c);  // the row above's pixel x+1 (the last column: its own)
+      if (tp > seen_up) {
+        if (!wait_full(up, tp)) return false;
+        seen_up = tp;
+      }
+    } else {
+      if (!wait(up, min(x + 2, W), seen_up)) return false;
+    }
     if (has_consumer && x >= kWRing && !wait(cons_idx, x - kWRing + 2 - (cons_idx == kWRows + 1 ? 1 : 0), seen_cons))
       return false;
     // ---- revisits that the reference runs before this visit (they may produce this visit's path-2 input) ----
@@ -366,7 +388,10 @@ __global__ void __launch_bounds__(kWWarps * 32, 1) k_wave(const WaveArgs wa) {
       agg_store<LPT>(ap, acc, active);
     }
     __syncwarp();
-    if (lane == 0) st_release_cta(&prog[w], x + 1);
+    if (lane == 0) {
+      if constexpr (MB) mbar_arrive(&full_bar[w * kWRing + sl]);
+      st_release_cta(&prog[w], x + 1);
+    }
     if constexpr (KIND != 3) {
       if (!PASS2 || a.keep_agg) agg_store<LPT>(ap, acc, active);
       if constexpr (PASS2) {  // WTA; the last column waits for its revisits (k_wta_column)
@@ -438,15 +463,28 @@ WaveLayout wave_layout(int W, int H, int n) {
   return L;
 }
 
-template <int LPT, bool FULL, bool PASS2>
-void launch_wave_t(const WaveArgs& wa, int nCB, cudaStream_t s) {
+template <int LPT, bool FULL, bool PASS2, bool MB>
+void launch_wave_tm(const WaveArgs& wa, int nCB, cudaStream_t s) {
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(k_wave<LPT, FULL, PASS2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wave_smem_bytes<LPT>());
+    cudaFuncSetAttribute(k_wave<LPT, FULL, PASS2, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wave_smem_bytes<LPT>());
     configured = true;
   }
-  k_wave<LPT, FULL, PASS2><<<nCB, kWWarps * 32, wave_smem_bytes<LPT>(), s>>>(wa);
+  k_wave<LPT, FULL, PASS2, MB><<<nCB, kWWarps * 32, wave_smem_bytes<LPT>(), s>>>(wa);
   count_launches(1);
+}
+bool wave_mbar() {
+  static int v = -1;
+  if (v < 0) {
+    const char* e = getenv("LUX_WAVE_SYNC");
+    v = (e && e[0] == 'c') ? 0 : 1;
+  }
+  return v == 1;
+}
+template <int LPT, bool FULL, bool PASS2>
+void launch_wave_t(const WaveArgs& wa, int nCB, cudaStream_t s) {
+  if (wave_mbar()) launch_wave_tm<LPT, FULL, PASS2, true>(wa, nCB, s);
+  else launch_wave_tm<LPT, FULL, PASS2, false>(wa, nCB, s);
 }
 template <int LPT>
 void launch_wave(const WaveArgs& wa, int nCB, cudaStream_t s) {
