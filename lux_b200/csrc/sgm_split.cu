@@ -132,6 +132,10 @@ LUX_DEV void chain_above(const SplitArgs& a, const uint16_t* bnd_up, const uint1
   }
 }
 
+// Bytes of one chain's staging slot of a step: [agg 2n B when read][raw n B], rounded up to 16 bytes (the kernel's layout
+// and the launch's shared-memory size both come from here).
+__host__ __device__ constexpr int chain_slot_bytes(int n, bool read_agg) { return ((read_agg ? 2 * n : 0) + n + 15) & ~15; }
+
 // Vector loads and stores of a lane's planes in shared memory (16, 8 or 4 bytes).
 template <int LPT>
 LUX_DEV void sload(V<LPT>& v, const uint16_t* base, int lane) {
@@ -388,7 +392,7 @@ __global__ void __launch_bounds__(kMaxWarpsS * 32, 1) k_chains(const SplitArgs a
   // Raw costs and aggregates are staged kStageS steps ahead by cp.async into this warp's slots: per step and chain
   // [agg 2n B (when read)][raw n B]; lane j < n/8 copies planes 8j..8j+7 (16 B of aggregates, 8 B of raw costs), and
   // each lane then reads its own LPT planes. One commit group per step (empty past the chain's end).
-  const int cbytes = ((kReadAgg ? 2 * n : 0) + n + 15) & ~15;  // one chain's bytes of a step, in 16-byte units
+  const int cbytes = chain_slot_bytes(n, kReadAgg);  // one chain's bytes of a step
   const int gran = n >> 3;
   uint8_t* stage = stage_base + (size_t)w * kStageS * 2 * cbytes;
   auto stage_at = [&](int slot, int k) { return stage + ((size_t)slot * 2 + k) * cbytes; };
@@ -667,7 +671,7 @@ template <int LPT>
 size_t chain_smem_bytes(int nw, int n, bool read_agg) {
   const size_t rings = (size_t)(kMaxChainWarps + 1) * kRingS * Dp_of(LPT) * 2 + (size_t)(kMaxChainWarps + 1) * kRingS * 4 +
                        (size_t)2 * (kMaxChainWarps + 1) * kRingS * 8;
-  const size_t staging = (size_t)nw * kStageS * 2 * (size_t)(((read_agg ? 2 * n : 0) + n + 15) & ~15);
+  const size_t staging = (size_t)nw * kStageS * 2 * (size_t)chain_slot_bytes(n, read_agg);
   return rings + staging;
 }
 
