@@ -66,8 +66,10 @@ def args_():
                    help="the served mixed request stream (Poisson arrivals of preview pairs, 13 MP pairs and module captures) "
                         "through the request server, against the plain one-request-at-a-time path on the same arrivals")
     p.add_argument("--requests", type=int, default=400)
-    p.add_argument("--rate", type=float, default=40.0, help="mean arrivals per second of the served stream")
-    p.add_argument("--slots", type=int, default=3)
+    p.add_argument("--rate", type=float, default=60.0,
+                   help="mean arrivals per second of the served stream (60/s: above what one request at a time keeps up with)")
+    p.add_argument("--slots", type=int, default=2,
+                   help="worker contexts of the request server (2 measured best: 3 stretches large requests' tails)")
     p.add_argument("--sweep", action="store_true",
                    help="throughput with 1, 4, 16 and 64 module captures in flight through the request server")
     p.add_argument("--cache", action="store_true",

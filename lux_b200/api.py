@@ -773,7 +773,7 @@ class Server:
     admitted in arrival order against an HBM budget and run on `slots` worker contexts, overlapping on the GPU. A request
     is one layer solved from unfiltered images exactly as DenseLayer.compute(..., prefilter=True) solves it."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, slots: int = 3):
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, slots: int = 2):
         self.lib = L.load()
         h = ctypes.c_void_p()
         rc = self.lib.lux_server_create(device, hbm_budget_bytes, slots, ctypes.byref(h))
