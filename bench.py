@@ -42,9 +42,10 @@ W_, H_, D_, TILE, BITS, DESC = WORKLOADS["pair13mp"]
 # pass +1 reads the u8 raw volume (1) and writes the u16 aggregates (2); pass -1 reads both again (1 + 2).
 BYTES_PER_DE_AGG = 6
 # DRAM bytes (read + write) per DE of a layer's aggregation as built (the path-group chains: 4 launches per layer),
-# from ncu dram__bytes_read.sum + dram__bytes_write.sum on the 2080x1560 D=256 pair: 13.74 GB for 830.7 MDE. The split
-# design trades these extra bytes (agg read/written by both path groups, raw read by each) for a short critical path.
-TRAFFIC_PER_DE_LAYER = 13.74e9 / (2080 * 1560 * 256)
+# from ncu dram__bytes_read.sum + dram__bytes_write.sum of the four k_chains launches of the 2080x1560 D=256 pair:
+# 2.655 + 4.315 + 4.317 + 2.730 GB = 14.02 GB for 830.7 MDE. The split design trades these extra bytes (aggregates read
+# and written by both path groups, raw costs read by each) for a critical path of W or H steps.
+TRAFFIC_PER_DE_LAYER = 14.02e9 / (2080 * 1560 * 256)
 
 
 def metric():
@@ -60,6 +61,9 @@ def args_():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="lux", choices=["lux", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--sgm", default="auto", choices=["auto", "split", "wave", "fused"],
+                   help="aggregation form of the timed solves (auto: the autotuner's choice, timed on the first solve of the "
+                        "shape; a fixed form for profiler runs, whose timings would mislead the tuner)")
     p.add_argument("--no-served", action="store_true",
                    help="leave out the served stream and the batched capture objects of the default line")
     p.add_argument("--serve", action="store_true",
@@ -234,7 +238,7 @@ def run_lux(a):
     infos = []
 
     def solve(imgs):
-        L = api.DenseLayer.compute(imgs, wl.gray, wl.calibs, wl.near, wl.far, wl.params, prefilter=True, ctx=ctx)
+        L = api.DenseLayer.compute(imgs, wl.gray, wl.calibs, wl.near, wl.far, wl.params, prefilter=True, sgm=a.sgm, ctx=ctx)
         infos.append((L.gpu_ms_cost, L.gpu_ms_sgm, L.gpu_ms_wta, L.sgm_kernel))
         return L
 
@@ -302,12 +306,13 @@ def run_lux(a):
         "config": {"workload": DESC,
                    "parallelism": f"replicas x{world}", "l2": l2_note(),
                    "stages_ms": {"cost": cost_ms, "sgm_2_passes": sgm_ms, "wta": wta_ms},
-                   "sgm_kernel": {0: "exact-replay", 1: "fused-wavefront", 2: "path-group-chains"}.get(inf_v[0][3] if inf_v else -1)},
+                   "sgm_kernel": {0: "exact-replay", 1: "fused-wavefront", 2: "path-group-chains", 3: "lean-wavefront"}.get(
+                       inf_v[0][3] if inf_v else -1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk.get("hbm_gbs"), "unit": "GB/s",
                      "frac": achieved / pk.get("hbm_gbs"), "traffic": TRAFFIC_PER_DE_LAYER * de,
                      "kernel": "SGM aggregation of one layer (both passes; 4 chain launches, or 2 fused ones below 2 MP)",
                      "bytes_per_de": BYTES_PER_DE_AGG, "traffic_per_de": TRAFFIC_PER_DE_LAYER,
-                     "traffic_source": "ncu dram__bytes_read+write of the 2080x1560 D=256 chain launches, scaled by DE",
+                     "traffic_source": "ncu dram__bytes_read+write of the four 2080x1560 D=256 k_chains launches, scaled by DE",
                      "peak_source": "fallback" if pk.get("fallback") else "MEASURED_PEAKS.json hbm_gbs (measured)"},
         "e2e": {"value": e2e, "unit": "MDE/s", "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": W_ * H_ * 4,
                 "path": ("host uint16 12-bit samples -> lux_image_from_grey16 -> lux_sgm_layer -> depth read back"
