@@ -142,7 +142,8 @@ struct EmuBuffers {
   int* ticket;    // [2]
   int* progress;  // [2 * bands * kEmuParts]
 };
-constexpr int kEmuParts = 4;  // at most, blocks per band of the exact replay (parts of min(16, T/2) rows)
+constexpr int kEmuPartRows = 8;  // rows of a block (part) of the exact replay's row form: min(8, T/2)
+constexpr int kEmuParts = 16;    // at most, blocks per band (parts of at least 4 rows, T <= 64)
 size_t emu_line_buffer_elems(int W, int max_hi);
 void emu_init_buffers(const EmuBuffers& b, int W, int max_hi, int align, int bands, cudaStream_t s);
 void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xsw, uint16_t p1, float p2scale, const float gw[4],

@@ -5,21 +5,23 @@
 // past a block see whatever the flat buffer holds there, and pass -1 starts from the state pass +1 left. This kernel
 // keeps the flat buffer (2 halves x (W+2) slots x (4·MaxHi+5) u16, plus Min/RangeS/RangeC/Pix) in global memory and runs
 // every Pixel() call of the reference in an order that gives each read the same last writer:
-//   * a band of T >= 4 rows runs on blocks (parts) of min(16, T/2) rows, a warp per row (one block below); blocks take
+//   * a band of T >= 4 rows runs on blocks (parts) of min(8, T/2) rows, a warp per row (one block below); blocks take
 //     tickets in order, so a part only ever waits on a running one;
 //   * a part runs its tiles in order (a block barrier between tiles); inside a tile, row r runs its offset u (pixel
 //     column iT - r + u) once row r-1 has finished offset u, and a part's first row follows the part above's last row:
 //     at the same tile and offset within a band, at offset u of tile i+1 across bands (the same sheared frame);
 //   * two calls touch a common element only when at most two columns apart, and the one pair this leaves unordered,
 //     the upper row's pixel two columns right of the lower one, touches nothing in common (see the row hand-over);
-//   * the revisits of the last column do not follow the sheared columns: a band's first part waits for tile i+2 of
-//     the band above when that tile revisits, and a part whose rows revisit in tile i first waits for the band's last
-//     part to finish tile i-1 (a band's tiles come in order in the reference);
+//   * the revisits of the last column do not follow the sheared columns: all of a band's revisits lie at offset 0 of its
+//     last tile, and the next band's first part waits for that offset before a tile that reaches column W-3; a part
+//     whose rows revisit in tile i first waits for the band's last part to finish tile i-1 (a band's tiles come in order
+//     in the reference);
 //   * tiles taller than the flag rows step with a block barrier instead, pixel (r, u) at step u + 2r (pixels of one step
 //     are three or more columns apart), one block per band, three tiles behind the band above.
 // tests/test_replay_schedule_cpu.py checks these waits against the reference's order as a happens-before model.
-// Within a Pixel() call a warp handles the lanes. The four paths run in order (a path may spill into the next), or at
-// once on four groups of eight lanes where no window of the call leaves its block.
+// Within a Pixel() call a warp handles the lanes, with all of the call's line-buffer reads in one batch where its windows
+// allow. The four paths run in order (a path may spill into the next), or at once on four groups of eight lanes where
+// no window of the call leaves its block.
 #include "common.cuh"
 #include "internal.h"
 
@@ -113,37 +115,50 @@ LUX_DEV int emu_path_batched(const uint16_t* Ln, uint16_t* Lw, int p1, int cap, 
   return runMin;
 }
 
-// One batch of the grouped form: KB chunks of 8 planes from plane b0, lane j of group grp on plane b0 + 8u + j.
-template <int KB>
-LUX_DEV void emu_group_load(const uint16_t* Ln, int b0, int cap, int count, bool skipped, const uint8_t* rawp,
-                            const uint16_t* aggp, int j, int grp, int (&Lm)[KB], int (&L0)[KB], int (&Lp)[KB], int (&rv)[KB],
-                            int (&ag)[KB]) {
+// The forms below take a Pixel() call's line-buffer reads in one batch, issued together with its line state, and make
+// each plane's three neighbours (window elements k-1, k, k+1) from one load per element by shuffles. R holds the batch in
+// registers (compile-time indices only).
+
+// Plane k's window neighbours from the lanes of a segment of `width` lanes: element e of the window sits in chunk
+// (e + 1) / width at lane (e + 1) % width, so lane i of chunk c holds element c·width + i - 1, its own Lm.
+template <int width>
+LUX_DEV void emu_neighbours(int x0, int x1, int i, int& L0, int& Lp) {
+  const int d1 = __shfl_down_sync(0xffffffffu, x0, 1, width), d2 = __shfl_down_sync(0xffffffffu, x0, 2, width);
+  const int n0 = __shfl_sync(0xffffffffu, x1, 0, width), n1 = __shfl_sync(0xffffffffu, x1, 1, width);
+  L0 = i < width - 1 ? d1 : n0;
+  Lp = i < width - 2 ? d2 : i == width - 2 ? n0 : n1;
+}
+
+// The grouped form in one batch (cap <= 8·KBG): lane j of group grp holds elements 8u + j - 1 of path grp's read window
+// Ln[-1 .. cap] in R[u] (u = 0..KBG), the raw costs of planes 8u + j in R[KBG + 1 + u] and (group 0) their aggregates in
+// R[2·KBG + 1 + u].
+template <int KBG, int NR>
+LUX_DEV void emu_group_load1(const uint16_t* Ln, int cap, int count, bool skipped, const uint8_t* rawp, const uint16_t* aggp,
+                             int j, int grp, int (&R)[NR]) {
+  static_assert(3 * KBG + 1 <= NR, "register batch too small");
 #pragma unroll
-  for (int u = 0; u < KB; u++) {
-    if (b0 + 8 * u < cap) {
-      const int k = b0 + 8 * u + j;
-      Lm[u] = __ldcg(Ln + k - 1);
-      L0[u] = __ldcg(Ln + k);
-      Lp[u] = __ldcg(Ln + k + 1);
-      rv[u] = skipped ? (k < count ? 0 : 255) : rawp[k];
-      ag[u] = grp == 0 ? (int)aggp[k] : 0;
-    }
+  for (int u = 0; u <= KBG; u++) {
+    const int e = 8 * u + j - 1;
+    R[u] = e <= cap ? (int)__ldcg(Ln + e) : 0;
+  }
+#pragma unroll
+  for (int u = 0; u < KBG; u++) {
+    const int k = 8 * u + j;
+    R[KBG + 1 + u] = k < cap ? (skipped ? (k < count ? 0 : 255) : (int)rawp[k]) : 0;
+    R[2 * KBG + 1 + u] = k < cap && grp == 0 ? (int)aggp[k] : 0;
   }
 }
 
-// The four paths of a Pixel() call at once, lanes 8p..8p+7 on path p, where every write and cleanup window of the call
-// lies inside its own block (q + cap and q0 + cp at most MaxHi + 1) and every read inside the buffer. Then no path
-// reads what another writes (the reads are neighbour slots or the other half; the writes are this slot's four blocks),
-// so the paths may run together, and the cleanup need only write the part of the old range the new one does not
-// overwrite. The aggregate takes the four paths' sum at once: saturating adds of non-negative terms commute,
-// min(min(a + x, C) + y, C) = min(a + x + y, C). KB chunks of 8 planes have their loads issued before their stores;
-// the first batch comes in loaded (its reads are neighbour slots, which no write of this call touches). Caps are
-// multiples of 8 here (checked before the launch), so every lane of a chunk has a plane.
-template <int KB>
-LUX_DEV void emu_pixel_grouped(const EmuArgs& a, const uint16_t* Ln, long long baseCur, long long q, long long q0, int cap,
-                               int cp, int count, bool skipped, const uint8_t* rawp, uint16_t* aggp, int P2p, int minPrev,
-                               uint16_t* minOut, int lane, int (&Lm)[KB], int (&L0)[KB], int (&Lp)[KB], int (&rv)[KB],
-                               int (&ag)[KB]) {
+// The four paths of a Pixel() call at once, lanes 8p..8p+7 on path p, from the batch emu_group_load1 loaded, where every
+// write and cleanup window of the call lies inside its own block (q + cap and q0 + cp at most MaxHi + 1) and every read
+// inside the buffer. Then no path reads what another writes (the reads are neighbour slots or the other half; the writes
+// are this slot's four blocks), so the paths may run together, and the cleanup need only write the part of the old range
+// the new one does not overwrite. The aggregate takes the four paths' sum at once: saturating adds of non-negative terms
+// commute, min(min(a + x, C) + y, C) = min(a + x + y, C). Caps are multiples of 8 here (checked before the launch), so
+// every lane of a chunk has a plane.
+template <int KBG, int NR>
+LUX_DEV void emu_pixel_grouped1(const EmuArgs& a, long long baseCur, long long q, long long q0, int cap, int cp, uint16_t* aggp,
+                                int P2p, int minPrev, uint16_t* minOut, int lane, const int (&R)[NR]) {
   const int j = lane & 7, grp = lane >> 3;
   for (long long k = (q0 < 0 ? -q0 : 0) + j; k < cp; k += 8) {  // stale cleanup (:261-263), outside the new range
     const long long idx = q0 + k;
@@ -151,26 +166,91 @@ LUX_DEV void emu_pixel_grouped(const EmuArgs& a, const uint16_t* Ln, long long b
   }
   uint16_t* Lw = a.L + (baseCur + q);
   int runMin = 0xffff;
-  for (int b0 = 0; b0 < cap; b0 += 8 * KB) {  // warp-uniform: the cap is the pixel's
-    if (b0 > 0) emu_group_load<KB>(Ln, b0, cap, count, skipped, rawp, aggp, j, grp, Lm, L0, Lp, rv, ag);
 #pragma unroll
-    for (int u = 0; u < KB; u++) {
-      if (b0 + 8 * u >= cap) break;
-      const int k = b0 + 8 * u + j;
-      const int m = min(min(min(Lm[u] + a.p1, 65535), L0[u]), min(min(Lp[u] + a.p1, 65535), P2p));
-      int lc = min(rv[u] + m, 65535) - minPrev;
-      if (lc < 0) lc = 0;
-      __stcg(Lw + k, (uint16_t)lc);
-      runMin = min(runMin, lc);
-      int sum = lc + __shfl_xor_sync(0xffffffffu, lc, 8);
-      sum += __shfl_xor_sync(0xffffffffu, sum, 16);
-      if (grp == 0) aggp[k] = (uint16_t)min(ag[u] + sum, 65535);
-    }
+  for (int u = 0; u < KBG; u++) {
+    if (8 * u >= cap) break;  // warp-uniform: the cap is the pixel's
+    const int k = 8 * u + j;
+    int L0, Lp;
+    emu_neighbours<8>(R[u], R[u + 1], j, L0, Lp);
+    const int m = min(min(min(R[u] + a.p1, 65535), L0), min(min(Lp + a.p1, 65535), P2p));
+    int lc = min(R[KBG + 1 + u] + m, 65535) - minPrev;
+    if (lc < 0) lc = 0;
+    __stcg(Lw + k, (uint16_t)lc);
+    runMin = min(runMin, lc);
+    int sum = lc + __shfl_xor_sync(0xffffffffu, lc, 8);
+    sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+    if (grp == 0) aggp[k] = (uint16_t)min(R[2 * KBG + 1 + u] + sum, 65535);
   }
   runMin = min(runMin, __shfl_xor_sync(0xffffffffu, runMin, 1));
   runMin = min(runMin, __shfl_xor_sync(0xffffffffu, runMin, 2));
   runMin = min(runMin, __shfl_xor_sync(0xffffffffu, runMin, 4));
   if (j == 0) __stcg(minOut, (uint16_t)runMin);
+}
+
+// The path-serial form in one batch (cap <= 32·CH - 2): R[p·CH + c] holds element 32c + lane - 1 of path p's read window
+// Ln_p[-1 .. cap], R[4·CH + c] the raw cost and R[5·CH + c] the aggregate of plane 32c + lane.
+template <int CH, int NR>
+LUX_DEV void emu_serial_load1(const uint16_t* L, const long long (&win)[4], int cap, int count, bool skipped, const uint8_t* rawp,
+                              const uint16_t* aggp, int lane, int (&R)[NR]) {
+  static_assert(6 * CH <= NR, "register batch too small");
+#pragma unroll
+  for (int c = 0; c < CH; c++) {
+    const int e = 32 * c + lane - 1;
+#pragma unroll
+    for (int p = 0; p < 4; p++) R[p * CH + c] = e <= cap ? (int)__ldcg(L + win[p] + e) : 0;
+    const int k = 32 * c + lane;
+    R[4 * CH + c] = k < cap ? (skipped ? (k < count ? 0 : 255) : (int)rawp[k]) : 0;
+    R[5 * CH + c] = k < cap ? (int)aggp[k] : 0;
+  }
+}
+
+// The four paths in the reference's order (a path's cleanup and writes may spill into the next block), each from its
+// window in the batch. The batch went out before any of the call's writes, which reads no element earlier than the
+// reference does: paths 1-3 read the other half, which the call does not write; path 0 reads the slot beside its own,
+// which only path 3's spill can reach (pass -1), after path 0; and the windows stay clear of the call's own slot (checked
+// by the caller: q + cap + 2 <= slot stride). The aggregate takes the four paths' sum at once (saturating adds of
+// non-negative terms commute).
+template <int CH, int NR>
+LUX_DEV void emu_pixel_serial1(const EmuArgs& a, int cur, int slot, long long q, int sp, int cp, int cap, uint16_t* aggp,
+                               int gMinPrev, int gP2, int lane, int (&R)[NR]) {
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    const long long baseCur = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
+    {  // stale cleanup of the previously stored range (:261-263)
+      const long long q0 = sp - a.min_lo, k0 = q0 < 0 ? -q0 : 0;
+      const long long k1 = min((long long)cp, a.Llen - baseCur - q0);
+      for (long long k = k0 + lane; k < k1; k += 32) __stcg(a.L + baseCur + q0 + k, (uint16_t)2000);
+    }
+    __syncwarp();
+    const int minPrev = __shfl_sync(0xffffffffu, gMinPrev, 8 * p), P2 = __shfl_sync(0xffffffffu, gP2, 8 * p);
+    const int P2p = min(P2 + minPrev, 65535);
+    uint16_t* Lw = a.L + (baseCur + q);
+    int runMin = 0xffff;
+#pragma unroll
+    for (int c = 0; c < CH; c++) {
+      if (32 * c >= cap) break;  // warp-uniform
+      const int k = 32 * c + lane;
+      const int x0 = R[p * CH + c];
+      int L0, Lp;
+      emu_neighbours<32>(x0, R[p * CH + (c + 1 < CH ? c + 1 : c)], lane, L0, Lp);  // chunk CH-1's lanes 30, 31 have no plane
+      const int m = min(min(min(x0 + a.p1, 65535), L0), min(min(Lp + a.p1, 65535), P2p));
+      int lc = min(R[4 * CH + c] + m, 65535) - minPrev;
+      if (lc < 0) lc = 0;
+      if (k < cap) {
+        __stcg(Lw + k, (uint16_t)lc);
+        runMin = min(runMin, lc);
+        R[5 * CH + c] += lc;
+      }
+    }
+    runMin = __reduce_min_sync(0xffffffffu, (unsigned)runMin);
+    __syncwarp();  // this path's stores (a spill reaches the next block) before the next path's cleanup
+    if (lane == 0) __stcg(a.Min + cur * a.halfM + slot * 4 + p, (uint16_t)runMin);
+  }
+#pragma unroll
+  for (int c = 0; c < CH; c++) {
+    const int k = 32 * c + lane;
+    if (k < cap) aggp[k] = (uint16_t)min(R[5 * CH + c], 65535);
+  }
 }
 
 // A pixel's read-only inputs, loaded before the hand-over that lets it run.
@@ -191,10 +271,13 @@ LUX_DEV EmuPix emu_load_pix(const EmuArgs& a, int x, int y) {
   return s;
 }
 
-// Pixel (DenseStereoSgm.cs:234-317), one warp; KB iterations of a path's plane loop share one L2 round trip. The
-// line-state loads (own Range, neighbours' Min and Pix, the grouped form's first batch) go out together.
-template <int KB>
+// Pixel (DenseStereoSgm.cs:234-317), one warp. The line-state loads (own Range, neighbours' Min and Pix) and, where the
+// windows allow, every line-buffer read of the call go out as one batch: the grouped form for caps up to 8·KBG, the
+// path-serial form for caps up to 32·CH - 2. Otherwise (larger caps, windows at the buffer's ends) the paths run one at
+// a time below, KB iterations of a path's plane loop sharing one L2 round trip.
+template <int KB, int KBG, int CH>
 LUX_DEV void emu_pixel(const EmuArgs& a, int x, const EmuPix& px, int cur, int other, int lane) {
+  constexpr int NR = 6 * CH > 3 * KBG + 1 ? 6 * CH : 3 * KBG + 1;
   const int slot = x + 1;
   const int start = px.start, count = px.count, cap = px.cap;
   const bool skipped = px.skip != 0;
@@ -210,13 +293,27 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, const EmuPix& px, int cur, int o
   const float4 pn4 = __ldcg(a.Pix + ghalf * a.halfR + gns);
   const long long q = start - a.min_lo;
   const long long gnb = (long long)ghalf * a.halfL + (long long)gns * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
-  // The grouped form pays where the one-path-at-a-time form would take one batch a path (cap <= 32·KB): it makes the
-  // four round trips one. Larger caps take as many batches either way and stay on the form below. Its read and own
-  // write windows are checked here; the cleanup window (from the Range entries) decides below.
-  const bool maybe_grouped = cap <= 32 * KB && q + cap <= a.max_hi + 1 && __all_sync(0xffffffffu, gnb + q + cap + 1 <= a.Llen);
-  int Lm[KB], L0[KB], Lp[KB], rv[KB], ag[KB];
-  const uint16_t* Ln = a.L + (gnb + q);
-  if (maybe_grouped) emu_group_load<KB>(Ln, 0, cap, count, skipped, rawp, aggp, lane & 7, gp, Lm, L0, Lp, rv, ag);
+  // The grouped form needs every write window inside its own block and every read inside the buffer (checked here) and
+  // the cleanup window inside its block (checked once the Range entries are in). The path-serial batch needs its four
+  // read windows and write ranges inside the buffer and clear of each other.
+  const bool grouped = cap <= 8 * KBG && q + cap <= a.max_hi + 1 && __all_sync(0xffffffffu, gnb + q + cap + 1 <= a.Llen);
+  bool serial = false;
+  long long win[4];
+  if (!grouped) {
+    const long long own = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1;
+    serial = cap <= 32 * CH - 2 && q + cap + 2 <= a.slot_stride;
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const int ns = slot + (p == 2 ? 0 : p == 3 ? a.dir : -a.dir);
+      const long long nb = (long long)(p == 0 ? cur : other) * a.halfL + (long long)ns * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
+      const long long wb = own + (long long)p * (a.max_hi + 1) + q;
+      win[p] = nb + q;
+      serial = serial && nb + q - 1 >= 0 && nb + q + cap + 1 <= a.Llen && wb >= 0 && wb + cap <= a.Llen;
+    }
+  }
+  int R[NR];
+  if (grouped) emu_group_load1<KBG>(a.L + (gnb + q), cap, count, skipped, rawp, aggp, lane & 7, gp, R);
+  else if (serial) emu_serial_load1<CH>(a.L, win, cap, count, skipped, rawp, aggp, lane, R);
   const float g[4] = {(float)px.gb.x, (float)px.gb.y, (float)px.gb.z, (float)px.gb.w};
   if (lane == 0) __stcg(a.Pix + cur * a.halfR + slot, make_float4(g[0], g[1], g[2], g[3]));
   int gP2;
@@ -224,19 +321,26 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, const EmuPix& px, int cur, int o
     const float pn[4] = {pn4.x, pn4.y, pn4.z, pn4.w};
     gP2 = sgm_p2(g, pn, a.gw, a.p2base);
   }
-  {
+  bool done = false;
+  if (grouped) {
     const long long q0 = sp - a.min_lo;
-    const long long gbase = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
-    if (maybe_grouped && (cp == 0 || q0 + cp <= a.max_hi + 1)) {
-      emu_pixel_grouped<KB>(a, Ln, gbase, q, q0, cap, cp, count, skipped, rawp, aggp, min(gP2 + gMinPrev, 65535), gMinPrev,
-                            a.Min + cur * a.halfM + slot * 4 + gp, lane, Lm, L0, Lp, rv, ag);
-      if (lane == 0) {
-        __stcg(a.RangeS + cur * a.halfR + slot, (uint16_t)start);
-        __stcg(a.RangeC + cur * a.halfR + slot, (uint16_t)cap);
-      }
-      __syncwarp();
-      return;
+    if (cp == 0 || q0 + cp <= a.max_hi + 1) {
+      const long long gbase = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
+      emu_pixel_grouped1<KBG>(a, gbase, q, q0, cap, cp, aggp, min(gP2 + gMinPrev, 65535), gMinPrev,
+                              a.Min + cur * a.halfM + slot * 4 + gp, lane, R);
+      done = true;
     }
+  } else if (serial) {
+    emu_pixel_serial1<CH>(a, cur, slot, q, sp, cp, cap, aggp, gMinPrev, gP2, lane, R);
+    done = true;
+  }
+  if (done) {
+    if (lane == 0) {
+      __stcg(a.RangeS + cur * a.halfR + slot, (uint16_t)start);
+      __stcg(a.RangeC + cur * a.halfR + slot, (uint16_t)cap);
+    }
+    __syncwarp();
+    return;
   }
 #pragma unroll 1
   for (int p = 0; p < 4; p++) {
@@ -311,10 +415,12 @@ LUX_DEV bool emu_tile_pixel(const EmuArgs& a, const EmuTileRow& t, int i, int r,
 
 constexpr int kFlagRows = 64;  // tiles up to this many rows hand over row to row (a warp a row); taller ones step with a barrier
 
-// kThreads bounds the block: 512 for the row form (parts of at most 16 rows; four iterations a round trip within the
-// register budget), 1024 for the barrier form (T/2 warps, one iteration). kFlags: the row hand-over below (even
-// T <= kFlagRows), else a barrier per
-// step of the sheared schedule, pixel (r, u) at step u + 2r (pixels of one step are three or more columns apart).
+// kThreads bounds the block and with it the registers a thread may hold for a Pixel() call's batch: 256 for the row form
+// (parts of at most 8 rows; caps up to 574 planes in one batch, the plane counts of the whole L16 pyramid), 1024 for
+// the barrier form. KB, KBG, CH: emu_pixel's batch sizes. kFlags: the row hand-over below (even T <= kFlagRows), else a
+// barrier per step of the sheared schedule, pixel (r, u) at step u + 2r (pixels of one step are three or more columns
+// apart).
+//
 //
 // Each warp owns one row of its part and runs the row's offsets u in order through all tiles; row r runs offset u of a
 // tile once row r-1 has finished offset u (a CTA-scope release/acquire of the row's count in shared memory): the
@@ -332,7 +438,7 @@ constexpr int kFlagRows = 64;  // tiles up to this many rows hand over row to ro
 //     block 0's last element (index MaxHi >= 8 with align 8; with align 2 nothing spills).
 // Rows then advance at their own pace, one pixel apart, instead of two pixels apart with each step waiting for its
 // slowest pixel.
-template <int kThreads, int KB, bool kFlags>
+template <int kThreads, int KB, int KBG, int CH, bool kFlags>
 __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
   __shared__ int s_part;
   __shared__ volatile int s_stop;
@@ -371,18 +477,20 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
       const EmuTileRow row = emu_tile_row(a, j, i, r);
       // Another block reads what this part's last two rows write (the row above it in the other half, the row two
       // above in its own half: the Range entries of its stale cleanup, the line state it overwrites), and, on a tile
-      // before the part above revisits, what any row writes near the last column. Those rows' lanes make their
-      // writes visible to the GPU before the row's count moves on; the CTA-scope hand-over alone only orders them
-      // for this block.
-      const bool fence = r >= r_pub - 1 || (part > 0 && (i + 1) * T >= a.W);
+      // before the part above revisits, what any row writes near the last column. No fence is needed for that: every
+      // hand-over is a release / acquire pair (a row's lanes __syncwarp, lane 0 releases its count at CTA scope, the
+      // next row's lanes acquire it; the publishing row releases at GPU scope, the next block's lanes acquire), so a
+      // write of any row is ordered, through the chain of hand-overs, before every read that waits on it (the PTX
+      // memory model's causality order is transitive across the CTA- and GPU-scope links).
       // Waits at the tile's start, around revisits of the last column (which do not follow the sheared columns):
-      // the first part's first row waits for tile i+2 of the band above when that tile revisits (the band above comes
+      // the first part's first row waits, before a tile that reaches column W-3 (whose calls touch the last column's
+      // slots), for the band above's revisits: offset 0 of its last tile, where all of them lie (the band above comes
       // first in the reference); a first row whose part revisits in tile i waits for the band's last part (and so
       // every part below it) to finish tile i-1, and any revisiting row for its own part's last row (a band's tiles
       // come in order in the reference).
       int gneed = 0;
       int* gflag = above;
-      if (r == r0 && part == 0 && k > 0 && (i + 2) * T >= a.W) gneed = min(i + 3, a.gwN) * T;
+      if (r == r0 && part == 0 && k > 0 && (i + 1) * T >= a.W - 2) gneed = (a.gwN - 1) * T + 1;
       const int last = min(a.parts - 1, (a.H - j * T - 1) / a.part_rows);  // the band's last part inside the image
       if (r == r0 && part < last && i > 0 && i * T - r0 >= a.W) {
         gneed = i * T;  // (a first part's row r0 revisiting at tile i has no tile i+2 wait: i * T >= W)
@@ -434,9 +542,8 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
         }
         if (has) {
           const int cur = (r & 1) == 0 ? 1 : 0;
-          emu_pixel<KB>(a, x, px, cur, 1 - cur, lane);
+          emu_pixel<KB, KBG, CH>(a, x, px, cur, 1 - cur, lane);
         }
-        if (fence) __threadfence();
         __syncwarp();
         if (lane == 0) {
           st_release_cta(&s_row[r], i * T + u + 1);
@@ -462,7 +569,7 @@ __global__ void __launch_bounds__(kThreads) k_sgm_emulate(const EmuArgs a) {
         int x, y;
         if (!emu_tile_pixel(a, row, i, r, u, x, y)) continue;
         const int cur = (r & 1) == 0 ? 1 : 0;
-        emu_pixel<KB>(a, x, emu_load_pix(a, x, y), cur, 1 - cur, lane);
+        emu_pixel<KB, KBG, CH>(a, x, emu_load_pix(a, x, y), cur, 1 - cur, lane);
       }
       __syncthreads();
     }
@@ -517,12 +624,14 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   a.p2base = p1f * p2scale;  // (float)P1 * P2Scale (:256)
   for (int i = 0; i < 4; i++) a.gw[i] = gw[i];
   int pass = dir > 0 ? 0 : 1;
-  // The row form splits a band of T >= 4 rows between blocks (parts) of min(16, T/2) rows, a warp a row (up to 16
-  // warps a block: 128 registers a thread, four iterations a round trip). It needs an even T: the line-buffer half of a row follows its row in the tile (as in the reference), so with an odd T
-  // a band's last row and the next band's first row share a half, and the pair two columns apart that the row form
-  // leaves unordered would then meet (the upper pixel's path-0 read of the slot the lower one spills into).
+  // The row form splits a band of T >= 4 rows between blocks (parts) of min(8, T/2) rows, a warp a row (up to 8 warps
+  // a block, so that a thread may hold a whole Pixel() call's batch; shorter parts also spread a band over more SMs,
+  // which measured faster than 16-row parts on every L16 layer). It needs an even T: the line-buffer half of a row
+  // follows its row in the tile (as in the reference), so with an odd T a band's last row and the next band's first
+  // row share a half, and the pair two columns apart that the row form leaves unordered would then meet (the upper
+  // pixel's path-0 read of the slot the lower one spills into).
   const bool flags = g.tile <= kFlagRows && g.tile % 2 == 0;
-  a.part_rows = flags && g.tile >= 4 ? min(16, g.tile / 2) : g.tile;
+  a.part_rows = flags && g.tile >= 4 ? min(kEmuPartRows, g.tile / 2) : g.tile;
   a.parts = (g.tile + a.part_rows - 1) / a.part_rows;  // at most kEmuParts (T <= kFlagRows = 64)
   a.ticket = b.ticket + pass;
   a.progress = b.progress + (size_t)pass * a.ghN * kEmuParts;
@@ -534,8 +643,8 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   if (nw < 1) nw = 1;
   if (nw > 32) nw = 32;
   const int blocks = a.ghN * a.parts;
-  if (!flags) k_sgm_emulate<1024, 1, false><<<blocks, nw * 32, 0, s>>>(a);
-  else k_sgm_emulate<512, 4, true><<<blocks, nw * 32, 0, s>>>(a);  // nw = part_rows <= 16
+  if (!flags) k_sgm_emulate<1024, 1, 4, 2, false><<<blocks, nw * 32, 0, s>>>(a);
+  else k_sgm_emulate<256, 4, 8, 18, true><<<blocks, nw * 32, 0, s>>>(a);  // nw = part_rows <= 8
   count_launches(1);
 }
 

@@ -20,7 +20,6 @@
 //     three-input adds per word.
 // Exactness without saturation is as in k_sgm_uniform: with P2 <= 1744 every stored L is below 2000 (a never-written
 // word), every candidate of the minimum is at least the previous minimum, and 16 contributions never exceed 65535.
-#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -473,18 +472,11 @@ void launch_wave_tm(const WaveArgs& wa, int nCB, cudaStream_t s) {
   k_wave<LPT, FULL, PASS2, MB><<<nCB, kWWarps * 32, wave_smem_bytes<LPT>(), s>>>(wa);
   count_launches(1);
 }
-bool wave_mbar() {
-  static int v = -1;
-  if (v < 0) {
-    const char* e = getenv("LUX_WAVE_SYNC");
-    v = (e && e[0] == 'c') ? 0 : 1;
-  }
-  return v == 1;
-}
+// The hand-over in waits on the ring slots' full mbarriers (MB = true): measured faster than polling the row counters
+// (MB = false, which the kernel keeps as the plain form of the same schedule).
 template <int LPT, bool FULL, bool PASS2>
 void launch_wave_t(const WaveArgs& wa, int nCB, cudaStream_t s) {
-  if (wave_mbar()) launch_wave_tm<LPT, FULL, PASS2, true>(wa, nCB, s);
-  else launch_wave_tm<LPT, FULL, PASS2, false>(wa, nCB, s);
+  launch_wave_tm<LPT, FULL, PASS2, true>(wa, nCB, s);
 }
 template <int LPT>
 void launch_wave(const WaveArgs& wa, int nCB, cudaStream_t s) {

@@ -2,10 +2,11 @@
 
 The reference runs DenseLayer.Pixel() (DenseStereoSgm.cs:234-317) band by band, tile by tile, row by row, column by
 column (DenseStereoSgm.cs:206-224), and its result depends on that order through the flat line buffer. The GPU replay
-runs pixels concurrently: a band of T rows is split into parts (blocks) of min(16, T/2) rows, a warp per row, and each row goes
+runs pixels concurrently: a band of T rows is split into parts (blocks) of min(8, T/2) rows, a warp per row, and each row goes
 through its tiles on its own; row r runs offset u of tile i once row r-1 has finished it; a part's first row follows
 the last row of the part above (same tile and offset within a band, offset u of tile i+1 across bands); waits at a
-tile's start cover the revisits of the last column. This test builds the happens-before graph of those waits and
+tile's start cover the revisits of the last column (a band's first row waits for the band above's revisits, all at
+offset 0 of its last tile, before a tile that reaches column W-3). This test builds the happens-before graph of those waits and
 checks that every two Pixel() calls that touch a common line-buffer region, one of them writing, are ordered as the
 reference orders them, and that the graph has no cycle (no wait can deadlock).
 
@@ -89,15 +90,17 @@ def _count_unordered(ids, preds, pixels):
 
 
 def launcher_part_rows(T):
-    """Rows per part (block) of a band, as the launcher splits it: min(16, T/2) rows for T >= 4, the whole band below."""
-    return min(16, T // 2) if T >= 4 else T
+    """Rows per part (block) of a band, as the launcher splits it: min(8, T/2) rows for T >= 4, the whole band below."""
+    return min(8, T // 2) if T >= 4 else T
 
 
-def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False, own_part_rule=True, part_rows=None):
+def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False, own_part_rule=True, part_rows=None, band_reach=3):
     """Conflicting pairs the waits leave unordered (or -1 for a cycle). The band is split into parts of part_rows rows
-    (the last part holds the rest: 16 + 16 + 8 at T = 40), or into `parts` equal parts when part_rows is None. Planted
-    mistakes: lower_part_rule makes a lower part wait for the part above to finish its revisiting tile i+1 (instead of
-    the part above waiting for it); own_part_rule=False drops the wait of a revisiting row for its own part's last row."""
+    (the last part holds the rest: 8 + 8 + 8 + 8 + 2 at T = 34), or into `parts` equal parts when part_rows is None. A
+    band's first row waits for the band above's revisits (offset 0 of its last tile) before a tile that reaches column
+    W - band_reach (W - 3 in the kernel). Planted mistakes: lower_part_rule makes a lower part wait for the part above to
+    finish its revisiting tile i+1 (instead of the part above waiting for it); own_part_rule=False drops the wait of a
+    revisiting row for its own part's last row; band_reach=2 waits one column too late."""
     ghN, gwN = (H + T - 1) // T, (W + 2 * T - 1) // T
     R = part_rows if part_rows is not None else (T + parts - 1) // parts
     parts = (T + R - 1) // R
@@ -140,8 +143,8 @@ def unordered_pairs(W, H, T, parts, dirn, lower_part_rule=False, own_part_rule=T
                             edge(node(key), n)
                         if u == 0:  # waits at the tile's start
                             waits = []
-                            if r == r0 and part == 0 and j > 0 and (i + 2) * T >= W:
-                                waits.append((j - 1, parts - 1, min(i + 3, gwN) - 1))
+                            if r == r0 and part == 0 and j > 0 and (i + 1) * T >= W - band_reach + 1:
+                                edge(node((j - 1, parts - 1, pub_row(j - 1, parts - 1), gwN - 1, 0)), n)
                             if lower_part_rule:
                                 if r == r0 and part > 0 and (i + 1) * T - (r0 - R) >= W:
                                     waits.append((j, part - 1, min(i + 2, gwN) - 1))
@@ -205,8 +208,8 @@ def unordered_pairs_barrier_form(W, H, T, dirn, lag=3):
                                    (40, 10, 4), (20, 11, 6), (75, 70, 34), (83, 90, 40), (61, 55, 50), (90, 130, 62)])
 @pytest.mark.parametrize("dirn", [1, -1])
 def test_replay_waits_keep_the_reference_order(W, H, T, dirn):
-    """Even tiles whose band the launcher splits into parts of min(16, T/2) rows, including the tiles between 32 and 64
-    rows that are not multiples of 16, where the last part is shorter (T = 34: 16 + 16 + 2; T = 40: 16 + 16 + 8)."""
+    """Even tiles whose band the launcher splits into parts of min(8, T/2) rows, including the tiles that are not
+    multiples of 8, where the last part is shorter (T = 34: four parts of 8 and one of 2; T = 50: six of 8 and one of 2)."""
     assert unordered_pairs(W, H, T, 0, dirn, part_rows=launcher_part_rows(T)) == 0
 
 
@@ -217,6 +220,21 @@ def test_order_check_catches_a_wrong_revisit_rule():
     assert unordered_pairs(30, 20, 4, 2, -1, lower_part_rule=True) > 0
     assert unordered_pairs(70, 45, 32, 2, 1, own_part_rule=False) > 0
     assert unordered_pairs(40, 10, 4, 2, -1, own_part_rule=False) > 0
+
+
+@pytest.mark.parametrize("W,H,T,dirn", [(66, 65, 64, 1), (130, 98, 16, 1), (66, 40, 4, 1)])
+def test_order_check_catches_a_late_band_wait(W, H, T, dirn):
+    """A band whose first row waits for the band above's revisits only before a tile reaching column W-2 (one column
+    late) writes the slots that those revisits still read."""
+    assert unordered_pairs(W, H, T, 0, dirn, part_rows=launcher_part_rows(T), band_reach=2) > 0
+    assert unordered_pairs(W, H, T, 0, dirn, part_rows=launcher_part_rows(T)) == 0
+
+
+@pytest.mark.parametrize("W,H,T,dirn", [(66, 65, 64, 1), (130, 100, 64, -1), (70, 45, 32, 1), (83, 90, 40, -1)])
+def test_shorter_parts_keep_the_reference_order(W, H, T, dirn):
+    """Parts of 4 rows (up to 16 a band) and 16 rows: the waits do not depend on the part size."""
+    assert unordered_pairs(W, H, T, 0, dirn, part_rows=4) == 0
+    assert unordered_pairs(W, H, T, 0, dirn, part_rows=16) == 0
 
 
 def test_four_parts_wait_for_the_last_part():
