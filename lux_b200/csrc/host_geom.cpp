@@ -286,27 +286,10 @@ void host_flow_matrix(const lux_calib& a, const lux_calib& b, float out[16]) {
     for (int r = 0; r < 4; r++) out[4 * c + r] = (float)M[4 * r + c];
 }
 
-int host_skip_mask(int mode, int w, int h, std::vector<uint8_t>& m) {
-  m.assign((size_t)w * h, 0);
-  if (mode == 0) return LUX_OK;
-  if (mode != 2) return LUX_ERR_SKIPMODE;
-  std::fill(m.begin(), m.end(), (uint8_t)0xff);
-  int nx = w / 64 + (64 < 2 * (w % 64) ? 1 : 0), ny = h / 64 + (64 < 2 * (h % 64) ? 1 : 0);
-  if (nx < 1) nx = 1;
-  if (ny < 1) ny = 1;
-  for (int j = 0; j < ny; j++)
-    for (int i = 0; i < nx; i++) {  // one computed pixel per 2x2 cell, a fresh default-seeded generator per 64x64 tile
-      int x0 = 64 * i, x1 = std::min(w, x0 + 64 * (i == nx - 1 ? 2 : 1));
-      int y0 = 64 * j, y1 = std::min(h, y0 + 64 * (j == ny - 1 ? 2 : 1));
-      Twister mt(5489u);
-      for (int y = y0; y < y1; y += 2)
-        for (int x = x0; x < x1; x += 2) {
-          int dy = (int)(mt.next() & 1), dx = (int)(mt.next() & 1);
-          int yy = y + dy, xx = x + dx;
-          if (xx >= 0 && xx < w && yy >= 0 && yy < h) m[(size_t)yy * w + xx] = 0;
-        }
-    }
-  return LUX_OK;
+void host_skip_stream_bits(uint32_t out[256]) {
+  Twister mt(5489u);  // the default seed, as every tile of DenseLayer.SkipMask uses (DenseStereoSgm.cs:74-84)
+  for (int w = 0; w < 256; w++) out[w] = 0;
+  for (int k = 0; k < 8192; k++) out[k >> 5] |= (mt.next() & 1u) << (k & 31);
 }
 
 bool host_range_bounds(const std::vector<float>& planes, std::vector<float>& b) {

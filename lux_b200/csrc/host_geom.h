@@ -17,8 +17,10 @@ const uint32_t* host_rcp_table();      // the 4096-entry table (uploaded to the 
 int host_planes(float near_, float far_, const lux_calib* calibs, int ncams, float density, int align, std::vector<float>& out);
 // Mat4D.FlowMatrix (ViewTransform.cs:126-133): column-major float M = (K_b·E_b)·(K_a·E_a)^-1 computed in double.
 void host_flow_matrix(const lux_calib& a, const lux_calib& b, float out[16]);
-// DenseLayer.SkipMask (DenseStereoSgm.cs:65-87); returns a LUX_ERR_* code.
-int host_skip_mask(int mode, int w, int h, std::vector<uint8_t>& m);
+// DenseLayer.SkipMask (DenseStereoSgm.cs:65-87) seeds a fresh generator for every 64x64 tile, so every tile reads the
+// same stream: the low bits of its first 8192 draws (enough for a tile's at most 64 x 64 cells of two draws), draw k at
+// bit k % 32 of word k / 32. k_skip_mask builds the mask from them on the device.
+void host_skip_stream_bits(uint32_t out[256]);
 // The plane-index boundaries of RangeFromPrevious (DenseStereoSgm.cs:94-96); returns whether they are non-decreasing.
 bool host_range_bounds(const std::vector<float>& planes, std::vector<float>& b);
 

@@ -49,6 +49,8 @@ struct CostArgs {
 
 // prep.cu
 void launch_box_filter3(const uint8_t* src, int w, int h, int stride, uint8_t* dst, cudaStream_t s);
+// DenseLayer.SkipMask for SkipMode 0 or 2 (checked by the caller); bits: host_skip_stream_bits on the device.
+void launch_skip_mask(int mode, int w, int h, const uint32_t* bits, uint8_t* m, cudaStream_t s);
 void launch_guidance(const uint8_t* img0, int w0, int h0, int w, int h, int scale, uchar4* out, cudaStream_t s);
 // b: the n plane-index boundaries (device); monotone: b is non-decreasing (bisection gives the scan's answer)
 void launch_range_from_previous(const float* prev_depth, const uint8_t* prev_skip, int pw, int ph, const float* b, int monotone,

@@ -28,6 +28,7 @@ struct lux_sgm_ctx {
   std::mutex mu;
   std::string last_error;
   uint32_t* d_rcp = nullptr;  // 4096-entry rcp table
+  uint32_t* d_skip_bits = nullptr;  // the skip mask's generator stream (host_skip_stream_bits)
   uint32_t* d_warp = nullptr; // the rsqrt tables (exponents 127, 128; 4096 entries each), then the 384-float Lanczos table
   int* d_err = nullptr;       // device error word of the current call
   cudaEvent_t ev[4] = {};
@@ -249,8 +250,7 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   L->h = (ih[0] + p.scale - 1) / p.scale;
   const int W = L->w, H = L->h;
   const size_t npx = (size_t)W * H;
-  std::vector<uint8_t> skip;
-  if ((rc = host_skip_mask(p.skip_mode, W, H, skip))) return set_err(ctx, rc, "%s", default_message(rc));
+  if (p.skip_mode != 0 && p.skip_mode != 2) return set_err(ctx, LUX_ERR_SKIPMODE, "%s", default_message(LUX_ERR_SKIPMODE));
   auto& B = L->bufs;
   if ((rc = alloc_t(ctx, B, (size_t)L->n, &L->planes))) return rc;
   if ((rc = alloc_t(ctx, B, npx, &L->guidance))) return rc;
@@ -262,7 +262,7 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   if ((rc = alloc_t(ctx, B, npx, &L->depth))) return rc;
   cudaStream_t s = ctx->stream;
   CK(cudaMemcpyAsync(L->planes, L->planes_h.data(), (size_t)L->n * 4, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(L->skip, skip.data(), npx, cudaMemcpyHostToDevice, s));
+  launch_skip_mask(p.skip_mode, W, H, ctx->d_skip_bits, L->skip, s);
   launch_guidance(dimg[0], iw[0], ih[0], W, H, p.scale, L->guidance, s);
   std::vector<DevBuf> tmp;
   struct TmpGuard {
@@ -502,6 +502,12 @@ int lux_sgm_create(int device, uint64_t hbm_budget_bytes, lux_sgm_ctx** out) {
   ctx->d_never = ctx->d_err + 1;
   cudaMemcpy(ctx->d_rcp, host_rcp_table(), 4096 * 4, cudaMemcpyHostToDevice);
   {
+    uint32_t bits[256];
+    host_skip_stream_bits(bits);
+    if (cudaMalloc(&ctx->d_skip_bits, sizeof bits) != cudaSuccess) return fail(LUX_ERR_ALLOC);
+    cudaMemcpy(ctx->d_skip_bits, bits, sizeof bits, cudaMemcpyHostToDevice);
+  }
+  {
     std::vector<uint32_t> wt(8192 + 384);
     std::memcpy(wt.data(), host_rsqrt_table(false), 4096 * 4);
     std::memcpy(wt.data() + 4096, host_rsqrt_table(true), 4096 * 4);
@@ -521,6 +527,7 @@ void lux_sgm_destroy(lux_sgm_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (auto& e : ctx->ev) cudaEventDestroy(e);
   cudaFree(ctx->d_rcp);
+  cudaFree(ctx->d_skip_bits);
   cudaFree(ctx->d_warp);
   cudaFree(ctx->d_err);
   cudaStreamDestroy(ctx->stream);
@@ -736,9 +743,6 @@ int lux_sgm_pyramid(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* image
         if (rc) { set_err(ctx, rc, "%s", default_message(rc)); break; }
         const int W = (iw[0] + pars[i].scale - 1) / pars[i].scale, H = (ih[0] + pars[i].scale - 1) / pars[i].scale;
         const size_t npx = (size_t)W * H;
-        std::vector<uint8_t> sk;
-        rc = host_skip_mask(pars[i].skip_mode, W, H, sk);
-        if (rc) { set_err(ctx, rc, "%s", default_message(rc)); break; }
         std::vector<DevBuf> tmp;
         uint16_t *st = nullptr, *ct = nullptr;
         uint8_t* dsk = nullptr;
@@ -751,7 +755,7 @@ int lux_sgm_pyramid(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* image
         if (!rc) rc = ranges_from_previous(ctx, tmp, pl, prev, W, H, pars[i].margin, st, ct, &rr);
         unsigned long long cost = 0;
         if (!rc) {
-          cudaMemcpyAsync(dsk, sk.data(), npx, cudaMemcpyHostToDevice, ctx->stream);
+          launch_skip_mask(pars[i].skip_mode, W, H, ctx->d_skip_bits, dsk, ctx->stream);
           cudaMemsetAsync(acc, 0, 8, ctx->stream);
           launch_estimate_terms(ct, dsk, (int)npx, aligns[t], acc, ctx->stream);
           cudaMemcpyAsync(&cost, acc, 8, cudaMemcpyDeviceToHost, ctx->stream);

@@ -16,6 +16,34 @@ void count_launches(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order
 uint64_t kernel_launches() { return g_launches.load(); }
 
 // ---- DenseStereo.BoxFilter3 (DenseStereo.cs:93-159): per channel float(Σ)·(1/(cols·rows)), RNE, saturated ----
+// DenseLayer.SkipMask (DenseStereoSgm.cs:65-87), SkipMode 2: the image is cut into 64x64 tiles (the last tile of a row or
+// column takes the remainder, nx = w/64 + (64 < 2·(w%64))), each drawing from a fresh default-seeded mt19937; its 2x2
+// cells in row order take two draws each, dy then dx, and the cell's pixel (x + dx, y + dy) is computed (0), every
+// other pixel skipped (0xff). Tiles start at multiples of 64, so a pixel's cell is (x & ~1, y & ~1) and it is the
+// chosen one when its parities are (dx, dy). bits: the stream's low bits (host_skip_stream_bits).
+__global__ void k_skip_mask(uint8_t* __restrict__ m, int w, int h, int nx, int ny, const uint32_t* __restrict__ bits) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= w || y >= h) return;
+  const int i = min(x >> 6, nx - 1), j = min(y >> 6, ny - 1);
+  const int x0 = 64 * i, x1 = min(w, x0 + (i == nx - 1 ? 128 : 64)), y0 = 64 * j;
+  const int c = ((y - y0) >> 1) * ((x1 - x0 + 1) >> 1) + ((x - x0) >> 1);  // the cell's index in its tile
+  const int k = 2 * c;
+  const int dy = (__ldg(bits + (k >> 5)) >> (k & 31)) & 1, dx = (__ldg(bits + ((k + 1) >> 5)) >> ((k + 1) & 31)) & 1;
+  m[(size_t)y * w + x] = ((x & 1) == dx && (y & 1) == dy) ? 0 : 0xff;
+}
+
+void launch_skip_mask(int mode, int w, int h, const uint32_t* bits, uint8_t* m, cudaStream_t s) {
+  if (mode == 0) {
+    cudaMemsetAsync(m, 0, (size_t)w * h, s);
+    return;
+  }
+  int nx = w / 64 + (64 < 2 * (w % 64) ? 1 : 0), ny = h / 64 + (64 < 2 * (h % 64) ? 1 : 0);
+  if (nx < 1) nx = 1;
+  if (ny < 1) ny = 1;
+  k_skip_mask<<<dim3((w + 255) / 256, h), 256, 0, s>>>(m, w, h, nx, ny, bits);
+  count_launches(1);
+}
+
 __global__ void k_box_filter3(const uint8_t* __restrict__ src, int w, int h, int stride, uint8_t* __restrict__ dst) {
   int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
   if (x >= w) return;

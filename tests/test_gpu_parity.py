@@ -200,6 +200,21 @@ def test_uniform_layer_with_skip_mask(ctx, oracle, kernel):
         gl.close()
 
 
+@pytest.mark.parametrize("w,h", [(2080, 1560), (1040, 780), (191, 127), (127, 191), (95, 97), (33, 25)])
+def test_skip_mask_on_the_device(ctx, oracle, w, h):
+    """SkipMode 2's mask (DenseStereoSgm.cs:65-87), made on the device from the generator stream every 64x64 tile
+    restarts: the pyramid's two finest layer sizes, last tiles that absorb a remainder of at most 32 pixels or stand on
+    their own past it, and a layer smaller than one tile (eight planes, so the solve itself is cheap)."""
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(w, h, 8, seed=5, tile=8)
+    p = api.StereoParams(**{**wl.params.__dict__, "skip_mode": 2})
+    gl = api.DenseLayer.compute(wl.images, wl.gray, wl.calibs, wl.near, wl.far, p, prefilter=True, ctx=ctx)
+    try:
+        assert np.array_equal(gl.Skip.reshape(h, w), oracle.skip_mask(2, w, h).reshape(h, w))
+    finally:
+        gl.close()
+
+
 @pytest.mark.parametrize("kernel", ["fused", "split", "wave"])
 @pytest.mark.parametrize("n_cams,colour", [(4, False), (6, True), (6, False)])
 def test_multicamera_layers_bit_exact(ctx, oracle, n_cams, colour, kernel):
