@@ -465,12 +465,13 @@ def capture_batched_vs_plain(a, steps=5, warmup=3):
     pairs = [([dev_imgs[0], dev_imgs[k]], [mc.gray[0], mc.gray[k]], [mc.calibs[0], mc.calibs[k]]) for k in range(1, len(dev_imgs))]
     n_k = [len(api.DenseStereo.planes(mc.near, mc.far, c, mc.params.plane_density, 8)) for _, _, c in pairs]
 
-    def batched():
-        api.DenseLayer.compute(dev_imgs, mc.gray, mc.calibs, mc.near, mc.far, mc.params, prefilter=True, ctx=ctx).close()
+    def batched(sgm="auto"):
+        api.DenseLayer.compute(dev_imgs, mc.gray, mc.calibs, mc.near, mc.far, mc.params, prefilter=True, sgm=sgm,
+                               ctx=ctx).close()
 
-    def plain():
+    def plain(sgm="auto"):
         for imgs_k, g_k, c_k in pairs:
-            api.DenseLayer.compute(imgs_k, g_k, c_k, mc.near, mc.far, mc.params, prefilter=True, ctx=ctx).close()
+            api.DenseLayer.compute(imgs_k, g_k, c_k, mc.near, mc.far, mc.params, prefilter=True, sgm=sgm, ctx=ctx).close()
 
     def timed(fn):
         for _ in range(warmup):
@@ -485,12 +486,18 @@ def capture_batched_vs_plain(a, steps=5, warmup=3):
         return e0.elapsed_time(e1) / steps
 
     ms_b, ms_p = timed(batched), timed(plain)
+    # the size rule the autotuner replaces (path-group chains from about 2 MP, so every layer here): the same work
+    ms_bf, ms_pf = timed(lambda: batched("split")), timed(lambda: plain("split"))
+    form = api.SGM_FORM_NAMES.get(api.tuned_form(2080, 1560, n, mc.params.tile), "untuned")
     ctx.close()
     return {"workload": "2080x1560 reference + 10 module cameras (1-6 MP crops, focal 1.0-2.7x, D_k 64-192), u8",
-            "batched": {"ms_per_capture": ms_b, "planes": n, "mde_per_s": 2080 * 1560 * n / ms_b / 1e3,
+            "batched": {"ms_per_capture": ms_b, "planes": n, "mde_per_s": 2080 * 1560 * n / ms_b / 1e3, "sgm": form,
                         "note": "one layer summing the ten cameras' costs (the reference's multi-view sum)"},
             "plain": {"ms_per_capture": ms_p, "planes": n_k, "mde_per_s": sum(2080 * 1560 * k for k in n_k) / ms_p / 1e3,
-                      "note": "ten two-camera layers one after another"}}
+                      "note": "ten two-camera layers one after another"},
+            "size_rule": {"batched_ms": ms_bf, "plain_ms": ms_pf,
+                          "note": "the same two jobs with the aggregation form fixed by size (path-group chains), "
+                                  "against the autotuned forms above"}}
 
 
 def run_serve(a):

@@ -393,9 +393,9 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
       return run_sgm_uniform(g, xsw, p.p1, p.p2scale, p.guidance, L->raw, L->agg, L->agg_pass1, L->depth, keep, scr, sb, ctx->d_err, s);
     };
     if (tune) {
-      // The first solve of this shape times every form on the layer's own volume and keeps the fastest for later solves.
-      // Each form writes every aggregate and depth it produces and all forms give the same bits, so the layer keeps the
-      // last run's results. The reported aggregation time is the chosen form's.
+      // The first solve of this shape times every form on the layer's own volume (the second of two runs) and keeps the
+      // fastest for later solves. Each form writes every aggregate and depth it produces and all forms give the same
+      // bits, so the layer keeps the last run's results. The reported aggregation time is the chosen form's.
       static const int kForms[3] = {3, 2, 1};
       size_t sb = 0;
       for (int f : kForms) sb = std::max(sb, scratch_of(f));
@@ -406,6 +406,9 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
       float best_ms = 0.f;
       int best = 0;
       for (int f : kForms) {
+        // an untimed run first: a form's first launch in the process also loads its kernels (lazy module loading) and
+        // sets their shared-memory limits, which is not the form's speed
+        if ((rc = run_form(f, scr, sb))) return set_err(ctx, LUX_ERR_CUDA, "uniform aggregation launch failed (%d)", rc);
         CK(cudaEventRecord(ctx->ev[1], s));
         if ((rc = run_form(f, scr, sb))) return set_err(ctx, LUX_ERR_CUDA, "uniform aggregation launch failed (%d)", rc);
         CK(cudaEventRecord(ctx->ev[2], s));

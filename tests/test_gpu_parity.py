@@ -87,6 +87,23 @@ def test_replay_barrier_form_bit_exact(ctx, oracle, w, h, d, tile):
         gl.close()
 
 
+@pytest.mark.parametrize("w,h,d,tile", [(120, 90, 24, 20), (150, 100, 16, 34), (140, 130, 16, 50)])
+def test_replay_partial_last_part_bit_exact(ctx, oracle, w, h, d, tile):
+    """The row form splits a band into parts of min(8, T/2) rows; these tiles leave a shorter last part (T = 20: 8 + 8 +
+    4; T = 34: four parts of 8 and one of 2; T = 50: six of 8 and one of 2), whose last row publishes to the next band."""
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(w, h, d, seed=w + h, tile=tile)
+    filt = _filtered(oracle, wl.images)
+    ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True)
+    gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, keep_agg=True,
+                                ctx=ctx, force_replay=True)
+    try:
+        assert gl.sgm_kernel == SGM_FORMS["replay"]
+        _compare_layer(gl, ol, f"{w}x{h} D{d} T{tile} replay")
+    finally:
+        gl.close()
+
+
 @pytest.mark.parametrize("kernel", ["fused", "split", "wave"])
 def test_uniform_fast_depth_without_kept_aggregates(ctx, oracle, kernel):
     """The production form (no Agg kept, WTA fused into the last kernel of pass -1) gives the same depth."""
