@@ -931,15 +931,21 @@ def pyramid_job(a, w, h, steps, warmup, cpu=True):
     out = torch.empty((2 * h, 2 * w), dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
     info = []
+    ups = []  # the upsample's (start, end) events of the timed steps
 
-    def step():
+    def step(timed=False):
         layers = api.DenseStereoPyramid.run(d_imgs, cap.gray, cap.calibs, cap.near, cap.far, ctx=ctx)
         top = layers[-1]
         info[:] = [(L.W, L.H, L.n_planes, L.sgm_kernel, L.cost_kernel, L.gpu_ms_cost, L.gpu_ms_sgm, L.gpu_ms_wta, L.volume / (L.W * L.H))
                    for L in layers]
         gi = api.L.Img(guide.data_ptr(), 2 * w, 2 * h, 2 * w, 1)
+        if timed:
+            ups.append((torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)))
+            ups[-1][0].record(stream)
         ctx.check(lib.lux_sgm_upsample(ctx.handle, top.device_ptr(0), top.W, top.H, 1, ctypes.byref(gi), w, h, 12.0, 2, None,
                                        out.data_ptr(), None))
+        if timed:
+            ups[-1][1].record(stream)
         for L in layers:
             L.close()
 
@@ -951,16 +957,21 @@ def pyramid_job(a, w, h, steps, warmup, cpu=True):
     with ClockSampler(0) as clk:
         e0.record(stream)
         for _ in range(steps):
-            step()
+            step(timed=True)
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     launches = api.kernel_launches() - n0
+    ms_up = float(np.median([a.elapsed_time(b) for a, b in ups]))
+    up_bytes = 2 * w * 2 * h * 8 + w * h * 8  # DenseUpsampleLayer: full-size depth out + guide in, layer depth in + shifted copy
+    peak = float(peaks()["hbm_gbs"])
     ctx.close()
     de = sum(W * H * n for (W, H, n, *_) in info)
     res = {"workload": f"L16 pyramid on 5 colour cameras {w}x{h} + upsample to {2 * w}x{2 * h}", "ms_per_capture": ms,
            "captures_per_s": 1e3 / ms, "mde_per_s": de / (ms / 1e3) / 1e6, "gpu_launches": int(launches),
            "clocks": clk.summary(),
+           "upsample": {"ms": ms_up, "gb_per_s": up_bytes / ms_up / 1e6, "frac": up_bytes / ms_up / 1e6 / peak,
+                        "bytes": up_bytes, "note": "k_shift_resize + k_bilateral, of the measured HBM copy bandwidth"},
            "layers": [{"w": W, "h": H, "planes": n, "mean_cap": round(mc, 1), "sgm_kernel": sk, "cost_kernel": ck,
                        "ms_cost": round(c, 3), "ms_sgm": round(g, 3), "ms_wta": round(t, 3)}
                       for (W, H, n, sk, ck, c, g, t, mc) in info]}
