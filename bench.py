@@ -996,7 +996,7 @@ def run_pyramid(a):
             "unit": "captures/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": r["ms_per_capture"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 cost / u16 aggregation",
             "data": "synthetic (colour capture, planar scene 0.4-6 m, 8-40 mm baselines)",
-            "config": {"workload": r["workload"], "layers": r["layers"], "mde_per_s": r["mde_per_s"]},
+            "config": {"workload": r["workload"], "layers": r["layers"], "mde_per_s": r["mde_per_s"], "upsample": r["upsample"]},
             "gpu_launches": r["gpu_launches"], "clocks": r["clocks"]}
     if "cpu_baseline" in r:
         line["cpu_baseline"] = r["cpu_baseline"]

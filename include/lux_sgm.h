@@ -340,6 +340,11 @@ int lux_server_wait(lux_server* server, uint64_t ticket, uint64_t timeout_ns, lu
 int lux_server_estimate(const lux_request* req, uint64_t* bytes);
 /* How many requests started ahead of an earlier-queued one that had to wait (light requests passing a heavy one). */
 uint64_t lux_server_passed(const lux_server* server);
+/* Cancels a request that has not started: its lux_server_wait then reports status LUX_ERR_CANCELED
+ * (OperationCanceledException). The reference is cancelable between the states of a capture's registration, and a state
+ * once started runs to its end (StereoAsyncApi.cs:51-64); here a request that has started runs to its end and the call
+ * returns LUX_ERR_CANCELED without changing it. LUX_ERR_ARG for an unknown ticket. */
+int lux_server_cancel(lux_server* server, uint64_t ticket);
 /* The high-water mark of the device memory this library's allocations hold in the device's memory pool (the stream-
  * ordered pool every context allocates from), in bytes; reset != 0 resets it to the current use afterwards. */
 int lux_sgm_pool_high_water(int device, int32_t reset, uint64_t* bytes);

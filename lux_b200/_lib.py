@@ -142,6 +142,7 @@ SIGNATURES = [
     ("lux_server_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(Result)]),
     ("lux_server_estimate", ctypes.c_int, [ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]),
     ("lux_server_passed", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("lux_server_cancel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     ("lux_sgm_pool_high_water", ctypes.c_int, [ctypes.c_int, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
     ("lux_sgm_upsample_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.POINTER(Img), ctypes.c_int32, ctypes.c_int32, ctypes.c_float,

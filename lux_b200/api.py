@@ -37,9 +37,13 @@ class LuxIndexError(LuxError, IndexError):
     """The reference indexes outside an array for these inputs (IndexOutOfRangeException)."""
 
 
+class OperationCanceledError(LuxError):
+    """OperationCanceledException of the reference: a request canceled before it started."""
+
+
 _EXC = {1: InvalidOperationError, 2: InvalidOperationError, 3: InvalidOperationError, 6: InvalidOperationError,
-        4: NotSupportedError, 5: NotSupportedError, 7: LuxIndexError, 14: InvalidOperationError, 15: InvalidOperationError,
-        17: InvalidOperationError}
+        4: NotSupportedError, 5: NotSupportedError, 7: LuxIndexError, 13: OperationCanceledError, 14: InvalidOperationError,
+        15: InvalidOperationError, 17: InvalidOperationError}
 
 
 def _raise(code, msg):
@@ -833,6 +837,16 @@ class Server:
             _raise(rc, self.lib.lux_server_last_error(self.handle).decode())
         self._pending[t.value] = (out, keep, arr, g, cc)  # the image data and the output stay alive until wait
         return t.value
+
+    def cancel(self, ticket: int) -> bool:
+        """Cancels a request that has not started (its wait then reports status 13, LUX_ERR_CANCELED); returns False
+        when it has started already, which leaves it running to its end (a started state of the reference runs on)."""
+        rc = self.lib.lux_server_cancel(self.handle, ticket)
+        if rc == 13:
+            return False
+        if rc:
+            _raise(rc, self.lib.lux_server_last_error(self.handle).decode())
+        return True
 
     def wait(self, ticket: int, timeout_ns: int = 0) -> ServedResult:
         r = L.Result()

@@ -241,6 +241,32 @@ uint64_t lux_server_passed(const lux_server* s) {
   return s->passed;
 }
 
+int lux_server_cancel(lux_server* s, uint64_t ticket) {
+  if (!s) return LUX_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->results.find(ticket);
+    if (it == s->results.end()) {
+      s->last_error = "unknown ticket";
+      return LUX_ERR_ARG;
+    }
+    size_t i = 0;
+    while (i < s->queue.size() && s->queue[i].ticket != ticket) i++;
+    if (i == s->queue.size()) {  // running or finished: a started request runs to its end
+      s->last_error = "the request has started";
+      return LUX_ERR_CANCELED;
+    }
+    s->queue.erase(s->queue.begin() + (long)i);
+    lux_result r{};
+    r.status = LUX_ERR_CANCELED;
+    it->second.result = r;
+    it->second.done = true;
+  }
+  s->cv_done.notify_all();
+  s->cv_work.notify_all();  // a heavy request held back behind it may start now
+  return LUX_OK;
+}
+
 int lux_server_wait(lux_server* s, uint64_t ticket, uint64_t timeout_ns, lux_result* out) {
   if (!s) return LUX_ERR_ARG;
   std::unique_lock<std::mutex> lk(s->mu);

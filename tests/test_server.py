@@ -131,3 +131,37 @@ def test_estimate_covers_the_device_high_water():
             assert peak > 0 and est >= peak, (r[0][0].shape, est, peak)
     finally:
         ctx.close()
+
+
+def test_cancel_before_start():
+    """A queued request canceled before it starts reports LUX_ERR_CANCELED (OperationCanceledException); a finished one
+    is not changed (a started state of the reference runs to its end, StereoAsyncApi.cs:51-64); the rest run as if the
+    canceled one had never been submitted."""
+    from lux_b200 import api
+    heavy, light = _heavy_and_light()
+    ctx = api.Context(0)
+    solo = []
+    for r in light:
+        L = api.DenseLayer.compute(*r, prefilter=True, ctx=ctx)
+        solo.append(L.Depth.copy())
+        L.close()
+    ctx.close()
+    srv = api.Server(0, hbm_budget_bytes=0, slots=1)
+    try:
+        first = srv.submit(*heavy[0])  # occupies the only worker while the others queue
+        t = [srv.submit(*r) for r in light]
+        assert srv.cancel(t[1])
+        with pytest.raises(api.LuxError):
+            srv.cancel(123456789)  # unknown ticket
+        srv.wait(first)
+        res = {k: srv.wait(x) for k, x in enumerate(t) if k != 0}
+        assert not srv.cancel(t[0])  # finished (its wait not yet taken): left as it is
+        res[0] = srv.wait(t[0])
+    finally:
+        srv.close()
+    assert res[1].status == 13
+    for k in range(len(light)):
+        if k == 1:
+            continue
+        assert res[k].status == 0
+        assert np.array_equal(res[k].Depth.view(np.uint32), solo[k].view(np.uint32)), k
