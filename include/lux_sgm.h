@@ -114,9 +114,11 @@ int lux_sgm_box_filter3(lux_sgm_ctx* ctx, const lux_img_rgba8* src, uint8_t* dst
 #define LUX_LAYER_KEEP_AGG 2     /* keep the final aggregates (DenseLayer.Agg); the depth never needs them */
 #define LUX_LAYER_PREFILTER 4    /* images are unfiltered: apply DenseStereo.BoxFilter3 on the device first */
 #define LUX_LAYER_FORCE_REPLAY 8 /* aggregate with the exact traversal replay even where the fast uniform kernel applies */
-/* The fast uniform aggregation has two forms with the same results: the four paths fused in one wavefront (faster on
- * small layers) and the path groups {0,1} / {2,3} as row and column chains (faster from about 2 MP). By default the
- * library picks by size; these flags force one form (tuning and tests). */
+/* The fast uniform aggregation has three forms with the same results: the four paths fused in one wavefront (faster on
+ * small layers), the same in a lean form, and the path groups {0,1} / {2,3} as row and column chains (faster from about
+ * 2 MP). It takes uniform layers of up to 768 planes; past 256 planes (the L16 pyramid's first layer has 552) only the
+ * fused form runs them, whatever these flags ask. By default the library picks by timing (below); these flags force
+ * one form (tuning and tests). */
 #define LUX_LAYER_SGM_FUSED 16
 #define LUX_LAYER_SGM_SPLIT 32
 #define LUX_LAYER_SGM_WAVE 64    /* the fused wavefront in its lean form (progress counters, packed minima) */

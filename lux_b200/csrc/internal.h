@@ -161,6 +161,8 @@ struct UniformBuffers {
   void* events;         // host-built revisit schedule
 };
 size_t uniform_supported_planes();
+// Layers past 256 planes: only the fused form (k_sgm_uniform, LPT 16 or 24) runs them.
+bool uniform_wide_planes(int n_planes);
 bool uniform_fast_supported(int W, int H, int n_planes, int tile, uint16_t p1, float p2scale);
 size_t uniform_scratch_bytes(int W, int H, int n_planes, int tile);
 // Both passes, WTA into depth. agg holds pass +1's aggregates afterwards, and the final ones when keep_agg.

@@ -375,7 +375,9 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   CK(cudaEventRecord(ctx->ev[1], s));
   const int xsw = 0;  // LUX_SGM_XSW unset: the reference default (DenseStereoSgm.cs:31)
   if (fast) {
-    const int forced = (flags & LUX_LAYER_SGM_WAVE) ? 3 : (flags & LUX_LAYER_SGM_SPLIT) ? 2 : (flags & LUX_LAYER_SGM_FUSED) ? 1 : 0;
+    // past 256 planes the fused form is the only fast one: no tuning, and a requested chain or wave form runs fused
+    const bool wide = uniform_wide_planes(L->n);
+    const int forced = wide ? 1 : (flags & LUX_LAYER_SGM_WAVE) ? 3 : (flags & LUX_LAYER_SGM_SPLIT) ? 2 : (flags & LUX_LAYER_SGM_FUSED) ? 1 : 0;
     int form = forced;
     bool tune = false;
     if (!forced) {

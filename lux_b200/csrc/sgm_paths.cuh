@@ -69,6 +69,12 @@ LUX_DEV void vload(V<LPT>& v, const uint16_t* p, int lane) {
   } else if constexpr (LPT == 4) {
     uint2 t = __ldcg(reinterpret_cast<const uint2*>(q));
     v.r[0] = t.x; v.r[1] = t.y;
+  } else if constexpr (LPT % 8 == 0) {  // LPT > 8: one 16-byte load per octet of planes
+#pragma unroll
+    for (int o = 0; o < LPT / 8; o++) {
+      uint4 t = __ldcg(reinterpret_cast<const uint4*>(q) + o);
+      v.r[4 * o] = t.x; v.r[4 * o + 1] = t.y; v.r[4 * o + 2] = t.z; v.r[4 * o + 3] = t.w;
+    }
   } else {
     v.r[0] = __ldcg(q);
   }
@@ -78,7 +84,11 @@ LUX_DEV void vstore(const V<LPT>& v, uint16_t* p, int lane) {
   uint32_t* q = reinterpret_cast<uint32_t*>(p + lane * LPT);
   if constexpr (LPT == 8) __stcg(reinterpret_cast<uint4*>(q), make_uint4(v.r[0], v.r[1], v.r[2], v.r[3]));
   else if constexpr (LPT == 4) __stcg(reinterpret_cast<uint2*>(q), make_uint2(v.r[0], v.r[1]));
-  else __stcg(q, v.r[0]);
+  else if constexpr (LPT % 8 == 0) {
+#pragma unroll
+    for (int o = 0; o < LPT / 8; o++)
+      __stcg(reinterpret_cast<uint4*>(q) + o, make_uint4(v.r[4 * o], v.r[4 * o + 1], v.r[4 * o + 2], v.r[4 * o + 3]));
+  } else __stcg(q, v.r[0]);
 }
 template <int LPT>
 LUX_DEV void vload_s(V<LPT>& v, const uint16_t* p, int lane) {  // shared memory
@@ -98,10 +108,20 @@ LUX_DEV void vinit(V<LPT>& v) {
   for (int i = 0; i < LPT / 2; i++) v.r[i] = kInit2;
 }
 
+// A lane's planes in use, counted in octets (the plane count is a multiple of 8): the `active` argument of the helpers
+// below. A lane of LPT <= 8 planes holds at most one octet, so it is 0 or 1 (any true value); past 256 planes (LPT 16 or
+// 24) the last lane below the plane count may hold padding octets after its planes. Word i of a lane (planes 2i, 2i+1)
+// is in use when i / 4 < active.
+template <int LPT>
+LUX_DEV int lane_octets(int n, int lane) {
+  if constexpr (LPT <= 8) return lane * LPT < n ? 1 : 0;
+  else return max(0, min(LPT / 8, (n - lane * LPT) / 8));
+}
+
 // One path step (DenseStereoSgm.cs:276-313) for a lane's planes. nb: the neighbour's L (2000 past the plane range),
 // mp: its minimum, p2p: min(P2 + mp, 65535). Returns the new L; adds lc to acc; folds lc into rmin.
 template <int LPT>
-LUX_DEV void path_step(const V<LPT>& nb, uint32_t mp, uint32_t p2p, uint32_t p1x2, const V<LPT>& raw2, bool active, int lane,
+LUX_DEV void path_step(const V<LPT>& nb, uint32_t mp, uint32_t p2p, uint32_t p1x2, const V<LPT>& raw2, int active, int lane,
                        V<LPT>& out, V<LPT>& acc, uint32_t& rmin) {
   constexpr int NR = LPT / 2;
   uint32_t prev = __shfl_up_sync(0xffffffffu, nb.r[NR - 1], 1);
@@ -119,7 +139,7 @@ LUX_DEV void path_step(const V<LPT>& nb, uint32_t mp, uint32_t p2p, uint32_t p1x
     uint32_t t = vmin2(lm[i], lm[i + 1]) + p1x2;       // min(L[d-1], L[d+1]) + P1
     t = vmin2(vmin2(t, nb.r[i]), p2x2);                 // with L[d] and P2 + minPrev
     uint32_t lc = t + raw2.r[i] - mp2;                   // raw + m - minPrev, each half in [0, 2000)
-    lc = active ? lc : kInit2;                           // padding lanes keep 2000
+    lc = (i >> 2) < active ? lc : kInit2;                // padding planes keep 2000
     out.r[i] = lc;
     rmin = vmin2(rmin, lc);
     acc.r[i] += lc;
@@ -136,7 +156,7 @@ LUX_DEV uint32_t warp_min(uint32_t rmin) {  // min over both halves and all lane
 // first, then the min/add chains, then the four warp minima. nb[p]/mp[p]: neighbour L and minimum of path p; p2[p]: P2.
 template <int LPT, bool FULL>
 LUX_DEV void four_paths(const V<LPT> (&nb)[4], const uint32_t (&mp)[4], const uint32_t (&p2)[4], uint32_t p1x2, const V<LPT>& raw2,
-                        bool active, int lane, V<LPT> (&out)[4], V<LPT>& acc, uint32_t (&mins)[4]) {
+                        int active, int lane, V<LPT> (&out)[4], V<LPT>& acc, uint32_t (&mins)[4]) {
   constexpr int NR = LPT / 2;
   uint32_t prev[4], next[4];
 #pragma unroll
@@ -160,7 +180,7 @@ LUX_DEV void four_paths(const V<LPT> (&nb)[4], const uint32_t (&mp)[4], const ui
       uint32_t t = vmin2(lm, lp) + p1x2;
       t = vmin2(vmin2(t, nb[p].r[i]), dup16(p2[p] + mp[p]));  // P2 <= 1744 and minPrev <= 2000: no u16 overflow
       uint32_t lc = t + raw2.r[i] - dup16(mp[p]);  // raw + m - minPrev, each half in [0, 2000)
-      if (!FULL) lc = active ? lc : kInit2;          // padding lanes keep 2000
+      if (!FULL) lc = (i >> 2) < active ? lc : kInit2;  // padding planes keep 2000
       out[p].r[i] = lc;
       rmin[p] = vmin2(rmin[p], lc);
       acc.r[i] += lc;
@@ -230,7 +250,7 @@ LUX_DEV void cs_put(const UniArgs& a, const V<LPT>& L, uint32_t mn, int row, int
 }
 
 template <int LPT>
-LUX_DEV void load_raw(const UniArgs& a, int xm, int ym, V<LPT>& raw2, bool active, int lane) {
+LUX_DEV void load_raw(const UniArgs& a, int xm, int ym, V<LPT>& raw2, int active, int lane) {
   const int x = a.dir > 0 ? xm : a.W - 1 - xm, y = a.dir > 0 ? ym : a.H - 1 - ym;
   const uint8_t* p = a.raw + ((size_t)y * a.W + x) * a.n + lane * LPT;
   if (!active) {
@@ -245,6 +265,13 @@ LUX_DEV void load_raw(const UniArgs& a, int xm, int ym, V<LPT>& raw2, bool activ
   } else if constexpr (LPT == 4) {
     uint32_t b = __ldcs(reinterpret_cast<const unsigned int*>(p));
     raw2.r[0] = __byte_perm(b, 0, 0x4140); raw2.r[1] = __byte_perm(b, 0, 0x4342);
+  } else if constexpr (LPT % 8 == 0) {  // LPT > 8: the octets in use, 8 bytes each
+#pragma unroll
+    for (int o = 0; o < LPT / 8; o++) {
+      uint2 b = o < active ? __ldcs(reinterpret_cast<const uint2*>(p) + o) : make_uint2(0u, 0u);
+      raw2.r[4 * o] = __byte_perm(b.x, 0, 0x4140); raw2.r[4 * o + 1] = __byte_perm(b.x, 0, 0x4342);
+      raw2.r[4 * o + 2] = __byte_perm(b.y, 0, 0x4140); raw2.r[4 * o + 3] = __byte_perm(b.y, 0, 0x4342);
+    }
   } else {
     uint32_t b = __ldcs(reinterpret_cast<const unsigned short*>(p));
     raw2.r[0] = __byte_perm(b, 0, 0x4140);
@@ -257,7 +284,7 @@ LUX_DEV uint16_t* agg_ptr(const UniArgs& a, int xm, int ym, int lane) {
   return a.agg + ((size_t)y * a.W + x) * a.n + lane * LPT;
 }
 template <int LPT>
-LUX_DEV void agg_load(const uint16_t* p, V<LPT>& v, bool active) {
+LUX_DEV void agg_load(const uint16_t* p, V<LPT>& v, int active) {
   if (!active) {
 #pragma unroll
     for (int i = 0; i < LPT / 2; i++) v.r[i] = 0;
@@ -269,25 +296,36 @@ LUX_DEV void agg_load(const uint16_t* p, V<LPT>& v, bool active) {
   } else if constexpr (LPT == 4) {
     uint2 t = __ldcs(reinterpret_cast<const uint2*>(p));
     v.r[0] = t.x; v.r[1] = t.y;
+  } else if constexpr (LPT % 8 == 0) {  // LPT > 8: the octets in use (a padding octet would read the next pixel's planes)
+#pragma unroll
+    for (int o = 0; o < LPT / 8; o++) {
+      uint4 t = o < active ? __ldcs(reinterpret_cast<const uint4*>(p) + o) : make_uint4(0u, 0u, 0u, 0u);
+      v.r[4 * o] = t.x; v.r[4 * o + 1] = t.y; v.r[4 * o + 2] = t.z; v.r[4 * o + 3] = t.w;
+    }
   } else {
     v.r[0] = __ldcs(reinterpret_cast<const unsigned int*>(p));
   }
 }
 template <int LPT>
-LUX_DEV void agg_store(uint16_t* p, const V<LPT>& v, bool active) {
+LUX_DEV void agg_store(uint16_t* p, const V<LPT>& v, int active) {
   if (!active) return;
   if constexpr (LPT == 8) __stcs(reinterpret_cast<uint4*>(p), make_uint4(v.r[0], v.r[1], v.r[2], v.r[3]));
   else if constexpr (LPT == 4) __stcs(reinterpret_cast<uint2*>(p), make_uint2(v.r[0], v.r[1]));
-  else __stcs(reinterpret_cast<unsigned int*>(p), v.r[0]);
+  else if constexpr (LPT % 8 == 0) {  // LPT > 8: the octets in use only (the next pixel's planes follow)
+#pragma unroll
+    for (int o = 0; o < LPT / 8; o++)
+      if (o < active) __stcs(reinterpret_cast<uint4*>(p) + o, make_uint4(v.r[4 * o], v.r[4 * o + 1], v.r[4 * o + 2], v.r[4 * o + 3]));
+  } else __stcs(reinterpret_cast<unsigned int*>(p), v.r[0]);
 }
 
 // First minimum of the lane's planes, then over the warp (DenseStereoSgm.cs:228-230): key = value·4096 + plane.
 template <int LPT>
-LUX_DEV int wta_arg(const V<LPT>& agg, bool active, int lane) {
+LUX_DEV int wta_arg(const V<LPT>& agg, int active, int lane) {
   uint32_t best = 0xffffu, arg = 0xfffu;
   if (active) {
 #pragma unroll
     for (int i = 0; i < LPT / 2; i++) {
+      if ((i >> 2) >= active) break;  // padding planes of the lane
       uint32_t lo = agg.r[i] & 0xffffu, hi = agg.r[i] >> 16;
       if (lo < best) { best = lo; arg = lane * LPT + 2 * i; }
       if (hi < best) { best = hi; arg = lane * LPT + 2 * i + 1; }
@@ -297,24 +335,27 @@ LUX_DEV int wta_arg(const V<LPT>& agg, bool active, int lane) {
   return key >= (0xffffu << 12) ? 0 : (int)(key & 0xfffu);
 }
 
-// Raw bytes of a lane's planes as loaded (8, 4 or 2 bytes), unpacked to u16 pairs when used.
+// Raw bytes of a lane's planes as loaded (LPT, 4 or 2 bytes), unpacked to u16 pairs when used.
 template <int LPT>
 struct RawB {
-  uint32_t r[LPT >= 8 ? 2 : 1];
+  uint32_t r[LPT >= 8 ? LPT / 4 : 1];
 };
 template <int LPT>
 LUX_DEV void raw_unpack(const RawB<LPT>& b, V<LPT>& raw2) {
   raw2.r[0] = __byte_perm(b.r[0], 0, 0x4140);
   if constexpr (LPT >= 4) raw2.r[1] = __byte_perm(b.r[0], 0, 0x4342);
-  if constexpr (LPT == 8) {
-    raw2.r[2] = __byte_perm(b.r[1], 0, 0x4140);
-    raw2.r[3] = __byte_perm(b.r[1], 0, 0x4342);
+  if constexpr (LPT >= 8) {
+#pragma unroll
+    for (int w = 1; w < LPT / 4; w++) {
+      raw2.r[2 * w] = __byte_perm(b.r[w], 0, 0x4140);
+      raw2.r[2 * w + 1] = __byte_perm(b.r[w], 0, 0x4342);
+    }
   }
 }
 
 // A revisit R(c, y) (DenseStereoSgm.cs:234-317 replayed at the last column), run by one warp.
 template <int LPT>
-LUX_DEV void run_revisit(const UniArgs& a, int y, int lane, bool active) {
+LUX_DEV void run_revisit(const UniArgs& a, int y, int lane, int active) {
   const int c = a.W - 1;
   Src<LPT> s[4];
   const int e[3] = {a.src0[y], a.src1[y], a.src2[y]};

@@ -28,16 +28,26 @@
 
 namespace lux {
 
-constexpr int kRows = 14;      // rows of the recurrence per block (one warp each)
-constexpr int kWarps = kRows + 2;  // plus the loader and the publisher warps
+// kRows: rows of the recurrence per block (one warp each), kWarps: plus the loader and the publisher warps, kRing: slots
+// of the hand-over ring between neighbouring rows of a block. Past 256 planes (LPT 16 or 24) a ring slot holds 32·LPT
+// planes of three paths, so the block runs 4 rows to keep its rings in an SM's shared memory (184 KB at LPT 24). The
+// ring keeps 8 slots: the loader frees a batch of 4 slots before it fills them, which a ring of 4 could never do while
+// row 0 holds the slots of the pixels it reads.
+template <int LPT>
+struct UniCfg {
+  static constexpr int kRows = LPT > 8 ? 4 : 14;
+  static constexpr int kRing = 8;
+  static constexpr int kWarps = kRows + 2;
+};
+constexpr int uni_rows(int lpt) { return lpt > 8 ? UniCfg<16>::kRows : UniCfg<8>::kRows; }
 constexpr int kBandBufs = 4;   // band buffers in rotation
-constexpr int kRing = 8;       // slots of the hand-over ring between neighbouring rows of a block
 constexpr int kPublish = 8;    // the publisher releases the global band progress every kPublish pixels
 
 // Shared memory of a block: kRows + 1 hand-over rings (ring kRows is the row above the block, filled by the loader warp),
 // their minima, and a full and an empty mbarrier per ring slot.
 template <int LPT>
 constexpr size_t ring_bytes() {
+  constexpr int kRows = UniCfg<LPT>::kRows, kRing = UniCfg<LPT>::kRing;
   return (size_t)(kRows + 1) * kRing * 3 * Dp_of(LPT) * 2 + (size_t)(kRows + 1) * kRing * 3 * 2 + 16 +
          (size_t)2 * (kRows + 1) * kRing * 8;
 }
@@ -90,8 +100,10 @@ LUX_DEV void row_above(const UniArgs& a, const uint16_t* bnd_up, const uint16_t*
 // waits only on its neighbours (shared-memory acquire/release), so the global latencies of the block boundary stay
 // off the rows' own critical path.
 template <int LPT, bool FULL, bool PASS2>
-__global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a) {
+__global__ void __launch_bounds__(UniCfg<LPT>::kWarps * 32, 1) k_sgm_uniform(const UniArgs a) {
   constexpr int NR = LPT / 2, Dp = Dp_of(LPT), kBatch = 4;
+  constexpr int kRows = UniCfg<LPT>::kRows, kRing = UniCfg<LPT>::kRing, kWarps = UniCfg<LPT>::kWarps;
+  static_assert(kBatch < kRing, "the loader frees a batch of slots before filling them");
   extern __shared__ __align__(16) uint16_t smem_ring[];
   auto ring = [&](int set, int slot, int p) { return smem_ring + (((size_t)set * kRing + slot) * 3 + p) * Dp; };
   uint16_t* ring_min = smem_ring + (size_t)(kRows + 1) * kRing * 3 * Dp;
@@ -102,7 +114,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
   auto empty = [&](int set, int slot) { return bars + (kRows + 1) * kRing + set * kRing + slot; };
   __shared__ int s_cb;
   __shared__ volatile int s_stop;
-  __shared__ float s_planes[256];  // the WTA's plane depths (pass -1)
+  __shared__ float s_planes[LPT > 8 ? 32 * LPT : 256];  // the WTA's plane depths (pass -1)
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   if (PASS2)
     for (int i = tid; i < a.n; i += blockDim.x) s_planes[i] = a.planes[i];
@@ -116,7 +128,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
   const int cb = s_cb;
   const int y0 = cb * kRows;
   const bool below_exists = y0 + kRows < a.H;  // a block below reads this block's last row
-  const bool active = FULL || lane * LPT < a.n;
+  const int active = FULL ? (LPT > 8 ? LPT / 8 : 1) : lane_octets<LPT>(a.n, lane);  // planes in use, in octets
   const uint16_t* bnd_up = a.bnd + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3 * Dp;
   const uint16_t* bnd_up_min = a.bnd_min + (size_t)((cb + kBandBufs - 1) % kBandBufs) * a.W * 3;
   uint16_t* bnd_me = a.bnd + (size_t)(cb % kBandBufs) * a.W * 3 * Dp;
@@ -223,7 +235,14 @@ __global__ void __launch_bounds__(kWarps * 32, 1) k_sgm_uniform(const UniArgs a)
   auto fetch = [&](int xq, Queued& q) {
     const int off = col_of(xq) * a.n;
     const uint8_t* rp = raw_row + off;
-    if (!active) {
+    if constexpr (LPT > 8) {  // the octets in use, 8 bytes each
+#pragma unroll
+      for (int o = 0; o < LPT / 8; o++) {
+        const uint2 t = o < active ? __ldcs(reinterpret_cast<const uint2*>(rp) + o) : make_uint2(0u, 0u);
+        q.raw.r[2 * o] = t.x;
+        q.raw.r[2 * o + 1] = t.y;
+      }
+    } else if (!active) {
       q.raw.r[0] = 0;
       if constexpr (LPT >= 8) q.raw.r[1] = 0;
     } else if constexpr (LPT == 8) {
@@ -384,12 +403,13 @@ void launch_wta_column(const uint16_t* agg, int W, int H, int n, const float* pl
   count_launches(1);
 }
 
-size_t uniform_supported_planes() { return 256; }
+size_t uniform_supported_planes() { return 256; }  // the chain and wave forms; the fused form takes up to 768
+bool uniform_wide_planes(int n) { return n > 256; }
 
-static int lpt_for(int n) { return n <= 64 ? 2 : n <= 128 ? 4 : 8; }
+static int lpt_for(int n) { return n <= 64 ? 2 : n <= 128 ? 4 : n <= 256 ? 8 : n <= 512 ? 16 : 24; }
 
 bool uniform_fast_supported(int W, int H, int n, int tile, uint16_t p1, float p2scale) {
-  if (n <= 0 || n > 256 || (n & 7) != 0) return false;
+  if (n <= 0 || n > 768 || (n & 7) != 0) return false;  // past 256 planes the fused form only (uniform_wide_planes)
   if ((tile & 1) != 0 || tile < 2) return false;  // a row's half of the line buffer is its parity only for even tiles
   if (W < 3 || H < 2) return false;
   volatile float p1f = (float)p1;
@@ -404,7 +424,8 @@ struct UniScratchLayout {
 
 static UniScratchLayout layout_of(int W, int H, int n) {
   const size_t Dp = 32 * (size_t)lpt_for(n);
-  const int nCB = (H + kRows - 1) / kRows;
+  const int rows = uni_rows(lpt_for(n));
+  const int nCB = (H + rows - 1) / rows;
   auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
   UniScratchLayout L;
   size_t o = 0;
@@ -433,7 +454,7 @@ static void launch_pass_t(const UniArgs& a, cudaStream_t s) {
     cudaFuncSetAttribute(k_sgm_uniform<LPT, FULL, PASS2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring_bytes<LPT>());
     configured = true;
   }
-  k_sgm_uniform<LPT, FULL, PASS2><<<a.nCB, kWarps * 32, ring_bytes<LPT>(), s>>>(a);
+  k_sgm_uniform<LPT, FULL, PASS2><<<a.nCB, UniCfg<LPT>::kWarps * 32, ring_bytes<LPT>(), s>>>(a);
   count_launches(1);
 }
 template <int LPT>
@@ -468,7 +489,8 @@ int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, con
   }
   int* dsched = reinterpret_cast<int*>(base + L.sched);
   if (cudaMemcpyAsync(dsched, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return 10;
-  const int nCB = (H + kRows - 1) / kRows;
+  const int rows = uni_rows(lpt_for(n));
+  const int nCB = (H + rows - 1) / rows;
   int* progress = reinterpret_cast<int*>(base + L.progress);
   cudaMemsetAsync(progress, 0, (size_t)(nCB + 2) * 4 * 2, s);
   UniArgs a;
@@ -509,7 +531,9 @@ int run_sgm_uniform(const LayerGeom& g, int xsw, uint16_t p1, float p2scale, con
     count_launches(1);
     if (lpt == 2) launch_pass<2>(a, s);
     else if (lpt == 4) launch_pass<4>(a, s);
-    else launch_pass<8>(a, s);
+    else if (lpt == 8) launch_pass<8>(a, s);
+    else if (lpt == 16) launch_pass<16>(a, s);
+    else launch_pass<24>(a, s);
     if (pass == 0 && agg_pass1) cudaMemcpyAsync(agg_pass1, agg, (size_t)W * H * n * 2, cudaMemcpyDeviceToDevice, s);
   }
   k_wta_column<<<(H * 32 + 255) / 256, 256, 0, s>>>(agg, W, H, n, 0, g.planes, depth);

@@ -87,6 +87,24 @@ def test_replay_barrier_form_bit_exact(ctx, oracle, w, h, d, tile):
         gl.close()
 
 
+@pytest.mark.parametrize("w,h,d,tile", [(600, 40, 264, 8), (520, 48, 400, 16), (700, 30, 552, 4), (300, 20, 768, 2)])
+def test_wide_uniform_layer_fused_bit_exact(ctx, oracle, w, h, d, tile):
+    """Uniform layers past 256 planes (the L16 pyramid's first layer has 552) on the fused fast kernel, a lane holding 16
+    or 24 planes with the padding octets of the last lane masked; a chain or wave form asked for runs fused there."""
+    from lux_b200 import api, synth
+    wl = synth.rectified_pair(w, h, d, seed=d + tile, tile=tile)
+    filt = _filtered(oracle, wl.images)
+    ol = oracle.layer(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True)
+    for sgm in ("auto", "split"):
+        gl = api.DenseLayer.compute(filt, wl.gray, wl.calibs, wl.near, wl.far, wl.params, keep_pass1=True, keep_agg=True,
+                                    sgm=sgm, ctx=ctx)
+        try:
+            assert gl.n_planes == d and gl.sgm_kernel == SGM_FORMS["fused"]
+            _compare_layer(gl, ol, f"{w}x{h} D{d} T{tile} fused ({sgm})")
+        finally:
+            gl.close()
+
+
 @pytest.mark.parametrize("w,h,d,tile", [(120, 90, 24, 20), (150, 100, 16, 34), (140, 130, 16, 50)])
 def test_replay_partial_last_part_bit_exact(ctx, oracle, w, h, d, tile):
     """The row form splits a band into parts of min(8, T/2) rows; these tiles leave a shorter last part (T = 20: 8 + 8 +
