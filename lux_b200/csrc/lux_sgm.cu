@@ -450,6 +450,8 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   const int bands = (H + p.tile - 1) / p.tile;
   EmuBuffers eb;
   eb.Llen = emu_line_buffer_elems(W, L->max_hi);
+  if (eb.Llen > (size_t)INT_MAX - 65536)  // the replay indexes its line buffer with 32-bit integers
+    return set_err(ctx, LUX_ERR_UNSUPPORTED, "the exact replay's line buffer of %zu elements is past 32-bit indexing", eb.Llen);
   if ((rc = alloc_t(ctx, tmp, eb.Llen, &eb.L))) return rc;
   if ((rc = alloc_t(ctx, tmp, (size_t)2 * (W + 2) * 4, &eb.Min))) return rc;
   if ((rc = alloc_t(ctx, tmp, (size_t)2 * (W + 2), &eb.RangeS))) return rc;

@@ -30,7 +30,7 @@ namespace lux {
 struct EmuArgs {
   int W, H, T, dir, xsw, min_lo, max_hi, slot_stride, halfL, halfM, halfR, gwN, ghN;
   int parts, part_rows;  // blocks per band and rows per block
-  long long Llen;
+  int Llen;  // line-buffer elements; the host keeps it below 2^31 - 2^16, so every index of it fits 32 bits
   uint16_t* L;
   uint16_t* Min;
   uint16_t* RangeS;
@@ -55,23 +55,23 @@ struct EmuArgs {
   const int* never;
 };
 
-LUX_DEV int rd(const EmuArgs& a, long long i) {  // Rd (DenseStereoSgm.cs:324)
+LUX_DEV int rd(const EmuArgs& a, int i) {  // Rd (DenseStereoSgm.cs:324)
   return i < 0 ? 2000 : i < a.Llen ? (int)__ldcg(a.L + i) : 0;
 }
 
 // One path of a Pixel() call (:276-314) over its cap planes, a lane per plane, each index through Rd's bounds and each
 // write checked: the form for windows that reach past the buffer. Returns the lane's running minimum.
-LUX_DEV int emu_path_checked(const EmuArgs& a, long long nb, long long baseCur, long long q, int cap, int count, bool skipped,
+LUX_DEV int emu_path_checked(const EmuArgs& a, int nb, int baseCur, int q, int cap, int count, bool skipped,
                              const uint8_t* rawp, uint16_t* aggp, int P2p, int minPrev, int lane) {
   int runMin = 0xffff;
   for (int k = lane; k < cap; k += 32) {
-    const long long qi = q + k;
+    const int qi = q + k;
     const int Lm = rd(a, nb + qi - 1), L0 = rd(a, nb + qi), Lp = rd(a, nb + qi + 1);
     const int m = min(min(min(Lm + a.p1, 65535), L0), min(min(Lp + a.p1, 65535), P2p));
     const int rv = skipped ? (k < count ? 0 : 255) : rawp[k];
     int lc = min(rv + m, 65535) - minPrev;
     if (lc < 0) lc = 0;
-    const long long wi = baseCur + qi;
+    const int wi = baseCur + qi;
     if (wi < 0 || wi >= a.Llen) atomicCAS(a.err, 0, 7);
     else __stcg(a.L + wi, (uint16_t)lc);
     runMin = min(runMin, lc);
@@ -157,11 +157,11 @@ LUX_DEV void emu_group_load1(const uint16_t* Ln, int cap, int count, bool skippe
 // commute, min(min(a + x, C) + y, C) = min(a + x + y, C). Caps are multiples of 8 here (checked before the launch), so
 // every lane of a chunk has a plane.
 template <int KBG, int NR>
-LUX_DEV void emu_pixel_grouped1(const EmuArgs& a, long long baseCur, long long q, long long q0, int cap, int cp, uint16_t* aggp,
+LUX_DEV void emu_pixel_grouped1(const EmuArgs& a, int baseCur, int q, int q0, int cap, int cp, uint16_t* aggp,
                                 int P2p, int minPrev, uint16_t* minOut, int lane, const int (&R)[NR]) {
   const int j = lane & 7, grp = lane >> 3;
-  for (long long k = (q0 < 0 ? -q0 : 0) + j; k < cp; k += 8) {  // stale cleanup (:261-263), outside the new range
-    const long long idx = q0 + k;
+  for (int k = (q0 < 0 ? -q0 : 0) + j; k < cp; k += 8) {  // stale cleanup (:261-263), outside the new range
+    const int idx = q0 + k;
     if (idx < q || idx >= q + cap) __stcg(a.L + baseCur + idx, (uint16_t)2000);
   }
   uint16_t* Lw = a.L + (baseCur + q);
@@ -190,7 +190,7 @@ LUX_DEV void emu_pixel_grouped1(const EmuArgs& a, long long baseCur, long long q
 // The path-serial form in one batch (cap <= 32·CH - 2): R[p·CH + c] holds element 32c + lane - 1 of path p's read window
 // Ln_p[-1 .. cap], R[4·CH + c] the raw cost and R[5·CH + c] the aggregate of plane 32c + lane.
 template <int CH, int NR>
-LUX_DEV void emu_serial_load1(const uint16_t* L, const long long (&win)[4], int cap, int count, bool skipped, const uint8_t* rawp,
+LUX_DEV void emu_serial_load1(const uint16_t* L, const int (&win)[4], int cap, int count, bool skipped, const uint8_t* rawp,
                               const uint16_t* aggp, int lane, int (&R)[NR]) {
   static_assert(6 * CH <= NR, "register batch too small");
 #pragma unroll
@@ -211,15 +211,15 @@ LUX_DEV void emu_serial_load1(const uint16_t* L, const long long (&win)[4], int 
 // by the caller: q + cap + 2 <= slot stride). The aggregate takes the four paths' sum at once (saturating adds of
 // non-negative terms commute).
 template <int CH, int NR>
-LUX_DEV void emu_pixel_serial1(const EmuArgs& a, int cur, int slot, long long q, int sp, int cp, int cap, uint16_t* aggp,
+LUX_DEV void emu_pixel_serial1(const EmuArgs& a, int cur, int slot, int q, int sp, int cp, int cap, uint16_t* aggp,
                                int gMinPrev, int gP2, int lane, int (&R)[NR]) {
 #pragma unroll
   for (int p = 0; p < 4; p++) {
-    const long long baseCur = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
+    const int baseCur = (int)cur * a.halfL + (int)slot * a.slot_stride + 1 + (int)p * (a.max_hi + 1);
     {  // stale cleanup of the previously stored range (:261-263)
-      const long long q0 = sp - a.min_lo, k0 = q0 < 0 ? -q0 : 0;
-      const long long k1 = min((long long)cp, a.Llen - baseCur - q0);
-      for (long long k = k0 + lane; k < k1; k += 32) __stcg(a.L + baseCur + q0 + k, (uint16_t)2000);
+      const int q0 = sp - a.min_lo, k0 = q0 < 0 ? -q0 : 0;
+      const int k1 = min((int)cp, a.Llen - baseCur - q0);
+      for (int k = k0 + lane; k < k1; k += 32) __stcg(a.L + baseCur + q0 + k, (uint16_t)2000);
     }
     __syncwarp();
     const int minPrev = __shfl_sync(0xffffffffu, gMinPrev, 8 * p), P2 = __shfl_sync(0xffffffffu, gP2, 8 * p);
@@ -291,22 +291,22 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, const EmuPix& px, int cur, int o
   const int ghalf = gp == 0 ? cur : other;
   const int gMinPrev = __ldcg(a.Min + ghalf * a.halfM + gns * 4 + gp);
   const float4 pn4 = __ldcg(a.Pix + ghalf * a.halfR + gns);
-  const long long q = start - a.min_lo;
-  const long long gnb = (long long)ghalf * a.halfL + (long long)gns * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
+  const int q = start - a.min_lo;
+  const int gnb = (int)ghalf * a.halfL + (int)gns * a.slot_stride + 1 + (int)gp * (a.max_hi + 1);
   // The grouped form needs every write window inside its own block and every read inside the buffer (checked here) and
   // the cleanup window inside its block (checked once the Range entries are in). The path-serial batch needs its four
   // read windows and write ranges inside the buffer and clear of each other.
   const bool grouped = cap <= 8 * KBG && q + cap <= a.max_hi + 1 && __all_sync(0xffffffffu, gnb + q + cap + 1 <= a.Llen);
   bool serial = false;
-  long long win[4];
+  int win[4];
   if (!grouped) {
-    const long long own = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1;
+    const int own = (int)cur * a.halfL + (int)slot * a.slot_stride + 1;
     serial = cap <= 32 * CH - 2 && q + cap + 2 <= a.slot_stride;
 #pragma unroll
     for (int p = 0; p < 4; p++) {
       const int ns = slot + (p == 2 ? 0 : p == 3 ? a.dir : -a.dir);
-      const long long nb = (long long)(p == 0 ? cur : other) * a.halfL + (long long)ns * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
-      const long long wb = own + (long long)p * (a.max_hi + 1) + q;
+      const int nb = (int)(p == 0 ? cur : other) * a.halfL + (int)ns * a.slot_stride + 1 + (int)p * (a.max_hi + 1);
+      const int wb = own + (int)p * (a.max_hi + 1) + q;
       win[p] = nb + q;
       serial = serial && nb + q - 1 >= 0 && nb + q + cap + 1 <= a.Llen && wb >= 0 && wb + cap <= a.Llen;
     }
@@ -323,9 +323,9 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, const EmuPix& px, int cur, int o
   }
   bool done = false;
   if (grouped) {
-    const long long q0 = sp - a.min_lo;
+    const int q0 = sp - a.min_lo;
     if (cp == 0 || q0 + cp <= a.max_hi + 1) {
-      const long long gbase = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)gp * (a.max_hi + 1);
+      const int gbase = (int)cur * a.halfL + (int)slot * a.slot_stride + 1 + (int)gp * (a.max_hi + 1);
       emu_pixel_grouped1<KBG>(a, gbase, q, q0, cap, cp, aggp, min(gP2 + gMinPrev, 65535), gMinPrev,
                               a.Min + cur * a.halfM + slot * 4 + gp, lane, R);
       done = true;
@@ -344,11 +344,11 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, const EmuPix& px, int cur, int o
   }
 #pragma unroll 1
   for (int p = 0; p < 4; p++) {
-    const long long baseCur = (long long)cur * a.halfL + (long long)slot * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
+    const int baseCur = (int)cur * a.halfL + (int)slot * a.slot_stride + 1 + (int)p * (a.max_hi + 1);
     {  // stale cleanup of the previously stored range (:261-263)
-      long long q0 = sp - a.min_lo, k0 = q0 < 0 ? -q0 : 0;
-      long long k1 = min((long long)cp, a.Llen - baseCur - q0);
-      for (long long k = k0 + lane; k < k1; k += 32) __stcg(a.L + baseCur + q0 + k, (uint16_t)2000);
+      int q0 = sp - a.min_lo, k0 = q0 < 0 ? -q0 : 0;
+      int k1 = min((int)cp, a.Llen - baseCur - q0);
+      for (int k = k0 + lane; k < k1; k += 32) __stcg(a.L + baseCur + q0 + k, (uint16_t)2000);
     }
     __syncwarp();
     const int ns = slot + (p == 2 ? 0 : p == 3 ? a.dir : -a.dir);
@@ -361,8 +361,8 @@ LUX_DEV void emu_pixel(const EmuArgs& a, int x, const EmuPix& px, int cur, int o
       __syncwarp();
       continue;
     }
-    const long long nb = (long long)half * a.halfL + (long long)ns * a.slot_stride + 1 + (long long)p * (a.max_hi + 1);
-    const long long q = start - a.min_lo;
+    const int nb = (int)half * a.halfL + (int)ns * a.slot_stride + 1 + (int)p * (a.max_hi + 1);
+    const int q = start - a.min_lo;
     // A path reads L[nb + q - 1 .. nb + q + cap] and writes L[baseCur + q .. baseCur + q + cap - 1]. The bases lie a
     // whole half apart (paths 1-3) or one slot stride apart (path 0), so the windows meet only if cap + 2 exceeds the
     // slot stride (4·MaxHi + 5). Where they stay apart and inside the buffer, the batched form runs; otherwise one plane
@@ -615,7 +615,7 @@ void launch_sgm_emulate(const LayerGeom& g, const EmuBuffers& b, int dir, int xs
   a.halfR = g.W + 2;
   a.gwN = (g.W + 2 * g.tile - 1) / g.tile;
   a.ghN = (g.H + g.tile - 1) / g.tile;
-  a.Llen = (long long)b.Llen;
+  a.Llen = (int)b.Llen;
   a.L = b.L; a.Min = b.Min; a.RangeS = b.RangeS; a.RangeC = b.RangeC; a.Pix = b.Pix;
   a.guidance = g.guidance; a.skip = g.skip; a.start = g.start; a.count = g.count; a.cap = g.cap; a.off = g.off;
   a.raw = raw; a.agg = agg;
