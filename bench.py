@@ -70,8 +70,9 @@ def args_():
                    help="the served mixed request stream (Poisson arrivals of preview pairs, 13 MP pairs and module captures) "
                         "through the request server, against the plain one-request-at-a-time path on the same arrivals")
     p.add_argument("--requests", type=int, default=400)
-    p.add_argument("--rate", type=float, default=60.0,
-                   help="mean arrivals per second of the served stream (60/s: above what one request at a time keeps up with)")
+    p.add_argument("--rate", type=float, default=40.0,
+                   help="mean arrivals per second of the served stream (40/s: below what one request at a time keeps up "
+                        "with, about 53/s, so the latencies compare the serving forms, not a growing backlog)")
     p.add_argument("--slots", type=int, default=2,
                    help="worker contexts of the request server (2 measured best: 3 stretches large requests' tails)")
     p.add_argument("--sweep", action="store_true",
@@ -409,9 +410,11 @@ def serve_stream(a):
 
     def served():
         srv = api.Server(0, hbm_budget_bytes=120 * 10**9, slots=a.slots)
-        for kind in pool:  # the worker contexts' first solves (module loading, pools) are not part of the stream
-            for r in pool[kind]:
-                srv.wait(srv.submit(r[0], *r[1:6]))
+        # the worker contexts' first solves (module loading) and the memory pool's growth to what concurrent requests
+        # hold are not part of the stream: every input twice, submitted at once so the slots run them side by side
+        warm = [srv.submit(r[0], *r[1:6]) for _ in range(2) for kind in pool for r in pool[kind]]
+        for t in warm:
+            srv.wait(t)
         tickets = [None] * len(picks)
         t0 = time.perf_counter()
 
@@ -446,8 +449,12 @@ def serve_stream(a):
         return {"req_per_s": len(picks) / tot, "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mde_per_s": de / tot / 1e6, "wall_s": tot}
 
+    shapes = {"preview": (520, 390, 32), "pair13mp": (4160, 3120, 128), "capture10": (2080, 1560, n_mc)}
+    # plain: the library's default (the autotuner's choice); served: the server's choice by size
+    forms = {k: {"plain": api.SGM_FORM_NAMES.get(api.tuned_form(w, h, n, 64), "size rule"),
+                 "served": "split" if w * h >= 2000000 else "fused"} for k, (w, h, n) in shapes.items()}
     return {"workload": f"{a.requests} Poisson arrivals at {a.rate}/s: {mix}", "slots": a.slots, "hbm_budget_gb": 120,
-            "served": stats(lat_s, tot_s), "plain": stats(lat_p, tot_p)}
+            "sgm_forms": forms, "served": stats(lat_s, tot_s), "plain": stats(lat_p, tot_p)}
 
 
 def capture_batched_vs_plain(a, steps=5, warmup=3):
@@ -507,7 +514,8 @@ def run_serve(a):
     out = {"metric": "served depth requests/s (mixed Poisson stream), with p50/p99 latency, served vs plain",
            "value": st["served"]["req_per_s"], "unit": "req/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u8 cost / u16 aggregation", "data": "synthetic (seeded pools per kind)",
-           "config": {"workload": st["workload"], "slots": st["slots"], "hbm_budget_gb": st["hbm_budget_gb"]},
+           "config": {"workload": st["workload"], "slots": st["slots"], "hbm_budget_gb": st["hbm_budget_gb"],
+                      "sgm_forms": st["sgm_forms"]},
            "served": st["served"], "plain": st["plain"]}
     print(json.dumps(out))
 

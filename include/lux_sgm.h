@@ -308,12 +308,16 @@ int lux_depth_cache_fetch(lux_sgm_ctx* ctx, const float* cache, int32_t cw, int3
  * `slots` worker contexts is free, the first waiting request whose host-side estimate of device memory fits what the
  * running requests leave of the HBM budget starts (0 = no limit; when nothing runs, the first request starts
  * regardless). A heavy request (estimate above 1.5 GiB, the queue's LightBytes) that does not fit holds back every heavy
- * request behind it (no overtaking), while light ones may pass it. Each worker has its own CUDA stream, so requests
+ * request behind it (no overtaking), while light ones may pass it; one heavy request runs at a time (a heavy solve fills
+ * the GPU, and two side by side only interleave their blocks). Each worker has its own CUDA stream, so requests
  * that arrive while others are on the GPU start as soon as a slot and memory are free and overlap on the device. A
  * request is one layer, solved exactly as lux_sgm_layer solves it from unfiltered images (LUX_LAYER_PREFILTER is
  * implied; prev = NULL, align 8), its depth map copied into out_depth (host, the layer's w*h floats, out_bytes long;
  * NULL: nothing copied). The server copies the request's small arrays at submit; the caller keeps the image data and
- * out_depth alive until lux_server_wait has returned for the ticket. Every result equals the same request solved alone. */
+ * out_depth alive until lux_server_wait has returned for the ticket. Every result equals the same request solved alone.
+ * The workers pick the aggregation form by size (path-group chains from about 2 MP, the fused wavefront below) unless
+ * the request's flags name one: the autotuner's choices are timed on an idle GPU and need not be the best beside other
+ * requests; the workers do not autotune either. */
 typedef struct lux_server lux_server;
 typedef struct {
   int32_t n_cams;

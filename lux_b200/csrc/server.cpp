@@ -5,7 +5,8 @@
 // walks that order and starts the first request that may start: one whose estimated device memory fits what the running
 // requests leave of the HBM budget (or any request when nothing runs). A heavy request (estimate above 1.5 GiB, the
 // queue's LightBytes) that does not fit holds back every heavy request behind it, so heavy requests never overtake each
-// other, while light ones (previews) may pass it. Requests run on `slots` worker contexts (each its own CUDA stream,
+// other, while light ones (previews) may pass it. On the GPU one heavy request runs at a time (a heavy solve fills every
+// SM; two side by side only interleave): a heavy request waits while another one runs, as if it did not fit. Requests run on `slots` worker contexts (each its own CUDA stream,
 // error word and events, all drawing on the device's memory pool), so requests that arrive while others are on the GPU
 // start as soon as a slot and memory are free and their work overlaps on the device with the host-side work (copies,
 // planes, schedules) of the others. A request is one layer solved exactly as lux_sgm_layer solves it (prefilter
@@ -63,6 +64,7 @@ struct lux_server {
   uint64_t next_ticket = 1;
   uint64_t in_use = 0;  // estimated device bytes of the requests running
   int running = 0;
+  int heavy_running = 0;  // requests above kLightBytes on the GPU (at most one)
   bool stop = false;
   std::string last_error;
   uint64_t passed = 0;  // requests started ahead of an earlier-queued request that had to wait
@@ -99,7 +101,9 @@ long pick(const lux_server* s) {
     const bool heavy = p.estimate > kLightBytes;
     if (heavy && heavy_blocked) continue;
     const bool fits = s->budget == 0 || s->in_use + p.estimate <= s->budget;
-    if (anything && !fits) {
+    // one heavy request on the GPU at a time: a heavy solve's launches fill every SM, and two of them side by side
+    // only interleave their blocks (measured: two 13 MP solves at once took 0.3-1.3 s each instead of 36 ms)
+    if ((anything && !fits) || (heavy && s->heavy_running > 0)) {
       if (heavy) heavy_blocked = true;
       continue;
     }
@@ -121,12 +125,23 @@ void worker(lux_server* s, lux_sgm_ctx* ctx) {
       s->queue.erase(s->queue.begin() + i);
       s->in_use += p.estimate;
       s->running++;
+      if (p.estimate > kLightBytes) s->heavy_running++;
     }
     p.started = Clock::now();
     lux_result r{};
     lux_layer* L = nullptr;
+    // The aggregation form by size (path-group chains from about 2 MP, the fused wavefront below), unless the request
+    // names one: the autotuner's choices are timed on an idle GPU, and beside other requests they need not be the best
+    // (measured in the 60/s mixed stream: the lean wavefront for the 520x390 previews, their solo choice, gave a served
+    // p99 of 441 ms, the fused wavefront 181 ms).
+    int32_t flags = p.flags | LUX_LAYER_PREFILTER;
+    if (!(flags & (LUX_LAYER_SGM_FUSED | LUX_LAYER_SGM_SPLIT | LUX_LAYER_SGM_WAVE))) {
+      const int sc = p.params.scale > 0 ? p.params.scale : 1;
+      const int64_t w = (p.images[0].w + sc - 1) / sc, h = (p.images[0].h + sc - 1) / sc;
+      flags |= w * h >= 2000000 ? LUX_LAYER_SGM_SPLIT : LUX_LAYER_SGM_FUSED;
+    }
     r.status = lux_sgm_layer(ctx, (int32_t)p.images.size(), p.images.data(), p.gray.data(), p.calibs.data(), p.near_, p.far_,
-                             &p.params, 0, 8, nullptr, p.flags | LUX_LAYER_PREFILTER, &L);
+                             &p.params, 0, 8, nullptr, flags, &L);
     if (r.status == LUX_OK) {
       lux_layer_info info{};
       lux_layer_get_info(L, &info);
@@ -143,6 +158,7 @@ void worker(lux_server* s, lux_sgm_ctx* ctx) {
       std::lock_guard<std::mutex> lk(s->mu);
       s->in_use -= p.estimate;
       s->running--;
+      if (p.estimate > kLightBytes) s->heavy_running--;
       Done& d = s->results[p.ticket];
       d.result = r;
       d.done = true;
@@ -170,6 +186,9 @@ int lux_server_create(int device, uint64_t hbm_budget_bytes, int32_t slots, lux_
       delete s;
       return rc;
     }
+    // Workers do not time the aggregation forms: on a GPU shared with the other workers' requests the timings would
+    // measure the contention, not the form (requests pick their form by size, see worker()).
+    lux_sgm_set_autotune(c, 0);
     s->ctxs.push_back(c);
   }
   for (auto* c : s->ctxs) s->workers.emplace_back(worker, s, c);
