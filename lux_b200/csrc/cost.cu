@@ -595,11 +595,17 @@ static void launch_rows(int nk, int blocks, const CostArgs& a, const LayerGeom& 
   }
 }
 
+// The row kernels give a warp 32 pixels of a row and walk the planes in each lane: a small layer with many planes (the
+// L16 pyramid's first layer: 65x49 pixels, 552 planes, 147 row tiles) leaves most SMs idle for a long walk, so it takes
+// the warp-per-pixel kernel, lanes over planes (same bits), with the horizontal phase images that kernel reads.
+bool cost_small_wide_layer(int W, int H, int n_planes) { return ((W + 31) / 32) * H < 148 * 4 && n_planes > 256; }
+
 int launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t* raw, int* err, cudaStream_t s) {
   const int npx = g.W * g.H;
   const bool grey = cost_all_grey(a);
   int kind = 0;
-  if (g.uniform && g.n_planes % 8 == 0 && a.n_others >= 1 && a.n_others <= kMaxCams - 1) {
+  if (g.uniform && !cost_small_wide_layer(g.W, g.H, g.n_planes) && g.n_planes % 8 == 0 && a.n_others >= 1 &&
+      a.n_others <= kMaxCams - 1) {
     const int tiles = ((g.W + 31) / 32) * g.H;
     int blocks = (tiles + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;

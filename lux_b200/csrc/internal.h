@@ -132,6 +132,8 @@ void launch_colour_apply(const float* yuv, int npx, const ColourF& F, uint8_t* o
 bool cost_all_grey(const CostArgs& a);
 void launch_phases(const CostArgs& a, cudaStream_t s);
 // Returns the kernel it used: 0 per-pixel warps, 1 per-row warps (uniform layers), 2 per-row warps of an axis-aligned pair.
+// Small layers with many planes: the warp-per-pixel cost kernel (and horizontal phase images) instead of the row kernels.
+bool cost_small_wide_layer(int W, int H, int n_planes);
 int launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t* raw, int* err, cudaStream_t s);
 
 // sgm_emulate.cu: the exact replay of the reference's sheared-tile traversal on its line-buffer layout (any layer)

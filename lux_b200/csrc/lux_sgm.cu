@@ -361,7 +361,7 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   if ((rc = alloc_t(ctx, tmp, zt_h.size() / 4, &zt))) return rc;
   CK(cudaMemcpyAsync(zt, zt_h.data(), zt_h.size() * 4, cudaMemcpyHostToDevice, s));
   // an axis-aligned grey pair at scale 1 with the fast layout: the cost kernel that shares block columns between pixels
-  ca.vcols = ca.axis && ca.scale == 1 && cost_all_grey(ca) && uniform && L->n % 8 == 0 ? 1 : 0;
+  ca.vcols = ca.axis && ca.scale == 1 && cost_all_grey(ca) && uniform && L->n % 8 == 0 && !cost_small_wide_layer(W, H, L->n) ? 1 : 0;
   const size_t phase_words = cost_all_grey(ca) ? 8 : 4;  // per pixel: four phases of {u16 pairs} (grey) or RGBA words
   for (int k = 0; k < ca.n_others; k++) {  // the half-pixel phase images of the other cameras
     uint32_t* ph = nullptr;
