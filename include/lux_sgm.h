@@ -136,7 +136,8 @@ int lux_sgm_set_tuned_form(int32_t w, int32_t h, int32_t n_planes, int32_t tile,
  * images: n_cams camera images (camera 0 = reference), box-FILTERED already unless LUX_LAYER_PREFILTER (as
  * DenseStereoPyramid.Run filters them, DenseStereoSgm.cs:335); gray[k] selects the grey cost weights; prev = the
  * previous layer (NULL for a first layer: every pixel searches all planes). The layer object owns its device state
- * until lux_layer_destroy. */
+ * until lux_layer_destroy. LUX_ERR_UNSUPPORTED where the exact replay would need a line buffer (2·(w+2)·(4·MaxHi+5)
+ * u16) past 2^31 - 2^16 elements, which it indexes with 32-bit integers (w beyond about 65,000 pixels). */
 int lux_sgm_layer(lux_sgm_ctx* ctx, int32_t n_cams, const lux_img_rgba8* images, const uint8_t* gray, const lux_calib* calibs,
                   float near_, float far_, const lux_stereo_params* params, int32_t index, int32_t align, const lux_layer* prev,
                   int32_t flags, lux_layer** out);
