@@ -322,7 +322,7 @@ def run_lux(a):
         "clocks": clk.summary(),
     }
     if BITS == 0 and world == 1:
-        # the survey's plain comparator of the batched capture: the reference against each module camera alone, one
+        # the plain comparator of the batched capture: the reference against each module camera alone, one
         # two-camera solve (its own planes, D_k) after the other, inputs on the device
         pairs = []
         for k in range(1, len(wl.images)):
