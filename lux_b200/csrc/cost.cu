@@ -448,22 +448,32 @@ LUX_DEV uint32_t col_cost(uint2 t, const ColRef& c) {
 
 // Uniform layers of one axis-aligned grey pair at scale 1 (the plain stereo pair): the 3x3 blocks of neighbouring
 // pixels overlap, and so do their target blocks wherever the target column advances by one whole pixel with the same
-// half-pixel phase from one pixel to the next. A warp covers 30 pixels of a row (lanes 2..31; lanes 0 and 1 are the two
-// pixels to the left): per plane every lane computes only the right column of its block (reference column x + 1,
-// clamped as the reference clamps its block, against target column ix + 1) and takes the middle and left columns from
-// lanes x - 1 and x - 2 when their target positions are exactly 2 and 4 half-pixels to the left. Where they are not, the
-// lane computes the two columns itself. The terms, and so the sums, are the reference's (:222-246); only who computes a
-// term changes. Normalise (:378-379) of one camera's cost is a function of S0 (0..18), a 19-entry table.
-__global__ void __launch_bounds__(256) k_cost_axis_v(const CostArgs a, const LayerGeom g, const float4* __restrict__ zt,
-                                                     uint8_t* __restrict__ raw, int* err) {
+// half-pixel phase from one pixel to the next. A lane holds P neighbouring pixels of a row (slots 0..P-1) and a warp a
+// run of 32·P - 2 pixels (slots 0 and 1 of lane 0 are the two pixels to the left of the run, computed and not stored).
+// Per plane every slot computes only the right column of its block (reference column x + 1, clamped as the reference
+// clamps its block, against target column ix + 1) and takes the middle and left columns from the two pixels to its left
+// (the lane's own slots, or slots P-2 and P-1 of the lane to the left by shuffle) when their target positions are
+// exactly 2 and 4 half-pixels to the left; a warp vote keeps the common case, where every slot that needs its block has
+// it that way, free of per-slot branches. Elsewhere a slot computes the two columns itself. The terms, and so the sums,
+// are the reference's (:222-246); only who computes a term changes. The plane terms, the target row and the neighbour
+// exchange are shared by the lane's P pixels. Normalise (:378-379) of one camera's cost is a function of S0 (0..18), a
+// 19-entry table. Two pixels a lane: 4 (79 registers) take more issue slots a DE, and staging each 32-plane group in
+// shared memory (whole-sector stores) saves DRAM traffic the kernel is not bound by at the price of instructions it is.
+constexpr int kAxPx = 2;                 // pixels a lane
+constexpr int kAxRun = 32 * kAxPx - 2;  // pixels a warp stores
+
+template <int P>
+__global__ void __launch_bounds__(256, P > 2 ? 3 : 4)
+    k_cost_axis_v(const CostArgs a, const LayerGeom g, const float4* __restrict__ zt, uint8_t* __restrict__ raw, int* err) {
+  constexpr int kRun = 32 * P - 2;
   __shared__ uint8_t s_norm[32];
   if (threadIdx.x < 32)
     s_norm[threadIdx.x] =
         (uint8_t)(f2i(__fmul_rn((float)(((uint32_t)(min((int)threadIdx.x, 18) * 12240 + 16) >> 5) & 0xffffu), a.norm)) & 0xff);
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int tiles_x = (g.W + 29) / 30;
-  const int ntiles = tiles_x * g.H;
+  const int runs_x = (g.W + kRun - 1) / kRun;
+  const int nruns = runs_x * g.H;
   const int n = g.n_planes;
   const uint8_t* ref8 = a.ref;
   const float* Wm = a.warp[0];
@@ -472,95 +482,153 @@ __global__ void __launch_bounds__(256) k_cost_axis_v(const CostArgs a, const Lay
   const uint2* q = reinterpret_cast<const uint2*>(a.phase[0]);
   const int plane_stride = ih * iw;
   constexpr int kNoRow = INT_MIN;
-  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += (gridDim.x * blockDim.x) >> 5) {
-    const int y = t / tiles_x, x = (t - y * tiles_x) * 30 + lane - 2;
-    const bool in_row = lane >= 2 && x < g.W;
-    const size_t pi = (size_t)y * g.W + min(max(x, 0), g.W - 1);
-    uint8_t* out = raw + pi * n;
-    const bool skipped = in_row && g.skip[pi] != 0;
-    const bool live = in_row && !skipped;
-    if (skipped)
-      for (int d = 0; d < n; d += 8) *reinterpret_cast<uint2*>(out + d) = make_uint2(0u, 0u);
-    if (__ballot_sync(0xffffffffu, live) == 0) continue;
-    // reference column triples (rows y-1, y, y+1 clamped): this lane's right column, and the left and middle ones of
-    // lanes x - 2 and x - 1 (their right columns)
-    const int xImg = min(x, a.rw - 1);  // scale 1: the reference grid is the layer grid
-    ColRef cr;
-    {
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nruns; t += (gridDim.x * blockDim.x) >> 5) {
+    const int y = t / runs_x;
+    const int x0 = (t - y * runs_x) * kRun - 2;  // x of slot 0 of lane 0
+    const int xs = x0 + lane * P;                // x of this lane's slot 0
+    const long long row0 = (long long)y * g.W;
+    bool live[P];
+    float xf[P];
+    ColRef cr[P];
+    const int ya = max(y - 1, 0), yb = min(y + 1, a.rh - 1);
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < P; j++) {
+      const int x = xs + j;
+      const bool in_row = lane * P + j >= 2 && x < g.W;  // slots 0 and 1 of lane 0 belong to the run to the left
+      const bool skipped = in_row && g.skip[row0 + x] != 0;
+      live[j] = in_row && !skipped;
+      any = any || live[j];
+      if (skipped) {  // skipped pixels aggregate raw 0 (DenseStereoSgm.cs:242)
+        uint8_t* out = raw + (row0 + x) * n;
+        for (int d = 0; d < n; d += 8) *reinterpret_cast<uint2*>(out + d) = make_uint2(0u, 0u);
+      }
+      xf[j] = (float)min(x, a.rw - 1);  // scale 1: the reference grid is the layer grid
+      // this slot's right reference column (rows y-1, y, y+1 and the column clamped like the reference's block)
       const int c = min(max(x + 1, 0), a.rw - 1);
-      const int ya = max(y - 1, 0), yb = min(y + 1, a.rh - 1);
       const uint32_t r0 = ref8[((size_t)ya * a.rw + c) * 4], r1 = ref8[((size_t)y * a.rw + c) * 4], r2 = ref8[((size_t)yb * a.rw + c) * 4];
-      cr = col_ref(r0 | (r2 << 16), r1);
+      cr[j] = col_ref(r0 | (r2 << 16), r1);
     }
-    const ColRef cm{__shfl_up_sync(0xffffffffu, cr.ea, 1), __shfl_up_sync(0xffffffffu, cr.eb, 1), __shfl_up_sync(0xffffffffu, cr.oa, 1),
-                    __shfl_up_sync(0xffffffffu, cr.ob, 1)};
-    const ColRef cl{__shfl_up_sync(0xffffffffu, cr.ea, 2), __shfl_up_sync(0xffffffffu, cr.eb, 2), __shfl_up_sync(0xffffffffu, cr.oa, 2),
-                    __shfl_up_sync(0xffffffffu, cr.ob, 2)};
-    const float xf = (float)xImg, yf = (float)y;
-    uint32_t last = 0;  // the normalised cost of the last plane computed (:273-274)
-    auto block = [&](size_t base) {  // the whole block from the target columns base, base + 1, base + 2
-      const uint32_t s = col_cost(__ldg(q + base), cl) + col_cost(__ldg(q + base + 1), cm) + col_cost(__ldg(q + base + 2), cr);
-      return (uint32_t)s_norm[(s & 0xffffu) + (s >> 16) - 12 * 256];
-    };
+    if (__ballot_sync(0xffffffffu, any) == 0) continue;
+    // slots P-2 and P-1 of the lane to the left. Slot j's left and middle block columns are entries j and j + 1 of
+    // {left lane's P-2, left lane's P-1, own 0, ..., own P-1}, its right column entry j + 2.
+    const ColRef lA{__shfl_up_sync(0xffffffffu, cr[P - 2].ea, 1), __shfl_up_sync(0xffffffffu, cr[P - 2].eb, 1),
+                    __shfl_up_sync(0xffffffffu, cr[P - 2].oa, 1), __shfl_up_sync(0xffffffffu, cr[P - 2].ob, 1)};
+    const ColRef lB{__shfl_up_sync(0xffffffffu, cr[P - 1].ea, 1), __shfl_up_sync(0xffffffffu, cr[P - 1].eb, 1),
+                    __shfl_up_sync(0xffffffffu, cr[P - 1].oa, 1), __shfl_up_sync(0xffffffffu, cr[P - 1].ob, 1)};
+    auto ext_ref = [&](int e) -> const ColRef& { return e == 0 ? lA : e == 1 ? lB : cr[e - 2]; };
+    uint32_t last[P];  // the normalised cost of the last plane computed, per slot (:273-274)
     {  // plane 0: the general projection, clamped into the rect (:263-269)
       const float z = __ldg(g.planes);
-      const float xz = __fmul_rn(xf, z), yz = __fmul_rn(yf, z);
       const float4 zk = __ldg(zt);
-      const float px = __fadd_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0)), __fmul_rn(yz, w4));
-      const float py = __fadd_rn(__fadd_rn(zk.y, __fmul_rn(xz, w1)), __fmul_rn(yz, w5));
-      const float pz = __fadd_rn(__fadd_rn(zk.z, __fmul_rn(xz, w2)), __fmul_rn(yz, w6));
-      const float inv = __frcp_rn(pz);
-      const float fx = cs_minf(cs_maxf(__fadd_rn(__fmul_rn(px, inv), 0.25f), 1.0f), (float)(x1 - 1));
-      const float fy = cs_minf(cs_maxf(__fadd_rn(__fmul_rn(py, inv), 0.25f), 1.0f), (float)(y1 - 1));
-      const int tx = f2i(__fadd_rn(fx, fx)), ty = f2i(__fadd_rn(fy, fy));
-      const int ix = tx >> 1, iy = ty >> 1;
-      if (ix >= 1 && ix < x1 && iy >= 1 && iy < y1) {
-        if (live) last = block(((size_t)(((ty & 1) << 1) | (tx & 1)) * ih + (iy - 1)) * iw + (ix - 1));
-      } else if (live) {  // the scalar fallback of the reference would read out of the image
-        atomicCAS(err, 0, 7);
+      const float yz = __fmul_rn((float)y, z);
+#pragma unroll
+      for (int j = 0; j < P; j++) {
+        last[j] = 0;
+        const float xz = __fmul_rn(xf[j], z);
+        const float px = __fadd_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0)), __fmul_rn(yz, w4));
+        const float py = __fadd_rn(__fadd_rn(zk.y, __fmul_rn(xz, w1)), __fmul_rn(yz, w5));
+        const float pz = __fadd_rn(__fadd_rn(zk.z, __fmul_rn(xz, w2)), __fmul_rn(yz, w6));
+        const float inv = __frcp_rn(pz);
+        const float fx = cs_minf(cs_maxf(__fadd_rn(__fmul_rn(px, inv), 0.25f), 1.0f), (float)(x1 - 1));
+        const float fy = cs_minf(cs_maxf(__fadd_rn(__fmul_rn(py, inv), 0.25f), 1.0f), (float)(y1 - 1));
+        const int tx = f2i(__fadd_rn(fx, fx)), ty = f2i(__fadd_rn(fy, fy));
+        const int ix = tx >> 1, iy = ty >> 1;
+        if (ix >= 1 && ix < x1 && iy >= 1 && iy < y1) {
+          if (live[j]) {
+            const size_t base = ((size_t)(((ty & 1) << 1) | (tx & 1)) * ih + (iy - 1)) * iw + (ix - 1);
+            const uint32_t s = col_cost(__ldg(q + base), ext_ref(j)) + col_cost(__ldg(q + base + 1), ext_ref(j + 1)) +
+                               col_cost(__ldg(q + base + 2), cr[j]);
+            last[j] = s_norm[(s & 0xffffu) + (s >> 16) - 12 * 256];
+          }
+        } else if (live[j]) {  // the scalar fallback of the reference would read out of the image
+          atomicCAS(err, 0, 7);
+        }
       }
     }
-    // planes in groups of eight (one 8-byte store each); the row offset of plane d comes from lane d % 32
-    int rowoff = 0;
-    for (int d8 = 0; d8 < n; d8 += 8) {
-      if ((d8 & 31) == 0) {  // lane j: the offset of row iy - 1 of phase 2·hy of plane d8 + j (kNoRow: off the rect)
-        const int dj = min(d8 + lane, n - 1);
-        const float4 zj = __ldg(zt + dj);
-        const float yz = __fmul_rn(yf, __ldg(g.planes + dj));
-        const float fy = __fadd_rn(__fmul_rn(__fadd_rn(zj.y, __fmul_rn(yz, w5)), zj.w), 0.25f);
-        const int ty = f2i(__fadd_rn(fy, fy)), iy = ty >> 1;
-        rowoff = (iy >= 1 && iy < y1) ? (((ty & 1) << 1) * ih + iy - 1) * iw : kNoRow;
-      }
-      uint32_t pk0 = 0, pk1 = 0;
+    const float yf = (float)y;
+    auto row_offset = [&](int d) {  // lane j: the offset of row iy - 1 of phase 2·hy of plane d + j (kNoRow: off the rect)
+      const int dj = min(d + lane, n - 1);
+      const float4 zj = __ldg(zt + dj);
+      const float yz = __fmul_rn(yf, __ldg(g.planes + dj));
+      const float fy = __fadd_rn(__fmul_rn(__fadd_rn(zj.y, __fmul_rn(yz, w5)), zj.w), 0.25f);
+      const int ty = f2i(__fadd_rn(fy, fy)), iy = ty >> 1;
+      return (iy >= 1 && iy < y1) ? (((ty & 1) << 1) * ih + iy - 1) * iw : kNoRow;
+    };
+    int rowoff = row_offset(0);
+    // eight planes of u8 costs a slot as one 64-bit value {lo, hi}, plane d at byte d % 8: each plane shifts it right by
+    // one byte and enters at the top
+    uint32_t lo[P], hi[P];
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const int d = d8 + k;
-        const int ro_d = __shfl_sync(0xffffffffu, rowoff, d & 31);
-        if (d != 0 && ro_d != kNoRow) {  // plane 0 was done above; ro_d is the same for the whole warp
-          const float4 zk = __ldg(zt + d);
-          const float xz = __fmul_rn(xf, __ldg(g.planes + d));
+    for (int j = 0; j < P; j++) {
+      lo[j] = 0;
+      hi[j] = last[j] << 24;
+    }
+    for (int d = 1; d < n; d++) {
+      if ((d & 31) == 0) rowoff = row_offset(d);
+      const int ro_d = __shfl_sync(0xffffffffu, rowoff, d & 31);
+      if (ro_d != kNoRow) {  // the same for the whole warp
+        const float4 zk = __ldg(zt + d);
+        const float z = __ldg(g.planes + d);
+        int tx[P], ix[P], rb[P];
+        uint32_t c[P];
+        bool inr[P];
+#pragma unroll
+        for (int j = 0; j < P; j++) {
+          const float xz = __fmul_rn(xf[j], z);
           const float fx = __fadd_rn(__fmul_rn(__fadd_rn(zk.x, __fmul_rn(xz, w0)), zk.w), 0.25f);
-          const int tx = f2i(__fadd_rn(fx, fx)), ix = tx >> 1;
-          const int base = ro_d + (tx & 1) * plane_stride;
-          const uint32_t c = col_cost(__ldg(q + base + min(max(ix + 1, 0), iw - 1)), cr);
-          const uint32_t c1 = __shfl_up_sync(0xffffffffu, c, 1), c2 = __shfl_up_sync(0xffffffffu, c, 2);
-          // lanes 1..31 whose target is one pixel right of the target of the lane to their left; where all are, the
-          // lane two to the left is two pixels left too
-          const int t1 = __shfl_up_sync(0xffffffffu, tx, 1);
-          const bool all = __all_sync(0xffffffffu, lane == 0 || t1 == tx - 2);
-          int t2 = tx - 4;
-          if (!all) t2 = __shfl_up_sync(0xffffffffu, tx, 2);  // the same branch for the whole warp
-          if (live && ix >= 1 && ix < x1) {
-            uint32_t sum;
-            if (t1 == tx - 2 && t2 == tx - 4) sum = c + c1 + c2;
-            else sum = col_cost(__ldg(q + base + ix - 1), cl) + col_cost(__ldg(q + base + ix), cm) + c;
-            last = s_norm[(sum & 0xffffu) + (sum >> 16) - 12 * 256];
+          tx[j] = f2i(__fadd_rn(fx, fx));
+          ix[j] = tx[j] >> 1;
+          inr[j] = ix[j] >= 1 && ix[j] < x1;
+          rb[j] = ro_d + (tx[j] & 1) * plane_stride;  // row iy - 1 of the slot's phase
+          c[j] = col_cost(__ldg(q + rb[j] + min(max(ix[j] + 1, 0), iw - 1)), cr[j]);
+        }
+        // slots P-2 and P-1 of the lane to the left; slot P-1's target is sent as kNoRow unless slot P-2's is one pixel
+        // left of it, so that one comparison checks both neighbours of slot 0. A neighbour pair found unequal (by this
+        // or by the wrapping compares below) only sends a slot to its own columns, which is always exact.
+        const int tl = (uint32_t)tx[P - 1] - (uint32_t)tx[P - 2] == 2u ? tx[P - 1] : kNoRow;
+        const uint32_t cA = __shfl_up_sync(0xffffffffu, c[P - 2], 1), cB = __shfl_up_sync(0xffffffffu, c[P - 1], 1);
+        const int tB = __shfl_up_sync(0xffffffffu, tl, 1);
+        bool fast[P];
+        bool pair[P];  // pair[j]: slot j's target is one pixel right of slot j-1's (j >= 1)
+#pragma unroll
+        for (int j = 1; j < P; j++) pair[j] = (uint32_t)tx[j] - (uint32_t)tx[j - 1] == 2u;
+        fast[0] = (uint32_t)tx[0] - (uint32_t)tB == 2u;
+#pragma unroll
+        for (int j = 1; j < P; j++) fast[j] = pair[j] && (j == 1 ? fast[0] : pair[j - 1]);
+        bool ok = true;  // every slot that needs its block has it from its neighbours
+#pragma unroll
+        for (int j = 0; j < P; j++) ok = ok && (fast[j] || !(live[j] && inr[j]));
+        auto ext_c = [&](int e) { return e == 0 ? cA : e == 1 ? cB : c[e - 2]; };
+        if (__all_sync(0xffffffffu, ok)) {
+#pragma unroll
+          for (int j = 0; j < P; j++) {
+            const uint32_t sum = ext_c(j) + ext_c(j + 1) + c[j];
+            if (inr[j]) last[j] = s_norm[(sum & 0xffffu) + (sum >> 16) - 12 * 256];
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < P; j++) {
+            if (inr[j]) {
+              uint32_t sum;
+              if (fast[j]) sum = ext_c(j) + ext_c(j + 1) + c[j];
+              else sum = col_cost(__ldg(q + rb[j] + ix[j] - 1), ext_ref(j)) + col_cost(__ldg(q + rb[j] + ix[j]), ext_ref(j + 1)) + c[j];
+              last[j] = s_norm[(sum & 0xffffu) + (sum >> 16) - 12 * 256];
+            }
           }
         }
-        if (k < 4) pk0 |= last << (8 * k);
-        else pk1 |= last << (8 * (k - 4));
       }
-      if (live) *reinterpret_cast<uint2*>(out + d8) = make_uint2(pk0, pk1);
+#pragma unroll
+      for (int j = 0; j < P; j++) {
+        lo[j] = __funnelshift_r(lo[j], hi[j], 8);
+        hi[j] = __funnelshift_r(hi[j], last[j], 8);
+      }
+      if ((d & 7) == 7) {
+        const int d0 = d - 7;
+#pragma unroll
+        for (int j = 0; j < P; j++)
+          if (live[j]) *reinterpret_cast<uint2*>(raw + (row0 + xs + j) * n + d0) = make_uint2(lo[j], hi[j]);
+      }
     }
   }
 }
@@ -610,10 +678,10 @@ int launch_cost(const CostArgs& a, const LayerGeom& g, const float4* zt, uint8_t
     int blocks = (tiles + 7) / 8;
     if (blocks > 148 * 16) blocks = 148 * 16;
     if (a.vcols) {
-      const int vtiles = ((g.W + 29) / 30) * g.H;
-      int vb = (vtiles + 7) / 8;
+      const int vruns = ((g.W + kAxRun - 1) / kAxRun) * g.H;
+      int vb = (vruns + 7) / 8;
       if (vb > 148 * 16) vb = 148 * 16;
-      k_cost_axis_v<<<vb, 256, 0, s>>>(a, g, zt, raw, err);
+      k_cost_axis_v<kAxPx><<<vb, 256, 0, s>>>(a, g, zt, raw, err);
       kind = 3;
     } else if (a.axis) {
       if (grey) k_cost_axis<true><<<blocks, 256, 0, s>>>(a, g, zt, raw, err);

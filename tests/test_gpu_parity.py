@@ -154,9 +154,10 @@ def test_multicamera_colour_layer_bit_exact(ctx, oracle):
         gl.close()
 
 
-@pytest.mark.parametrize("focal,skip,w", [(1.0, 0, 157), (1.0, 2, 211), (1.3, 0, 130), (0.77, 2, 97), (1.0, 0, 30)])
+@pytest.mark.parametrize("focal,skip,w", [(1.0, 0, 157), (1.0, 2, 211), (1.3, 0, 130), (0.77, 2, 97), (1.0, 0, 30),
+                                           (1.0, 0, 124), (1.0, 2, 253), (1.3, 2, 125)])
 def test_axis_pair_shared_columns(ctx, oracle, focal, skip, w):
-    """The shared-column grey cost kernel: widths that are and are not multiples of its 30-pixel warps, skipped pixels,
+    """The shared-column grey cost kernel: widths below, at and past its 62-pixel warp runs, skipped pixels,
     and a second camera with another focal length, where neighbouring target positions step by more (1.3) or less
     (0.77) than one pixel so that lanes compute their own block columns."""
     from lux_b200 import api, synth
