@@ -445,6 +445,12 @@ LUX_DEV ColRef col_ref(uint32_t even, uint32_t odd) { return ColRef{0x01000100u 
 LUX_DEV uint32_t col_cost(uint2 t, const ColRef& c) {
   return vmin2c(vmax2c(t.x + c.ea, c.eb - t.x), 0x01020102u) + vmin2c(vmax2c(t.y + c.oa, c.ob - t.y), 0x01000102u);
 }
+// The same with the four adds as multiply-adds by one = 1 and neg = 0xffffffff (kernel-argument values, so they stay
+// multiply-adds and issue on the FMA pipe; the ALU pipe bounds the kernel that uses this). Equal mod 2^32.
+LUX_DEV uint32_t col_cost_m(uint2 t, const ColRef& c, uint32_t one, uint32_t neg) {
+  return vmin2c(vmax2c(t.x * one + c.ea, t.x * neg + c.eb), 0x01020102u) +
+         vmin2c(vmax2c(t.y * one + c.oa, t.y * neg + c.ob), 0x01000102u);
+}
 
 // Uniform layers of one axis-aligned grey pair at scale 1 (the plain stereo pair): the 3x3 blocks of neighbouring
 // pixels overlap, and so do their target blocks wherever the target column advances by one whole pixel with the same
@@ -482,6 +488,8 @@ __global__ void __launch_bounds__(256, P > 2 ? 3 : 4)
   const uint2* q = reinterpret_cast<const uint2*>(a.phase[0]);
   const int plane_stride = ih * iw;
   constexpr int kNoRow = INT_MIN;
+  // (s · 0x10001) >> 16 is the sum of the two u16 lanes of a block sum s (each lane under 2^15, so nothing carries)
+  const uint32_t one = a.one, neg = 0u - a.one, k10001 = 0x10001u * a.one;
   for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nruns; t += (gridDim.x * blockDim.x) >> 5) {
     const int y = t / runs_x;
     const int x0 = (t - y * runs_x) * kRun - 2;  // x of slot 0 of lane 0
@@ -581,7 +589,9 @@ __global__ void __launch_bounds__(256, P > 2 ? 3 : 4)
           ix[j] = tx[j] >> 1;
           inr[j] = ix[j] >= 1 && ix[j] < x1;
           rb[j] = ro_d + (tx[j] & 1) * plane_stride;  // row iy - 1 of the slot's phase
-          c[j] = col_cost(__ldg(q + rb[j] + min(max(ix[j] + 1, 0), iw - 1)), cr[j]);
+          // column ix + 1, clamped only to stay in the image: a column a neighbour takes (ix + 1 of a slot whose right
+          // neighbour is in the rect one pixel on) lies in [0, iw - 3] already, so a negative ix + 1 may map to iw - 1
+          c[j] = col_cost_m(__ldg(q + rb[j] + min((uint32_t)(ix[j] + 1), (uint32_t)(iw - 1))), cr[j], one, neg);
         }
         // slots P-2 and P-1 of the lane to the left; slot P-1's target is sent as kNoRow unless slot P-2's is one pixel
         // left of it, so that one comparison checks both neighbours of slot 0. A neighbour pair found unequal (by this
@@ -604,7 +614,7 @@ __global__ void __launch_bounds__(256, P > 2 ? 3 : 4)
 #pragma unroll
           for (int j = 0; j < P; j++) {
             const uint32_t sum = ext_c(j) + ext_c(j + 1) + c[j];
-            if (inr[j]) last[j] = s_norm[(sum & 0xffffu) + (sum >> 16) - 12 * 256];
+            if (inr[j]) last[j] = s_norm[((sum * k10001) >> 16) - 12 * 256];
           }
         } else {
 #pragma unroll

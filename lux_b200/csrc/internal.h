@@ -45,6 +45,7 @@ struct CostArgs {
   int scale;
   int axis;                         // one other camera, axis-aligned flow matrix: zt.w holds 1/pz per plane
   int vcols;                        // axis, grey, scale 1: phase images as vertical triples, blocks from shared columns
+  uint32_t one;                     // 1: a multiplier the compiler cannot fold, so that adds can issue on the FMA pipe
 };
 
 // prep.cu

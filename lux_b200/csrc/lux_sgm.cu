@@ -309,6 +309,7 @@ int build_layer(lux_sgm_ctx* ctx, int n_cams, const uint8_t* const* dimg, const 
   // matching cost (DenseStereo.BuildContext + MatchingCost + Normalise)
   CostArgs ca;
   std::memset(&ca, 0, sizeof ca);
+  ca.one = 1;
   ca.ref = dimg[0]; ca.rw = iw[0]; ca.rh = ih[0];
   ca.n_others = n_cams - 1;
   for (int k = 1; k < n_cams; k++) {
